@@ -1,0 +1,293 @@
+"""Groundwater problem description mirroring the reference configuration.
+
+The dataclasses follow the groundwater subset of frehg2's ``FrehgConfig``
+(``src/core/Config.hpp``): ``DomainConfig`` (:56-80), ``SoilType``
+(:395-420), ``GroundwaterTimestepConfig`` (:253-260), ``GroundwaterConfig``
+(:285-350), ``SolverSystemConfig`` (:673-698), ``GroundwaterInitialConfig``
+(:493-498) and ``BoundaryConditionConfig`` (:564-578).  Names, defaults and
+meanings are the reference's.
+
+:func:`rasterize` turns a config into the per-cell / per-column arrays the
+C ABI (``include/frehg_gw.h``) takes, following the reference's own setup:
+soil staging by type map (``RichardsSolver.cpp:207-329``) and polygon
+boundary membership by cell centre (``BoundarySet.cpp:33-150``,
+``Polygon.cpp:45-80``; on-edge counts as inside).
+"""
+from __future__ import annotations
+
+import dataclasses
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+ArrayOrFloat = Union[float, np.ndarray]
+
+BC_NOFLUX, BC_HEAD, BC_FLUX, BC_GRAVITY, BC_HEAD_HYDROSTATIC = 0, 1, 2, 3, 4
+IC_FORMS = {"moisture": 0, "head": 1, "water_table": 2}
+
+
+@dataclass
+class SoilType:
+    """One van Genuchten-Mualem soil (``SoilType``, Config.hpp:395-420)."""
+
+    name: str
+    ksx: float
+    ksy: float
+    ksz: float
+    theta_s: float
+    theta_r: float
+    vg_alpha: float
+    vg_n: float
+    aev: float = 0.0
+
+
+@dataclass
+class Domain:
+    """``DomainConfig`` (Config.hpp:56-80); ``bottom_elevation`` is a
+    constant or an (ny, nx) raster."""
+
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    dy: float
+    dz: float
+    dz_stretch: float = 1.0
+    bottom_elevation: ArrayOrFloat = 0.0
+    follow_terrain: bool = False
+    terrain_layers: str = "scaled"  # "scaled" | "uniform"
+
+    def dz_layers(self) -> np.ndarray:
+        """Nominal layer thicknesses dz * dz_stretch**k (``Grid::dzK``)."""
+        return np.array([self.dz * (float(self.dz_stretch) ** k) for k in range(self.nz)])
+
+
+@dataclass
+class Timestep:
+    """``GroundwaterTimestepConfig`` (Config.hpp:253-260)."""
+
+    dt_init: float
+    dt_min: float
+    dt_max: float
+    dq_grow: float = 0.01
+    dq_shrink: float = 0.02
+    courant_max: float = 2.0
+
+
+@dataclass
+class Groundwater:
+    """``GroundwaterConfig`` (Config.hpp:285-350) with the reference defaults."""
+
+    timestep: Timestep
+    use_full3d: bool = True
+    specific_storage: float = 0.0
+    reallocation_surplus: str = "drop"  # "drop" | "redistribute"
+    reallocation: str = "legacy"  # "legacy" | "disabled"
+    predictor_corrector: str = "consistent"  # "consistent" | "legacy"
+    face_conductivity: str = "arithmetic"  # "arithmetic" | "harmonic"
+    saturated_contact: str = "head"  # "head" ("legacy" is order-dependent)
+
+
+@dataclass
+class Solver:
+    """``SolverSystemConfig`` for the gw_ system (Config.hpp:673-698).
+
+    ``preconditioner`` names the lane: the B200 form runs Jacobi-PCG (the
+    reference's ``-gw_pc_type jacobi`` lane); the reference default
+    ``bjacobi-icc`` exists only in the CPU oracle.  ``precision`` selects the
+    plain FP64 solve or the FP32-inner / FP64-outer defect correction.
+    """
+
+    rtol: float = 1.0e-8
+    atol: float = 1.0e-14
+    max_iterations: int = 1000
+    preconditioner: str = "jacobi"
+    precision: str = "fp64"  # "fp64" | "mixed"
+    outer_rtol: float = 1.0e-10
+    max_outer: int = 30
+
+
+@dataclass
+class InitialCondition:
+    """``GroundwaterInitialConfig`` (Config.hpp:493-498).  ``value`` is a
+    constant, an (ny, nx, nz) field (moisture, head) or an (ny, nx) raster
+    (water table)."""
+
+    form: str  # "moisture" | "head" | "water_table"
+    value: ArrayOrFloat
+
+
+@dataclass
+class BoundaryCondition:
+    """``BoundaryConditionConfig`` (Config.hpp:564-578), groundwater targets."""
+
+    name: str
+    polygon: Sequence[Tuple[float, float]]
+    target: str  # "groundwater_top" | "groundwater_bottom" | "groundwater_side"
+    kind: str  # "head" | "flux"
+    form: str = "constant"  # "constant" | "gravity" | "hydrostatic"
+    value: float = 0.0
+    hydrostatic_eta: float = 0.0
+
+    def code(self) -> int:
+        if self.kind == "head":
+            return BC_HEAD_HYDROSTATIC if self.form == "hydrostatic" else BC_HEAD
+        if self.kind == "flux":
+            return BC_GRAVITY if self.form == "gravity" else BC_FLUX
+        raise ValueError(f"groundwater boundary condition '{self.name}' must be head or flux")
+
+    def value_at(self, t: float) -> float:
+        """``BoundaryCondition::value`` (BoundarySet.cpp:19-31)."""
+        if self.form == "gravity":
+            return 0.0
+        if self.form == "hydrostatic":
+            return self.hydrostatic_eta
+        return self.value
+
+
+@dataclass
+class GwConfig:
+    """The groundwater part of one frehg2 run."""
+
+    domain: Domain
+    soil_types: List[SoilType]
+    groundwater: Groundwater
+    initial: InitialCondition
+    solver: Solver = field(default_factory=Solver)
+    boundary_conditions: List[BoundaryCondition] = field(default_factory=list)
+    soil_map: Optional[np.ndarray] = None  # (ny, nx, nz) type ids; None = type 0
+    # Optional per-cell soil arrays (name -> (ny, nx, nz)) overriding the
+    # type table; the reference reaches the same state with one type per cell.
+    cell_soil: Optional[dict] = None
+
+    def replace(self, **kw) -> "GwConfig":
+        return dataclasses.replace(self, **kw)
+
+
+# ----------------------------------------------------------------- rasterizing
+def _on_segment(a, b, x, y) -> bool:
+    cross = (b[0] - a[0]) * (y - a[1]) - (b[1] - a[1]) * (x - a[0])
+    scale = max(abs(a[0]), abs(a[1]), abs(b[0]), abs(b[1]), abs(x), abs(y), 1.0)
+    if abs(cross) > 1.0e-12 * scale * scale:
+        return False
+    dot = (x - a[0]) * (b[0] - a[0]) + (y - a[1]) * (b[1] - a[1])
+    len2 = (b[0] - a[0]) ** 2 + (b[1] - a[1]) ** 2
+    return -1.0e-12 * scale * scale <= dot <= len2 + 1.0e-12 * scale * scale
+
+
+def polygon_contains(poly: Sequence[Tuple[float, float]], x: float, y: float) -> bool:
+    """Point-in-polygon with on-edge counted inside (Polygon.cpp:45-80)."""
+    xs = [p[0] for p in poly]
+    ys = [p[1] for p in poly]
+    if x < min(xs) - 1e-12 or x > max(xs) + 1e-12 or y < min(ys) - 1e-12 or y > max(ys) + 1e-12:
+        return False
+    n = len(poly)
+    for v in range(n):
+        if _on_segment(poly[v], poly[(v + 1) % n], x, y):
+            return True
+    inside = False
+    for v in range(n):
+        a, b = poly[v], poly[(v + 1) % n]
+        if (a[1] > y) != (b[1] > y):
+            xint = a[0] + (y - a[1]) / (b[1] - a[1]) * (b[0] - a[0])
+            if x < xint:
+                inside = not inside
+    return inside
+
+
+@dataclass
+class Rasterized:
+    """Per-cell / per-column arrays for ``frehg_gw_desc``."""
+
+    dz_layers: np.ndarray
+    bath: np.ndarray  # (ny, nx)
+    soil: dict  # name -> (ny, nx, nz) float64
+    top_code: np.ndarray
+    bot_code: np.ndarray
+    xm_code: np.ndarray
+    xp_code: np.ndarray
+    ym_code: np.ndarray
+    yp_code: np.ndarray
+    top_value: np.ndarray
+    bot_value: np.ndarray
+    xm_value: np.ndarray
+    xp_value: np.ndarray
+    ym_value: np.ndarray
+    yp_value: np.ndarray
+
+
+SOIL_FIELDS = ("ksx", "ksy", "ksz", "vg_alpha", "vg_n", "theta_s", "theta_r", "aev")
+
+
+def rasterize(cfg: GwConfig, t: float = 0.0) -> Rasterized:
+    d = cfg.domain
+    ny, nx, nz = d.ny, d.nx, d.nz
+    if np.isscalar(d.bottom_elevation):
+        bath = np.full((ny, nx), float(d.bottom_elevation))
+    else:
+        bath = np.asarray(d.bottom_elevation, dtype=np.float64).reshape(ny, nx)
+    if cfg.soil_map is None:
+        ids = np.zeros((ny, nx, nz), dtype=np.int64)
+    else:
+        ids = np.asarray(cfg.soil_map, dtype=np.int64).reshape(ny, nx, nz)
+    if ids.min() < 0 or ids.max() >= len(cfg.soil_types):
+        raise ValueError("soil_map ids must index soil_types")
+    soil = {}
+    for name in SOIL_FIELDS:
+        table = np.array([getattr(s, name) for s in cfg.soil_types], dtype=np.float64)
+        soil[name] = np.ascontiguousarray(table[ids])
+        if cfg.cell_soil is not None and name in cfg.cell_soil:
+            soil[name] = np.ascontiguousarray(
+                np.broadcast_to(np.asarray(cfg.cell_soil[name], np.float64), (ny, nx, nz)))
+
+    codes = {k: None for k in ("top", "bot", "xm", "xp", "ym", "yp")}
+    codes["top"] = np.zeros((ny, nx), np.int32)
+    codes["bot"] = np.zeros((ny, nx), np.int32)
+    codes["xm"] = np.zeros(ny, np.int32)
+    codes["xp"] = np.zeros(ny, np.int32)
+    codes["ym"] = np.zeros(nx, np.int32)
+    codes["yp"] = np.zeros(nx, np.int32)
+    vals = {k: np.zeros(v.shape, np.float64) for k, v in codes.items()}
+    for bc in cfg.boundary_conditions:
+        code = bc.code()
+        v = bc.value_at(t)
+        for j in range(ny):
+            yc = (j + 0.5) * d.dy
+            for i in range(nx):
+                xc = (i + 0.5) * d.dx
+                if not polygon_contains(bc.polygon, xc, yc):
+                    continue
+                if bc.target == "groundwater_top":
+                    codes["top"][j, i] = code
+                    vals["top"][j, i] = v
+                elif bc.target == "groundwater_bottom":
+                    codes["bot"][j, i] = code
+                    vals["bot"][j, i] = v
+                elif bc.target == "groundwater_side":
+                    if i == 0:
+                        codes["xm"][j], vals["xm"][j] = code, v
+                    if i == nx - 1:
+                        codes["xp"][j], vals["xp"][j] = code, v
+                    if j == 0:
+                        codes["ym"][i], vals["ym"][i] = code, v
+                    if j == ny - 1:
+                        codes["yp"][i], vals["yp"][i] = code, v
+                else:
+                    raise ValueError(f"unknown target {bc.target}")
+    return Rasterized(
+        dz_layers=d.dz_layers(),
+        bath=bath,
+        soil=soil,
+        top_code=codes["top"], bot_code=codes["bot"], xm_code=codes["xm"],
+        xp_code=codes["xp"], ym_code=codes["ym"], yp_code=codes["yp"],
+        top_value=vals["top"], bot_value=vals["bot"], xm_value=vals["xm"],
+        xp_value=vals["xp"], ym_value=vals["ym"], yp_value=vals["yp"],
+    )
+
+
+def whole_footprint(nx: int, ny: int, dx: float = 1.0, dy: float = 1.0):
+    """Polygon covering every column (tests/unit/test_gw.cpp:124-129)."""
+    x1 = nx * dx + 0.1
+    y1 = ny * dy + 0.1
+    return [(-0.1, -0.1), (x1, -0.1), (x1, y1), (-0.1, y1)]

@@ -1,0 +1,205 @@
+/* frehg_gw.h — C ABI of the B200 groundwater (3D mixed-form Richards) step.
+ *
+ * Drop-in for the frehg2 groundwater module's step path.  Each entry point
+ * replaces one piece of the reference's C++ interface (paths are within the
+ * frehg2 project):
+ *
+ *   frehg_gw_create        gw::RichardsSolver::RichardsSolver
+ *                          (src/gw/RichardsSolver.hpp:177-178,
+ *                          RichardsSolver.cpp:61-205) together with the
+ *                          setup it consumes: gw::TerrainMetric
+ *                          (TerrainMetric.cpp:69-430), Grid::buildGlobalIds
+ *                          (Grid.cpp:160-238) and the BC markers of
+ *                          RichardsSolver::buildBoundaryLists (:429-524).
+ *   frehg_gw_init_state    RichardsSolver::applyInitialConditions (:331-427)
+ *   frehg_gw_set_state     a restart read + RichardsSolver::refreshDerivedState
+ *                          (RichardsSolver.hpp:336, RichardsSolver.cpp:880-890)
+ *   frehg_gw_set_bc_values RichardsSolver::updateBoundaryValues (:526-566);
+ *                          the caller evaluates BoundaryCondition::value(t)
+ *   frehg_gw_step          RichardsSolver::step(t, dtg) (RichardsSolver.hpp:257,
+ *                          RichardsSolver.cpp:729-794), including the
+ *                          LinearSystem::setValues/solve KSP call it makes
+ *                          (core/LinearSystem.hpp:119-133)
+ *   frehg_gw_next_dt       RichardsSolver::nextDt (RichardsSolver.hpp:261)
+ *   frehg_gw_get_field     head(), waterContent(), fluxXVolumetric(),
+ *                          fluxYVolumetric(), fluxZFaceVolumetric(),
+ *                          faceConductivityX/Y/ZFace(), waterContentStart()
+ *                          (RichardsSolver.hpp:265-358)
+ *   frehg_gw_owned_volume  RichardsSolver::ownedVolume (RichardsSolver.hpp:423)
+ *   frehg_gw_destroy       ~RichardsSolver
+ *
+ * Conventions (kept from the reference): cell (j, i, k), k = 0 at the land
+ * surface, k increasing downward, k unit-stride; interior host arrays are
+ * indexed ((j * nx) + i) * nz + k.  x/y fluxes are positive toward -axis,
+ * z fluxes positive upward, all carrying the face area [m^3/s].  z-face
+ * plane k is the face above cell k; plane nz the bottom boundary face.
+ *
+ * Errors never cross the ABI as exceptions: every call returns a
+ * frehg_gw_status; frehg_gw_last_error() describes the last failure on the
+ * calling thread.  One handle may be used by one host thread at a time.
+ * All device work of a handle runs on its stream (frehg_gw_set_stream).
+ */
+#ifndef FREHG_GW_H
+#define FREHG_GW_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FREHG_GW_ABI_VERSION 1
+
+typedef enum frehg_gw_status {
+  FREHG_GW_OK = 0,
+  FREHG_GW_EINVAL = 1,       /* bad argument or descriptor (reference: log::fatal) */
+  FREHG_GW_EUNSUPPORTED = 2, /* a branch outside the groundwater-only step */
+  FREHG_GW_ENOMEM = 3,       /* device allocation failed */
+  FREHG_GW_ECUDA = 4,        /* a CUDA runtime call failed */
+  FREHG_GW_ESOLVER = 5,      /* CG diverged or hit max_iterations (reference: fatal) */
+  FREHG_GW_ENONFINITE = 6,   /* non-finite head or moisture after the step */
+  FREHG_GW_ESTATE = 7        /* call order violated (e.g. step before init_state) */
+} frehg_gw_status;
+
+/* GwBcCode (src/gw/RichardsSolver.hpp:66-72). */
+enum {
+  FREHG_GW_BC_NOFLUX = 0,
+  FREHG_GW_BC_HEAD = 1,
+  FREHG_GW_BC_FLUX = 2,
+  FREHG_GW_BC_GRAVITY = 3,
+  FREHG_GW_BC_HEAD_HYDROSTATIC = 4
+};
+
+/* GroundwaterInitialConfig::Form (src/core/Config.hpp:493-498). */
+enum { FREHG_GW_IC_MOISTURE = 0, FREHG_GW_IC_HEAD = 1, FREHG_GW_IC_WATER_TABLE = 2 };
+
+/* Arithmetic of the predictor's linear solve. */
+enum {
+  FREHG_GW_PRECISION_FP64 = 0, /* FP64 Jacobi-PCG, PETSc KSPCG semantics */
+  FREHG_GW_PRECISION_MIXED = 1 /* FP32 inner PCG inside FP64 defect correction */
+};
+
+/* Fields for frehg_gw_get_field. */
+enum {
+  FREHG_GW_FIELD_HEAD = 0,      /* (ny, nx, nz)   */
+  FREHG_GW_FIELD_WC = 1,        /* (ny, nx, nz)   */
+  FREHG_GW_FIELD_QX = 2,        /* (ny, nx+1, nz) faces i-1/2 .. nx-1/2 */
+  FREHG_GW_FIELD_QY = 3,        /* (ny+1, nx, nz) faces j-1/2 .. ny-1/2 */
+  FREHG_GW_FIELD_QZ = 4,        /* (ny, nx, nz+1) */
+  FREHG_GW_FIELD_KX = 5,        /* like QX */
+  FREHG_GW_FIELD_KY = 6,        /* like QY */
+  FREHG_GW_FIELD_KZ = 7,        /* like QZ */
+  FREHG_GW_FIELD_WC_START = 8,  /* theta^n of the last step, (ny, nx, nz) */
+  FREHG_GW_FIELD_DZ = 9,        /* cell thickness (ny, nx, nz) */
+  FREHG_GW_FIELD_BOT = 10,      /* cell bottom elevation, offset frame */
+  FREHG_GW_FIELD_AX = 11,       /* x-face area, like QX */
+  FREHG_GW_FIELD_AY = 12,       /* y-face area, like QY */
+  FREHG_GW_FIELD_SINX = 13,     /* like QX */
+  FREHG_GW_FIELD_COSX = 14,
+  FREHG_GW_FIELD_SINY = 15,     /* like QY */
+  FREHG_GW_FIELD_COSY = 16,
+  FREHG_GW_FIELD_VLOSS = 17,    /* cumulative clamp volume per cell */
+  FREHG_GW_FIELD_COUNT = 18
+};
+
+/* Static description of one domain.  Host pointers; the library copies what
+ * it needs during frehg_gw_create.  Mirrors the reference's DomainConfig,
+ * SoilConfig, GroundwaterConfig and SolverSystemConfig (src/core/Config.hpp:
+ * 56-80, 253-260, 285-350, 673-698) after rasterization: soil and boundary
+ * codes arrive per cell / per column rather than as type maps and polygons. */
+typedef struct frehg_gw_desc {
+  int abi_version; /* FREHG_GW_ABI_VERSION */
+  int nx, ny, nz;
+  double dx, dy;
+  const double* dz_layers; /* nz nominal layer thicknesses (Grid::dzK) */
+  double dz_stretch;       /* domain.dz_stretch (scaled terrain layer weights) */
+  const double* bath;      /* ny*nx bed elevation, unshifted datum; NULL = flat 0 */
+  int follow_terrain;      /* domain.follow_terrain */
+  int terrain_uniform;     /* domain.terrain_layers: 1 uniform, 0 scaled */
+  /* Per-cell soil, ny*nx*nz each (SoilType, Config.hpp:395-420). */
+  const double *ksx, *ksy, *ksz, *vg_alpha, *vg_n, *theta_s, *theta_r, *aev;
+  double specific_storage;
+  /* Boundary codes (FREHG_GW_BC_*): top/bottom per column (ny*nx); side
+   * codes per edge column: xm/xp indexed by j (ny), ym/yp by i (nx). */
+  const int *top_code, *bot_code, *xm_code, *xp_code, *ym_code, *yp_code;
+  /* Scheme switches (GroundwaterConfig). */
+  int use_full3d;
+  int pc_consistent;          /* predictor_corrector: 1 consistent, 0 legacy */
+  int face_harmonic;          /* face_conductivity: 1 harmonic, 0 arithmetic */
+  int reallocation_off;       /* reallocation: 1 disabled, 0 legacy */
+  int surplus_redistribute;   /* reallocation_surplus: 1 redistribute, 0 drop */
+  int saturated_contact_head; /* must be 1; the legacy in-place rule is order-dependent */
+  /* Adaptive controller (GroundwaterTimestepConfig). */
+  double dt_init, dt_min, dt_max, dq_grow, dq_shrink, courant_max;
+  /* Predictor solve (SolverSystemConfig; the preconditioner is Jacobi). */
+  double rtol, atol;
+  int max_iterations;
+  int precision;      /* FREHG_GW_PRECISION_* */
+  double outer_rtol;  /* mixed: ||b - A x|| / ||b|| target of the FP64 outer loop */
+  int max_outer;      /* mixed: outer-iteration cap */
+} frehg_gw_desc;
+
+/* GwStepAudit (src/gw/RichardsSolver.hpp:86-130) plus the solve statistics
+ * of RichardsSolver::lastSolve (:402) and the controller output (:261). */
+typedef struct frehg_gw_step_info {
+  int status;
+  int cg_iterations;     /* total inner iterations of the predictor solve */
+  int outer_iterations;  /* mixed precision: defect-correction sweeps; fp64: 1 */
+  double residual_norm;  /* final preconditioned residual norm ||D^-1 r|| */
+  double boundary_in;
+  double ss_storage;
+  double realloc_adjust;
+  double realloc_dropped;
+  double vloss;
+  double next_dt;
+} frehg_gw_step_info;
+
+typedef struct frehg_gw_handle frehg_gw_handle;
+
+/* Last error message of the calling thread ("" if none). */
+const char* frehg_gw_last_error(void);
+
+/* Build geometry, masks, global ids and device state for one domain. */
+int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out);
+int frehg_gw_destroy(frehg_gw_handle* h);
+
+/* Run all device work of h on this cudaStream_t (NULL = the library's own). */
+int frehg_gw_set_stream(frehg_gw_handle* h, void* cuda_stream);
+
+/* Boundary values (host arrays shaped like the codes; NULL keeps the current
+ * values).  Hydrostatic stages are given in the unshifted datum. */
+int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top_value,
+                           const double* bot_value, const double* xm_value,
+                           const double* xp_value, const double* ym_value,
+                           const double* yp_value);
+
+/* Initial state from one of the three IC forms; field is ny*nx*nz (moisture,
+ * head) or ny*nx (water table), NULL = the constant. */
+int frehg_gw_init_state(frehg_gw_handle* h, int form, double constant, const double* field);
+
+/* Overwrite the interior head and moisture (host, ny*nx*nz each). */
+int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc);
+
+/* One groundwater step of size dtg ending at time t. */
+int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* info);
+
+/* The controller's next dtg (dt_init before the first step). */
+int frehg_gw_next_dt(frehg_gw_handle* h, double* out);
+
+/* Copy a field to host memory (shape per FREHG_GW_FIELD_*). */
+int frehg_gw_get_field(frehg_gw_handle* h, int field, double* host_out);
+
+/* Number of doubles frehg_gw_get_field writes for this field. */
+size_t frehg_gw_field_size(const frehg_gw_handle* h, int field);
+
+/* Sum over active cells of theta * dx * dy * dz (FP64, fixed order). */
+int frehg_gw_owned_volume(frehg_gw_handle* h, double* out);
+
+/* Number of active cells. */
+long long frehg_gw_active_cells(const frehg_gw_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FREHG_GW_H */

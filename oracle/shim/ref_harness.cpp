@@ -1,0 +1,359 @@
+// C entry points around the reference's own, unmodified frehg::gw::
+// RichardsSolver (compiled from the reference's sources against the host
+// shims in oracle/shim/include).  Test infrastructure only: it builds the
+// solver exactly the way the reference's unit-test harness does
+// (tests/unit/test_gw.cpp:33-61, MiniGw::build) from an in-code FrehgConfig,
+// so python tests can drive the real reference step and read its fields.
+//
+// Field transfers use the reference's own (ny+2, nx+2, nz[+1]) halo layout
+// with k fastest (src/core/Types.hpp:35-43).
+
+#include "bc/BoundarySet.hpp"
+#include "core/Config.hpp"
+#include "core/Grid.hpp"
+#include "core/HaloExchanger.hpp"
+#include "core/Types.hpp"
+#include "gw/RichardsSolver.hpp"
+#include "gw/TerrainMetric.hpp"
+
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <memory>
+#include <string>
+#include <vector>
+
+extern "C" void frehg_shim_set_pc(const char* pc);
+
+extern "C" {
+
+/// Flat description of one groundwater case.  Soil types carry 8 numbers
+/// each: ksx, ksy, ksz, theta_s, theta_r, alpha, n, aev.  Boundary
+/// conditions: target (1 top, 2 bottom, 3 side), kind (4 head, 5 flux), value
+/// form (0 constant, 2 gravity, 3 hydrostatic), value, hydrostatic stage and
+/// polygon vertices (x, y pairs; bc_npts per condition, concatenated).
+typedef struct ref_case {
+  int nx, ny, nz;
+  double dx, dy, dz, dz_stretch;
+  int follow_terrain, terrain_uniform;
+  const double* bath;  // ny*nx (j*nx + i), or NULL for a flat bed at 0
+  int n_soil_types;
+  const double* soil_types;
+  const int* soil_map;  // ny*nx*nz ids ((j*nx + i)*nz + k), or NULL
+  int ic_form;          // 0 moisture, 1 head, 2 water table
+  double ic_const;
+  const double* ic_field;  // 3D for moisture/head, 2D for water table, or NULL
+  double ss;
+  int use_full3d, pc_consistent, harmonic, realloc_off, surplus_redistribute, sc_head;
+  double dt_init, dt_min, dt_max, dq_grow, dq_shrink, courant_max;
+  double rtol, atol;
+  int maxit;
+  int n_bc;
+  const int* bc_target;
+  const int* bc_kind;
+  const int* bc_form;
+  const double* bc_value;
+  const double* bc_eta;
+  const int* bc_npts;
+  const double* bc_pts;
+  const char* workdir;
+  const char* pc;  // "jacobi" | "icc"
+} ref_case;
+
+}  // extern "C"
+
+namespace {
+
+struct RefSim {
+  frehg::FrehgConfig cfg;
+  std::unique_ptr<frehg::Grid> grid;
+  std::unique_ptr<frehg::HaloExchanger> halo;
+  std::unique_ptr<frehg::gw::TerrainMetric> mesh;
+  std::unique_ptr<frehg::BoundarySet> boundaries;
+  std::unique_ptr<frehg::gw::RichardsSolver> gw;
+};
+
+std::string g_error;
+
+void writeFlat(const std::string& path, const double* v, std::size_t n) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) throw frehg::FatalError("cannot write " + path);
+  for (std::size_t k = 0; k < n; ++k) std::fprintf(f, "%.17g\n", v[k]);
+  std::fclose(f);
+}
+
+void copyOut(const frehg::Field3<double>& f, double* out) {
+  std::memcpy(out, f.data(), f.span() * sizeof(double));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_error.c_str(); }
+
+void* ref_create(const ref_case* c) {
+  try {
+    frehg_shim_set_pc(c->pc ? c->pc : "");
+    auto sim = std::make_unique<RefSim>();
+    frehg::FrehgConfig& cfg = sim->cfg;
+    const std::string dir = c->workdir ? c->workdir : ".";
+    std::filesystem::create_directories(dir);
+    cfg.configDir = dir;
+    cfg.simulation.id = "oracle-ref";
+    cfg.domain.nx = c->nx;
+    cfg.domain.ny = c->ny;
+    cfg.domain.nz = c->nz;
+    cfg.domain.dx = c->dx;
+    cfg.domain.dy = c->dy;
+    cfg.domain.dz = c->dz;
+    cfg.domain.dzStretch = c->dz_stretch;
+    cfg.domain.followTerrain = c->follow_terrain != 0;
+    cfg.domain.terrainLayers = c->terrain_uniform ? frehg::DomainConfig::TerrainLayers::Uniform
+                                                  : frehg::DomainConfig::TerrainLayers::Scaled;
+    const std::size_t ncol = static_cast<std::size_t>(c->nx) * static_cast<std::size_t>(c->ny);
+    const std::size_t ncell = ncol * static_cast<std::size_t>(c->nz);
+    if (c->bath) {
+      writeFlat(dir + "/bath.dat", c->bath, ncol);
+      cfg.domain.bottomElevation.fromFile = true;
+      cfg.domain.bottomElevation.file = "bath.dat";
+    } else {
+      cfg.domain.bottomElevation.constant = 0.0;
+    }
+    cfg.time.dt = c->dt_init;
+    cfg.time.tEnd = 1.0e9;
+    cfg.time.outputInterval = 1.0e9;
+    cfg.modules.groundwater = true;
+    auto& gw = cfg.groundwater;
+    gw.timestep.dtInit = c->dt_init;
+    gw.timestep.dtMin = c->dt_min;
+    gw.timestep.dtMax = c->dt_max;
+    gw.timestep.dqGrow = c->dq_grow;
+    gw.timestep.dqShrink = c->dq_shrink;
+    gw.timestep.courantMax = c->courant_max;
+    gw.specificStorage = c->ss;
+    gw.useFull3d = c->use_full3d != 0;
+    gw.predictorCorrector = c->pc_consistent
+                                ? frehg::GroundwaterConfig::PredictorCorrector::Consistent
+                                : frehg::GroundwaterConfig::PredictorCorrector::Legacy;
+    gw.faceConductivity = c->harmonic ? frehg::GroundwaterConfig::FaceConductivity::Harmonic
+                                      : frehg::GroundwaterConfig::FaceConductivity::Arithmetic;
+    gw.reallocation = c->realloc_off ? frehg::GroundwaterConfig::Reallocation::Off
+                                     : frehg::GroundwaterConfig::Reallocation::Legacy;
+    gw.reallocationSurplus = c->surplus_redistribute
+                                 ? frehg::GroundwaterConfig::ReallocationSurplus::Redistribute
+                                 : frehg::GroundwaterConfig::ReallocationSurplus::Drop;
+    gw.saturatedContact = c->sc_head ? frehg::GroundwaterConfig::SaturatedContact::Head
+                                     : frehg::GroundwaterConfig::SaturatedContact::Legacy;
+    cfg.solver.groundwater.rtol = c->rtol;
+    cfg.solver.groundwater.atol = c->atol;
+    cfg.solver.groundwater.maxIterations = c->maxit;
+
+    cfg.soil.types.clear();
+    for (int t = 0; t < c->n_soil_types; ++t) {
+      const double* s = c->soil_types + 8 * t;
+      frehg::SoilType st;
+      st.name = "type" + std::to_string(t);
+      st.ksx = s[0];
+      st.ksy = s[1];
+      st.ksz = s[2];
+      st.thetaS = s[3];
+      st.thetaR = s[4];
+      st.vgAlpha = s[5];
+      st.vgN = s[6];
+      st.aev = s[7];
+      cfg.soil.types.push_back(st);
+    }
+    if (c->soil_map) {
+      std::vector<double> ids(ncell);
+      for (std::size_t n = 0; n < ncell; ++n) ids[n] = c->soil_map[n];
+      writeFlat(dir + "/soil_id.dat", ids.data(), ncell);
+      cfg.soil.map.fromFile = true;
+      cfg.soil.map.file = "soil_id.dat";
+    } else {
+      cfg.soil.map.constantName = "type0";
+    }
+
+    auto& ic = cfg.initialConditions.groundwater;
+    ic.form = (c->ic_form == 0)   ? frehg::GroundwaterInitialConfig::Form::Moisture
+              : (c->ic_form == 1) ? frehg::GroundwaterInitialConfig::Form::Head
+                                  : frehg::GroundwaterInitialConfig::Form::WaterTable;
+    if (c->ic_field) {
+      writeFlat(dir + "/ic.dat", c->ic_field, c->ic_form == 2 ? ncol : ncell);
+      ic.value.fromFile = true;
+      ic.value.file = "ic.dat";
+    } else {
+      ic.value.constant = c->ic_const;
+    }
+
+    int off = 0;
+    for (int b = 0; b < c->n_bc; ++b) {
+      frehg::BoundaryConditionConfig bc;
+      bc.name = "bc" + std::to_string(b);
+      bc.target = static_cast<frehg::BcTarget>(c->bc_target[b]);
+      bc.kind = static_cast<frehg::BcKind>(c->bc_kind[b]);
+      bc.value.form = static_cast<frehg::BcValueConfig::Form>(c->bc_form[b]);
+      bc.value.constant = c->bc_value[b];
+      bc.value.hydrostaticEta = c->bc_eta[b];
+      for (int p = 0; p < c->bc_npts[b]; ++p) {
+        bc.polygon.push_back({c->bc_pts[2 * (off + p)], c->bc_pts[2 * (off + p) + 1]});
+      }
+      off += c->bc_npts[b];
+      cfg.boundaryConditions.push_back(bc);
+    }
+
+    sim->grid = std::make_unique<frehg::Grid>(MPI_COMM_WORLD, cfg.domain);
+    sim->halo = std::make_unique<frehg::HaloExchanger>(*sim->grid, false);
+    sim->mesh = std::make_unique<frehg::gw::TerrainMetric>(*sim->grid, cfg, *sim->halo);
+    sim->grid->buildGlobalIds(sim->mesh->ktop());
+    sim->boundaries =
+        std::make_unique<frehg::BoundarySet>(*sim->grid, cfg.boundaryConditions, cfg.configDir);
+    sim->gw = std::make_unique<frehg::gw::RichardsSolver>(*sim->grid, cfg, *sim->mesh,
+                                                          *sim->boundaries, *sim->halo);
+    return sim.release();
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return nullptr;
+  }
+}
+
+void ref_destroy(void* h) { delete static_cast<RefSim*>(h); }
+
+/// One RichardsSolver::step(t, dtg); t is the end-of-step time.
+int ref_step(void* h, double t, double dtg) {
+  try {
+    static_cast<RefSim*>(h)->gw->step(t, dtg);
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+double ref_next_dt(void* h) { return static_cast<RefSim*>(h)->gw->nextDt(); }
+
+double ref_owned_volume(void* h) { return static_cast<RefSim*>(h)->gw->ownedVolume(); }
+
+/// audit[0..6] = boundaryIn, ssStorage, reallocAdjust, reallocDropped, vloss,
+/// cplVent, pcClampVolume.
+void ref_audit(void* h, double* out) {
+  const auto& gw = *static_cast<RefSim*>(h)->gw;
+  const auto& a = gw.audit();
+  out[0] = a.boundaryIn;
+  out[1] = a.ssStorage;
+  out[2] = a.reallocAdjust;
+  out[3] = a.reallocDropped;
+  out[4] = a.vloss;
+  out[5] = a.cplVent;
+  out[6] = gw.pcClampVolume();
+}
+
+void ref_last_solve(void* h, int* iterations, double* residual) {
+  const auto& s = static_cast<RefSim*>(h)->gw->lastSolve();
+  *iterations = s.iterations;
+  *residual = s.residualNorm;
+}
+
+double ref_elevation_offset(void* h) { return static_cast<RefSim*>(h)->mesh->elevationOffset(); }
+
+/// Copy a named field out in the reference's halo layout.
+int ref_get(void* h, const char* name, double* out) {
+  RefSim& s = *static_cast<RefSim*>(h);
+  auto& gw = *s.gw;
+  auto& mesh = *s.mesh;
+  const std::string n(name);
+  if (n == "h") copyOut(gw.head(), out);
+  else if (n == "wc") copyOut(gw.waterContent(), out);
+  else if (n == "wcn") copyOut(gw.waterContentStart(), out);
+  else if (n == "qx") copyOut(gw.fluxXVolumetric(), out);
+  else if (n == "qy") copyOut(gw.fluxYVolumetric(), out);
+  else if (n == "qz") copyOut(gw.fluxZFaceVolumetric(), out);
+  else if (n == "kx") copyOut(gw.faceConductivityX(), out);
+  else if (n == "ky") copyOut(gw.faceConductivityY(), out);
+  else if (n == "kz") copyOut(gw.faceConductivityZFace(), out);
+  else if (n == "vloss") copyOut(gw.vlossField(), out);
+  else if (n == "dz3d") copyOut(mesh.dz3d(), out);
+  else if (n == "bot3d") copyOut(mesh.bot3d(), out);
+  else if (n == "ax") copyOut(mesh.areaX(), out);
+  else if (n == "ay") copyOut(mesh.areaY(), out);
+  else if (n == "sinx") copyOut(mesh.sinX(), out);
+  else if (n == "cosx") copyOut(mesh.cosX(), out);
+  else if (n == "siny") copyOut(mesh.sinY(), out);
+  else if (n == "cosy") copyOut(mesh.cosY(), out);
+  else if (n == "bath") std::memcpy(out, mesh.bath().data(), mesh.bath().span() * sizeof(double));
+  else {
+    g_error = "unknown field " + n;
+    return 1;
+  }
+  return 0;
+}
+
+/// Overwrite h and wc (halo layout; interiors authoritative) and rebuild the
+/// derived state, as a restart read does (RichardsSolver::refreshDerivedState).
+void ref_set_state(void* h, const double* head, const double* wc) {
+  auto& gw = *static_cast<RefSim*>(h)->gw;
+  std::memcpy(gw.head().data(), head, gw.head().span() * sizeof(double));
+  std::memcpy(gw.waterContent().data(), wc, gw.waterContent().span() * sizeof(double));
+  gw.refreshDerivedState();
+}
+
+/// Global ids (halo layout, -1 inactive) and the per-column ktop.
+void ref_gid(void* h, int* gid, int* ktop) {
+  RefSim& s = *static_cast<RefSim*>(h);
+  const auto& g = s.grid->gid3Host();
+  for (std::size_t n = 0; n < g.span(); ++n) gid[n] = g.data()[n];
+  const auto& kt = s.mesh->ktop();
+  for (std::size_t n = 0; n < kt.span(); ++n) ktop[n] = kt.data()[n];
+}
+
+/// The rasterized boundary markers, rebuilt from the BoundarySet exactly as
+/// RichardsSolver::buildBoundaryLists / updateBoundaryValues do
+/// (RichardsSolver.cpp:429-566), each (ny+2)*(nx+2): codes[0..5] =
+/// top, bottom, xm, xp, ym, yp; values likewise at time t.
+void ref_bc_masks(void* h, double t, int* codes, double* values) {
+  RefSim& s = *static_cast<RefSim*>(h);
+  const std::size_t n2 = static_cast<std::size_t>(s.grid->nyLocal() + 2) *
+                         static_cast<std::size_t>(s.grid->nxLocal() + 2);
+  const std::size_t nx2 = static_cast<std::size_t>(s.grid->nxLocal() + 2);
+  std::memset(codes, 0, 6 * n2 * sizeof(int));
+  std::memset(values, 0, 6 * n2 * sizeof(double));
+  for (const frehg::BoundaryCondition& bc : s.boundaries->all()) {
+    if (bc.target() != frehg::BcTarget::GroundwaterTop &&
+        bc.target() != frehg::BcTarget::GroundwaterBottom &&
+        bc.target() != frehg::BcTarget::GroundwaterSide) {
+      continue;
+    }
+    int code = 0;
+    if (bc.kind() == frehg::BcKind::Head) {
+      code = (bc.valueForm() == frehg::BcValueConfig::Form::Hydrostatic) ? 4 : 1;
+    } else if (bc.kind() == frehg::BcKind::Flux) {
+      code = (bc.valueForm() == frehg::BcValueConfig::Form::Gravity) ? 3 : 2;
+    } else {
+      continue;
+    }
+    double v = bc.value(t);
+    if (code == 4) v += s.mesh->elevationOffset();
+    for (const frehg::BcCell& cell : bc.cells()) {
+      frehg::BcFace face = cell.face;
+      if (bc.target() == frehg::BcTarget::GroundwaterTop) face = frehg::BcFace::Top;
+      if (bc.target() == frehg::BcTarget::GroundwaterBottom) face = frehg::BcFace::Bottom;
+      int slot = 0;
+      switch (face) {
+        case frehg::BcFace::Top: slot = 0; break;
+        case frehg::BcFace::Bottom: slot = 1; break;
+        case frehg::BcFace::XMinus: slot = 2; break;
+        case frehg::BcFace::XPlus: slot = 3; break;
+        case frehg::BcFace::YMinus: slot = 4; break;
+        case frehg::BcFace::YPlus: slot = 5; break;
+      }
+      const std::size_t at = static_cast<std::size_t>(cell.j) * nx2 + static_cast<std::size_t>(cell.i);
+      codes[static_cast<std::size_t>(slot) * n2 + at] = code;
+      values[static_cast<std::size_t>(slot) * n2 + at] = v;
+    }
+  }
+}
+
+void ref_reallocate_only(void* h) { static_cast<RefSim*>(h)->gw->reallocateWaterContent(); }
+
+}  // extern "C"
