@@ -1,0 +1,281 @@
+"""Throughput of the B200 groundwater step (cell-steps/s).
+
+Workload: the terrain-following heterogeneous slab of
+``frehg_b200.workloads.hillslope`` (512x512x128 by default, 33.5M cells,
+seeded synthetic inputs), one groundwater step (``RichardsSolver::step``:
+predictor assembly, Jacobi-PCG head solve, corrector, post-allocation,
+clamp, audit, adaptive controller) per timed step, dt driven by the
+step's own controller from dt0 = 60 s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   # the reference's CPU step
+
+With N > 1 the script runs under torchrun, one rank per GPU; every rank
+steps its own independent domain (an ensemble member with its own seed), so
+the work per GPU is fixed (weak scaling) and there is no data-path
+collective; rank 0 prints the line with the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALG_BYTES_PER_CG_ITER = 128  # FP64 Jacobi-PCG iteration, bytes per active cell
+ALG_BYTES_FIXED = 536        # FP64 step outside the solve, bytes per active cell
+METRIC = "cell-steps/s at 512x512x128"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--size", default="512,512,128")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-sample", default="64,64,128")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(sample: str, threads: int):
+    """The reference's own CPU step (its src/gw compiled on host shims, OpenMP
+    shim backend, the reference's default bjacobi-ICC(0) CG) on a bounded crop
+    of the same workload."""
+    from frehg_b200 import workloads
+    from oracle import ref as refmod
+    if not refmod.available(omp=True):
+        return None
+    nx, ny, nz = (int(v) for v in sample.split(","))
+    cfg = workloads.hillslope(nx, ny, nz, per_cell_soil=False)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    r = refmod.RefSolver(cfg, pc="icc", omp=True)
+    r.advance()  # warm-up step
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        r.advance()
+        steps += 1
+        if time.perf_counter() - t0 > 10.0 or steps >= 20:
+            break
+    dt = time.perf_counter() - t0
+    _, ktop = r.gid()
+    active = int(sum(nz - k for k in ktop.ravel()))
+    r.close()
+    return {"value": active * steps / dt, "unit": "cell-steps/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{nx}x{ny}x{nz} crop of the slab, {steps} steps after 1 warm-up, "
+                      "reference src/gw on host shims (OpenMP), bjacobi-ICC(0) CG"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    res = cpu_baseline(args.cpu_sample, threads)
+    if res is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref (reference sources on host shims) not built"}))
+        return
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": f"terrain slab crop {args.cpu_sample} (CPU-sized sample of "
+                               f"{args.size})", "parallelism": "host threads"},
+        "cpu_baseline": {k: res[k] for k in ("kind", "cores", "sample")} | {"value": res["value"],
+                                                                           "unit": "cell-steps/s"},
+        "e2e": {"value": res["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from frehg_b200 import workloads
+    from frehg_b200.config import rasterize
+    from frehg_b200.gw import RichardsSolver
+
+    nx, ny, nz = (int(v) for v in args.size.split(","))
+    cfg = workloads.hillslope(nx, ny, nz, seed=20261203 + rank, precision=args.precision)
+    stream = torch.cuda.Stream()
+    gw = RichardsSolver(cfg, stream=stream.cuda_stream)
+    active = gw.activeCells()
+    for _ in range(args.warmup):
+        gw.advance()
+    gw.setProfiling(True)
+    launches0 = gw.kernelLaunches()
+    iters, solve_ms = 0, 0.0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            gw.advance()
+            iters += gw.lastSolve()[0]
+            solve_ms += gw.phaseTimes()["solve"]
+        end.record(stream)
+        torch.cuda.synchronize()
+    launches = gw.kernelLaunches() - launches0
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        a = torch.tensor([float(active)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(a)
+        total_cells = float(a.item())
+    else:
+        total_cells = float(active)
+    value = total_cells * args.steps / (ms / 1e3)
+
+    # End to end through the C ABI with host buffers: boundary values in from
+    # pinned host memory, head and moisture back to host, every step.
+    ras = rasterize(cfg)
+    h2d = sum(v.nbytes for v in (ras.top_value, ras.bot_value, ras.xm_value, ras.xp_value,
+                                 ras.ym_value, ras.yp_value))
+    d2h = 2 * active * 8
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        gw.setBoundaryValues(ras.top_value, ras.bot_value, ras.xm_value, ras.xp_value,
+                             ras.ym_value, ras.yp_value)
+        gw.advance()
+        _ = gw.head()
+        _ = gw.waterContent()
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": active * args.e2e_steps / e2e_s * (total_cells / active),
+           "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+    gw.close()
+
+    peak, peak_kind = peaks()
+    achieved = ALG_BYTES_PER_CG_ITER * active * iters / (solve_ms / 1e3) / 1e9 if solve_ms else 0.0
+    roof = {"bound": "hbm", "kernel": "k_cg64 (Jacobi-PCG solve, one launch per step)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_kind, "traffic": None,
+            "alg_bytes_per_cell_iter": ALG_BYTES_PER_CG_ITER,
+            "cg_iterations_per_step": iters / args.steps,
+            "solve_share": solve_ms / ms if ms else None}
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(args.cpu_sample,
+                                                                      os.cpu_count() or 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32-inner/f64",
+        "data": "synthetic",
+        "config": {"workload": f"terrain-following heterogeneous slab {nx}x{ny}x{nz} "
+                               f"(hillslope, seeded), dt0 60 s adaptive, {args.precision} solve",
+                   "active_cells_per_gpu": active, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (13 GB working set)"},
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -196,6 +196,35 @@ def polygon_contains(poly: Sequence[Tuple[float, float]], x: float, y: float) ->
     return inside
 
 
+def polygon_mask(poly: Sequence[Tuple[float, float]], x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """Vectorized :func:`polygon_contains` over arrays of points (same
+    arithmetic, element by element)."""
+    x = np.asarray(x, np.float64)
+    y = np.asarray(y, np.float64)
+    xs = [p[0] for p in poly]
+    ys = [p[1] for p in poly]
+    bbox = ((x >= min(xs) - 1e-12) & (x <= max(xs) + 1e-12) &
+            (y >= min(ys) - 1e-12) & (y <= max(ys) + 1e-12))
+    n = len(poly)
+    edge = np.zeros(x.shape, bool)
+    inside = np.zeros(x.shape, bool)
+    ax_ = np.abs(x)
+    ay_ = np.abs(y)
+    for v in range(n):
+        a, b = poly[v], poly[(v + 1) % n]
+        cross = (b[0] - a[0]) * (y - a[1]) - (b[1] - a[1]) * (x - a[0])
+        scale = np.maximum(np.maximum(ax_, ay_), max(abs(a[0]), abs(a[1]), abs(b[0]), abs(b[1]), 1.0))
+        s2 = scale * scale
+        dot = (x - a[0]) * (b[0] - a[0]) + (y - a[1]) * (b[1] - a[1])
+        len2 = (b[0] - a[0]) ** 2 + (b[1] - a[1]) ** 2
+        edge |= (np.abs(cross) <= 1.0e-12 * s2) & (dot >= -1.0e-12 * s2) & (dot <= len2 + 1.0e-12 * s2)
+        crosses = (a[1] > y) != (b[1] > y)
+        if b[1] != a[1]:
+            xint = a[0] + (y - a[1]) / (b[1] - a[1]) * (b[0] - a[0])
+            inside ^= crosses & (x < xint)
+    return bbox & (edge | inside)
+
+
 @dataclass
 class Rasterized:
     """Per-cell / per-column arrays for ``frehg_gw_desc``."""
@@ -249,32 +278,28 @@ def rasterize(cfg: GwConfig, t: float = 0.0) -> Rasterized:
     codes["ym"] = np.zeros(nx, np.int32)
     codes["yp"] = np.zeros(nx, np.int32)
     vals = {k: np.zeros(v.shape, np.float64) for k, v in codes.items()}
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    xc = (ii + 0.5) * d.dx
+    yc = (jj + 0.5) * d.dy
     for bc in cfg.boundary_conditions:
         code = bc.code()
         v = bc.value_at(t)
-        for j in range(ny):
-            yc = (j + 0.5) * d.dy
-            for i in range(nx):
-                xc = (i + 0.5) * d.dx
-                if not polygon_contains(bc.polygon, xc, yc):
-                    continue
-                if bc.target == "groundwater_top":
-                    codes["top"][j, i] = code
-                    vals["top"][j, i] = v
-                elif bc.target == "groundwater_bottom":
-                    codes["bot"][j, i] = code
-                    vals["bot"][j, i] = v
-                elif bc.target == "groundwater_side":
-                    if i == 0:
-                        codes["xm"][j], vals["xm"][j] = code, v
-                    if i == nx - 1:
-                        codes["xp"][j], vals["xp"][j] = code, v
-                    if j == 0:
-                        codes["ym"][i], vals["ym"][i] = code, v
-                    if j == ny - 1:
-                        codes["yp"][i], vals["yp"][i] = code, v
-                else:
-                    raise ValueError(f"unknown target {bc.target}")
+        sel = polygon_mask(bc.polygon, xc, yc)
+        if bc.target == "groundwater_top":
+            codes["top"][sel] = code
+            vals["top"][sel] = v
+        elif bc.target == "groundwater_bottom":
+            codes["bot"][sel] = code
+            vals["bot"][sel] = v
+        elif bc.target == "groundwater_side":
+            for key, m in (("xm", sel[:, 0]), ("xp", sel[:, nx - 1])):
+                codes[key][m] = code
+                vals[key][m] = v
+            for key, m in (("ym", sel[0, :]), ("yp", sel[ny - 1, :])):
+                codes[key][m] = code
+                vals[key][m] = v
+        else:
+            raise ValueError(f"unknown target {bc.target}")
     return Rasterized(
         dz_layers=d.dz_layers(),
         bath=bath,

@@ -1,0 +1,564 @@
+// The C ABI of the B200 groundwater step (include/frehg_gw.h): handle
+// lifetime, device memory, and the per-step orchestration of the kernels in
+// gw_kernels.cu and gw_cg.cu.  No exception crosses the ABI; every entry
+// point returns a frehg_gw_status and records a message for
+// frehg_gw_last_error().
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+#include "../../include/frehg_gw.h"
+#include "gw_internal.h"
+#include "gw_setup.h"
+
+struct frehg_gw_handle {
+  fgw::Device D;
+  double offset = 0.0;
+  long long nactive = 0;
+  double* bath_dev = nullptr;
+  std::vector<int> codes;      // host copy, 6 x ncol
+  std::vector<double> values;  // host staging, 6 x ncol
+  double rtol = 1e-8, atol = 1e-14, outer_rtol = 1e-10;
+  int maxit = 1000, max_outer = 30, precision = 0;
+  double dt_min = 0, dt_max = 0, dq_grow = 0.01, dq_shrink = 0.02, co_max = 2.0;
+  double next_dt = 0.0;
+  bool have_state = false;
+  int start_buf = 0;  // ping-pong index of the last step's theta^n
+  bool profiling = false;
+  cudaEvent_t ev[6] = {};
+  double phase_ms[5] = {0, 0, 0, 0, 0};
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int status, const std::string& msg) {
+  g_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(FREHG_GW_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(call, what)                    \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(fgw::Device& D, T** p, size_t n) {
+  void* raw = nullptr;
+  cudaError_t e = cudaMalloc(&raw, (n ? n : 1) * sizeof(T));
+  if (e != cudaSuccess) return e;
+  D.allocs.push_back(raw);
+  e = cudaMemset(raw, 0, (n ? n : 1) * sizeof(T));
+  *p = static_cast<T*>(raw);
+  return e;
+}
+
+// Solver arrays carry a zero margin of one j-row on both ends.
+template <class T>
+cudaError_t dalloc_margin(fgw::Device& D, T** p, long long ncell, long long margin) {
+  T* base = nullptr;
+  cudaError_t e = dalloc(D, &base, static_cast<size_t>(ncell + 2 * margin));
+  *p = base + margin;
+  return e;
+}
+
+void free_device(fgw::Device& D) {
+  for (void* p : D.allocs) cudaFree(p);
+  D.allocs.clear();
+  if (D.out_host) cudaFreeHost(D.out_host);
+  D.out_host = nullptr;
+  if (D.own_stream && D.stream) cudaStreamDestroy(D.stream);
+  D.stream = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* frehg_gw_last_error(void) { return g_error.c_str(); }
+
+int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
+  g_error.clear();
+  if (!desc || !out) return fail(FREHG_GW_EINVAL, "frehg_gw_create: null argument");
+  *out = nullptr;
+  try {
+    fgw::HostDomain H;
+    std::string err;
+    const int rc = fgw::build_host_domain(*desc, H, err);
+    if (rc != FREHG_GW_OK) return fail(rc, "frehg_gw_create: " + err);
+    if (desc->precision != FREHG_GW_PRECISION_FP64 && desc->precision != FREHG_GW_PRECISION_MIXED)
+      return fail(FREHG_GW_EINVAL, "frehg_gw_create: unknown precision");
+    if (!(desc->rtol >= 0.0) || !(desc->atol >= 0.0) || desc->max_iterations < 1)
+      return fail(FREHG_GW_EINVAL, "frehg_gw_create: invalid solver tolerances");
+
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    int coop = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "attribute");
+    if (!coop) return fail(FREHG_GW_ECUDA, "device lacks cooperative launch");
+
+    auto* hnd = new frehg_gw_handle();
+    fgw::Device& D = hnd->D;
+    CUDA_TRY(cudaDeviceGetAttribute(&D.sm_count, cudaDevAttrMultiProcessorCount, dev), "sm");
+    CUDA_TRY(cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking), "stream");
+    D.own_stream = true;
+
+    fgw::Dims& d = D.d;
+    d.nx = H.nx;
+    d.ny = H.ny;
+    d.nz = H.nz;
+    d.nx2 = H.nx + 2;
+    d.ny2 = H.ny + 2;
+    d.sx = H.nz;
+    d.sy = static_cast<long long>(H.nx + 2) * H.nz;
+    d.ncell = H.ncell;
+    d.ncol = H.ncol;
+    d.dx = desc->dx;
+    d.dy = desc->dy;
+    d.az = desc->dx * desc->dy;
+    d.ss = desc->specific_storage;
+    d.full3d = desc->use_full3d ? 1 : 0;
+    d.pc = desc->pc_consistent ? 1 : 0;
+    d.harm = (desc->pc_consistent && desc->face_harmonic) ? 1 : 0;
+    d.off = desc->reallocation_off ? 1 : 0;
+    d.redistribute = desc->surplus_redistribute ? 1 : 0;
+    d.terrain = desc->follow_terrain ? 1 : 0;
+
+    const long long n3 = d.ncell, nf = d.ncol * (d.nz + 1), m = d.sy;
+    auto up = [&](double** p, const std::vector<double>& v) -> cudaError_t {
+      cudaError_t e = dalloc(D, p, v.size());
+      if (e != cudaSuccess) return e;
+      return cudaMemcpy(*p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
+    };
+    cudaError_t e = cudaSuccess;
+    double** soil[8] = {&D.ksx, &D.ksy, &D.ksz, &D.vga, &D.vgn, &D.wcs, &D.wcr, &D.aev};
+    for (int f = 0; f < 8 && e == cudaSuccess; ++f) e = up(soil[f], H.soil[f]);
+    if (e == cudaSuccess) e = up(&D.dz, H.dz);
+    if (e == cudaSuccess) e = up(&D.bot, H.bot);
+    if (e == cudaSuccess) e = up(&D.ax, H.ax);
+    if (e == cudaSuccess) e = up(&D.ay, H.ay);
+    if (e == cudaSuccess) e = up(&D.sinx, H.sinx);
+    if (e == cudaSuccess) e = up(&D.cosx, H.cosx);
+    if (e == cudaSuccess) e = up(&D.siny, H.siny);
+    if (e == cudaSuccess) e = up(&D.cosy, H.cosy);
+    if (e == cudaSuccess) e = up(&hnd->bath_dev, H.bath);
+    if (e == cudaSuccess) e = dalloc(D, &D.act, static_cast<size_t>(n3));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(D.act, H.act.data(), static_cast<size_t>(n3), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = dalloc(D, &D.codes, 6 * static_cast<size_t>(d.ncol));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(D.codes, H.codes.data(), H.codes.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = dalloc(D, &D.values, 6 * static_cast<size_t>(d.ncol));
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+      e = dalloc(D, &D.h[b], n3);
+      if (e == cudaSuccess) e = dalloc(D, &D.wc[b], n3);
+    }
+    double** cellf[] = {&D.hp, &D.wcu, &D.kcx, &D.kcy, &D.kcz, &D.kx, &D.ky, &D.qx, &D.qy,
+                        &D.vloss, &D.room, &D.sup, &D.sdn};
+    for (double** p : cellf)
+      if (e == cudaSuccess) e = dalloc(D, p, n3);
+    if (e == cudaSuccess) e = dalloc(D, &D.kzf, nf);
+    if (e == cudaSuccess) e = dalloc(D, &D.qzf, nf);
+    if (e == cudaSuccess) e = dalloc(D, &D.colflag, d.ncol);
+    double** solv[] = {&D.diag, &D.gxp, &D.gyp, &D.gzp, &D.rhs, &D.x, &D.r, &D.p0, &D.p1, &D.w};
+    for (double** p : solv)
+      if (e == cudaSuccess) e = dalloc_margin(D, p, n3, m);
+    if (desc->precision == FREHG_GW_PRECISION_MIXED) {
+      float** solv32[] = {&D.diag32, &D.gxp32, &D.gyp32, &D.gzp32, &D.r32,
+                          &D.x32,    &D.p032,  &D.p132,  &D.w32};
+      for (float** p : solv32)
+        if (e == cudaSuccess) e = dalloc_margin(D, p, n3, m);
+    }
+    if (e != cudaSuccess) {
+      free_device(D);
+      delete hnd;
+      return fail(e == cudaErrorMemoryAllocation ? FREHG_GW_ENOMEM : FREHG_GW_ECUDA,
+                  std::string("frehg_gw_create: ") + cudaGetErrorString(e));
+    }
+    // Diagonal 1 everywhere outside the active rows (ghosts, margins), so the
+    // Jacobi scaling of those always-zero entries stays finite.
+    {
+      std::vector<double> ones(static_cast<size_t>(n3 + 2 * m), 1.0);
+      e = cudaMemcpy(D.diag - m, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess && D.diag32) {
+        std::vector<float> onesf(ones.size(), 1.0f);
+        e = cudaMemcpy(D.diag32 - m, onesf.data(), onesf.size() * sizeof(float),
+                       cudaMemcpyHostToDevice);
+      }
+    }
+    D.nblk = static_cast<int>(std::min<long long>((n3 + fgw::kBlock - 1) / fgw::kBlock,
+                                                  static_cast<long long>(D.sm_count) * 8));
+    if (D.nblk < 1) D.nblk = 1;
+    D.cg_grid = fgw::cg64_grid(D.sm_count, n3);
+    D.cg_grid32 = fgw::cg32_grid(D.sm_count, n3);
+    if (e == cudaSuccess)
+      e = dalloc(D, &D.partial, static_cast<size_t>(fgw::kPSlots) * D.nblk);
+    if (e == cudaSuccess)
+      e = dalloc(D, &D.cgpart, 4 * static_cast<size_t>(std::max(D.cg_grid, D.cg_grid32)));
+    if (e == cudaSuccess) e = dalloc(D, &D.out, 1);
+    if (e == cudaSuccess) e = cudaMallocHost(&D.out_host, sizeof(fgw::StepOut));
+    if (e != cudaSuccess) {
+      free_device(D);
+      delete hnd;
+      return fail(FREHG_GW_ECUDA, std::string("frehg_gw_create: ") + cudaGetErrorString(e));
+    }
+
+    fgw::Fields& f = D.f;
+    f.ksx = D.ksx;
+    f.ksy = D.ksy;
+    f.ksz = D.ksz;
+    f.vga = D.vga;
+    f.vgn = D.vgn;
+    f.wcs = D.wcs;
+    f.wcr = D.wcr;
+    f.aev = D.aev;
+    f.dz = D.dz;
+    f.bot = D.bot;
+    f.ax = D.ax;
+    f.ay = D.ay;
+    f.sinx = D.sinx;
+    f.cosx = D.cosx;
+    f.siny = D.siny;
+    f.cosy = D.cosy;
+    f.act = D.act;
+    f.topc = D.codes;
+    f.botc = D.codes + d.ncol;
+    f.xmc = D.codes + 2 * d.ncol;
+    f.xpc = D.codes + 3 * d.ncol;
+    f.ymc = D.codes + 4 * d.ncol;
+    f.ypc = D.codes + 5 * d.ncol;
+    f.topv = D.values;
+    f.botv = D.values + d.ncol;
+    f.xmv = D.values + 2 * d.ncol;
+    f.xpv = D.values + 3 * d.ncol;
+    f.ymv = D.values + 4 * d.ncol;
+    f.ypv = D.values + 5 * d.ncol;
+
+    hnd->offset = H.offset;
+    hnd->nactive = H.nactive;
+    hnd->codes = H.codes;
+    hnd->values.assign(6 * static_cast<size_t>(d.ncol), 0.0);
+    hnd->rtol = desc->rtol;
+    hnd->atol = desc->atol;
+    hnd->maxit = desc->max_iterations;
+    hnd->precision = desc->precision;
+    hnd->outer_rtol = desc->outer_rtol > 0 ? desc->outer_rtol : 1e-10;
+    hnd->max_outer = desc->max_outer > 0 ? desc->max_outer : 30;
+    hnd->dt_min = desc->dt_min;
+    hnd->dt_max = desc->dt_max;
+    hnd->dq_grow = desc->dq_grow;
+    hnd->dq_shrink = desc->dq_shrink;
+    hnd->co_max = desc->courant_max;
+    hnd->next_dt = desc->dt_init;
+    CUDA_TRY(cudaDeviceSynchronize(), "frehg_gw_create");
+    *out = hnd;
+    return FREHG_GW_OK;
+  } catch (const std::exception& ex) {
+    return fail(FREHG_GW_ENOMEM, std::string("frehg_gw_create: ") + ex.what());
+  }
+}
+
+int frehg_gw_destroy(frehg_gw_handle* h) {
+  if (!h) return FREHG_GW_OK;
+  cudaStreamSynchronize(h->D.stream);
+  for (cudaEvent_t& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  free_device(h->D);
+  delete h;
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_set_stream(frehg_gw_handle* h, void* stream) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  CUDA_TRY(cudaStreamSynchronize(h->D.stream), "set_stream");
+  if (h->D.own_stream) cudaStreamDestroy(h->D.stream);
+  if (stream) {
+    h->D.stream = static_cast<cudaStream_t>(stream);
+    h->D.own_stream = false;
+  } else {
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->D.stream, cudaStreamNonBlocking), "stream");
+    h->D.own_stream = true;
+  }
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* bot,
+                           const double* xm, const double* xp, const double* ym, const double* yp) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  const fgw::Dims& d = h->D.d;
+  const long long nc = d.ncol;
+  auto put = [&](int slot, long long col, double v) {
+    const int code = h->codes[slot * nc + col];
+    h->values[slot * nc + col] = v + (code == FREHG_GW_BC_HEAD_HYDROSTATIC ? h->offset : 0.0);
+  };
+  for (int j = 1; j <= d.ny; ++j) {
+    for (int i = 1; i <= d.nx; ++i) {
+      const long long q = static_cast<long long>(j - 1) * d.nx + (i - 1);
+      if (top) put(0, fgw::col2(d, j, i), top[q]);
+      if (bot) put(1, fgw::col2(d, j, i), bot[q]);
+    }
+  }
+  for (int j = 1; j <= d.ny; ++j) {
+    if (xm) put(2, fgw::col2(d, j, 1), xm[j - 1]);
+    if (xp) put(3, fgw::col2(d, j, d.nx), xp[j - 1]);
+  }
+  for (int i = 1; i <= d.nx; ++i) {
+    if (ym) put(4, fgw::col2(d, 1, i), ym[i - 1]);
+    if (yp) put(5, fgw::col2(d, d.ny, i), yp[i - 1]);
+  }
+  for (double v : h->values)
+    if (!std::isfinite(v)) return fail(FREHG_GW_EINVAL, "non-finite boundary value");
+  CUDA_TRY(cudaMemcpyAsync(h->D.values, h->values.data(), h->values.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, h->D.stream),
+           "set_bc_values");
+  CUDA_TRY(cudaStreamSynchronize(h->D.stream), "set_bc_values");
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_init_state(frehg_gw_handle* h, int form, double constant, const double* field) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  if (form < FREHG_GW_IC_MOISTURE || form > FREHG_GW_IC_WATER_TABLE)
+    return fail(FREHG_GW_EINVAL, "unknown initial-condition form");
+  fgw::Device& D = h->D;
+  const fgw::Dims& d = D.d;
+  double* fdev = nullptr;
+  if (field) {
+    const size_t n = (form == FREHG_GW_IC_WATER_TABLE)
+                         ? static_cast<size_t>(d.nx) * d.ny
+                         : static_cast<size_t>(d.nx) * d.ny * d.nz;
+    CUDA_TRY(cudaMalloc(&fdev, n * sizeof(double)), "init_state");
+    CUDA_TRY(cudaMemcpy(fdev, field, n * sizeof(double), cudaMemcpyHostToDevice), "init_state");
+  }
+  D.cur = 0;
+  fgw::launch_init_state(D, form, constant, fdev, h->bath_dev, h->offset);
+  fgw::launch_ghosts(D, D.h[0], D.wc[0]);
+  CUDA_TRY(cudaMemcpyAsync(D.h[1], D.h[0], d.ncell * sizeof(double), cudaMemcpyDeviceToDevice,
+                           D.stream), "init_state");
+  CUDA_TRY(cudaMemcpyAsync(D.wc[1], D.wc[0], d.ncell * sizeof(double), cudaMemcpyDeviceToDevice,
+                           D.stream), "init_state");
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "init_state");
+  if (fdev) cudaFree(fdev);
+  CUDA_TRY(cudaGetLastError(), "init_state kernel");
+  h->have_state = true;
+  h->start_buf = 0;
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc) {
+  if (!h || !head || !wc) return fail(FREHG_GW_EINVAL, "null argument");
+  fgw::Device& D = h->D;
+  const fgw::Dims& d = D.d;
+  std::vector<double> hh(static_cast<size_t>(d.ncell)), ww(static_cast<size_t>(d.ncell));
+  CUDA_TRY(cudaMemcpy(hh.data(), D.h[D.cur], d.ncell * sizeof(double), cudaMemcpyDeviceToHost),
+           "set_state");
+  CUDA_TRY(cudaMemcpy(ww.data(), D.wc[D.cur], d.ncell * sizeof(double), cudaMemcpyDeviceToHost),
+           "set_state");
+  for (int j = 1; j <= d.ny; ++j)
+    for (int i = 1; i <= d.nx; ++i)
+      for (int k = 0; k < d.nz; ++k) {
+        const long long q = (static_cast<long long>(j - 1) * d.nx + (i - 1)) * d.nz + k;
+        hh[fgw::cidx(d, j, i, k)] = head[q];
+        ww[fgw::cidx(d, j, i, k)] = wc[q];
+      }
+  for (int b = 0; b < 2; ++b) {
+    CUDA_TRY(cudaMemcpy(D.h[b], hh.data(), d.ncell * sizeof(double), cudaMemcpyHostToDevice),
+             "set_state");
+    CUDA_TRY(cudaMemcpy(D.wc[b], ww.data(), d.ncell * sizeof(double), cudaMemcpyHostToDevice),
+             "set_state");
+    fgw::launch_ghosts(D, D.h[b], D.wc[b]);
+  }
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "set_state");
+  h->have_state = true;
+  h->start_buf = D.cur;
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* info) {
+  (void)t;  // boundary values arrive through frehg_gw_set_bc_values
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  if (!h->have_state) return fail(FREHG_GW_ESTATE, "frehg_gw_step before frehg_gw_init_state");
+  if (!(dtg > 0.0) || !std::isfinite(dtg)) return fail(FREHG_GW_EINVAL, "dtg must be positive");
+  fgw::Device& D = h->D;
+  const int cur = D.cur, nxt = 1 - cur;
+  double* hn = D.h[cur];
+  double* wcn = D.wc[cur];
+  const bool prof = h->profiling;
+  auto mark = [&](int n) {
+    if (prof) cudaEventRecord(h->ev[n], D.stream);
+  };
+  // Step-start refresh, predictor, solve.
+  mark(0);
+  fgw::launch_ghosts(D, hn, wcn);
+  fgw::launch_closure_pred(D, hn);
+  fgw::launch_assemble(D, hn, wcn, dtg);
+  mark(1);
+  cudaError_t e;
+  if (h->precision == FREHG_GW_PRECISION_MIXED) {
+    e = fgw::launch_cg_mixed(D, h->rtol, h->atol, h->maxit, h->outer_rtol, h->max_outer);
+  } else {
+    e = fgw::launch_cg64(D, h->rtol, h->atol, h->maxit);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "predictor solve launch");
+  mark(2);
+  // Corrector, post-allocation, clamp, audit, controller.
+  fgw::launch_closure_corr(D, hn);
+  fgw::launch_flux(D, wcn, dtg);
+  fgw::launch_update_wc(D, hn, wcn, dtg);
+  mark(3);
+  fgw::launch_classify(D, D.wc[nxt], D.h[nxt]);
+  fgw::launch_walk(D, D.wc[nxt], dtg);
+  mark(4);
+  fgw::launch_finalize(D, D.wc[nxt], dtg, h->co_max);
+  fgw::launch_step_info(D, dtg, h->dq_grow, h->dq_shrink, h->dt_min, h->dt_max);
+  mark(5);
+  CUDA_TRY(cudaMemcpyAsync(D.out_host, D.out, sizeof(fgw::StepOut), cudaMemcpyDeviceToHost,
+                           D.stream), "step readback");
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "step");
+  CUDA_TRY(cudaGetLastError(), "step kernels");
+  if (prof) {
+    for (int n = 0; n < 5; ++n) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, h->ev[n], h->ev[n + 1]);
+      h->phase_ms[n] = ms;
+    }
+  }
+  const fgw::StepOut& o = *D.out_host;
+  frehg_gw_step_info s{};
+  s.cg_iterations = o.cg.its;
+  s.outer_iterations = o.cg.outer;
+  s.residual_norm = o.cg.dp;
+  s.boundary_in = o.boundary_in;
+  s.ss_storage = o.ss_storage;
+  s.realloc_adjust = o.realloc_adjust;
+  s.realloc_dropped = o.realloc_dropped;
+  s.vloss = o.vloss;
+  s.next_dt = o.next_dt;
+  int status = FREHG_GW_OK;
+  if (o.cg.err) {
+    status = fail(FREHG_GW_ECUDA, "predictor solve: grid barrier timed out");
+  } else if (o.cg.reason < 0) {
+    status = fail(FREHG_GW_ESOLVER, "predictor solve diverged after " + std::to_string(o.cg.its) +
+                                        " iterations (KSP reason " +
+                                        std::to_string(o.cg.reason) + ")");
+  } else if (!std::isfinite(o.volume)) {
+    status = fail(FREHG_GW_ENONFINITE, "non-finite moisture after the step");
+  }
+  s.status = status;
+  if (info) *info = s;
+  if (status != FREHG_GW_OK) return status;
+  h->start_buf = cur;
+  D.cur = nxt;
+  h->next_dt = o.next_dt;
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_next_dt(frehg_gw_handle* h, double* out) {
+  if (!h || !out) return fail(FREHG_GW_EINVAL, "null argument");
+  *out = h->next_dt;
+  return FREHG_GW_OK;
+}
+
+size_t frehg_gw_field_size(const frehg_gw_handle* h, int field) {
+  if (!h) return 0;
+  const fgw::Dims& d = h->D.d;
+  const size_t nx = d.nx, ny = d.ny, nz = d.nz;
+  switch (field) {
+    case FREHG_GW_FIELD_QX: case FREHG_GW_FIELD_KX: case FREHG_GW_FIELD_AX:
+    case FREHG_GW_FIELD_SINX: case FREHG_GW_FIELD_COSX:
+      return ny * (nx + 1) * nz;
+    case FREHG_GW_FIELD_QY: case FREHG_GW_FIELD_KY: case FREHG_GW_FIELD_AY:
+    case FREHG_GW_FIELD_SINY: case FREHG_GW_FIELD_COSY:
+      return (ny + 1) * nx * nz;
+    case FREHG_GW_FIELD_QZ: case FREHG_GW_FIELD_KZ:
+      return ny * nx * (nz + 1);
+    default:
+      return (field >= 0 && field < FREHG_GW_FIELD_COUNT) ? ny * nx * nz : 0;
+  }
+}
+
+int frehg_gw_get_field(frehg_gw_handle* h, int field, double* out) {
+  if (!h || !out) return fail(FREHG_GW_EINVAL, "null argument");
+  fgw::Device& D = h->D;
+  const fgw::Dims& d = D.d;
+  const double* src = nullptr;
+  int kind = 0;  // 0 cell, 1 x face, 2 y face, 3 z face
+  switch (field) {
+    case FREHG_GW_FIELD_HEAD: src = D.h[D.cur]; break;
+    case FREHG_GW_FIELD_WC: src = D.wc[D.cur]; break;
+    case FREHG_GW_FIELD_WC_START: src = D.wc[h->start_buf]; break;
+    case FREHG_GW_FIELD_DZ: src = D.dz; break;
+    case FREHG_GW_FIELD_BOT: src = D.bot; break;
+    case FREHG_GW_FIELD_VLOSS: src = D.vloss; break;
+    case FREHG_GW_FIELD_QX: src = D.qx; kind = 1; break;
+    case FREHG_GW_FIELD_KX: src = D.kx; kind = 1; break;
+    case FREHG_GW_FIELD_AX: src = D.ax; kind = 1; break;
+    case FREHG_GW_FIELD_SINX: src = D.sinx; kind = 1; break;
+    case FREHG_GW_FIELD_COSX: src = D.cosx; kind = 1; break;
+    case FREHG_GW_FIELD_QY: src = D.qy; kind = 2; break;
+    case FREHG_GW_FIELD_KY: src = D.ky; kind = 2; break;
+    case FREHG_GW_FIELD_AY: src = D.ay; kind = 2; break;
+    case FREHG_GW_FIELD_SINY: src = D.siny; kind = 2; break;
+    case FREHG_GW_FIELD_COSY: src = D.cosy; kind = 2; break;
+    case FREHG_GW_FIELD_QZ: src = D.qzf; kind = 3; break;
+    case FREHG_GW_FIELD_KZ: src = D.kzf; kind = 3; break;
+    default: return fail(FREHG_GW_EINVAL, "unknown field");
+  }
+  const size_t n = static_cast<size_t>(kind == 3 ? d.ncol * (d.nz + 1) : d.ncell);
+  std::vector<double> full(n);
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "get_field");
+  CUDA_TRY(cudaMemcpy(full.data(), src, n * sizeof(double), cudaMemcpyDeviceToHost), "get_field");
+  size_t q = 0;
+  if (kind == 3) {
+    for (int j = 1; j <= d.ny; ++j)
+      for (int i = 1; i <= d.nx; ++i)
+        for (int k = 0; k <= d.nz; ++k) out[q++] = full[fgw::fidx(d, j, i, k)];
+    return FREHG_GW_OK;
+  }
+  const int j0 = (kind == 2) ? 0 : 1, i0 = (kind == 1) ? 0 : 1;
+  for (int j = j0; j <= d.ny; ++j)
+    for (int i = i0; i <= d.nx; ++i)
+      for (int k = 0; k < d.nz; ++k) out[q++] = full[fgw::cidx(d, j, i, k)];
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_owned_volume(frehg_gw_handle* h, double* out) {
+  if (!h || !out) return fail(FREHG_GW_EINVAL, "null argument");
+  fgw::Device& D = h->D;
+  fgw::launch_volume(D, D.wc[D.cur]);
+  CUDA_TRY(cudaMemcpyAsync(D.out_host, D.out, sizeof(fgw::StepOut), cudaMemcpyDeviceToHost,
+                           D.stream), "owned_volume");
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "owned_volume");
+  *out = D.out_host->volume;
+  return FREHG_GW_OK;
+}
+
+long long frehg_gw_active_cells(const frehg_gw_handle* h) { return h ? h->nactive : 0; }
+
+int frehg_gw_set_profiling(frehg_gw_handle* h, int on) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  if (on && !h->ev[0]) {
+    for (cudaEvent_t& e : h->ev) CUDA_TRY(cudaEventCreate(&e), "set_profiling");
+  }
+  h->profiling = on != 0;
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5) {
+  if (!h || !ms5) return fail(FREHG_GW_EINVAL, "null argument");
+  for (int n = 0; n < 5; ++n) ms5[n] = h->phase_ms[n];
+  return FREHG_GW_OK;
+}
+
+long long frehg_gw_kernel_launches(const frehg_gw_handle* h) { return h ? h->D.launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,246 @@
+// Device-side building blocks of the B200 groundwater step: the van
+// Genuchten-Mualem closures, the face-conductivity rules and the layout
+// helpers shared by the kernels in gw_kernels.cu and gw_cg.cu.
+//
+// Layout.  Every cell field lives in the halo layout of the reference
+// (src/core/Types.hpp:35-43): (ny+2, nx+2, nz) with k unit-stride, so cell
+// (j, i, k) is at ((j * (nx+2)) + i) * nz + k.  z-face fields carry nz+1
+// planes per column (plane k = face above cell k).  Solver vectors add a
+// zero margin of one j-row on both ends so the 7-point stencil reads of
+// ghost cells stay in bounds and multiply zero coefficients.
+#pragma once
+
+#include <cstdint>
+
+namespace fgw {
+
+enum BcCode : int { kNoFlux = 0, kHead = 1, kFlux = 2, kGravity = 3, kHydro = 4 };
+
+struct Soil {
+  double vga, vgn, ts, tr, aev;
+};
+
+// Static geometry and parameters of one domain, by value in every launch.
+struct Dims {
+  int nx, ny, nz;
+  int nx2, ny2;          // nx + 2, ny + 2
+  long long sx, sy;      // strides of i and j in a cell field (nz, (nx+2) nz)
+  long long ncell;       // (ny+2)(nx+2)nz
+  long long ncol;        // (ny+2)(nx+2)
+  double dx, dy, az;
+  double ss;             // specific storage
+  int full3d, pc, harm, off, redistribute, terrain;
+};
+
+// Device pointers of one domain (see gw_internal.h for ownership).
+struct Fields {
+  // soil (halo layout, mirrored ghosts)
+  const double *ksx, *ksy, *ksz, *vga, *vgn, *wcs, *wcr, *aev;
+  // geometry
+  const double *dz, *bot, *ax, *ay, *sinx, *cosx, *siny, *cosy;
+  const int8_t* act;   // 1 = active cell (gid >= 0), 0 = inactive or ghost
+  // boundary markers, (ny+2)(nx+2); side codes live on the edge columns
+  const int *topc, *botc, *xmc, *xpc, *ymc, *ypc;
+  const double *topv, *botv, *xmv, *xpv, *ymv, *ypv;
+};
+
+__host__ __device__ inline long long cidx(const Dims& d, int j, int i, int k) {
+  return (static_cast<long long>(j) * d.nx2 + i) * d.nz + k;
+}
+__host__ __device__ inline long long fidx(const Dims& d, int j, int i, int k) {
+  return (static_cast<long long>(j) * d.nx2 + i) * (d.nz + 1) + k;
+}
+__host__ __device__ inline long long col2(const Dims& d, int j, int i) {
+  return static_cast<long long>(j) * d.nx2 + i;
+}
+__device__ inline void unflatten(const Dims& d, long long c, int& j, int& i, int& k) {
+  const long long col = c / d.nz;
+  k = static_cast<int>(c - col * d.nz);
+  j = static_cast<int>(col / d.nx2);
+  i = static_cast<int>(col - static_cast<long long>(j) * d.nx2);
+}
+__device__ inline bool is_head(int code) { return code == kHead || code == kHydro; }
+
+__device__ inline Soil soil_at(const Fields& f, long long c) {
+  return Soil{f.vga[c], f.vgn[c], f.wcs[c], f.wcr[c], f.aev[c]};
+}
+
+// ---------------------------------------------------------------- closures
+// The pointwise van Genuchten-Mualem relations of the frehg2 groundwater
+// module (src/gw/VanGenuchten.hpp:45-128): theta(h) with the air-entry cutoff
+// and [theta_r, theta_s] clamp, h(theta) with the theta_r + 1e-7 floor, C(h)
+// and K(h) cut off at h > 0, K capped at Ks, dK/dtheta with the 0.9999
+// theta_s limiter.  Every power goes through the CUDA math library's pow.
+
+__device__ inline double vg_theta(const Soil& s, double h) {
+  const double m = 1.0 - 1.0 / s.vgn;
+  double wc;
+  if (h > s.aev) {
+    wc = s.ts;
+  } else {
+    const double se = pow(1.0 + pow(fabs(s.vga * h), s.vgn), -m);
+    wc = s.tr + (s.ts - s.tr) * se;
+  }
+  if (wc > s.ts) {
+    wc = s.ts;
+  } else if (wc < s.tr) {
+    wc = s.tr;
+  }
+  return wc;
+}
+
+__device__ inline double vg_head(const Soil& s, double wc) {
+  const double m = 1.0 - 1.0 / s.vgn;
+  if (wc - s.tr < 1.0e-7) wc = s.tr + 1.0e-7;
+  if (wc < s.ts) {
+    const double ratio = (s.ts - s.tr) / (wc - s.tr);
+    return -(1.0 / s.vga) * pow(pow(ratio, 1.0 / m) - 1.0, 1.0 / s.vgn);
+  }
+  return 0.0;
+}
+
+__device__ inline double vg_capacity(const Soil& s, double h) {
+  if (h > 0.0) return 0.0;
+  const double m = 1.0 - 1.0 / s.vgn;
+  const double ah = fabs(s.vga * h);
+  const double nume = s.vga * s.vgn * m * (s.ts - s.tr) * pow(ah, s.vgn - 1.0);
+  const double deno = pow(1.0 + pow(ah, s.vgn), m + 1.0);
+  return nume / deno;
+}
+
+// Relative-permeability pieces of K(h) shared by the three directional Ks of
+// one cell: K = ((ks * root) * br) * br, capped at ks, ks for h > 0.
+struct KrParts {
+  double root, br;
+  bool sat;
+};
+__device__ inline KrParts vg_kr_parts(const Soil& s, double h) {
+  const double m = 1.0 - 1.0 / s.vgn;
+  const double se = pow(1.0 + pow(fabs(s.vga * h), s.vgn), -m);
+  KrParts p;
+  p.br = 1.0 - pow(1.0 - pow(se, 1.0 / m), m);
+  p.root = pow(se, 0.5);
+  p.sat = h > 0.0;
+  return p;
+}
+__device__ inline double vg_k_from(const KrParts& p, double ks) {
+  double k = ks * p.root * p.br * p.br;
+  if (k > ks) k = ks;
+  if (p.sat) k = ks;
+  return k;
+}
+__device__ inline double vg_k(const Soil& s, double h, double ks) {
+  return vg_k_from(vg_kr_parts(s, h), ks);
+}
+
+__device__ inline double vg_dkdtheta(const Soil& s, double wc, double ks) {
+  if (wc > 0.9999 * s.ts && wc < s.ts) wc = 0.9999 * s.ts;
+  const double m = 1.0 - 1.0 / s.vgn;
+  const double se = (wc - s.tr) / (s.ts - s.tr);
+  const double t0 = pow(1.0 - pow(se, 1.0 / m), m);
+  const double t1 = 0.5 * ks * pow(se, -0.5) * (1.0 - t0) * (1.0 - t0);
+  const double t2 = 2.0 * ks * pow(se, (2.0 - m) / (2.0 * m)) * (1.0 - t0) *
+                    pow(1.0 - pow(se, 1.0 / m), m - 1.0);
+  return (t1 + t2) / (s.ts - s.tr);
+}
+
+// Harmonic-Ks x arithmetic-kr face rule (src/gw/FaceConductivity.hpp:48-59)
+// from the flanks' own conductivities ka = K(h_a, Ks_a), kb = K(h_b, Ks_b).
+__device__ inline double face_harm(double ka, double ksa, double la, double kb, double ksb,
+                                   double lb) {
+  if (ksa <= 0.0 || ksb <= 0.0) return 0.0;
+  const double ksh = (la + lb) / (la / ksa + lb / ksb);
+  return ksh * 0.5 * (ka / ksa + kb / ksb);
+}
+
+// ---------------------------------------------------------------- face rules
+// Face conductivities of one pass (predictor or corrector), built from the
+// per-cell directional conductivities Kc = K(h_c, Ks_c) of that pass with the
+// reference's overrides applied in its order (src/gw/Predictor.cpp:105-386):
+// interior mean -> domain-edge rule -> top rule -> use_full3d -> inactive seal.
+struct PassK {
+  const double *kcx, *kcy, *kcz;  // per-cell K with Ksx, Ksy, Ksz
+  const double* wc;               // moisture at the pass (use_full3d test)
+};
+
+// x face between (j, i) and (j, i+1), i in [0, nx], j in [1, ny].
+__device__ inline double face_kx(const Dims& d, const Fields& f, const PassK& p, int j, int i,
+                                 int k) {
+  const long long a = cidx(d, j, i, k), b = a + d.sx;
+  double kf;
+  if (d.harm) {
+    kf = face_harm(p.kcx[a], f.ksx[a], 1.0, p.kcx[b], f.ksx[b], 1.0);
+  } else {
+    kf = 0.5 * (p.kcx[a] + p.kcx[b]);
+  }
+  if (i == 0) {  // west edge face, owned by cell i = 1
+    const int code = f.xmc[col2(d, j, 1)];
+    if (code == kNoFlux) kf = 0.0;
+    else if (is_head(code)) kf = p.kcx[b];
+  } else if (i == d.nx) {
+    const int code = f.xpc[col2(d, j, d.nx)];
+    if (code == kNoFlux) kf = 0.0;
+    else if (is_head(code)) kf = p.kcx[a];
+  }
+  if (!d.full3d) {
+    if ((f.act[a] && p.wc[a] < f.wcs[a]) || (f.act[b] && p.wc[b] < f.wcs[b])) kf = 0.0;
+  }
+  const bool ina = (i >= 1) && !f.act[a];
+  const bool inb = (i + 1 <= d.nx) && !f.act[b];
+  if (ina || inb) kf = 0.0;
+  return kf;
+}
+
+// y face between (j, i) and (j+1, i), j in [0, ny], i in [1, nx].
+__device__ inline double face_ky(const Dims& d, const Fields& f, const PassK& p, int j, int i,
+                                 int k) {
+  const long long a = cidx(d, j, i, k), b = a + d.sy;
+  double kf;
+  if (d.harm) {
+    kf = face_harm(p.kcy[a], f.ksy[a], 1.0, p.kcy[b], f.ksy[b], 1.0);
+  } else {
+    kf = 0.5 * (p.kcy[a] + p.kcy[b]);
+  }
+  if (j == 0) {
+    const int code = f.ymc[col2(d, 1, i)];
+    if (code == kNoFlux) kf = 0.0;
+    else if (is_head(code)) kf = p.kcy[b];
+  } else if (j == d.ny) {
+    const int code = f.ypc[col2(d, d.ny, i)];
+    if (code == kNoFlux) kf = 0.0;
+    else if (is_head(code)) kf = p.kcy[a];
+  }
+  if (!d.full3d) {
+    if ((f.act[a] && p.wc[a] < f.wcs[a]) || (f.act[b] && p.wc[b] < f.wcs[b])) kf = 0.0;
+  }
+  const bool ina = (j >= 1) && !f.act[a];
+  const bool inb = (j + 1 <= d.ny) && !f.act[b];
+  if (ina || inb) kf = 0.0;
+  return kf;
+}
+
+// z face plane k in [0, nz] of interior column (j, i): the face above cell k.
+__device__ inline double face_kz(const Dims& d, const Fields& f, const PassK& p, int j, int i,
+                                 int k) {
+  const long long base = cidx(d, j, i, 0);
+  const bool below = (k < d.nz) && f.act[base + k];
+  const bool above = (k >= 1) && f.act[base + k - 1];
+  // Seal (applied last in the reference): a face with an inactive cell on
+  // either side is closed.  This also closes the face above the top cell of
+  // a masked column (k > 0), whose top rule the seal overrides.
+  if ((k < d.nz && !below) || (k >= 1 && !above)) return 0.0;
+  if (k == 0) {
+    const int code = f.topc[col2(d, j, i)];
+    if (code == kHead) return f.ksz[base];
+    if (code == kNoFlux) return 0.0;
+    return p.kcz[base];
+  }
+  if (k == d.nz) {
+    return (f.botc[col2(d, j, i)] == kNoFlux) ? 0.0 : p.kcz[base + d.nz - 1];
+  }
+  const long long up = base + k - 1, lo = base + k;
+  if (d.harm) return face_harm(p.kcz[up], f.ksz[up], f.dz[up], p.kcz[lo], f.ksz[lo], f.dz[lo]);
+  return 0.5 * (p.kcz[up] + p.kcz[lo]);
+}
+
+}  // namespace fgw

@@ -1,0 +1,224 @@
+"""Host-side mirror of frehg2's ``gw::RichardsSolver`` over the B200 C ABI.
+
+:class:`RichardsSolver` keeps the reference's method names and meanings
+(``src/gw/RichardsSolver.hpp:166-423``): ``step(t, dtg)`` with t the
+end-of-step time, ``nextDt()``, ``head()``, ``waterContent()``, the
+volumetric flux accessors, ``audit()``, ``lastSolve()`` and
+``ownedVolume()``.  Errors raise :class:`FatalError`, the reference's
+``frehg::FatalError`` (``src/core/Types.hpp:53-62``), carrying the ABI
+status.  Every call goes through ``libfrehg_gw.so`` (``include/frehg_gw.h``);
+there is no CPU fallback: without the built library the constructor fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from .abi import FIELD, STATUS_NAMES, GwDesc, StepInfo, field_shape, make_desc
+from .config import IC_FORMS, GwConfig, rasterize
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfrehg_gw.so")
+
+_dp = C.POINTER(C.c_double)
+_lib = None
+
+
+class FatalError(RuntimeError):
+    """A non-OK status from the C ABI (reference: ``frehg::FatalError``)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def load_library(path: str = LIB_PATH):
+    """Load ``libfrehg_gw.so`` and declare its C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FatalError(4, f"{path} is not built; run __graft_entry__.build()")
+    lib = C.CDLL(path)
+    H = C.c_void_p
+    lib.frehg_gw_last_error.restype = C.c_char_p
+    lib.frehg_gw_create.argtypes = [C.POINTER(GwDesc), C.POINTER(H)]
+    lib.frehg_gw_destroy.argtypes = [H]
+    lib.frehg_gw_set_stream.argtypes = [H, C.c_void_p]
+    lib.frehg_gw_set_bc_values.argtypes = [H] + [_dp] * 6
+    lib.frehg_gw_init_state.argtypes = [H, C.c_int, C.c_double, _dp]
+    lib.frehg_gw_set_state.argtypes = [H, _dp, _dp]
+    lib.frehg_gw_step.argtypes = [H, C.c_double, C.c_double, C.POINTER(StepInfo)]
+    lib.frehg_gw_next_dt.argtypes = [H, _dp]
+    lib.frehg_gw_get_field.argtypes = [H, C.c_int, _dp]
+    lib.frehg_gw_field_size.argtypes = [H, C.c_int]
+    lib.frehg_gw_field_size.restype = C.c_size_t
+    lib.frehg_gw_owned_volume.argtypes = [H, _dp]
+    lib.frehg_gw_active_cells.argtypes = [H]
+    lib.frehg_gw_active_cells.restype = C.c_longlong
+    lib.frehg_gw_set_profiling.argtypes = [H, C.c_int]
+    lib.frehg_gw_set_profiling.restype = C.c_int
+    lib.frehg_gw_phase_times.argtypes = [H, _dp]
+    lib.frehg_gw_phase_times.restype = C.c_int
+    lib.frehg_gw_kernel_launches.argtypes = [H]
+    lib.frehg_gw_kernel_launches.restype = C.c_longlong
+    for name in ("frehg_gw_create", "frehg_gw_destroy", "frehg_gw_set_stream",
+                 "frehg_gw_set_bc_values", "frehg_gw_init_state", "frehg_gw_set_state",
+                 "frehg_gw_step", "frehg_gw_next_dt", "frehg_gw_get_field",
+                 "frehg_gw_owned_volume"):
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _check(lib, rc: int):
+    if rc != 0:
+        raise FatalError(rc, lib.frehg_gw_last_error().decode())
+
+
+class RichardsSolver:
+    """The B200 groundwater step for one domain."""
+
+    def __init__(self, cfg: GwConfig, stream: Optional[int] = None):
+        self.lib = load_library()
+        self.cfg = cfg
+        d = cfg.domain
+        self.nx, self.ny, self.nz = d.nx, d.ny, d.nz
+        ras = rasterize(cfg)
+        desc, keep = make_desc(cfg, ras)
+        h = C.c_void_p()
+        _check(self.lib, self.lib.frehg_gw_create(C.byref(desc), C.byref(h)))
+        self.h = h
+        if stream is not None:
+            _check(self.lib, self.lib.frehg_gw_set_stream(self.h, C.c_void_p(stream)))
+        self._values = [np.ascontiguousarray(v, np.float64) for v in
+                        (ras.top_value, ras.bot_value, ras.xm_value, ras.xp_value,
+                         ras.ym_value, ras.yp_value)]
+        _check(self.lib, self.lib.frehg_gw_set_bc_values(
+            self.h, *[v.ctypes.data_as(_dp) for v in self._values]))
+        ic = cfg.initial
+        if np.isscalar(ic.value):
+            _check(self.lib, self.lib.frehg_gw_init_state(self.h, IC_FORMS[ic.form],
+                                                          float(ic.value), None))
+        else:
+            fld = np.ascontiguousarray(ic.value, np.float64)
+            _check(self.lib, self.lib.frehg_gw_init_state(self.h, IC_FORMS[ic.form], 0.0,
+                                                          fld.ctypes.data_as(_dp)))
+        self.t = 0.0
+        self._info = None
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.frehg_gw_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- stepping ---------------------------------------------------------------
+    def step(self, t: float, dtg: float) -> dict:
+        """``RichardsSolver::step(t, dtg)``; returns the step record."""
+        info = StepInfo()
+        _check(self.lib, self.lib.frehg_gw_step(self.h, t, dtg, C.byref(info)))
+        self._info = info.as_dict()
+        return self._info
+
+    def nextDt(self) -> float:
+        out = C.c_double()
+        _check(self.lib, self.lib.frehg_gw_next_dt(self.h, C.byref(out)))
+        return out.value
+
+    next_dt = nextDt
+
+    def advance(self) -> float:
+        """One adaptive step the way the reference's driver loop takes it
+        (``Simulation::runGroundwaterLoop``, Simulation.cpp:1695-1700)."""
+        dtg = self.nextDt()
+        self.t += dtg
+        self.step(self.t, dtg)
+        return dtg
+
+    def setBoundaryValues(self, top=None, bottom=None, xm=None, xp=None, ym=None, yp=None):
+        """``updateBoundaryValues``: per-column / per-edge values (None keeps)."""
+        arrs = [None if v is None else np.ascontiguousarray(v, np.float64)
+                for v in (top, bottom, xm, xp, ym, yp)]
+        _check(self.lib, self.lib.frehg_gw_set_bc_values(
+            self.h, *[None if a is None else a.ctypes.data_as(_dp) for a in arrs]))
+
+    def setState(self, head: np.ndarray, wc: np.ndarray) -> None:
+        """Restart read + ``refreshDerivedState``."""
+        hh = np.ascontiguousarray(head, np.float64)
+        ww = np.ascontiguousarray(wc, np.float64)
+        _check(self.lib, self.lib.frehg_gw_set_state(self.h, hh.ctypes.data_as(_dp),
+                                                     ww.ctypes.data_as(_dp)))
+
+    # -- observation -----------------------------------------------------------
+    def field(self, name: str) -> np.ndarray:
+        out = np.empty(field_shape(name, self.nx, self.ny, self.nz))
+        _check(self.lib, self.lib.frehg_gw_get_field(self.h, FIELD[name],
+                                                     out.ctypes.data_as(_dp)))
+        return out
+
+    def head(self) -> np.ndarray:
+        return self.field("h")
+
+    def waterContent(self) -> np.ndarray:
+        return self.field("wc")
+
+    def fluxXVolumetric(self) -> np.ndarray:
+        return self.field("qx")
+
+    def fluxYVolumetric(self) -> np.ndarray:
+        return self.field("qy")
+
+    def fluxZFaceVolumetric(self) -> np.ndarray:
+        return self.field("qz")
+
+    def audit(self) -> dict:
+        """``GwStepAudit`` of the last step."""
+        i = self._info or {}
+        return {k: i.get(k, 0.0) for k in
+                ("boundary_in", "ss_storage", "realloc_adjust", "realloc_dropped", "vloss")}
+
+    def lastSolve(self):
+        """(iterations, final preconditioned residual norm) of the last solve."""
+        i = self._info or {}
+        return i.get("cg_iterations", 0), i.get("residual_norm", 0.0)
+
+    def ownedVolume(self) -> float:
+        out = C.c_double()
+        _check(self.lib, self.lib.frehg_gw_owned_volume(self.h, C.byref(out)))
+        return out.value
+
+    owned_volume = ownedVolume
+
+    def activeCells(self) -> int:
+        return int(self.lib.frehg_gw_active_cells(self.h))
+
+    # -- tracing ----------------------------------------------------------------
+    PHASES = ("predictor", "solve", "corrector", "post_allocation", "finalize")
+
+    def setProfiling(self, on: bool = True) -> None:
+        _check(self.lib, self.lib.frehg_gw_set_profiling(self.h, int(bool(on))))
+
+    def phaseTimes(self) -> dict:
+        """Device ms per phase of the last step (profiling on)."""
+        out = (C.c_double * 5)()
+        _check(self.lib, self.lib.frehg_gw_phase_times(self.h, out))
+        return dict(zip(self.PHASES, list(out)))
+
+    def kernelLaunches(self) -> int:
+        return int(self.lib.frehg_gw_kernel_launches(self.h))

@@ -1,0 +1,62 @@
+"""The C ABI library loads and exports every entry point include/*.h
+declares (no compute calls: this runs without a GPU)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "frehg_b200", "libfrehg_gw.so")
+
+
+def declared_symbols():
+    names = set()
+    for header in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(header).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(frehg_gw_\w+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_headers_declare_entry_points():
+    names = declared_symbols()
+    for required in ("frehg_gw_create", "frehg_gw_step", "frehg_gw_destroy",
+                     "frehg_gw_get_field", "frehg_gw_next_dt", "frehg_gw_owned_volume"):
+        assert required in names
+
+
+@pytest.mark.skipif(not os.path.exists(LIB), reason="libfrehg_gw.so not built")
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(LIB)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+@pytest.mark.skipif(not os.path.exists(LIB), reason="libfrehg_gw.so not built")
+def test_descriptor_layout_matches_header():
+    # The ctypes mirror must agree with the C struct: compile-free check on
+    # field order by name.
+    from frehg_b200.abi import GwDesc, StepInfo
+    text = open(os.path.join(ROOT, "include", "frehg_gw.h")).read()
+    body = text[text.index("typedef struct frehg_gw_desc"):text.index("} frehg_gw_desc;")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    decl = re.findall(r"(\*?\s*\w+)\s*[,;]", body.split("{", 1)[1])
+    names = [d.replace("*", "").strip() for d in decl]
+    assert names == [f[0] for f in GwDesc._fields_]
+    body = text[text.index("typedef struct frehg_gw_step_info"):text.index("} frehg_gw_step_info;")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = [d.strip() for d in re.findall(r"(\w+)\s*;", body)]
+    assert names == [f[0] for f in StepInfo._fields_]
+
+
+def test_null_arguments_are_rejected_without_a_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("libfrehg_gw.so not built")
+    lib = ctypes.CDLL(LIB)
+    lib.frehg_gw_create.restype = ctypes.c_int
+    assert lib.frehg_gw_create(None, None) == 1  # FREHG_GW_EINVAL
+    lib.frehg_gw_last_error.restype = ctypes.c_char_p
+    assert b"null" in lib.frehg_gw_last_error()
