@@ -9,16 +9,16 @@
 // max_iterations.
 //
 // One persistent cooperative launch runs the whole solve.  Per iteration:
-//   phase A: p_new = z + b p_old (z recomputed from r and diag for the seven
-//            stencil points, so z is never stored), w = A p_new, partial p'w;
+//   phase A: p_new = z + b p_old (for the seven stencil points), w = A p_new,
+//            partial p'w;
 //   grid barrier; every block reduces the partials in block order;
 //   phase B: x += a p, r -= a w, z = r / diag, partials z'z and z'r;
 //   grid barrier; reduction; convergence test.
-// Per cell and iteration this moves 15 FP64 words (120 B) through HBM:
-// phase A reads r, p_old, diag, gxp, gyp, gzp and writes p_new, w; phase B
-// reads x, p_new, r, w, diag and writes x, r.  Neighbour reads are served by
-// L1/L2 because the grid-stride sweep keeps all resident blocks inside a few
-// j-rows of each other.
+// Per cell and iteration this moves 16 FP64 words (128 B) through HBM:
+// phase A reads z, p_old, diag, gxp, gyp, gzp and writes p_new, w; phase B
+// reads x, p_new, r, w, diag and writes x, r, z.  Neighbour reads are served
+// by L1/L2 because the grid-stride sweep keeps all resident blocks inside a
+// few j-rows of each other.
 //
 // The grid barrier is a bounded spin on a generation counter: a wait that
 // exceeds kSpinLimit polls sets CgState::err, and every block leaves at its
@@ -118,7 +118,7 @@ __device__ double reduce_partials(const double* part, int G) {
 struct Cg64Args {
   Dims d;
   const double *diag, *gxp, *gyp, *gzp, *b;
-  double *x, *r, *p0, *p1, *w;
+  double *x, *r, *z, *p0, *p1, *w;
   double* part;  // 3 x G
   CgState* st;
   double rtol, atol;
@@ -127,7 +127,7 @@ struct Cg64Args {
 
 __device__ inline int sgn(double v) { return (v > 0.0) - (v < 0.0); }
 
-__global__ void __launch_bounds__(kCgBlock) k_cg64(Cg64Args a) {
+__global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
   const long long N = a.d.ncell, sx = a.d.sx, sy = a.d.sy;
   const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
   const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(kCgBlock) k_cg64(Cg64Args a) {
     a.p0[c] = 0.0;
     a.p1[c] = 0.0;
     const double z = rc * (1.0 / a.diag[c]);
+    a.z[c] = z;
     zz += z * z;
     zr += z * rc;
   }
@@ -182,13 +183,13 @@ __global__ void __launch_bounds__(kCgBlock) k_cg64(Cg64Args a) {
     // Phase A: direction update fused into the stencil product.
     double pw = 0.0;
     for (long long c = t0; c < N; c += stride) {
-      const double pc = a.r[c] * (1.0 / a.diag[c]) + bc * pold[c];
-      const double pym = a.r[c - sy] * (1.0 / a.diag[c - sy]) + bc * pold[c - sy];
-      const double pxm = a.r[c - sx] * (1.0 / a.diag[c - sx]) + bc * pold[c - sx];
-      const double pzm = a.r[c - 1] * (1.0 / a.diag[c - 1]) + bc * pold[c - 1];
-      const double pzp = a.r[c + 1] * (1.0 / a.diag[c + 1]) + bc * pold[c + 1];
-      const double pxp = a.r[c + sx] * (1.0 / a.diag[c + sx]) + bc * pold[c + sx];
-      const double pyp = a.r[c + sy] * (1.0 / a.diag[c + sy]) + bc * pold[c + sy];
+      const double pc = a.z[c] + bc * pold[c];
+      const double pym = a.z[c - sy] + bc * pold[c - sy];
+      const double pxm = a.z[c - sx] + bc * pold[c - sx];
+      const double pzm = a.z[c - 1] + bc * pold[c - 1];
+      const double pzp = a.z[c + 1] + bc * pold[c + 1];
+      const double pxp = a.z[c + sx] + bc * pold[c + sx];
+      const double pyp = a.z[c + sy] + bc * pold[c + sy];
       double wv = a.gyp[c - sy] * pym;
       wv += a.gxp[c - sx] * pxm;
       wv += a.gzp[c - 1] * pzm;
@@ -220,6 +221,7 @@ __global__ void __launch_bounds__(kCgBlock) k_cg64(Cg64Args a) {
       const double rc = a.r[c] - al * a.w[c];
       a.r[c] = rc;
       const double z = rc * (1.0 / a.diag[c]);
+      a.z[c] = z;
       zz += z * z;
       zr += z * rc;
     }
@@ -270,6 +272,7 @@ cudaError_t launch_cg64(Device& D, double rtol, double atol, int maxit) {
   a.b = D.rhs;
   a.x = D.x;
   a.r = D.r;
+  a.z = D.z;
   a.p0 = D.p0;
   a.p1 = D.p1;
   a.w = D.w;

@@ -76,7 +76,7 @@ struct Device {
   // linear system: coefficients and vectors carry a zero margin of sy cells
   // on both ends; the pointers below point at cell 0.
   double *diag = nullptr, *gxp = nullptr, *gyp = nullptr, *gzp = nullptr, *rhs = nullptr;
-  double *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *w = nullptr;
+  double *x = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *w = nullptr;
   // mixed precision: FP32 copies and inner vectors (same margins)
   float *diag32 = nullptr, *gxp32 = nullptr, *gyp32 = nullptr, *gzp32 = nullptr;
   float *r32 = nullptr, *x32 = nullptr, *p032 = nullptr, *p132 = nullptr, *w32 = nullptr;

@@ -20,10 +20,22 @@ H_TOL = 1e-9
 F_TOL = 1e-8
 
 
-def rel_linf(a, b):
-    scale = np.max(np.abs(b)) if b.size else 0.0
+# Scale floors of the L-inf comparison: a field whose magnitude is below its
+# floor (e.g. rounding-level fluxes of a column at equilibrium) is compared
+# absolutely against the floor instead.
+FLOOR = {"h": 1.0, "wc": 1.0, "qx": 1e-12, "qy": 1e-12, "qz": 1e-12, "kx": 1e-12,
+         "ky": 1e-12, "kz": 1e-12}
+
+
+FLUX_SCALE = {"qx": ("kx", "ax"), "qy": ("ky", "ay"), "qz": ("kz", None)}
+
+
+def rel_linf(a, b, floor=0.0):
+    if not b.size:
+        return 0.0
+    scale = max(float(np.max(np.abs(b))), floor)
     if scale == 0.0:
-        return float(np.max(np.abs(a))) if a.size else 0.0
+        return float(np.max(np.abs(a)))
     return float(np.max(np.abs(a - b)) / scale)
 
 
@@ -31,8 +43,13 @@ def compare(cfg, steps, fields=("h", "wc", "qx", "qy", "qz", "kx", "ky", "kz")):
     gpu = RichardsSolver(cfg)
     cpu = OracleSolver(cfg)
     try:
-        for name in ("dz3d", "bot3d", "ax", "ay", "sinx", "cosx", "siny", "cosy", "h", "wc"):
+        # Geometry is host set-up: bitwise.  The initial state comes from the
+        # retention curve, whose pow() differs by ulps between CUDA and glibc.
+        for name in ("dz3d", "bot3d", "ax", "ay", "sinx", "cosx", "siny", "cosy"):
             np.testing.assert_array_equal(gpu.field(name), cpu.field(name), err_msg=name)
+        for name in ("h", "wc"):
+            np.testing.assert_allclose(gpu.field(name), cpu.field(name), rtol=1e-14, atol=1e-15,
+                                       err_msg=name)
         prev = gpu.ownedVolume()
         for n in range(steps):
             dtg = cpu.next_dt()
@@ -41,9 +58,20 @@ def compare(cfg, steps, fields=("h", "wc", "qx", "qy", "qz", "kx", "ky", "kz")):
             cpu.step(cpu.t, dtg)
             info = gpu.step(cpu.t, dtg)
             assert abs(info["cg_iterations"] - cpu.info["cg_iterations"]) <= 2, f"step {n}"
-            assert rel_linf(gpu.field("h"), cpu.field("h")) <= H_TOL, f"h step {n}"
+            assert rel_linf(gpu.field("h"), cpu.field("h"), FLOOR["h"]) <= H_TOL, f"h step {n}"
             for name in fields[1:]:
-                assert rel_linf(gpu.field(name), cpu.field(name)) <= F_TOL, f"{name} step {n}"
+                ref = cpu.field(name)
+                floor = FLOOR[name]
+                if name in FLUX_SCALE:
+                    # A net Darcy flux is a difference of a pressure and a
+                    # gravity term; near equilibrium it cancels to the solve's
+                    # residual, so its error is measured on the gravity scale
+                    # K * A of that direction.
+                    kname, area = FLUX_SCALE[name]
+                    a = cfg.domain.dx * cfg.domain.dy if area is None else cpu.field(area)
+                    floor = max(floor, float(np.max(np.abs(cpu.field(kname)) * a)))
+                err = rel_linf(gpu.field(name), ref, floor)
+                assert err <= F_TOL, f"{name} step {n}: {err}"
             v = gpu.ownedVolume()
             resid = (v - prev) - (info["boundary_in"] - info["ss_storage"] +
                                   info["realloc_adjust"] - info["vloss"])
