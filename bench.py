@@ -113,10 +113,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(sample: str, threads: int):
+def cpu_baseline(sample: str, threads: int, warmup: int = 1, steps=None, budget_s: float = 10.0):
     """The reference's own CPU step (its src/gw compiled on host shims, OpenMP
     shim backend, the reference's default bjacobi-ICC(0) CG) on a bounded crop
-    of the same workload."""
+    of the same workload.  Without `steps`, steps until `budget_s` elapses."""
     from frehg_b200 import workloads
     from oracle import ref as refmod
     if not refmod.available(omp=True):
@@ -125,29 +125,32 @@ def cpu_baseline(sample: str, threads: int):
     cfg = workloads.hillslope(nx, ny, nz, per_cell_soil=False)
     os.environ["OMP_NUM_THREADS"] = str(threads)
     r = refmod.RefSolver(cfg, pc="icc", omp=True)
-    r.advance()  # warm-up step
+    for _ in range(max(warmup, 1)):
+        r.advance()
     t0 = time.perf_counter()
-    steps = 0
+    n = 0
     while True:
         r.advance()
-        steps += 1
-        if time.perf_counter() - t0 > 10.0 or steps >= 20:
+        n += 1
+        if steps is not None and n >= steps:
+            break
+        if steps is None and (time.perf_counter() - t0 > budget_s or n >= 20):
             break
     dt = time.perf_counter() - t0
     _, ktop = r.gid()
     active = int(sum(nz - k for k in ktop.ravel()))
     r.close()
-    return {"value": active * steps / dt, "unit": "cell-steps/s", "cores": threads,
+    return {"value": active * n / dt, "unit": "cell-steps/s", "cores": threads,
             "kind": "reference",
-            "sample": f"{nx}x{ny}x{nz} crop of the slab, {steps} steps after 1 warm-up, "
-                      "reference src/gw on host shims (OpenMP), bjacobi-ICC(0) CG"}
+            "sample": f"{nx}x{ny}x{nz} crop of the slab, {n} steps after {max(warmup, 1)} "
+                      "warm-up, reference src/gw on host shims (OpenMP), bjacobi-ICC(0) CG"}
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    res = cpu_baseline(args.cpu_sample, threads)
+    res = cpu_baseline(args.cpu_sample, threads, warmup=args.warmup, steps=args.steps)
     if res is None:
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref (reference sources on host shims) not built"}))
@@ -157,14 +160,81 @@ def run_reference(args, rank):
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": f"terrain slab crop {args.cpu_sample} (CPU-sized sample of "
-                               f"{args.size})", "parallelism": "host threads"},
+        "config": {"workload": f"terrain-following heterogeneous slab, {args.cpu_sample} crop "
+                               f"(CPU-sized sample of {args.size}), dt0 60 s adaptive",
+                   "parallelism": f"{threads} host threads"},
         "cpu_baseline": {k: res[k] for k in ("kind", "cores", "sample")} | {"value": res["value"],
                                                                            "unit": "cell-steps/s"},
         "e2e": {"value": res["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
+    """Warm-up, then K timed steps of one solver form; optional e2e leg."""
+    import torch
+
+    from frehg_b200 import workloads
+    from frehg_b200.config import rasterize
+    from frehg_b200.gw import RichardsSolver
+
+    nx, ny, nz = (int(v) for v in args.size.split(","))
+    cfg = workloads.hillslope(nx, ny, nz, seed=20261203 + rank, precision=precision)
+    gw = RichardsSolver(cfg, stream=stream.cuda_stream)
+    active = gw.activeCells()
+    for _ in range(args.warmup):
+        gw.advance()
+    gw.setProfiling(True)
+    launches0 = gw.kernelLaunches()
+    iters, outer, solve_ms = 0, 0, 0.0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            gw.advance()
+            iters += gw.lastSolve()[0]
+            outer += gw._info["outer_iterations"]
+            solve_ms += gw.phaseTimes()["solve"]
+        end.record(stream)
+        torch.cuda.synchronize()
+    launches = gw.kernelLaunches() - launches0
+    ms = start.elapsed_time(end)
+    total_cells = float(active)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        a = torch.tensor([float(active)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(a)
+        total_cells = float(a.item())
+    out = dict(value=total_cells * args.steps / (ms / 1e3), ms=ms, iters=iters, outer=outer,
+               solve_ms=solve_ms, launches=launches, clocks=clocks.summary(), active=active,
+               e2e=None)
+    if e2e_steps:
+        # End to end through the C ABI with host buffers: boundary values in,
+        # head and moisture back to host memory, every step.
+        ras = rasterize(cfg)
+        vals = (ras.top_value, ras.bot_value, ras.xm_value, ras.xp_value, ras.ym_value,
+                ras.yp_value)
+        h2d = sum(v.nbytes for v in vals)
+        d2h = 2 * active * 8
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            gw.setBoundaryValues(*vals)
+            gw.advance()
+            gw.head()
+            gw.waterContent()
+        e2e_s = time.perf_counter() - t0
+        out["e2e"] = {"value": total_cells * e2e_steps / e2e_s, "unit": "cell-steps/s",
+                      "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+    gw.close()
+    return out
 
 
 def main():
@@ -176,7 +246,6 @@ def main():
         run_reference(args, rank)
         return
 
-    import numpy as np
     import torch
 
     torch.cuda.set_device(local)
@@ -186,91 +255,55 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    from frehg_b200 import workloads
-    from frehg_b200.config import rasterize
-    from frehg_b200.gw import RichardsSolver
-
-    nx, ny, nz = (int(v) for v in args.size.split(","))
-    cfg = workloads.hillslope(nx, ny, nz, seed=20261203 + rank, precision=args.precision)
     stream = torch.cuda.Stream()
-    gw = RichardsSolver(cfg, stream=stream.cuda_stream)
-    active = gw.activeCells()
-    for _ in range(args.warmup):
-        gw.advance()
-    gw.setProfiling(True)
-    launches0 = gw.kernelLaunches()
-    iters, solve_ms = 0, 0.0
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            gw.advance()
-            iters += gw.lastSolve()[0]
-            solve_ms += gw.phaseTimes()["solve"]
-        end.record(stream)
-        torch.cuda.synchronize()
-    launches = gw.kernelLaunches() - launches0
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        a = torch.tensor([float(active)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(a)
-        total_cells = float(a.item())
-    else:
-        total_cells = float(active)
-    value = total_cells * args.steps / (ms / 1e3)
-
-    # End to end through the C ABI with host buffers: boundary values in from
-    # pinned host memory, head and moisture back to host, every step.
-    ras = rasterize(cfg)
-    h2d = sum(v.nbytes for v in (ras.top_value, ras.bot_value, ras.xm_value, ras.xp_value,
-                                 ras.ym_value, ras.yp_value))
-    d2h = 2 * active * 8
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        gw.setBoundaryValues(ras.top_value, ras.bot_value, ras.xm_value, ras.xp_value,
-                             ras.ym_value, ras.yp_value)
-        gw.advance()
-        _ = gw.head()
-        _ = gw.waterContent()
-    e2e_s = time.perf_counter() - t0
-    e2e = {"value": active * args.e2e_steps / e2e_s * (total_cells / active),
-           "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
-    gw.close()
+    other = "fp64" if args.precision == "mixed" else "mixed"
+    res_other = timed_form(args, other, rank, local, dist, stream, 0)
+    res = timed_form(args, args.precision, rank, local, dist, stream, args.e2e_steps)
+    fp64 = res if args.precision == "fp64" else res_other
+    mixed = res if args.precision == "mixed" else res_other
 
     peak, peak_kind = peaks()
-    achieved = ALG_BYTES_PER_CG_ITER * active * iters / (solve_ms / 1e3) / 1e9 if solve_ms else 0.0
-    roof = {"bound": "hbm", "kernel": "k_cg64 (Jacobi-PCG solve, one launch per step)",
+    # Roofline of the dominant kernel of the plain FP64 form: its Jacobi-PCG
+    # solve (one cooperative launch per step), 128 B per active cell and
+    # iteration.
+    achieved = (ALG_BYTES_PER_CG_ITER * fp64["active"] * fp64["iters"] /
+                (fp64["solve_ms"] / 1e3) / 1e9) if fp64["solve_ms"] else 0.0
+    roof = {"bound": "hbm", "kernel": "k_cg64v (FP64 Jacobi-PCG solve, one launch per step)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_kind, "traffic": None,
             "alg_bytes_per_cell_iter": ALG_BYTES_PER_CG_ITER,
-            "cg_iterations_per_step": iters / args.steps,
-            "solve_share": solve_ms / ms if ms else None}
+            "cg_iterations_per_step": fp64["iters"] / args.steps,
+            "solve_share_of_step": fp64["solve_ms"] / fp64["ms"] if fp64["ms"] else None}
+    forms = {
+        "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms"] / args.steps,
+                 "cg_iterations_per_step": fp64["iters"] / args.steps,
+                 "solve_ms_per_step": fp64["solve_ms"] / args.steps},
+        "mixed": {"value": mixed["value"], "ms_per_step": mixed["ms"] / args.steps,
+                  "inner_iterations_per_step": mixed["iters"] / args.steps,
+                  "outer_sweeps_per_step": mixed["outer"] / args.steps,
+                  "solve_ms_per_step": mixed["solve_ms"] / args.steps},
+        "mixed_over_fp64": mixed["value"] / fp64["value"] if fp64["value"] else None,
+    }
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
-    cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(args.cpu_sample,
-                                                                      os.cpu_count() or 1)
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        cpu = cpu_baseline(args.cpu_sample, os.cpu_count() or 1)
+    nx, ny, nz = (int(v) for v in args.size.split(","))
     line = {
-        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32-inner/f64",
         "data": "synthetic",
         "config": {"workload": f"terrain-following heterogeneous slab {nx}x{ny}x{nz} "
                                f"(hillslope, seeded), dt0 60 s adaptive, {args.precision} solve",
-                   "active_cells_per_gpu": active, "parallelism": f"replicas x{world}",
+                   "active_cells_per_gpu": res["active"], "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (13 GB working set)"},
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clocks.summary(),
+        "roofline": roof, "forms": forms, "cpu_baseline": cpu, "e2e": res["e2e"],
+        "gpu_launches": res["launches"], "clocks": res["clocks"],
     }
     print(json.dumps(line))
     if dist:

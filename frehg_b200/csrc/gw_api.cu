@@ -174,10 +174,11 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     for (double** p : solv)
       if (e == cudaSuccess) e = dalloc_margin(D, p, n3, m);
     if (desc->precision == FREHG_GW_PRECISION_MIXED) {
-      float** solv32[] = {&D.diag32, &D.gxp32, &D.gyp32, &D.gzp32, &D.r32,
-                          &D.x32,    &D.p032,  &D.p132,  &D.w32};
+      float** solv32[] = {&D.diag32, &D.gxp32, &D.gyp32, &D.gzp32, &D.dinv32, &D.l32,
+                          &D.r32,    &D.z32,   &D.d32,   &D.p032,  &D.p132, &D.w32};
       for (float** p : solv32)
         if (e == cudaSuccess) e = dalloc_margin(D, p, n3, m);
+      if (e == cudaSuccess) e = dalloc_margin(D, &D.xalt, n3, m);
     }
     if (e != cudaSuccess) {
       free_device(D);
@@ -200,7 +201,7 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
                                                   static_cast<long long>(D.sm_count) * 8));
     if (D.nblk < 1) D.nblk = 1;
     D.cg_grid = fgw::cg64_grid(D.sm_count, n3);
-    D.cg_grid32 = fgw::cg32_grid(D.sm_count, n3);
+    D.cg_grid32 = D.sm_count * 4;
     if (e == cudaSuccess)
       e = dalloc(D, &D.partial, static_cast<size_t>(fgw::kPSlots) * D.nblk);
     if (e == cudaSuccess)

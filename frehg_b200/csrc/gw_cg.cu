@@ -27,93 +27,14 @@
 #include <cfloat>
 #include <cstdio>
 
+#include "gw_coop.cuh"
 #include "gw_internal.h"
 
 namespace fgw {
 
 namespace {
 
-constexpr int kCgBlock = 256;
-constexpr long long kSpinLimit = 20000000LL;  // ~2-4 s of polling
-
-__device__ inline unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ inline int ld_relaxed_int(const int* p) {
-  int v;
-  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Grid-wide barrier for a cooperative (co-resident) launch.  Returns false
-// when the barrier gave up; the caller then leaves the kernel.
-__device__ bool grid_sync(CgState* st, unsigned nblocks) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int good = 1;
-    if (ld_relaxed_int(&st->err) != 0) {
-      good = 0;
-    } else {
-      const unsigned my = ld_acquire(&st->bar_gen);
-      __threadfence();
-      const unsigned arrived = atomicAdd(&st->bar_count, 1u) + 1u;
-      if (arrived == nblocks) {
-        atomicExch(&st->bar_count, 0u);
-        __threadfence();
-        atomicAdd(&st->bar_gen, 1u);
-      } else {
-        long long spins = 0;
-        while (ld_acquire(&st->bar_gen) == my) {
-          if (++spins > kSpinLimit || ld_relaxed_int(&st->err) != 0) {
-            atomicExch(&st->err, 1);
-            good = 0;
-            break;
-          }
-          __nanosleep(64);
-        }
-      }
-      __threadfence();
-    }
-    ok = good;
-  }
-  __syncthreads();
-  return ok != 0;
-}
-
-__device__ inline double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Fixed-order block sum; result broadcast to every thread.
-__device__ double block_sum_all(double v) {
-  __shared__ double sh[32];
-  __shared__ double res;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  v = warp_sum(v);
-  if (lane == 0) sh[wid] = v;
-  __syncthreads();
-  if (wid == 0) {
-    v = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
-    v = warp_sum(v);
-    if (lane == 0) res = v;
-  }
-  __syncthreads();
-  const double out = res;
-  __syncthreads();
-  return out;
-}
-
-// Sum of the G per-block partials, identical in every block.
-__device__ double reduce_partials(const double* part, int G) {
-  double v = 0.0;
-  for (int b = threadIdx.x; b < G; b += blockDim.x) v += part[b];
-  return block_sum_all(v);
-}
+using namespace coop;
 
 struct Cg64Args {
   Dims d;
@@ -249,11 +170,171 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
   }
 }
 
+
+// The same solve with two consecutive k-cells per thread and 16-byte loads
+// and stores (used when nz is even, so every pair and every i/j-neighbour pair
+// is 16-byte aligned): half the load instructions per cell and twice the bytes
+// in flight per request.  The arithmetic per cell is the scalar kernel's.
+__device__ inline double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ inline void st2(double* p, double a, double b) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+
+__global__ void __launch_bounds__(kCgBlock, 3) k_cg64v(Cg64Args a) {
+  const long long N2 = a.d.ncell / 2, sx = a.d.sx, sy = a.d.sy;
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const int G = gridDim.x;
+  double* const pzz = a.part;
+  double* const pzr = a.part + G;
+  double* const ppw = a.part + 2 * G;
+
+  double zz = 0.0, zr = 0.0;
+  for (long long q = t0; q < N2; q += stride) {
+    const long long c = 2 * q;
+    const double2 rc = ld2(a.b + c);
+    const double2 dg = ld2(a.diag + c);
+    st2(a.x + c, 0.0, 0.0);
+    st2(a.r + c, rc.x, rc.y);
+    st2(a.p0 + c, 0.0, 0.0);
+    st2(a.p1 + c, 0.0, 0.0);
+    const double z0 = rc.x * (1.0 / dg.x), z1 = rc.y * (1.0 / dg.y);
+    st2(a.z + c, z0, z1);
+    zz += z0 * z0;
+    zz += z1 * z1;
+    zr += z0 * rc.x;
+    zr += z1 * rc.y;
+  }
+  double s = block_sum_all(zz);
+  if (threadIdx.x == 0) pzz[blockIdx.x] = s;
+  s = block_sum_all(zr);
+  if (threadIdx.x == 0) pzr[blockIdx.x] = s;
+  if (!grid_sync(a.st, G)) return;
+  double dp = sqrt(reduce_partials(pzz, G));
+  double beta = reduce_partials(pzr, G);
+  const double rnorm0 = dp;
+  const double ttol = fmax(a.rtol * rnorm0, a.atol);
+  int reason = 0, its = 0;
+  const auto test = [&](double rn) {
+    if (!isfinite(rn)) reason = -9;
+    else if (rn <= ttol) reason = (rn < a.atol) ? 3 : 2;
+    else if (rn >= 1.0e5 * rnorm0) reason = -4;
+  };
+  test(dp);
+  double betaold = 1.0, dpi = 0.0, dpiold = 0.0;
+  int i = 0;
+  while (reason == 0) {
+    its = i + 1;
+    if (beta == 0.0) {
+      reason = 3;
+      break;
+    }
+    if (i > 0 && beta * betaold < 0.0) {
+      reason = -8;
+      break;
+    }
+    const double bc = (i == 0) ? 0.0 : beta / betaold;
+    const double* __restrict__ pold = (i & 1) ? a.p1 : a.p0;
+    double* __restrict__ pnew = (i & 1) ? a.p0 : a.p1;
+    double pw = 0.0;
+    for (long long q = t0; q < N2; q += stride) {
+      const long long c = 2 * q;
+      const double2 zc = ld2(a.z + c), pc = ld2(pold + c);
+      const double2 zxm = ld2(a.z + c - sx), pxm = ld2(pold + c - sx);
+      const double2 zxp = ld2(a.z + c + sx), pxp = ld2(pold + c + sx);
+      const double2 zym = ld2(a.z + c - sy), pym = ld2(pold + c - sy);
+      const double2 zyp = ld2(a.z + c + sy), pyp = ld2(pold + c + sy);
+      const double zkm = a.z[c - 1], pkm = pold[c - 1];
+      const double zkp = a.z[c + 2], pkp = pold[c + 2];
+      const double2 dg = ld2(a.diag + c);
+      const double2 gx = ld2(a.gxp + c), gxm = ld2(a.gxp + c - sx);
+      const double2 gy = ld2(a.gyp + c), gym = ld2(a.gyp + c - sy);
+      const double2 gz = ld2(a.gzp + c);
+      const double gzm = a.gzp[c - 1];
+      const double P0 = zc.x + bc * pc.x, P1 = zc.y + bc * pc.y;
+      const double Pkm = zkm + bc * pkm, Pkp = zkp + bc * pkp;
+      const double Pxm0 = zxm.x + bc * pxm.x, Pxm1 = zxm.y + bc * pxm.y;
+      const double Pxp0 = zxp.x + bc * pxp.x, Pxp1 = zxp.y + bc * pxp.y;
+      const double Pym0 = zym.x + bc * pym.x, Pym1 = zym.y + bc * pym.y;
+      const double Pyp0 = zyp.x + bc * pyp.x, Pyp1 = zyp.y + bc * pyp.y;
+      double w0 = gym.x * Pym0;
+      w0 += gxm.x * Pxm0;
+      w0 += gzm * Pkm;
+      w0 += dg.x * P0;
+      w0 += gz.x * P1;
+      w0 += gx.x * Pxp0;
+      w0 += gy.x * Pyp0;
+      double w1 = gym.y * Pym1;
+      w1 += gxm.y * Pxm1;
+      w1 += gz.x * P0;
+      w1 += dg.y * P1;
+      w1 += gz.y * Pkp;
+      w1 += gx.y * Pxp1;
+      w1 += gy.y * Pyp1;
+      st2(pnew + c, P0, P1);
+      st2(a.w + c, w0, w1);
+      pw += P0 * w0;
+      pw += P1 * w1;
+    }
+    s = block_sum_all(pw);
+    if (threadIdx.x == 0) ppw[blockIdx.x] = s;
+    if (!grid_sync(a.st, G)) return;
+    dpiold = dpi;
+    dpi = reduce_partials(ppw, G);
+    betaold = beta;
+    if (dpi == 0.0 || (i > 0 && sgn(dpi) * sgn(dpiold) < 0)) {
+      reason = -10;
+      break;
+    }
+    const double al = beta / dpi;
+    zz = 0.0;
+    zr = 0.0;
+    for (long long q = t0; q < N2; q += stride) {
+      const long long c = 2 * q;
+      const double2 pc = ld2(pnew + c), xc = ld2(a.x + c), rc0 = ld2(a.r + c);
+      const double2 wc = ld2(a.w + c), dg = ld2(a.diag + c);
+      st2(a.x + c, xc.x + al * pc.x, xc.y + al * pc.y);
+      const double r0 = rc0.x - al * wc.x, r1 = rc0.y - al * wc.y;
+      st2(a.r + c, r0, r1);
+      const double z0 = r0 * (1.0 / dg.x), z1 = r1 * (1.0 / dg.y);
+      st2(a.z + c, z0, z1);
+      zz += z0 * z0;
+      zz += z1 * z1;
+      zr += z0 * r0;
+      zr += z1 * r1;
+    }
+    s = block_sum_all(zz);
+    if (threadIdx.x == 0) pzz[blockIdx.x] = s;
+    s = block_sum_all(zr);
+    if (threadIdx.x == 0) pzr[blockIdx.x] = s;
+    if (!grid_sync(a.st, G)) return;
+    dp = sqrt(reduce_partials(pzz, G));
+    test(dp);
+    if (reason != 0) break;
+    beta = reduce_partials(pzr, G);
+    ++i;
+    if (i >= a.maxit) {
+      reason = -3;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.st->dp = dp;
+    a.st->rnorm0 = rnorm0;
+    a.st->its = its;
+    a.st->reason = reason;
+    a.st->outer = 1;
+  }
+}
+
 }  // namespace
 
 int cg64_grid(int sm_count, long long ncell) {
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg64, kCgBlock, 0);
+  int per_sm_v = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, k_cg64v, kCgBlock, 0);
+  if (per_sm_v < per_sm) per_sm = per_sm_v;
   if (per_sm < 1) per_sm = 1;
   const long long want = (ncell + kCgBlock - 1) / kCgBlock;
   long long g = static_cast<long long>(per_sm) * sm_count;
@@ -283,21 +364,9 @@ cudaError_t launch_cg64(Device& D, double rtol, double atol, int maxit) {
   a.maxit = maxit;
   void* args[] = {&a};
   ++D.launches;
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg64), dim3(D.cg_grid),
-                                     dim3(kCgBlock), args, 0, D.stream);
-}
-
-int cg32_grid(int sm_count, long long ncell) { return cg64_grid(sm_count, ncell); }
-
-cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, double outer_rtol,
-                            int max_outer) {
-  (void)D;
-  (void)rtol;
-  (void)atol;
-  (void)maxit;
-  (void)outer_rtol;
-  (void)max_outer;
-  return cudaErrorNotSupported;
+  const void* kern = (D.d.nz % 2 == 0) ? reinterpret_cast<const void*>(k_cg64v)
+                                       : reinterpret_cast<const void*>(k_cg64);
+  return cudaLaunchCooperativeKernel(kern, dim3(D.cg_grid), dim3(kCgBlock), args, 0, D.stream);
 }
 
 }  // namespace fgw

@@ -1,0 +1,401 @@
+// Mixed-precision predictor solve: FP32 inner preconditioned CG inside FP64
+// defect correction on the true residual.
+//
+//   x = 0
+//   repeat (outer sweep o = 0, 1, ...):
+//     x <- x + d;  r = b - A x  in FP64 with the FP64 coefficients
+//     stop when ||r||_2 <= outer_rtol ||b||_2
+//     solve A d = r approximately in FP32: CG preconditioned by the exact
+//     solve of each column's vertical tridiagonal block (line Jacobi along
+//     k), stopped at inner_rtol of the initial preconditioned norm
+//
+// The line preconditioner follows the thin-layer anisotropy of the head
+// system (dz << dx makes the vertical legs 10^2-10^3 times the lateral ones):
+// it solves the dominant couplings exactly and cuts the inner iteration count
+// by an order of magnitude against point Jacobi.  Every iterate that leaves
+// the solve is an FP64 vector whose FP64 residual met outer_rtol, so the
+// solution's accuracy is set by the FP64 sweep, not by the FP32 arithmetic.
+//
+// Layout.  The tridiagonal solve needs whole columns: phase B and the outer
+// residual pass walk the domain in tiles of `tc` consecutive columns (one
+// contiguous run of tc*nz cells in the halo layout), stage the tile in shared
+// memory (row pitch nz+1 so the per-column sweeps are bank-conflict free),
+// let one thread per column run the LDL^T sweeps, and write back coalesced.
+// Phase A (direction update + stencil product) is cell-parallel as in the
+// FP64 kernel.  FP32 inner traffic per cell and iteration: phase A 8 words
+// (z, p_old, diag, gxp, gyp, gzp in; p_new, w out), phase B 9 words (d, p, r,
+// w, dinv, l in; d, r, z out) -> 68 B.
+#include <cfloat>
+
+#include "gw_coop.cuh"
+#include "gw_internal.h"
+
+namespace fgw {
+
+using namespace coop;
+
+namespace {
+
+constexpr int kFactorBlock = 256;
+constexpr int kTileCells = 4096;  // tc * nz <= kTileCells (64 KB of FP32 staging)
+
+// Cast the FP64 coefficients to FP32 and factor every column's tridiagonal
+// block T = LDL^T (pivots in FP64, stored as FP32 1/d_k and l_k).
+__global__ void __launch_bounds__(kFactorBlock) k_line_factor(Dims d, const double* __restrict__ diag,
+                                                              const double* __restrict__ gxp,
+                                                              const double* __restrict__ gyp,
+                                                              const double* __restrict__ gzp,
+                                                              float* diag32, float* gxp32,
+                                                              float* gyp32, float* gzp32,
+                                                              float* dinv32, float* l32, int tc) {
+  extern __shared__ double fsm[];
+  const int nz = d.nz, nzp = nz + 1;
+  double* s_a = fsm;
+  double* s_e = fsm + static_cast<long long>(tc) * nzp;
+  const long long ntiles = (d.ncol + tc - 1) / tc;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const long long base = t * tc * nz;
+    const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
+    const int ncells = ncols * nz;
+    for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
+      const long long c = base + f;
+      const int col = f / nz, k = f - col * nz;
+      s_a[col * nzp + k] = diag[c];
+      s_e[col * nzp + k] = gzp[c];
+      diag32[c] = static_cast<float>(diag[c]);
+      gxp32[c] = static_cast<float>(gxp[c]);
+      gyp32[c] = static_cast<float>(gyp[c]);
+      gzp32[c] = static_cast<float>(gzp[c]);
+    }
+    __syncthreads();
+    if (threadIdx.x < ncols) {
+      double* a = s_a + threadIdx.x * nzp;
+      double* e = s_e + threadIdx.x * nzp;
+      double dprev = a[0];
+      a[0] = dprev;
+      for (int k = 1; k < nz; ++k) {
+        const double l = e[k - 1] / dprev;
+        const double dk = a[k] - l * e[k - 1];
+        e[k - 1] = l;
+        a[k] = dk;
+        dprev = dk;
+      }
+      e[nz - 1] = 0.0;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
+      const long long c = base + f;
+      const int col = f / nz, k = f - col * nz;
+      const double dk = s_a[col * nzp + k];
+      dinv32[c] = (dk > 0.0 && isfinite(dk)) ? static_cast<float>(1.0 / dk)
+                                             : static_cast<float>(1.0 / diag[c]);
+      l32[c] = static_cast<float>(s_e[col * nzp + k]);
+    }
+    __syncthreads();
+  }
+}
+
+struct MixedArgs {
+  Dims d;
+  const double *diag, *gxp, *gyp, *gzp, *b;
+  double *x0, *x1;
+  const float *diag32, *gxp32, *gyp32, *gzp32, *dinv32, *l32;
+  float *r32, *z32, *p0, *p1, *w32, *d32;
+  double* part;  // 3 x G
+  CgState* st;
+  double outer_rtol, inner_rtol, atol;
+  int max_inner, max_outer, max_total;
+  int tc;
+};
+
+// Forward/backward LDL^T sweeps of one staged column: z = T^-1 r.
+__device__ inline void column_solve(const float* r, const float* dinv, const float* l, float* z,
+                                    int nz) {
+  float y = r[0];
+  z[0] = y;
+  for (int k = 1; k < nz; ++k) {
+    y = r[k] - l[k - 1] * y;
+    z[k] = y;
+  }
+  float zk = z[nz - 1] * dinv[nz - 1];
+  z[nz - 1] = zk;
+  for (int k = nz - 2; k >= 0; --k) {
+    zk = z[k] * dinv[k] - l[k] * zk;
+    z[k] = zk;
+  }
+}
+
+__global__ void __launch_bounds__(kCgBlock) k_cg_mixed(MixedArgs a) {
+  extern __shared__ float msm[];
+  const Dims& d = a.d;
+  const int nz = d.nz, nzp = nz + 1, tc = a.tc;
+  float* s_r = msm;
+  float* s_dinv = msm + tc * nzp;
+  float* s_l = msm + 2 * tc * nzp;
+  float* s_z = msm + 3 * tc * nzp;
+  const long long N = d.ncell, sx = d.sx, sy = d.sy;
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long ntiles = (d.ncol + tc - 1) / tc;
+  const int G = gridDim.x;
+  double* const q0 = a.part;
+  double* const q1 = a.part + G;
+  double* const q2 = a.part + 2 * G;
+
+  for (long long c = t0; c < N; c += stride) {
+    a.x0[c] = 0.0;
+    a.d32[c] = 0.0f;
+  }
+  if (!grid_sync(a.st, G)) return;
+
+  double bnorm = 0.0, rnorm = 0.0;
+  int total = 0, outer = 0, reason = 0, final_buf = 0;
+  for (int o = 0;; ++o) {
+    const double* __restrict__ xo = (o & 1) ? a.x1 : a.x0;
+    double* __restrict__ xn = (o & 1) ? a.x0 : a.x1;
+    // Outer pass: x_new = x + d, r = b - A x_new (FP64), r32, z = T^-1 r32.
+    double rn2 = 0.0, zz = 0.0, zr = 0.0;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const long long base = t * tc * nz;
+      const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
+      const int ncells = ncols * nz;
+      for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
+        const long long c = base + f;
+        const int col = f / nz, k = f - col * nz;
+        const double xc = xo[c] + static_cast<double>(a.d32[c]);
+        const double xym = xo[c - sy] + static_cast<double>(a.d32[c - sy]);
+        const double xxm = xo[c - sx] + static_cast<double>(a.d32[c - sx]);
+        const double xzm = xo[c - 1] + static_cast<double>(a.d32[c - 1]);
+        const double xzp = xo[c + 1] + static_cast<double>(a.d32[c + 1]);
+        const double xxp = xo[c + sx] + static_cast<double>(a.d32[c + sx]);
+        const double xyp = xo[c + sy] + static_cast<double>(a.d32[c + sy]);
+        double ax = a.gyp[c - sy] * xym;
+        ax += a.gxp[c - sx] * xxm;
+        ax += a.gzp[c - 1] * xzm;
+        ax += a.diag[c] * xc;
+        ax += a.gzp[c] * xzp;
+        ax += a.gxp[c] * xxp;
+        ax += a.gyp[c] * xyp;
+        const double rr = a.b[c] - ax;
+        xn[c] = xc;
+        rn2 += rr * rr;
+        const float r32 = static_cast<float>(rr);
+        a.r32[c] = r32;
+        s_r[col * nzp + k] = r32;
+        s_dinv[col * nzp + k] = a.dinv32[c];
+        s_l[col * nzp + k] = a.l32[c];
+      }
+      __syncthreads();
+      if (threadIdx.x < ncols) {
+        const int o2 = threadIdx.x * nzp;
+        column_solve(s_r + o2, s_dinv + o2, s_l + o2, s_z + o2, nz);
+      }
+      __syncthreads();
+      for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
+        const long long c = base + f;
+        const int col = f / nz, k = f - col * nz;
+        const float z = s_z[col * nzp + k];
+        a.z32[c] = z;
+        a.p0[c] = 0.0f;
+        zz += static_cast<double>(z) * z;
+        zr += static_cast<double>(z) * s_r[col * nzp + k];
+      }
+      __syncthreads();
+    }
+    double s = block_sum_all(rn2);
+    if (threadIdx.x == 0) q0[blockIdx.x] = s;
+    s = block_sum_all(zz);
+    if (threadIdx.x == 0) q1[blockIdx.x] = s;
+    s = block_sum_all(zr);
+    if (threadIdx.x == 0) q2[blockIdx.x] = s;
+    if (!grid_sync(a.st, G)) return;
+    rnorm = sqrt(reduce_partials(q0, G));
+    const double zn0 = sqrt(reduce_partials(q1, G));
+    double beta = reduce_partials(q2, G);
+    final_buf = (o & 1) ? 0 : 1;
+    if (o == 0) bnorm = rnorm;
+    if (!isfinite(rnorm)) {
+      reason = -9;
+      break;
+    }
+    if (rnorm <= fmax(a.outer_rtol * bnorm, a.atol)) {
+      reason = (rnorm < a.atol) ? 3 : 2;
+      break;
+    }
+    if (outer >= a.max_outer || total >= a.max_total) {
+      reason = -3;
+      break;
+    }
+    ++outer;
+    // d = 0 for this sweep's inner solve.
+    for (long long c = t0; c < N; c += stride) a.d32[c] = 0.0f;
+    // Inner FP32 PCG on A d = r32.
+    const double itol = a.inner_rtol * zn0;
+    double betaold = 1.0;
+    for (int i = 0; i < a.max_inner && total < a.max_total; ++i) {
+      if (beta == 0.0 || (i > 0 && beta * betaold <= 0.0)) break;
+      const float bc = (i == 0) ? 0.0f : static_cast<float>(beta / betaold);
+      const float* __restrict__ pold = (i & 1) ? a.p1 : a.p0;
+      float* __restrict__ pnew = (i & 1) ? a.p0 : a.p1;
+      double pw = 0.0;
+      for (long long c = t0; c < N; c += stride) {
+        const float pc = a.z32[c] + bc * pold[c];
+        const float pym = a.z32[c - sy] + bc * pold[c - sy];
+        const float pxm = a.z32[c - sx] + bc * pold[c - sx];
+        const float pzm = a.z32[c - 1] + bc * pold[c - 1];
+        const float pzp = a.z32[c + 1] + bc * pold[c + 1];
+        const float pxp = a.z32[c + sx] + bc * pold[c + sx];
+        const float pyp = a.z32[c + sy] + bc * pold[c + sy];
+        float wv = a.gyp32[c - sy] * pym;
+        wv += a.gxp32[c - sx] * pxm;
+        wv += a.gzp32[c - 1] * pzm;
+        wv += a.diag32[c] * pc;
+        wv += a.gzp32[c] * pzp;
+        wv += a.gxp32[c] * pxp;
+        wv += a.gyp32[c] * pyp;
+        pnew[c] = pc;
+        a.w32[c] = wv;
+        pw += static_cast<double>(pc) * wv;
+      }
+      s = block_sum_all(pw);
+      if (threadIdx.x == 0) q0[blockIdx.x] = s;
+      if (!grid_sync(a.st, G)) return;
+      const double dpi = reduce_partials(q0, G);
+      if (!(dpi > 0.0)) break;  // inner breakdown: keep d, let the FP64 sweep judge
+      const float al = static_cast<float>(beta / dpi);
+      betaold = beta;
+      ++total;
+      zz = 0.0;
+      zr = 0.0;
+      for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const long long base = t * tc * nz;
+        const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
+        const int ncells = ncols * nz;
+        for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
+          const long long c = base + f;
+          const int col = f / nz, k = f - col * nz;
+          a.d32[c] += al * pnew[c];
+          const float r = a.r32[c] - al * a.w32[c];
+          a.r32[c] = r;
+          s_r[col * nzp + k] = r;
+          s_dinv[col * nzp + k] = a.dinv32[c];
+          s_l[col * nzp + k] = a.l32[c];
+        }
+        __syncthreads();
+        if (threadIdx.x < ncols) {
+          const int o2 = threadIdx.x * nzp;
+          column_solve(s_r + o2, s_dinv + o2, s_l + o2, s_z + o2, nz);
+        }
+        __syncthreads();
+        for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
+          const long long c = base + f;
+          const int col = f / nz, k = f - col * nz;
+          const float z = s_z[col * nzp + k];
+          a.z32[c] = z;
+          zz += static_cast<double>(z) * z;
+          zr += static_cast<double>(z) * s_r[col * nzp + k];
+        }
+        __syncthreads();
+      }
+      s = block_sum_all(zz);
+      if (threadIdx.x == 0) q1[blockIdx.x] = s;
+      s = block_sum_all(zr);
+      if (threadIdx.x == 0) q2[blockIdx.x] = s;
+      if (!grid_sync(a.st, G)) return;
+      const double zn = sqrt(reduce_partials(q1, G));
+      if (zn <= itol) break;
+      beta = reduce_partials(q2, G);
+    }
+  }
+  // The solution of the last outer pass lives in x1 after even passes.
+  if (final_buf == 1) {
+    for (long long c = t0; c < N; c += stride) a.x0[c] = a.x1[c];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.st->dp = rnorm;
+    a.st->rnorm0 = bnorm;
+    a.st->its = total;
+    a.st->reason = reason;
+    a.st->outer = outer;
+  }
+}
+
+int host_tile_cols(int nz) {
+  int tc = kTileCells / nz;
+  if (tc < 1) tc = 1;
+  if (tc > 64) tc = 64;
+  return tc;
+}
+
+size_t mixed_smem(int nz) { return 4 * sizeof(float) * host_tile_cols(nz) * (nz + 1); }
+size_t factor_smem(int nz) { return 2 * sizeof(double) * host_tile_cols(nz) * (nz + 1); }
+
+}  // namespace
+
+int cg32_grid(int sm_count, long long ncell) {
+  (void)ncell;
+  return sm_count;  // refined per domain in launch_cg_mixed (depends on nz)
+}
+
+cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, double outer_rtol,
+                            int max_outer) {
+  (void)rtol;
+  const int nz = D.d.nz;
+  if (host_tile_cols(nz) * nz > kTileCells && nz > kTileCells) return cudaErrorInvalidValue;
+  const size_t fsm = factor_smem(nz), msm = mixed_smem(nz);
+  cudaFuncSetAttribute(k_line_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(fsm));
+  cudaFuncSetAttribute(k_cg_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(msm));
+  const int tc = host_tile_cols(nz);
+  const long long ntiles = (D.d.ncol + tc - 1) / tc;
+  const int fgrid = static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));
+  k_line_factor<<<fgrid, kFactorBlock, fsm, D.stream>>>(D.d, D.diag, D.gxp, D.gyp, D.gzp,
+                                                        D.diag32, D.gxp32, D.gyp32, D.gzp32,
+                                                        D.dinv32, D.l32, tc);
+  ++D.launches;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_mixed, kCgBlock, msm);
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  long long g = static_cast<long long>(per_sm) * D.sm_count;
+  if (g > ntiles) g = ntiles;
+  if (g < 1) g = 1;
+  cudaMemsetAsync(&D.out->cg, 0, sizeof(CgState), D.stream);
+  MixedArgs a;
+  a.d = D.d;
+  a.diag = D.diag;
+  a.gxp = D.gxp;
+  a.gyp = D.gyp;
+  a.gzp = D.gzp;
+  a.b = D.rhs;
+  a.x0 = D.x;
+  a.x1 = D.xalt;
+  a.diag32 = D.diag32;
+  a.gxp32 = D.gxp32;
+  a.gyp32 = D.gyp32;
+  a.gzp32 = D.gzp32;
+  a.dinv32 = D.dinv32;
+  a.l32 = D.l32;
+  a.r32 = D.r32;
+  a.z32 = D.z32;
+  a.p0 = D.p032;
+  a.p1 = D.p132;
+  a.w32 = D.w32;
+  a.d32 = D.d32;
+  a.part = D.cgpart;
+  a.st = &D.out->cg;
+  a.outer_rtol = outer_rtol;
+  a.inner_rtol = 1.0e-4;
+  a.atol = atol;
+  a.max_inner = maxit;
+  a.max_outer = max_outer;
+  a.max_total = maxit;
+  a.tc = tc;
+  void* args[] = {&a};
+  ++D.launches;
+  D.cg_grid32 = static_cast<int>(g);
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_cg_mixed), dim3(g),
+                                     dim3(kCgBlock), args, msm, D.stream);
+}
+
+}  // namespace fgw

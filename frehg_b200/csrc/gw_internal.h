@@ -79,7 +79,10 @@ struct Device {
   double *x = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *w = nullptr;
   // mixed precision: FP32 copies and inner vectors (same margins)
   float *diag32 = nullptr, *gxp32 = nullptr, *gyp32 = nullptr, *gzp32 = nullptr;
-  float *r32 = nullptr, *x32 = nullptr, *p032 = nullptr, *p132 = nullptr, *w32 = nullptr;
+  float *dinv32 = nullptr, *l32 = nullptr;  // LDL^T factors of the column blocks
+  float *r32 = nullptr, *z32 = nullptr, *d32 = nullptr, *p032 = nullptr, *p132 = nullptr,
+        *w32 = nullptr;
+  double* xalt = nullptr;  // FP64 ping-pong partner of x (mixed outer sweeps)
   // reductions
   double* partial = nullptr;   // kPSlots x nblk
   double* cgpart = nullptr;    // 3 x cg grid
@@ -116,6 +119,5 @@ cudaError_t launch_cg64(Device& D, double rtol, double atol, int maxit);
 cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, double outer_rtol,
                             int max_outer);
 int cg64_grid(int sm_count, long long ncell);
-int cg32_grid(int sm_count, long long ncell);
 
 }  // namespace fgw

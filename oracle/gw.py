@@ -60,6 +60,8 @@ def load():
         f = getattr(lib, "oracle_vg_" + name)
         f.restype = C.c_double
         f.argtypes = [C.c_double] * 7
+    lib.oracle_gw_last_system.restype = C.c_long
+    lib.oracle_gw_last_system.argtypes = [C.c_void_p, _dp, _lp, _dp]
     lib.oracle_cg7.restype = C.c_int
     lib.oracle_cg7.argtypes = [C.c_long, _dp, _lp, _dp, _dp, C.c_double, C.c_double, C.c_int, _dp]
     _lib = lib
@@ -134,6 +136,16 @@ class OracleSolver:
         hh = np.ascontiguousarray(head, np.float64)
         ww = np.ascontiguousarray(wc, np.float64)
         self.lib.oracle_gw_set_state(self.h, hh.ctypes.data_as(_dp), ww.ctypes.data_as(_dp))
+
+    def last_system(self):
+        """(vals7, cols7, rhs) of the last predictor system."""
+        n = self.active_cells()
+        v = np.empty((n, 7))
+        c = np.empty((n, 7), dtype=np.int64)
+        b = np.empty(n)
+        self.lib.oracle_gw_last_system(self.h, v.ctypes.data_as(_dp), c.ctypes.data_as(_lp),
+                                       b.ctypes.data_as(_dp))
+        return v, c, b
 
     def owned_volume(self) -> float:
         return self.lib.oracle_gw_owned_volume(self.h)

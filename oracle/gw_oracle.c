@@ -1449,6 +1449,15 @@ int oracle_gw_step(oracle_gw* s, double t, double dtg, frehg_gw_step_info* info)
 }
 
 double oracle_gw_next_dt(const oracle_gw* s) { return s->dtg_next; }
+
+/* The predictor system of the last step: 7 legs per row [diag, xm, xp, ym,
+ * yp, zm, zp], their neighbour rows (-1 = none) and the right-hand side. */
+long oracle_gw_last_system(const oracle_gw* s, double* vals7, long* cols7, double* rhs) {
+  if (vals7) memcpy(vals7, s->vals7, (size_t)s->nactive * 7 * sizeof(double));
+  if (cols7) memcpy(cols7, s->cols7, (size_t)s->nactive * 7 * sizeof(long));
+  if (rhs) memcpy(rhs, s->rhs, (size_t)s->nactive * sizeof(double));
+  return (long)s->nactive;
+}
 long long oracle_gw_active_cells(const oracle_gw* s) { return s->nactive; }
 double oracle_gw_elevation_offset(const oracle_gw* s) { return s->offset; }
 

@@ -32,6 +32,7 @@ int oracle_gw_init_state(oracle_gw* s, int form, double constant, const double* 
 int oracle_gw_set_state(oracle_gw* s, const double* head, const double* wc);
 int oracle_gw_step(oracle_gw* s, double t, double dtg, frehg_gw_step_info* info);
 double oracle_gw_next_dt(const oracle_gw* s);
+long oracle_gw_last_system(const oracle_gw* s, double* vals7, long* cols7, double* rhs);
 /* Fields in the ABI shapes (include/frehg_gw.h, FREHG_GW_FIELD_*). */
 int oracle_gw_get_field(const oracle_gw* s, int field, double* out);
 double oracle_gw_owned_volume(const oracle_gw* s);
