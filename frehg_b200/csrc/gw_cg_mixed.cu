@@ -37,7 +37,7 @@ using namespace coop;
 namespace {
 
 constexpr int kFactorBlock = 256;
-constexpr int kTileCells = 4096;  // tc * nz <= kTileCells (64 KB of FP32 staging)
+constexpr int kTileCells = 4096;  // tc * nz <= kTileCells (2 x 16 KB of FP32 staging)
 
 // Cast the FP64 coefficients to FP32 and factor every column's tridiagonal
 // block T = LDL^T (pivots in FP64, stored as FP32 1/d_k and l_k).
@@ -108,31 +108,96 @@ struct MixedArgs {
   int tc;
 };
 
-// Forward/backward LDL^T sweeps of one staged column: z = T^-1 r.
-__device__ inline void column_solve(const float* r, const float* dinv, const float* l, float* z,
-                                    int nz) {
+// Forward/backward LDL^T sweeps of one column: z = T^-1 r.  r and z live in
+// the staged shared-memory tile; the factors are read straight from global
+// memory (one thread walks its own contiguous column, so every 32-byte sector
+// it touches serves 8 consecutive steps from L1).
+__device__ inline void column_solve(const float* r, const float* __restrict__ dinv,
+                                    const float* __restrict__ l, float* z, int nz) {
   float y = r[0];
   z[0] = y;
   for (int k = 1; k < nz; ++k) {
-    y = r[k] - l[k - 1] * y;
+    y = r[k] - __ldg(l + k - 1) * y;
     z[k] = y;
   }
-  float zk = z[nz - 1] * dinv[nz - 1];
+  float zk = z[nz - 1] * __ldg(dinv + nz - 1);
   z[nz - 1] = zk;
   for (int k = nz - 2; k >= 0; --k) {
-    zk = z[k] * dinv[k] - l[k] * zk;
+    zk = z[k] * __ldg(dinv + k) - __ldg(l + k) * zk;
     z[k] = zk;
   }
 }
 
-__global__ void __launch_bounds__(kCgBlock) k_cg_mixed(MixedArgs a) {
+__device__ inline float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ inline void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+
+// Phase A for V consecutive k-cells per thread (V = 4: 16-byte loads; the
+// lower/upper z legs of the group come from gzp[c-1] and the group's own).
+template <int V>
+__device__ inline double phase_a(const MixedArgs& a, float bc, const float* __restrict__ pold,
+                                 float* __restrict__ pnew, long long t0, long long stride) {
+  const long long N = a.d.ncell, sx = a.d.sx, sy = a.d.sy;
+  double pw = 0.0;
+  if constexpr (V == 4) {
+    for (long long q = t0; q < N / 4; q += stride) {
+      const long long c = 4 * q;
+      const float4 z = ld4(a.z32 + c), p = ld4(pold + c);
+      const float4 zxm = ld4(a.z32 + c - sx), pxm = ld4(pold + c - sx);
+      const float4 zxp = ld4(a.z32 + c + sx), pxp = ld4(pold + c + sx);
+      const float4 zym = ld4(a.z32 + c - sy), pym = ld4(pold + c - sy);
+      const float4 zyp = ld4(a.z32 + c + sy), pyp = ld4(pold + c + sy);
+      const float pkm = a.z32[c - 1] + bc * pold[c - 1];
+      const float pkp = a.z32[c + 4] + bc * pold[c + 4];
+      const float4 dg = ld4(a.diag32 + c);
+      const float4 gx = ld4(a.gxp32 + c), gxm = ld4(a.gxp32 + c - sx);
+      const float4 gy = ld4(a.gyp32 + c), gym = ld4(a.gyp32 + c - sy);
+      const float4 gz = ld4(a.gzp32 + c);
+      const float gzm = a.gzp32[c - 1];
+      float4 P, W;
+      P.x = z.x + bc * p.x;
+      P.y = z.y + bc * p.y;
+      P.z = z.z + bc * p.z;
+      P.w = z.w + bc * p.w;
+      W.x = gym.x * (zym.x + bc * pym.x) + gxm.x * (zxm.x + bc * pxm.x) + gzm * pkm +
+            dg.x * P.x + gz.x * P.y + gx.x * (zxp.x + bc * pxp.x) + gy.x * (zyp.x + bc * pyp.x);
+      W.y = gym.y * (zym.y + bc * pym.y) + gxm.y * (zxm.y + bc * pxm.y) + gz.x * P.x +
+            dg.y * P.y + gz.y * P.z + gx.y * (zxp.y + bc * pxp.y) + gy.y * (zyp.y + bc * pyp.y);
+      W.z = gym.z * (zym.z + bc * pym.z) + gxm.z * (zxm.z + bc * pxm.z) + gz.y * P.y +
+            dg.z * P.z + gz.z * P.w + gx.z * (zxp.z + bc * pxp.z) + gy.z * (zyp.z + bc * pyp.z);
+      W.w = gym.w * (zym.w + bc * pym.w) + gxm.w * (zxm.w + bc * pxm.w) + gz.z * P.z +
+            dg.w * P.w + gz.w * pkp + gx.w * (zxp.w + bc * pxp.w) + gy.w * (zyp.w + bc * pyp.w);
+      st4(pnew + c, P);
+      st4(a.w32 + c, W);
+      pw += static_cast<double>(P.x) * W.x;
+      pw += static_cast<double>(P.y) * W.y;
+      pw += static_cast<double>(P.z) * W.z;
+      pw += static_cast<double>(P.w) * W.w;
+    }
+  } else {
+    for (long long c = t0; c < N; c += stride) {
+      const float pc = a.z32[c] + bc * pold[c];
+      float wv = a.gyp32[c - sy] * (a.z32[c - sy] + bc * pold[c - sy]);
+      wv += a.gxp32[c - sx] * (a.z32[c - sx] + bc * pold[c - sx]);
+      wv += a.gzp32[c - 1] * (a.z32[c - 1] + bc * pold[c - 1]);
+      wv += a.diag32[c] * pc;
+      wv += a.gzp32[c] * (a.z32[c + 1] + bc * pold[c + 1]);
+      wv += a.gxp32[c] * (a.z32[c + sx] + bc * pold[c + sx]);
+      wv += a.gyp32[c] * (a.z32[c + sy] + bc * pold[c + sy]);
+      pnew[c] = pc;
+      a.w32[c] = wv;
+      pw += static_cast<double>(pc) * wv;
+    }
+  }
+  return pw;
+}
+
+template <int V>
+__global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
   extern __shared__ float msm[];
   const Dims& d = a.d;
   const int nz = d.nz, nzp = nz + 1, tc = a.tc;
   float* s_r = msm;
-  float* s_dinv = msm + tc * nzp;
-  float* s_l = msm + 2 * tc * nzp;
-  float* s_z = msm + 3 * tc * nzp;
+  float* s_z = msm + tc * nzp;
   const long long N = d.ncell, sx = d.sx, sy = d.sy;
   const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
   const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
@@ -163,32 +228,25 @@ __global__ void __launch_bounds__(kCgBlock) k_cg_mixed(MixedArgs a) {
         const long long c = base + f;
         const int col = f / nz, k = f - col * nz;
         const double xc = xo[c] + static_cast<double>(a.d32[c]);
-        const double xym = xo[c - sy] + static_cast<double>(a.d32[c - sy]);
-        const double xxm = xo[c - sx] + static_cast<double>(a.d32[c - sx]);
-        const double xzm = xo[c - 1] + static_cast<double>(a.d32[c - 1]);
-        const double xzp = xo[c + 1] + static_cast<double>(a.d32[c + 1]);
-        const double xxp = xo[c + sx] + static_cast<double>(a.d32[c + sx]);
-        const double xyp = xo[c + sy] + static_cast<double>(a.d32[c + sy]);
-        double ax = a.gyp[c - sy] * xym;
-        ax += a.gxp[c - sx] * xxm;
-        ax += a.gzp[c - 1] * xzm;
+        double ax = a.gyp[c - sy] * (xo[c - sy] + static_cast<double>(a.d32[c - sy]));
+        ax += a.gxp[c - sx] * (xo[c - sx] + static_cast<double>(a.d32[c - sx]));
+        ax += a.gzp[c - 1] * (xo[c - 1] + static_cast<double>(a.d32[c - 1]));
         ax += a.diag[c] * xc;
-        ax += a.gzp[c] * xzp;
-        ax += a.gxp[c] * xxp;
-        ax += a.gyp[c] * xyp;
+        ax += a.gzp[c] * (xo[c + 1] + static_cast<double>(a.d32[c + 1]));
+        ax += a.gxp[c] * (xo[c + sx] + static_cast<double>(a.d32[c + sx]));
+        ax += a.gyp[c] * (xo[c + sy] + static_cast<double>(a.d32[c + sy]));
         const double rr = a.b[c] - ax;
         xn[c] = xc;
         rn2 += rr * rr;
         const float r32 = static_cast<float>(rr);
         a.r32[c] = r32;
         s_r[col * nzp + k] = r32;
-        s_dinv[col * nzp + k] = a.dinv32[c];
-        s_l[col * nzp + k] = a.l32[c];
       }
       __syncthreads();
       if (threadIdx.x < ncols) {
-        const int o2 = threadIdx.x * nzp;
-        column_solve(s_r + o2, s_dinv + o2, s_l + o2, s_z + o2, nz);
+        const long long cb = base + static_cast<long long>(threadIdx.x) * nz;
+        column_solve(s_r + threadIdx.x * nzp, a.dinv32 + cb, a.l32 + cb,
+                     s_z + threadIdx.x * nzp, nz);
       }
       __syncthreads();
       for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
@@ -227,7 +285,6 @@ __global__ void __launch_bounds__(kCgBlock) k_cg_mixed(MixedArgs a) {
       break;
     }
     ++outer;
-    // d = 0 for this sweep's inner solve.
     for (long long c = t0; c < N; c += stride) a.d32[c] = 0.0f;
     // Inner FP32 PCG on A d = r32.
     const double itol = a.inner_rtol * zn0;
@@ -237,26 +294,7 @@ __global__ void __launch_bounds__(kCgBlock) k_cg_mixed(MixedArgs a) {
       const float bc = (i == 0) ? 0.0f : static_cast<float>(beta / betaold);
       const float* __restrict__ pold = (i & 1) ? a.p1 : a.p0;
       float* __restrict__ pnew = (i & 1) ? a.p0 : a.p1;
-      double pw = 0.0;
-      for (long long c = t0; c < N; c += stride) {
-        const float pc = a.z32[c] + bc * pold[c];
-        const float pym = a.z32[c - sy] + bc * pold[c - sy];
-        const float pxm = a.z32[c - sx] + bc * pold[c - sx];
-        const float pzm = a.z32[c - 1] + bc * pold[c - 1];
-        const float pzp = a.z32[c + 1] + bc * pold[c + 1];
-        const float pxp = a.z32[c + sx] + bc * pold[c + sx];
-        const float pyp = a.z32[c + sy] + bc * pold[c + sy];
-        float wv = a.gyp32[c - sy] * pym;
-        wv += a.gxp32[c - sx] * pxm;
-        wv += a.gzp32[c - 1] * pzm;
-        wv += a.diag32[c] * pc;
-        wv += a.gzp32[c] * pzp;
-        wv += a.gxp32[c] * pxp;
-        wv += a.gyp32[c] * pyp;
-        pnew[c] = pc;
-        a.w32[c] = wv;
-        pw += static_cast<double>(pc) * wv;
-      }
+      const double pw = phase_a<V>(a, bc, pold, pnew, t0, stride);
       s = block_sum_all(pw);
       if (threadIdx.x == 0) q0[blockIdx.x] = s;
       if (!grid_sync(a.st, G)) return;
@@ -271,29 +309,67 @@ __global__ void __launch_bounds__(kCgBlock) k_cg_mixed(MixedArgs a) {
         const long long base = t * tc * nz;
         const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
         const int ncells = ncols * nz;
-        for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
-          const long long c = base + f;
-          const int col = f / nz, k = f - col * nz;
-          a.d32[c] += al * pnew[c];
-          const float r = a.r32[c] - al * a.w32[c];
-          a.r32[c] = r;
-          s_r[col * nzp + k] = r;
-          s_dinv[col * nzp + k] = a.dinv32[c];
-          s_l[col * nzp + k] = a.l32[c];
+        if constexpr (V == 4) {
+          for (int f = 4 * threadIdx.x; f < ncells; f += 4 * blockDim.x) {
+            const long long c = base + f;
+            const int col = f / nz, k = f - col * nz;
+            const float4 pn = ld4(pnew + c), w = ld4(a.w32 + c);
+            float4 dd = ld4(a.d32 + c), r = ld4(a.r32 + c);
+            dd.x += al * pn.x;
+            dd.y += al * pn.y;
+            dd.z += al * pn.z;
+            dd.w += al * pn.w;
+            r.x -= al * w.x;
+            r.y -= al * w.y;
+            r.z -= al * w.z;
+            r.w -= al * w.w;
+            st4(a.d32 + c, dd);
+            st4(a.r32 + c, r);
+            float* sr = s_r + col * nzp + k;
+            sr[0] = r.x;
+            sr[1] = r.y;
+            sr[2] = r.z;
+            sr[3] = r.w;
+          }
+        } else {
+          for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
+            const long long c = base + f;
+            const int col = f / nz, k = f - col * nz;
+            a.d32[c] += al * pnew[c];
+            const float r = a.r32[c] - al * a.w32[c];
+            a.r32[c] = r;
+            s_r[col * nzp + k] = r;
+          }
         }
         __syncthreads();
         if (threadIdx.x < ncols) {
-          const int o2 = threadIdx.x * nzp;
-          column_solve(s_r + o2, s_dinv + o2, s_l + o2, s_z + o2, nz);
+          const long long cb = base + static_cast<long long>(threadIdx.x) * nz;
+          column_solve(s_r + threadIdx.x * nzp, a.dinv32 + cb, a.l32 + cb,
+                       s_z + threadIdx.x * nzp, nz);
         }
         __syncthreads();
-        for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
-          const long long c = base + f;
-          const int col = f / nz, k = f - col * nz;
-          const float z = s_z[col * nzp + k];
-          a.z32[c] = z;
-          zz += static_cast<double>(z) * z;
-          zr += static_cast<double>(z) * s_r[col * nzp + k];
+        if constexpr (V == 4) {
+          for (int f = 4 * threadIdx.x; f < ncells; f += 4 * blockDim.x) {
+            const long long c = base + f;
+            const int col = f / nz, k = f - col * nz;
+            const float* sz = s_z + col * nzp + k;
+            const float* sr = s_r + col * nzp + k;
+            const float4 z = make_float4(sz[0], sz[1], sz[2], sz[3]);
+            st4(a.z32 + c, z);
+            zz += static_cast<double>(z.x) * z.x + static_cast<double>(z.y) * z.y +
+                  static_cast<double>(z.z) * z.z + static_cast<double>(z.w) * z.w;
+            zr += static_cast<double>(z.x) * sr[0] + static_cast<double>(z.y) * sr[1] +
+                  static_cast<double>(z.z) * sr[2] + static_cast<double>(z.w) * sr[3];
+          }
+        } else {
+          for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
+            const long long c = base + f;
+            const int col = f / nz, k = f - col * nz;
+            const float z = s_z[col * nzp + k];
+            a.z32[c] = z;
+            zz += static_cast<double>(z) * z;
+            zr += static_cast<double>(z) * s_r[col * nzp + k];
+          }
         }
         __syncthreads();
       }
@@ -327,7 +403,7 @@ int host_tile_cols(int nz) {
   return tc;
 }
 
-size_t mixed_smem(int nz) { return 4 * sizeof(float) * host_tile_cols(nz) * (nz + 1); }
+size_t mixed_smem(int nz) { return 2 * sizeof(float) * host_tile_cols(nz) * (nz + 1); }
 size_t factor_smem(int nz) { return 2 * sizeof(double) * host_tile_cols(nz) * (nz + 1); }
 
 }  // namespace
@@ -345,8 +421,10 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
   const size_t fsm = factor_smem(nz), msm = mixed_smem(nz);
   cudaFuncSetAttribute(k_line_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(fsm));
-  cudaFuncSetAttribute(k_cg_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(msm));
+  const bool vec = (nz % 4 == 0);
+  const void* kern = vec ? reinterpret_cast<const void*>(k_cg_mixed<4>)
+                         : reinterpret_cast<const void*>(k_cg_mixed<1>);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm));
   const int tc = host_tile_cols(nz);
   const long long ntiles = (D.d.ncol + tc - 1) / tc;
   const int fgrid = static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));
@@ -355,7 +433,7 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
                                                         D.dinv32, D.l32, tc);
   ++D.launches;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_mixed, kCgBlock, msm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCgBlock, msm);
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   long long g = static_cast<long long>(per_sm) * D.sm_count;
   if (g > ntiles) g = ntiles;
@@ -385,7 +463,7 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
   a.part = D.cgpart;
   a.st = &D.out->cg;
   a.outer_rtol = outer_rtol;
-  a.inner_rtol = 1.0e-4;
+  a.inner_rtol = 1.0e-5;
   a.atol = atol;
   a.max_inner = maxit;
   a.max_outer = max_outer;
@@ -394,8 +472,7 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
   void* args[] = {&a};
   ++D.launches;
   D.cg_grid32 = static_cast<int>(g);
-  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_cg_mixed), dim3(g),
-                                     dim3(kCgBlock), args, msm, D.stream);
+  return cudaLaunchCooperativeKernel(kern, dim3(g), dim3(kCgBlock), args, msm, D.stream);
 }
 
 }  // namespace fgw
