@@ -1,0 +1,127 @@
+// RichardsSolver.hpp — C++20 host mirror of frehg2's gw::RichardsSolver over
+// the B200 C ABI (include/frehg_gw.h).
+//
+// The class keeps the reference's member names and meanings
+// (src/gw/RichardsSolver.hpp:166-423): step(t, dtg) with t the end-of-step
+// time, nextDt(), head(), waterContent(), the volumetric flux accessors,
+// audit(), lastSolve() and ownedVolume().  Non-OK ABI statuses throw
+// frehg_b200::FatalError, as the reference's log::fatal throws
+// frehg::FatalError (src/core/Types.hpp:53-62), so driver-side error
+// semantics are unchanged.  Fields come back in the ABI shapes (interior
+// cells, k fastest); a driver that keeps the reference's halo-layout views
+// copies them in (INTEGRATION.md shows the wiring).
+#pragma once
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../include/frehg_gw.h"
+
+namespace frehg_b200 {
+
+class FatalError : public std::runtime_error {
+ public:
+  FatalError(int status, const std::string& message)
+      : std::runtime_error(message), status_(status) {}
+  int status() const { return status_; }
+
+ private:
+  int status_;
+};
+
+/// The reference's GwStepAudit terms returned by the step.
+struct GwStepAudit {
+  double boundaryIn = 0.0;
+  double ssStorage = 0.0;
+  double reallocAdjust = 0.0;
+  double reallocDropped = 0.0;
+  double vloss = 0.0;
+};
+
+/// The reference's SolveStats of the predictor solve.
+struct SolveStats {
+  int iterations = 0;
+  int outerSweeps = 0;
+  double residualNorm = 0.0;
+};
+
+class RichardsSolver {
+ public:
+  /// Build the domain from a rasterized descriptor and set the initial state
+  /// (`icForm` is FREHG_GW_IC_*; `icField` null means the constant).
+  RichardsSolver(const frehg_gw_desc& desc, int icForm, double icConstant,
+                 const double* icField = nullptr, void* cudaStream = nullptr)
+      : nx_(desc.nx), ny_(desc.ny), nz_(desc.nz) {
+    check(frehg_gw_create(&desc, &h_));
+    if (cudaStream) check(frehg_gw_set_stream(h_, cudaStream));
+    check(frehg_gw_init_state(h_, icForm, icConstant, icField));
+  }
+  RichardsSolver(const RichardsSolver&) = delete;
+  RichardsSolver& operator=(const RichardsSolver&) = delete;
+  ~RichardsSolver() { frehg_gw_destroy(h_); }
+
+  /// RichardsSolver::updateBoundaryValues with the caller's value(t); null
+  /// arrays keep their current values.
+  void setBoundaryValues(const double* top, const double* bottom, const double* xm,
+                         const double* xp, const double* ym, const double* yp) {
+    check(frehg_gw_set_bc_values(h_, top, bottom, xm, xp, ym, yp));
+  }
+
+  /// RichardsSolver::step(t, dtg).
+  void step(double t, double dtg) {
+    frehg_gw_step_info info{};
+    check(frehg_gw_step(h_, t, dtg, &info));
+    audit_ = {info.boundary_in, info.ss_storage, info.realloc_adjust, info.realloc_dropped,
+              info.vloss};
+    last_ = {info.cg_iterations, info.outer_iterations, info.residual_norm};
+  }
+
+  double nextDt() const {
+    double v = 0.0;
+    check(frehg_gw_next_dt(h_, &v));
+    return v;
+  }
+
+  std::vector<double> head() const { return field(FREHG_GW_FIELD_HEAD); }
+  std::vector<double> waterContent() const { return field(FREHG_GW_FIELD_WC); }
+  std::vector<double> waterContentStart() const { return field(FREHG_GW_FIELD_WC_START); }
+  std::vector<double> fluxXVolumetric() const { return field(FREHG_GW_FIELD_QX); }
+  std::vector<double> fluxYVolumetric() const { return field(FREHG_GW_FIELD_QY); }
+  std::vector<double> fluxZFaceVolumetric() const { return field(FREHG_GW_FIELD_QZ); }
+  std::vector<double> faceConductivityX() const { return field(FREHG_GW_FIELD_KX); }
+  std::vector<double> faceConductivityY() const { return field(FREHG_GW_FIELD_KY); }
+  std::vector<double> faceConductivityZFace() const { return field(FREHG_GW_FIELD_KZ); }
+
+  /// Restart read + refreshDerivedState (interior arrays).
+  void setState(const double* head, const double* wc) { check(frehg_gw_set_state(h_, head, wc)); }
+
+  const GwStepAudit& audit() const { return audit_; }
+  const SolveStats& lastSolve() const { return last_; }
+
+  double ownedVolume() const {
+    double v = 0.0;
+    check(frehg_gw_owned_volume(h_, &v));
+    return v;
+  }
+
+  long long activeCells() const { return frehg_gw_active_cells(h_); }
+  frehg_gw_handle* handle() const { return h_; }
+
+ private:
+  static void check(int rc) {
+    if (rc != FREHG_GW_OK) throw FatalError(rc, frehg_gw_last_error());
+  }
+  std::vector<double> field(int which) const {
+    std::vector<double> out(frehg_gw_field_size(h_, which));
+    check(frehg_gw_get_field(h_, which, out.data()));
+    return out;
+  }
+
+  frehg_gw_handle* h_ = nullptr;
+  int nx_, ny_, nz_;
+  GwStepAudit audit_;
+  SolveStats last_;
+};
+
+}  // namespace frehg_b200
