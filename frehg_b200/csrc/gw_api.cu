@@ -163,7 +163,7 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
       e = dalloc(D, &D.h[b], n3);
       if (e == cudaSuccess) e = dalloc(D, &D.wc[b], n3);
     }
-    double** cellf[] = {&D.hp, &D.wcu, &D.kcx, &D.kcy, &D.kcz, &D.kx, &D.ky, &D.qx, &D.qy,
+    double** cellf[] = {&D.hp, &D.wcu, &D.ch, &D.kcx, &D.kcy, &D.kcz, &D.kx, &D.ky, &D.qx, &D.qy,
                         &D.vloss, &D.room, &D.sup, &D.sdn};
     for (double** p : cellf)
       if (e == cudaSuccess) e = dalloc(D, p, n3);

@@ -68,6 +68,7 @@ struct Device {
   double* wc[2] = {nullptr, nullptr};
   int cur = 0;
   double *hp = nullptr, *wcu = nullptr;           // predicted head, corrected theta
+  double* ch = nullptr;                           // C(h^n) of the storage term
   double *kcx = nullptr, *kcy = nullptr, *kcz = nullptr;  // per-cell K of the pass
   double *kx = nullptr, *ky = nullptr, *kzf = nullptr;    // corrector face K
   double *qx = nullptr, *qy = nullptr, *qzf = nullptr;    // fluxes

@@ -99,14 +99,20 @@ __global__ void k_ghosts(Dims d, Fields f, double* h, double* wc) {
 // Per-cell directional conductivities K(h, Ksx|Ksy|Ksz) of the predictor pass
 // from the step-start head (ghosts included; Predictor.cpp:127-232 evaluates
 // them for both flanks of every face).
+// The same pass also evaluates C(h^n), the capacity of the storage term
+// (Predictor.cpp:445-452), from the same powers.
 __global__ void k_closure_pred(Dims d, Fields f, const double* __restrict__ h, double* kcx,
-                               double* kcy, double* kcz) {
+                               double* kcy, double* kcz, double* ch) {
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const KrParts p = vg_kr_parts(soil_at(f, c), h[c]);
+    const Soil so = soil_at(f, c);
+    const double hc = h[c];
+    const VgParts v = vg_parts(so, hc);
+    const KrParts p = vg_kr_from(v, hc);
     kcx[c] = vg_k_from(p, f.ksx[c]);
     kcy[c] = vg_k_from(p, f.ksy[c]);
     kcz[c] = vg_k_from(p, f.ksz[c]);
+    ch[c] = vg_capacity_from(so, v, hc);
   }
 }
 
@@ -156,9 +162,10 @@ __global__ void k_closure_corr(Dims d, Fields f, const double* __restrict__ x,
 // (the same expression on the same data, so the stored matrix is the
 // reference's up to the rounding of its z legs).  Legs toward an inactive
 // cell or out of the domain are stored as 0 (PETSc ignores column -1).
-__global__ void k_assemble(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
-                           const double* __restrict__ wcn, double dtg, double* diag, double* gxps,
-                           double* gyps, double* gzps, double* rhs) {
+__global__ void __launch_bounds__(kBlock, 3)
+    k_assemble(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
+               const double* __restrict__ wcn, const double* __restrict__ ch, double dtg,
+               double* diag, double* gxps, double* gyps, double* gzps, double* rhs) {
   const double dx = d.dx, dy = d.dy;
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -196,8 +203,7 @@ __global__ void k_assemble(Dims d, Fields f, PassK pk, const double* __restrict_
     dzf = top ? 0.5 * dzc : 0.5 * (dzc + f.dz[c - 1]);
     const double gzm = -kzm * dtg / (dzc * dzf) * volume;
 
-    const Soil so = soil_at(f, c);
-    const double storage = vg_capacity(so, hn[c]) + d.ss * wcn[c] / so.ts;
+    const double storage = ch[c] + d.ss * wcn[c] / f.wcs[c];
     double gct = storage * volume - (gxp + gxm + gyp + gym);
     if (east && cxp == kFlux) gct += gxp;
     if (west && cxm == kFlux) gct += gxm;
@@ -489,7 +495,7 @@ __device__ inline Split gradient_split(const Dims& d, const Fields& f, const dou
 // Reallocate.cpp:181-391, saturated_contact: head): reads the corrected theta
 // and predicted head as the pre-sweep snapshot, writes the restored state to
 // separate buffers, so the classification is race-free by construction.
-__global__ void k_classify(Dims d, Fields f, const double* __restrict__ kx,
+__global__ void __launch_bounds__(kBlock, 3) k_classify(Dims d, Fields f, const double* __restrict__ kx,
                            const double* __restrict__ ky, const double* __restrict__ kzf,
                            const double* __restrict__ wcR, const double* __restrict__ hR,
                            double* wc_out, double* h_out, double* room, double* sup, double* sdn,
@@ -575,7 +581,7 @@ __global__ void k_classify(Dims d, Fields f, const double* __restrict__ kx,
 
 // Phase 2: the vertical send walks, one thread per flagged column, k
 // ascending (Reallocate.cpp:410-540, uncoupled, no transport window).
-__global__ void k_walk(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
+__global__ void k_walk_thread(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
                        const double* __restrict__ sdn, double* qzf, const int* __restrict__ colflag,
                        double dtg, double* partial) {
   double lost = 0.0;
@@ -644,11 +650,126 @@ __global__ void k_walk(Dims d, Fields f, double* wc, double* room, const double*
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// The same walk with one warp per flagged column.  The column's room, theta,
+// cell volume, activity and face fluxes are staged in shared memory
+// (coalesced), a ballot over each 32-cell chunk finds the surplus cells in
+// ascending k, and lane 0 runs the sequential walk of each one on shared
+// memory, so the deposit order and every rounding step are those of the
+// per-thread walk above.  Shared memory per warp: walk_warp_bytes(nz).
+constexpr int kWalkWarps = kBlock / 32;
+__host__ __device__ inline size_t walk_warp_bytes(int nz) {
+  return static_cast<size_t>(4 * nz + 1) * sizeof(double) + ((nz + 7) & ~7);
+}
+
+__device__ inline void walk_deposit(double& dv, int ll, double* rs, double* ws, const double* vs,
+                                    double* qs, int face, double sign, double dtg) {
+  if (rs[ll] > 0.0) {
+    const double take = (rs[ll] > dv) ? dv : rs[ll];
+    ws[ll] += take / vs[ll];
+    rs[ll] -= take;
+    if (sign > 0.0) {
+      qs[face] += take / dtg;
+    } else {
+      qs[face] -= take / dtg;
+    }
+    dv -= take;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
+                                                 const double* __restrict__ room,
+                                                 const double* __restrict__ sup,
+                                                 const double* __restrict__ sdn, double* qzf,
+                                                 const int* __restrict__ colflag, double dtg,
+                                                 double* partial) {
+  extern __shared__ __align__(16) unsigned char walk_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nz = d.nz;
+  double* rs = reinterpret_cast<double*>(walk_smem + warp * walk_warp_bytes(nz));
+  double* ws = rs + nz;
+  double* vs = ws + nz;
+  double* qs = vs + nz;  // nz + 1 faces
+  signed char* as = reinterpret_cast<signed char*>(qs + nz + 1);
+  double lost = 0.0;
+  const long long ncolint = static_cast<long long>(d.nx) * d.ny;
+  const long long nwarps = static_cast<long long>(gridDim.x) * kWalkWarps;
+  for (long long t = blockIdx.x * static_cast<long long>(kWalkWarps) + warp; t < ncolint;
+       t += nwarps) {
+    const int j = static_cast<int>(t / d.nx) + 1, i = static_cast<int>(t % d.nx) + 1;
+    const long long col = col2(d, j, i);
+    if (!colflag[col]) continue;
+    const long long base = cidx(d, j, i, 0), fb = fidx(d, j, i, 0);
+    const bool topHead = f.topc[col] == kHead;
+    for (int k = lane; k < nz; k += 32) {
+      rs[k] = room[base + k];
+      ws[k] = wc[base + k];
+      vs[k] = d.az * f.dz[base + k];
+      as[k] = f.act[base + k];
+    }
+    for (int k = lane; k <= nz; k += 32) qs[k] = qzf[fb + k];
+    __syncwarp();
+    for (int k0 = 0; k0 < nz; k0 += 32) {
+      const int k = k0 + lane;
+      double su = 0.0, sd = 0.0;
+      bool any = false;
+      if (k < nz && as[k]) {
+        su = sup[base + k];
+        sd = sdn[base + k];
+        any = su > 0.0 || sd > 0.0;
+      }
+      unsigned mask = __ballot_sync(0xffffffffu, any);
+      while (mask) {
+        const int b = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const double up = __shfl_sync(0xffffffffu, su, b);
+        const double dn = __shfl_sync(0xffffffffu, sd, b);
+        if (lane == 0) {
+          const int kk = k0 + b;
+          double dv = up;
+          if (dv > 0.0) {
+            int ll = kk;
+            while (ll > 0 && as[ll - 1] && dv > 0.0) {
+              --ll;
+              walk_deposit(dv, ll, rs, ws, vs, qs, ll + 1, 1.0, dtg);
+            }
+            if (dv > 0.0) {
+              if (topHead) {
+                qs[ll] += dv / dtg;
+              } else {
+                while (ll + 1 < nz && dv > 0.0) {
+                  ++ll;
+                  walk_deposit(dv, ll, rs, ws, vs, qs, ll, -1.0, dtg);
+                }
+                lost -= dv;
+              }
+            }
+          }
+          dv = dn;
+          if (dv > 0.0) {
+            int ll = kk;
+            while (ll + 1 < nz && dv > 0.0) {
+              ++ll;
+              walk_deposit(dv, ll, rs, ws, vs, qs, ll, -1.0, dtg);
+            }
+            lost -= dv;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    for (int k = lane; k < nz; k += 32) wc[base + k] = ws[k];
+    for (int k = lane; k <= nz; k += 32) qzf[fb + k] = qs[k];
+    __syncwarp();
+  }
+  const double s = block_reduce(lost, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
 // ---------------------------------------------------------------- clamp, audit, controller
 // finalizeWaterContent (Corrector.cpp:758-792), accumulateBoundaryFlux
 // (RichardsSolver.cpp:961-1006), the adaptTimeStep inputs (AdaptiveStep.cpp:
 // 58-98) and the owned volume (RichardsSolver.cpp:892-912), in one sweep.
-__global__ void k_finalize(Dims d, Fields f, double* wc, double* vloss,
+__global__ void __launch_bounds__(kBlock, 3) k_finalize(Dims d, Fields f, double* wc, double* vloss,
                            const double* __restrict__ qx, const double* __restrict__ qy,
                            const double* __restrict__ qzf, double dtg, double co_max,
                            double* partial, int nblk) {
@@ -814,14 +935,15 @@ void launch_ghosts(const Device& D, double* h, double* wc) {
 }
 
 void launch_closure_pred(const Device& D, const double* h) {
-  k_closure_pred<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, h, D.kcx, D.kcy, D.kcz);
+  k_closure_pred<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, h, D.kcx, D.kcy, D.kcz,
+                                                         D.ch);
   ++D.launches;
 }
 
 void launch_assemble(const Device& D, const double* hn, const double* wcn, double dtg) {
   PassK pk{D.kcx, D.kcy, D.kcz, wcn};
-  k_assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, hn, wcn, dtg, D.diag, D.gxp,
-                                                     D.gyp, D.gzp, D.rhs);
+  k_assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, hn, wcn, D.ch, dtg, D.diag,
+                                                     D.gxp, D.gyp, D.gzp, D.rhs);
   ++D.launches;
 }
 
@@ -853,9 +975,20 @@ void launch_classify(const Device& D, double* wc_out, double* h_out) {
   ++D.launches;
 }
 
+// Columns deeper than the shared-memory staging allows take the per-thread walk.
+constexpr size_t kWalkSmemMax = 48 * 1024;
+
 void launch_walk(const Device& D, double* wc_out, double dtg) {
-  k_walk<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn, D.qzf,
-                                                 D.colflag, dtg, D.partial + kPLost * D.nblk);
+  const size_t smem = kWalkWarps * walk_warp_bytes(D.d.nz);
+  if (smem <= kWalkSmemMax) {
+    k_walk<<<cells_grid(D), kBlock, smem, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
+                                                      D.qzf, D.colflag, dtg,
+                                                      D.partial + kPLost * D.nblk);
+  } else {
+    k_walk_thread<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
+                                                          D.qzf, D.colflag, dtg,
+                                                          D.partial + kPLost * D.nblk);
+  }
   ++D.launches;
 }
 
