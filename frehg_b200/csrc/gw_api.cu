@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <exception>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -563,3 +564,86 @@ int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5) {
 long long frehg_gw_kernel_launches(const frehg_gw_handle* h) { return h ? h->D.launches : 0; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- init_state without allocation
+// frehg_gw_init_state stages a caller's IC field in a device buffer that it
+// allocates and frees on every call.  frehg_gw_init_state_static stages it in
+// one fixed array compiled into this library instead, so the call allocates
+// nothing.  It is meant for callers that cannot allocate at that point: a
+// driver that has handed all free HBM to its own memory pool (cudaMalloc
+// would fail), or one that re-initialises domains while other streams are
+// busy (cudaFree waits for the whole device).
+//
+// The array holds FREHG_GW_STATIC_FIELD_MAX doubles (2 MiB); larger fields
+// are rejected with FREHG_GW_EINVAL.  Nothing in it has to start at zero:
+// each call writes the values it then reads.  Every call on a device uses
+// the same array, so two calls that overlap in time (two host threads, or two
+// handles driven concurrently) race on it and must be serialised by the
+// caller.  The first call on each device does a one-time set-up (it looks up
+// the array's device address, which may load this library's device code on
+// that device); make that first call before any stream capture begins.
+static __device__ __align__(256) double g_static_field[FREHG_GW_STATIC_FIELD_MAX];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+double* g_static_ptr[kStaticMaxDevices] = {};
+
+// The array's device address on the current device, looked up once per
+// device with that device current.
+int static_field_address(double** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev), "init_state_static: cudaGetDevice");
+  if (dev < 0 || dev >= kStaticMaxDevices)
+    return fail(FREHG_GW_EUNSUPPORTED, "init_state_static: device ordinal above 63");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress(&p, g_static_field), "init_state_static: scratch address");
+    g_static_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_static_ptr[dev];
+  return FREHG_GW_OK;
+}
+
+}  // namespace
+
+int frehg_gw_init_state_static(frehg_gw_handle* h, int form, double constant,
+                               const double* field) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  if (form < FREHG_GW_IC_MOISTURE || form > FREHG_GW_IC_WATER_TABLE)
+    return fail(FREHG_GW_EINVAL, "unknown initial-condition form");
+  double* scratch = nullptr;
+  const int rc = static_field_address(&scratch);
+  if (rc != FREHG_GW_OK) return rc;
+  fgw::Device& D = h->D;
+  const fgw::Dims& d = D.d;
+  const double* fdev = nullptr;
+  if (field) {
+    const size_t n = (form == FREHG_GW_IC_WATER_TABLE)
+                         ? static_cast<size_t>(d.nx) * d.ny
+                         : static_cast<size_t>(d.nx) * d.ny * d.nz;
+    if (n > static_cast<size_t>(FREHG_GW_STATIC_FIELD_MAX))
+      return fail(FREHG_GW_EINVAL,
+                  "init_state_static: field has " + std::to_string(n) +
+                      " values; the static scratch holds at most " +
+                      std::to_string(FREHG_GW_STATIC_FIELD_MAX) +
+                      " (use frehg_gw_init_state)");
+    CUDA_TRY(cudaMemcpyAsync(scratch, field, n * sizeof(double), cudaMemcpyHostToDevice,
+                             D.stream), "init_state_static");
+    fdev = scratch;
+  }
+  D.cur = 0;
+  fgw::launch_init_state(D, form, constant, fdev, h->bath_dev, h->offset);
+  fgw::launch_ghosts(D, D.h[0], D.wc[0]);
+  CUDA_TRY(cudaMemcpyAsync(D.h[1], D.h[0], d.ncell * sizeof(double), cudaMemcpyDeviceToDevice,
+                           D.stream), "init_state_static");
+  CUDA_TRY(cudaMemcpyAsync(D.wc[1], D.wc[0], d.ncell * sizeof(double), cudaMemcpyDeviceToDevice,
+                           D.stream), "init_state_static");
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "init_state_static");
+  CUDA_TRY(cudaGetLastError(), "init_state_static kernel");
+  h->have_state = true;
+  h->start_buf = 0;
+  return FREHG_GW_OK;
+}

@@ -177,6 +177,19 @@ int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top_value,
  * head) or ny*nx (water table), NULL = the constant. */
 int frehg_gw_init_state(frehg_gw_handle* h, int form, double constant, const double* field);
 
+/* frehg_gw_init_state without any device allocation; it has no counterpart in
+ * the reference.  The field is staged in one array compiled into the library
+ * (FREHG_GW_STATIC_FIELD_MAX doubles, 2 MiB) instead of a buffer allocated and
+ * freed per call, for callers that cannot allocate there: all free HBM already
+ * given to their own pool, or other streams running that cudaFree would wait
+ * for.  Larger fields return FREHG_GW_EINVAL.  All calls on a device share the
+ * array: calls that overlap in time race on it and must be serialised.  The
+ * first call on each device does a one-time set-up; make it before any stream
+ * capture begins. */
+#define FREHG_GW_STATIC_FIELD_MAX 262144
+int frehg_gw_init_state_static(frehg_gw_handle* h, int form, double constant,
+                               const double* field);
+
 /* Overwrite the interior head and moisture (host, ny*nx*nz each). */
 int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc);
 
