@@ -16,11 +16,15 @@
 // the solve is an FP64 vector whose FP64 residual met outer_rtol, so the
 // solution's accuracy is set by the FP64 sweep, not by the FP32 arithmetic.
 //
-// Layout.  The tridiagonal solve needs whole columns: phase B and the outer
-// residual pass walk the domain in tiles of `tc` consecutive columns (one
-// contiguous run of tc*nz cells in the halo layout), stage the tile in shared
-// memory (row pitch nz+1 so the per-column sweeps are bank-conflict free),
-// let one thread per column run the LDL^T sweeps, and write back coalesced.
+// Layout.  The tridiagonal solve needs whole columns.  For nz <= 256 phase B
+// and the outer residual pass give each warp whole columns: row e of a column
+// holds cells k = 32 e + lane (coalesced loads and stores), and the two
+// bidiagonal sweeps of the LDL^T solve run as warp scans of affine maps, so
+// every thread works and no block barrier is needed.  Deeper columns walk the
+// domain in tiles of `tc` consecutive columns (one contiguous run of tc*nz
+// cells in the halo layout), stage the tile in shared memory (row pitch nz+1
+// so the per-column sweeps are bank-conflict free), let one thread per column
+// run the LDL^T sweeps, and write back coalesced.
 // Phase A (direction update + stencil product) is cell-parallel as in the
 // FP64 kernel.  FP32 inner traffic per cell and iteration: phase A 8 words
 // (z, p_old, diag, gxp, gyp, gzp in; p_new, w out), phase B 9 words (d, p, r,
@@ -128,11 +132,173 @@ __device__ inline void column_solve(const float* r, const float* __restrict__ di
   }
 }
 
+// Warp-per-column LDL^T solve (nz <= 32 * kMaxE).  Lane `lane` holds the
+// E consecutive cells k = lane * E + e of the column (E a power of two with
+// 32 E >= nz).  With the unit lower bidiagonal factor L (subdiagonal l) and
+// pivots 1/dinv, z = T^-1 r is
+//   y_k = r_k - l_{k-1} y_{k-1}            (k ascending, y_0 = r_0)
+//   z_k = dinv_k y_k - l_k z_{k+1}         (k descending, z_{nz-1} = dinv y)
+// Each step is an affine map of its predecessor.  A lane composes its E maps,
+// a Hillis-Steele scan over the 32 lanes composes the lane maps (inclusive
+// for the forward sweep, suffix for the backward one), and each lane then
+// replays its E steps from its exclusive prefix.  Cells past nz hold the
+// identity map.  FP32 throughout: this is the inner preconditioner, whose
+// rounding the FP64 outer residual absorbs.
+//
+// Every load of a column is issued before any of its stores: the arrays are
+// distinct, but the compiler cannot prove it, and loads placed after a store
+// would wait for it.
+constexpr int kMaxE = 8;
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ inline void scan_affine_up(float& A, float& B, int lane) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const float Ap = __shfl_up_sync(kFull, A, off);
+    const float Bp = __shfl_up_sync(kFull, B, off);
+    if (lane >= off) {
+      B = fmaf(A, Bp, B);
+      A *= Ap;
+    }
+  }
+}
+
+__device__ inline void scan_affine_down(float& C, float& Dv, int lane) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const float Cn = __shfl_down_sync(kFull, C, off);
+    const float Dn = __shfl_down_sync(kFull, Dv, off);
+    if (lane + off < 32) {
+      Dv = fmaf(C, Dn, Dv);
+      C *= Cn;
+    }
+  }
+}
+
+// Load / store a lane's E cells of the column starting at cb.  `vec` (nz a
+// multiple of E) makes every lane all-in or all-out, with E-aligned addresses.
+template <int E>
+__device__ inline void ld_col(const float* p, long long cb, int lane, int nz, bool vec,
+                              float (&v)[E]) {
+  const int k0 = lane * E;
+  if (vec) {
+    if (k0 < nz) {
+      const float* q = p + cb + k0;
+      if constexpr (E == 1) {
+        v[0] = q[0];
+      } else if constexpr (E == 2) {
+        const float2 t = *reinterpret_cast<const float2*>(q);
+        v[0] = t.x;
+        v[1] = t.y;
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; e += 4) {
+          const float4 t = *reinterpret_cast<const float4*>(q + e);
+          v[e] = t.x;
+          v[e + 1] = t.y;
+          v[e + 2] = t.z;
+          v[e + 3] = t.w;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) v[e] = 0.0f;
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = (k0 + e < nz) ? p[cb + k0 + e] : 0.0f;
+  }
+}
+
+template <int E>
+__device__ inline void st_col(float* p, long long cb, int lane, int nz, bool vec,
+                              const float (&v)[E]) {
+  const int k0 = lane * E;
+  if (vec) {
+    if (k0 < nz) {
+      float* q = p + cb + k0;
+      if constexpr (E == 1) {
+        q[0] = v[0];
+      } else if constexpr (E == 2) {
+        *reinterpret_cast<float2*>(q) = make_float2(v[0], v[1]);
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; e += 4)
+          *reinterpret_cast<float4*>(q + e) = make_float4(v[e], v[e + 1], v[e + 2], v[e + 3]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (k0 + e < nz) p[cb + k0 + e] = v[e];
+  }
+}
+
+// z = T^-1 r for the column whose factors this lane holds (lk = l_k,
+// di = dinv_k of its E cells).
+template <int E>
+__device__ inline void warp_column_solve(const float (&lk)[E], const float (&di)[E], int lane,
+                                         int nz, const float (&r)[E], float (&z)[E]) {
+  const int k0 = lane * E;
+  const float lprev = __shfl_up_sync(kFull, lk[E - 1], 1);  // l_{k0-1}
+  float a[E];
+  float A = 1.0f, B = 0.0f;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int k = k0 + e;
+    a[e] = (k >= nz) ? 1.0f : (k == 0) ? 0.0f : -(e == 0 ? lprev : lk[e - 1]);
+    const float b = (k < nz) ? r[e] : 0.0f;
+    B = fmaf(a[e], B, b);
+    A *= a[e];
+  }
+  scan_affine_up(A, B, lane);
+  float y = __shfl_up_sync(kFull, B, 1);
+  if (lane == 0) y = 0.0f;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    y = fmaf(a[e], y, (k0 + e < nz) ? r[e] : 0.0f);
+    z[e] = y;
+  }
+  float c[E];
+  float C = 1.0f, Dv = 0.0f;
+#pragma unroll
+  for (int e = E - 1; e >= 0; --e) {
+    const int k = k0 + e;
+    c[e] = (k >= nz) ? 1.0f : (k + 1 < nz) ? -lk[e] : 0.0f;
+    z[e] = (k < nz) ? di[e] * z[e] : 0.0f;
+    Dv = fmaf(c[e], Dv, z[e]);
+    C *= c[e];
+  }
+  scan_affine_down(C, Dv, lane);
+  float zn = __shfl_down_sync(kFull, Dv, 1);
+  if (lane == 31) zn = 0.0f;
+#pragma unroll
+  for (int e = E - 1; e >= 0; --e) {
+    zn = fmaf(c[e], zn, z[e]);
+    z[e] = zn;
+  }
+}
+
 __device__ inline float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ inline void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 
 // Phase A for V consecutive k-cells per thread (V = 4: 16-byte loads; the
 // lower/upper z legs of the group come from gzp[c-1] and the group's own).
+// (A (x + d))_c in FP64 with the FP64 coefficients, in the SpMV's fixed
+// summation order (ym, xm, zm, diag, zp, xp, yp).
+__device__ inline double outer_ax(const MixedArgs& a, const double* __restrict__ xo, long long c,
+                                  long long sx, long long sy) {
+  const double xc = xo[c] + static_cast<double>(a.d32[c]);
+  double ax = a.gyp[c - sy] * (xo[c - sy] + static_cast<double>(a.d32[c - sy]));
+  ax += a.gxp[c - sx] * (xo[c - sx] + static_cast<double>(a.d32[c - sx]));
+  ax += a.gzp[c - 1] * (xo[c - 1] + static_cast<double>(a.d32[c - 1]));
+  ax += a.diag[c] * xc;
+  ax += a.gzp[c] * (xo[c + 1] + static_cast<double>(a.d32[c + 1]));
+  ax += a.gxp[c] * (xo[c + sx] + static_cast<double>(a.d32[c + sx]));
+  ax += a.gyp[c] * (xo[c + sy] + static_cast<double>(a.d32[c + sy]));
+  return ax;
+}
+
 template <int V>
 __device__ inline double phase_a(const MixedArgs& a, float bc, const float* __restrict__ pold,
                                  float* __restrict__ pnew, long long t0, long long stride) {
@@ -191,7 +357,9 @@ __device__ inline double phase_a(const MixedArgs& a, float bc, const float* __re
   return pw;
 }
 
-template <int V>
+// E = 0: shared-memory tiled line solve; E > 0: warp-per-column solve with E
+// cells per lane.
+template <int V, int E>
 __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
   extern __shared__ float msm[];
   const Dims& d = a.d;
@@ -203,6 +371,10 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
   const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   const long long ntiles = (d.ncol + tc - 1) / tc;
   const int G = gridDim.x;
+  const int lane = threadIdx.x & 31;
+  const bool vec = (E > 0) && (nz % (E > 0 ? E : 1) == 0);
+  const long long gwarp = blockIdx.x * static_cast<long long>(kCgBlock / 32) + (threadIdx.x >> 5);
+  const long long nwarp = static_cast<long long>(G) * (kCgBlock / 32);
   double* const q0 = a.part;
   double* const q1 = a.part + G;
   double* const q2 = a.part + 2 * G;
@@ -220,6 +392,41 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
     double* __restrict__ xn = (o & 1) ? a.x0 : a.x1;
     // Outer pass: x_new = x + d, r = b - A x_new (FP64), r32, z = T^-1 r32.
     double rn2 = 0.0, zz = 0.0, zr = 0.0;
+    if constexpr (E > 0) {
+      for (long long col = gwarp; col < d.ncol; col += nwarp) {
+        const long long cb = col * nz;
+        const int k0 = lane * E;
+        float rv[E], zv[E], lk[E], di[E];
+        double xv[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          rv[e] = 0.0f;
+          xv[e] = 0.0;
+          if (k0 + e < nz) {
+            const long long c = cb + k0 + e;
+            const double rr = a.b[c] - outer_ax(a, xo, c, sx, sy);
+            xv[e] = xo[c] + static_cast<double>(a.d32[c]);
+            rn2 += rr * rr;
+            rv[e] = static_cast<float>(rr);
+          }
+        }
+        ld_col<E>(a.l32, cb, lane, nz, vec, lk);
+        ld_col<E>(a.dinv32, cb, lane, nz, vec, di);
+        warp_column_solve<E>(lk, di, lane, nz, rv, zv);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          if (k0 + e < nz) {
+            xn[cb + k0 + e] = xv[e];
+            zz += static_cast<double>(zv[e]) * zv[e];
+            zr += static_cast<double>(zv[e]) * rv[e];
+          }
+          lk[e] = 0.0f;
+        }
+        st_col<E>(a.r32, cb, lane, nz, vec, rv);
+        st_col<E>(a.z32, cb, lane, nz, vec, zv);
+        st_col<E>(a.p0, cb, lane, nz, vec, lk);
+      }
+    } else {
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
       const long long base = t * tc * nz;
       const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
@@ -259,6 +466,7 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
         zr += static_cast<double>(z) * s_r[col * nzp + k];
       }
       __syncthreads();
+    }
     }
     double s = block_sum_all(rn2);
     if (threadIdx.x == 0) q0[blockIdx.x] = s;
@@ -305,6 +513,35 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
       ++total;
       zz = 0.0;
       zr = 0.0;
+      if constexpr (E > 0) {
+        for (long long col = gwarp; col < d.ncol; col += nwarp) {
+          const long long cb = col * nz;
+          const int k0 = lane * E;
+          float pn[E], wv[E], rv[E], dv[E], lk[E], di[E], zv[E];
+          ld_col<E>(pnew, cb, lane, nz, vec, pn);
+          ld_col<E>(a.w32, cb, lane, nz, vec, wv);
+          ld_col<E>(a.r32, cb, lane, nz, vec, rv);
+          ld_col<E>(a.d32, cb, lane, nz, vec, dv);
+          ld_col<E>(a.l32, cb, lane, nz, vec, lk);
+          ld_col<E>(a.dinv32, cb, lane, nz, vec, di);
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            dv[e] += al * pn[e];
+            rv[e] -= al * wv[e];
+          }
+          warp_column_solve<E>(lk, di, lane, nz, rv, zv);
+          st_col<E>(a.d32, cb, lane, nz, vec, dv);
+          st_col<E>(a.r32, cb, lane, nz, vec, rv);
+          st_col<E>(a.z32, cb, lane, nz, vec, zv);
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            if (k0 + e < nz) {
+              zz += static_cast<double>(zv[e]) * zv[e];
+              zr += static_cast<double>(zv[e]) * rv[e];
+            }
+          }
+        }
+      } else {
       for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const long long base = t * tc * nz;
         const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
@@ -373,6 +610,7 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
         }
         __syncthreads();
       }
+      }
       s = block_sum_all(zz);
       if (threadIdx.x == 0) q1[blockIdx.x] = s;
       s = block_sum_all(zr);
@@ -422,9 +660,17 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
   cudaFuncSetAttribute(k_line_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(fsm));
   const bool vec = (nz % 4 == 0);
-  const void* kern = vec ? reinterpret_cast<const void*>(k_cg_mixed<4>)
-                         : reinterpret_cast<const void*>(k_cg_mixed<1>);
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm));
+  const bool wcol = nz <= 32 * kMaxE;
+  const int ecol = !wcol ? 0 : nz <= 32 ? 1 : nz <= 64 ? 2 : nz <= 128 ? 4 : 8;
+  using Kern = void (*)(MixedArgs);
+  static const Kern table[2][5] = {
+      {k_cg_mixed<1, 0>, k_cg_mixed<1, 1>, k_cg_mixed<1, 2>, k_cg_mixed<1, 4>, k_cg_mixed<1, 8>},
+      {k_cg_mixed<4, 0>, k_cg_mixed<4, 1>, k_cg_mixed<4, 2>, k_cg_mixed<4, 4>, k_cg_mixed<4, 8>}};
+  const int slot = ecol == 0 ? 0 : ecol == 1 ? 1 : ecol == 2 ? 2 : ecol == 4 ? 3 : 4;
+  const void* kern = reinterpret_cast<const void*>(table[vec ? 1 : 0][slot]);
+  const size_t ksm = wcol ? 0 : msm;
+  if (!wcol)
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm));
   const int tc = host_tile_cols(nz);
   const long long ntiles = (D.d.ncol + tc - 1) / tc;
   const int fgrid = static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));
@@ -433,10 +679,12 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
                                                         D.dinv32, D.l32, tc);
   ++D.launches;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCgBlock, msm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCgBlock, ksm);
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  // 3 x g reduction partials fit the 4 x sm_count x 4 doubles allocated at create.
+  if (per_sm > 4) per_sm = 4;
   long long g = static_cast<long long>(per_sm) * D.sm_count;
-  if (g > ntiles) g = ntiles;
+  if (!wcol && g > ntiles) g = ntiles;
   if (g < 1) g = 1;
   cudaMemsetAsync(&D.out->cg, 0, sizeof(CgState), D.stream);
   MixedArgs a;
@@ -472,7 +720,7 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
   void* args[] = {&a};
   ++D.launches;
   D.cg_grid32 = static_cast<int>(g);
-  return cudaLaunchCooperativeKernel(kern, dim3(g), dim3(kCgBlock), args, msm, D.stream);
+  return cudaLaunchCooperativeKernel(kern, dim3(g), dim3(kCgBlock), args, ksm, D.stream);
 }
 
 }  // namespace fgw

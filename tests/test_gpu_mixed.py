@@ -76,3 +76,13 @@ def test_mixed_box_32x32x50():
 
 def test_mixed_hillslope_crop():
     run(workloads.hillslope(24, 20, 32), 3)
+
+
+def test_mixed_hillslope_crop_nz128():
+    # The benchmark's column depth: four rows of 32 cells per warp-column solve.
+    run(workloads.hillslope(16, 12, 128), 3)
+
+
+def test_mixed_deep_columns_tiled_solve():
+    # Columns deeper than 256 cells take the shared-memory tiled line solve.
+    run(workloads.column_32x32x50(nx=4, ny=3, nz=300), 3)
