@@ -171,6 +171,7 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     if (e == cudaSuccess) e = dalloc(D, &D.kzf, nf);
     if (e == cudaSuccess) e = dalloc(D, &D.qzf, nf);
     if (e == cudaSuccess) e = dalloc(D, &D.colflag, d.ncol);
+    if (e == cudaSuccess) e = dalloc(D, &D.satf, n3);
     double** solv[] = {&D.diag, &D.gxp, &D.gyp, &D.gzp, &D.rhs, &D.x, &D.r, &D.z, &D.p0, &D.p1, &D.w};
     for (double** p : solv)
       if (e == cudaSuccess) e = dalloc_margin(D, p, n3, m);

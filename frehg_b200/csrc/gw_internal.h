@@ -74,6 +74,7 @@ struct Device {
   double *qx = nullptr, *qy = nullptr, *qzf = nullptr;    // fluxes
   double *vloss = nullptr, *room = nullptr, *sup = nullptr, *sdn = nullptr;
   int* colflag = nullptr;
+  uint8_t* satf = nullptr;  // per-cell saturation flag of the post-allocation snapshot
   // linear system: coefficients and vectors carry a zero margin of sy cells
   // on both ends; the pointers below point at cell 0.
   double *diag = nullptr, *gxp = nullptr, *gyp = nullptr, *gzp = nullptr, *rhs = nullptr;

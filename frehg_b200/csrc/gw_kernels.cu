@@ -413,30 +413,44 @@ __global__ void k_flux(Dims d, Fields f, PassK pk, const double* __restrict__ hp
 // theta from the flux divergence with the Ss factor, and the Ss audit term
 // (updateWaterContent, Corrector.cpp:629-672).  Cells outside the update keep
 // theta^n, so the output buffer is a full copy.
-__global__ void k_update_wc(Dims d, Fields f, const double* __restrict__ hp,
-                            const double* __restrict__ hn, const double* __restrict__ wcn,
-                            const double* __restrict__ qx, const double* __restrict__ qy,
-                            const double* __restrict__ qzf, double dtg, double* wcu,
-                            double* partial) {
+//
+// The same pass writes the saturation flag of every cell (theta >= theta_s or
+// h > h_ae on the corrected theta and predicted head, ghosts included) that
+// the post-allocation classification tests on the six neighbours of a cell.
+// All loads of a cell are issued before its first store and before any
+// branch on loaded data, so one memory round trip serves the cell.
+__global__ void __launch_bounds__(kBlock) k_update_wc(
+    Dims d, Fields f, const double* __restrict__ hp, const double* __restrict__ hn,
+    const double* __restrict__ wcn, const double* __restrict__ qx, const double* __restrict__ qy,
+    const double* __restrict__ qzf, double dtg, double* __restrict__ wcu,
+    uint8_t* __restrict__ satf, double* partial) {
   double acc = 0.0;
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
-    if (j < 1 || j > d.ny || i < 1 || i > d.nx || !f.act[c]) {
-      wcu[c] = wcn[c];
-      continue;
+    const bool in = j >= 1 && j <= d.ny && i >= 1 && i <= d.nx;
+    const double w0 = wcn[c], hpc = hp[c], ts = f.wcs[c], aev = f.aev[c];
+    double upd = w0;
+    if (in) {
+      const long long fz = fidx(d, j, i, k);
+      const int8_t ac = f.act[c];
+      const double hnc = hn[c], dzc = f.dz[c];
+      const double qxp = qx[c], qxm = qx[c - d.sx], qyp = qy[c], qym = qy[c - d.sy];
+      const double qzt = qzf[fz], qzb = qzf[fz + 1];
+      if (ac) {
+        const double volume = d.az * dzc;
+        const double dh = hpc - hnc;
+        const double coeff = volume * (1.0 + d.ss * dh / ts);
+        const double dqx = dtg * (qxp - qxm);
+        const double dqy = dtg * (qyp - qym);
+        const double dqz = dtg * (qzb - qzt);
+        upd = (w0 * volume + dqx + dqy + dqz) / coeff;
+        acc += upd * volume * d.ss * dh / ts;
+      }
     }
-    const double volume = d.az * f.dz[c];
-    const double dh = hp[c] - hn[c];
-    const double coeff = volume * (1.0 + d.ss * dh / f.wcs[c]);
-    const long long fz = fidx(d, j, i, k);
-    const double dqx = dtg * (qx[c] - qx[c - d.sx]);
-    const double dqy = dtg * (qy[c] - qy[c - d.sy]);
-    const double dqz = dtg * (qzf[fz + 1] - qzf[fz]);
-    const double upd = (wcn[c] * volume + dqx + dqy + dqz) / coeff;
     wcu[c] = upd;
-    acc += upd * volume * d.ss * dh / f.wcs[c];
+    satf[c] = (upd >= ts || hpc > aev) ? 1 : 0;
   }
   const double s = block_reduce(acc, SumOp(), 0.0);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
@@ -448,24 +462,32 @@ __global__ void k_update_wc(Dims d, Fields f, const double* __restrict__ hp,
 struct Split {
   double up, down;
 };
-__device__ inline Split gradient_split(const Dims& d, const Fields& f, const double* kx,
-                                       const double* ky, const double* kzf, const double* hR,
-                                       int j, int i, int k) {
-  const long long c = cidx(d, j, i, k), fz = fidx(d, j, i, k);
+// The six-face gradient split of a cell's surplus (Reallocate.cpp:235-300)
+// on values the caller has already loaded: heads hR of the cell and its six
+// neighbours (x+, x-, y+, y-, z+ below, z- above), the neighbours' activity,
+// the face conductivities and the three layer thicknesses.
+struct SplitIn {
+  double hc, hxp, hxm, hyp, hym, hzp, hzm;
+  double kxp, kxm, kyp, kym, kzb, kzt;
+  double dzc, dzp, dzm;
+  int8_t axp, axm, ayp, aym, azp, azm;
+};
+
+__device__ inline Split gradient_split(const Dims& d, const SplitIn& n, int k) {
   double dh0 = 0.0, dh1 = 0.0, dh2 = 0.0, dh3 = 0.0, dh4 = 0.0, dh5 = 0.0;
   if (d.full3d) {
-    if (f.act[c + d.sx] && kx[c] > 0.0) dh0 = (hR[c + d.sx] - hR[c]) / d.dx;
-    if (f.act[c - d.sx] && kx[c - d.sx] > 0.0) dh1 = (hR[c] - hR[c - d.sx]) / d.dx;
-    if (f.act[c + d.sy] && ky[c] > 0.0) dh2 = (hR[c + d.sy] - hR[c]) / d.dy;
-    if (f.act[c - d.sy] && ky[c - d.sy] > 0.0) dh3 = (hR[c] - hR[c - d.sy]) / d.dy;
+    if (n.axp && n.kxp > 0.0) dh0 = (n.hxp - n.hc) / d.dx;
+    if (n.axm && n.kxm > 0.0) dh1 = (n.hc - n.hxm) / d.dx;
+    if (n.ayp && n.kyp > 0.0) dh2 = (n.hyp - n.hc) / d.dy;
+    if (n.aym && n.kym > 0.0) dh3 = (n.hc - n.hym) / d.dy;
   }
-  if (k + 1 < d.nz && f.act[c + 1] && kzf[fz + 1] > 0.0) {
-    const double dzp = 0.5 * (f.dz[c] + f.dz[c + 1]);
-    dh4 = (hR[c + 1] - hR[c]) / dzp - 1.0;
+  if (k + 1 < d.nz && n.azp && n.kzb > 0.0) {
+    const double dzp = 0.5 * (n.dzc + n.dzp);
+    dh4 = (n.hzp - n.hc) / dzp - 1.0;
   }
-  if (k >= 1 && f.act[c - 1] && kzf[fz] > 0.0) {
-    const double dzm = 0.5 * (f.dz[c] + f.dz[c - 1]);
-    dh5 = (hR[c] - hR[c - 1]) / dzm - 1.0;
+  if (k >= 1 && n.azm && n.kzt > 0.0) {
+    const double dzm = 0.5 * (n.dzc + n.dzm);
+    dh5 = (n.hc - n.hzm) / dzm - 1.0;
   }
   double tot = 0.0, gz;
   if (dh0 * dh1 >= 0.0) tot += fabs(0.5 * (dh0 + dh1));
@@ -494,84 +516,102 @@ __device__ inline Split gradient_split(const Dims& d, const Fields& f, const dou
 // Phase 1 of the post-allocation (reallocateWaterContent's classification,
 // Reallocate.cpp:181-391, saturated_contact: head): reads the corrected theta
 // and predicted head as the pre-sweep snapshot, writes the restored state to
-// separate buffers, so the classification is race-free by construction.
-__global__ void __launch_bounds__(kBlock, 3) k_classify(Dims d, Fields f, const double* __restrict__ kx,
-                           const double* __restrict__ ky, const double* __restrict__ kzf,
-                           const double* __restrict__ wcR, const double* __restrict__ hR,
-                           double* wc_out, double* h_out, double* room, double* sup, double* sdn,
-                           int* colflag, double* part_adj, double* part_drop) {
+// separate buffers, so the classification is race-free by construction.  The
+// neighbour-saturation tests read the flags k_update_wc wrote from the same
+// snapshot.  Every load of an interior cell, its neighbours included, is
+// issued before the first branch on loaded data.
+__global__ void __launch_bounds__(kBlock, 3) k_classify(
+    Dims d, Fields f, const double* __restrict__ kx, const double* __restrict__ ky,
+    const double* __restrict__ kzf, const double* __restrict__ wcR,
+    const double* __restrict__ hR, const uint8_t* __restrict__ satf, double* __restrict__ wc_out,
+    double* __restrict__ h_out, double* __restrict__ room, double* __restrict__ sup,
+    double* __restrict__ sdn, int* colflag, double* part_adj, double* part_drop) {
   double adj = 0.0, drop = 0.0;
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     const double before = wcR[c];
-    wc_out[c] = before;
-    h_out[c] = hR[c];
-    if (j < 1 || j > d.ny || i < 1 || i > d.nx || !f.act[c]) {
-      room[c] = 0.0;
-      sup[c] = 0.0;
-      sdn[c] = 0.0;
-      continue;
-    }
-    const Soil so = soil_at(f, c);
-    const double volume = d.az * f.dz[c];
-    double up = 0.0, dn = 0.0;
-    if (before >= so.ts) {
-      if (d.off) {
-        room[c] = 0.0;
-        sup[c] = 0.0;
-        sdn[c] = 0.0;
-        continue;
-      }
-      const double excess = (before - so.ts) * volume;
-      const Split s = gradient_split(d, f, kx, ky, kzf, hR, j, i, k);
-      up = excess * s.up;
-      dn = excess * s.down;
-      adj -= excess - up - dn;
-      drop += excess - up - dn;
-      wc_out[c] = so.ts;
-      room[c] = 0.0;
-    } else {
-      room[c] = (so.ts - before) * volume;
-      const auto sat = [&](long long n) { return wcR[n] >= f.wcs[n] || hR[n] > f.aev[n]; };
-      bool adjsat = false;
-      const long long col = col2(d, j, i);
-      if (k + 1 < d.nz && f.act[c + 1] && sat(c + 1)) adjsat = true;
-      else if (kx[c] != 0.0 && sat(c + d.sx)) adjsat = true;
-      else if (kx[c - d.sx] != 0.0 && sat(c - d.sx)) adjsat = true;
-      else if (ky[c] != 0.0 && sat(c + d.sy)) adjsat = true;
-      else if (ky[c - d.sy] != 0.0 && sat(c - d.sy)) adjsat = true;
-      else {
-        const bool top = (k == 0) || !f.act[c - 1];
-        if (top) {
-          if (f.topc[col] == kHead && f.topv[col] >= 0.0) adjsat = true;
-        } else if (sat(c - 1)) {
-          adjsat = true;
-        }
-      }
-      if (!adjsat) {
-        if (before < 0.9999 * so.ts) h_out[c] = vg_head(so, before);
-      } else if (!d.off) {
-        const double after = vg_theta(so, hR[c]);
-        wc_out[c] = after;
-        room[c] = (so.ts - after) * volume;
-        if (d.redistribute && after < before) {
-          const double surplus = (before - after) * volume;
-          const Split s = gradient_split(d, f, kx, ky, kzf, hR, j, i, k);
-          up = surplus * s.up;
-          dn = surplus * s.down;
-          adj -= surplus - up - dn;
-          drop += surplus - up - dn;
+    double wout = before, hout = hR[c], rm = 0.0, up = 0.0, dn = 0.0;
+    const bool in = j >= 1 && j <= d.ny && i >= 1 && i <= d.nx;
+    if (in) {
+      const long long col = col2(d, j, i), fz = fidx(d, j, i, k);
+      const long long cp = (k + 1 < d.nz) ? c + 1 : c, cm = (k >= 1) ? c - 1 : c;
+      SplitIn n;
+      n.hc = hout;
+      n.hxp = hR[c + d.sx];
+      n.hxm = hR[c - d.sx];
+      n.hyp = hR[c + d.sy];
+      n.hym = hR[c - d.sy];
+      n.hzp = hR[cp];
+      n.hzm = hR[cm];
+      n.kxp = kx[c];
+      n.kxm = kx[c - d.sx];
+      n.kyp = ky[c];
+      n.kym = ky[c - d.sy];
+      n.kzt = kzf[fz];
+      n.kzb = kzf[fz + 1];
+      n.dzc = f.dz[c];
+      n.dzp = f.dz[cp];
+      n.dzm = f.dz[cm];
+      n.axp = f.act[c + d.sx];
+      n.axm = f.act[c - d.sx];
+      n.ayp = f.act[c + d.sy];
+      n.aym = f.act[c - d.sy];
+      n.azp = (k + 1 < d.nz) ? f.act[cp] : 0;
+      n.azm = (k >= 1) ? f.act[cm] : 0;
+      const int8_t ac = f.act[c];
+      const uint8_t sxp = satf[c + d.sx], sxm = satf[c - d.sx], syp = satf[c + d.sy],
+                    sym = satf[c - d.sy], szp = satf[cp], szm = satf[cm];
+      const int topc = f.topc[col];
+      const double topv = f.topv[col];
+      const Soil so = soil_at(f, c);
+      if (ac) {
+        const double volume = d.az * n.dzc;
+        if (before >= so.ts) {
+          if (!d.off) {
+            const double excess = (before - so.ts) * volume;
+            const Split sp = gradient_split(d, n, k);
+            up = excess * sp.up;
+            dn = excess * sp.down;
+            adj -= excess - up - dn;
+            drop += excess - up - dn;
+            wout = so.ts;
+          }
         } else {
-          adj += (after - before) * volume;
-          if (after < before) drop += (before - after) * volume;
+          rm = (so.ts - before) * volume;
+          const bool top = (k == 0) || !n.azm;
+          const bool adjsat = (n.azp && szp) || (n.kxp != 0.0 && sxp) ||
+                              (n.kxm != 0.0 && sxm) || (n.kyp != 0.0 && syp) ||
+                              (n.kym != 0.0 && sym) ||
+                              (top ? (topc == kHead && topv >= 0.0) : (szm != 0));
+          if (!adjsat) {
+            if (before < 0.9999 * so.ts) hout = vg_head(so, before);
+          } else if (!d.off) {
+            const double after = vg_theta(so, hout);
+            wout = after;
+            rm = (so.ts - after) * volume;
+            if (d.redistribute && after < before) {
+              const double surplus = (before - after) * volume;
+              const Split sp = gradient_split(d, n, k);
+              up = surplus * sp.up;
+              dn = surplus * sp.down;
+              adj -= surplus - up - dn;
+              drop += surplus - up - dn;
+            } else {
+              adj += (after - before) * volume;
+              if (after < before) drop += (before - after) * volume;
+            }
+          }
         }
+        if (up > 0.0 || dn > 0.0) colflag[col] = 1;
       }
     }
+    wc_out[c] = wout;
+    h_out[c] = hout;
+    room[c] = rm;
     sup[c] = up;
     sdn[c] = dn;
-    if (up > 0.0 || dn > 0.0) colflag[col2(d, j, i)] = 1;
   }
   const double s1 = block_reduce(adj, SumOp(), 0.0);
   if (threadIdx.x == 0) part_adj[blockIdx.x] = s1;
@@ -651,29 +691,67 @@ __global__ void k_walk_thread(Dims d, Fields f, double* wc, double* room, const 
 }
 
 // The same walk with one warp per flagged column.  The column's room, theta,
-// cell volume, activity and face fluxes are staged in shared memory
-// (coalesced), a ballot over each 32-cell chunk finds the surplus cells in
-// ascending k, and lane 0 runs the sequential walk of each one on shared
-// memory, so the deposit order and every rounding step are those of the
-// per-thread walk above.  Shared memory per warp: walk_warp_bytes(nz).
+// cell volume and face fluxes are staged in shared memory (coalesced), with
+// two bit sets per column: the cells that still have room and the inactive
+// cells.  A ballot over each 32-cell chunk finds the surplus cells in
+// ascending k, and lane 0 runs each walk on shared memory, jumping straight
+// to the next cell with room (a cell without room takes nothing, so the walk
+// may skip it) and stopping where the per-thread walk stops.  The deposit
+// order and every rounding step are those of the per-thread walk above.
+// Shared memory per warp: walk_warp_bytes(nz).
 constexpr int kWalkWarps = kBlock / 32;
+__host__ __device__ inline int walk_words(int nz) { return (nz + 31) / 32; }
 __host__ __device__ inline size_t walk_warp_bytes(int nz) {
-  return static_cast<size_t>(4 * nz + 1) * sizeof(double) + ((nz + 7) & ~7);
+  return static_cast<size_t>(4 * nz + 1) * sizeof(double) +
+         static_cast<size_t>(2 * walk_words(nz)) * sizeof(unsigned);
 }
 
-__device__ inline void walk_deposit(double& dv, int ll, double* rs, double* ws, const double* vs,
-                                    double* qs, int face, double sign, double dtg) {
-  if (rs[ll] > 0.0) {
-    const double take = (rs[ll] > dv) ? dv : rs[ll];
-    ws[ll] += take / vs[ll];
-    rs[ll] -= take;
-    if (sign > 0.0) {
-      qs[face] += take / dtg;
-    } else {
-      qs[face] -= take / dtg;
+// Largest m in [lo, hi] whose bit is set, or -1.
+__device__ inline int bits_highest(const unsigned* w, int lo, int hi) {
+  if (hi < lo) return -1;
+  int wi = hi >> 5;
+  unsigned m = w[wi] & (0xffffffffu >> (31 - (hi & 31)));
+  const int wlo = lo >> 5;
+  for (;;) {
+    if (m) {
+      const int pos = (wi << 5) + 31 - __clz(m);
+      return pos >= lo ? pos : -1;
     }
-    dv -= take;
+    if (--wi < wlo) return -1;
+    m = w[wi];
   }
+}
+
+// Smallest m in [lo, hi] whose bit is set, or -1.
+__device__ inline int bits_lowest(const unsigned* w, int lo, int hi) {
+  if (hi < lo) return -1;
+  int wi = lo >> 5;
+  unsigned m = w[wi] & (0xffffffffu << (lo & 31));
+  const int whi = hi >> 5;
+  for (;;) {
+    if (m) {
+      const int pos = (wi << 5) + __ffs(m) - 1;
+      return pos <= hi ? pos : -1;
+    }
+    if (++wi > whi) return -1;
+    m = w[wi];
+  }
+}
+
+// Deposit at cell m: take min(room, dv), add take / dtg to face `face` with
+// `plus` (true: +=, false: -=), and clear m's room bit once its room is used up.
+__device__ inline void walk_take(double& dv, int m, double* rs, double* ws, const double* vs,
+                                 double* qs, unsigned* rbits, int face, bool plus, double dtg) {
+  const double take = (rs[m] > dv) ? dv : rs[m];
+  ws[m] += take / vs[m];
+  rs[m] -= take;
+  if (plus) {
+    qs[face] += take / dtg;
+  } else {
+    qs[face] -= take / dtg;
+  }
+  dv -= take;
+  if (!(rs[m] > 0.0)) rbits[m >> 5] &= ~(1u << (m & 31));
 }
 
 __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
@@ -684,12 +762,13 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
                                                  double* partial) {
   extern __shared__ __align__(16) unsigned char walk_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nz = d.nz;
+  const int nz = d.nz, nw = walk_words(nz);
   double* rs = reinterpret_cast<double*>(walk_smem + warp * walk_warp_bytes(nz));
   double* ws = rs + nz;
   double* vs = ws + nz;
   double* qs = vs + nz;  // nz + 1 faces
-  signed char* as = reinterpret_cast<signed char*>(qs + nz + 1);
+  unsigned* rbits = reinterpret_cast<unsigned*>(qs + nz + 1);
+  unsigned* ibits = rbits + nw;  // inactive cells
   double lost = 0.0;
   const long long ncolint = static_cast<long long>(d.nx) * d.ny;
   const long long nwarps = static_cast<long long>(gridDim.x) * kWalkWarps;
@@ -700,11 +779,23 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
     if (!colflag[col]) continue;
     const long long base = cidx(d, j, i, 0), fb = fidx(d, j, i, 0);
     const bool topHead = f.topc[col] == kHead;
-    for (int k = lane; k < nz; k += 32) {
-      rs[k] = room[base + k];
-      ws[k] = wc[base + k];
-      vs[k] = d.az * f.dz[base + k];
-      as[k] = f.act[base + k];
+    for (int k0 = 0; k0 < nz; k0 += 32) {
+      const int k = k0 + lane;
+      double r = 0.0;
+      bool inact = false;
+      if (k < nz) {
+        r = room[base + k];
+        rs[k] = r;
+        ws[k] = wc[base + k];
+        vs[k] = d.az * f.dz[base + k];
+        inact = !f.act[base + k];
+      }
+      const unsigned rb = __ballot_sync(0xffffffffu, r > 0.0);
+      const unsigned ib = __ballot_sync(0xffffffffu, inact);
+      if (lane == 0) {
+        rbits[k0 >> 5] = rb;
+        ibits[k0 >> 5] = ib;
+      }
     }
     for (int k = lane; k <= nz; k += 32) qs[k] = qzf[fb + k];
     __syncwarp();
@@ -712,7 +803,7 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
       const int k = k0 + lane;
       double su = 0.0, sd = 0.0;
       bool any = false;
-      if (k < nz && as[k]) {
+      if (k < nz && f.act[base + k]) {
         su = sup[base + k];
         sd = sdn[base + k];
         any = su > 0.0 || sd > 0.0;
@@ -721,35 +812,47 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
       while (mask) {
         const int b = __ffs(mask) - 1;
         mask &= mask - 1;
-        const double up = __shfl_sync(0xffffffffu, su, b);
-        const double dn = __shfl_sync(0xffffffffu, sd, b);
+        const double upv = __shfl_sync(0xffffffffu, su, b);
+        const double dnv = __shfl_sync(0xffffffffu, sd, b);
         if (lane == 0) {
           const int kk = k0 + b;
-          double dv = up;
+          double dv = upv;
           if (dv > 0.0) {
+            // Upward: cells kk-1, kk-2, ... up to the first inactive cell above
+            // kk (exclusive) or the surface.
+            const int lim = bits_highest(ibits, 0, kk - 1) + 1;
             int ll = kk;
-            while (ll > 0 && as[ll - 1] && dv > 0.0) {
-              --ll;
-              walk_deposit(dv, ll, rs, ws, vs, qs, ll + 1, 1.0, dtg);
+            while (dv > 0.0) {
+              const int m = bits_highest(rbits, lim, ll - 1);
+              if (m < 0) {
+                ll = lim;
+                break;
+              }
+              walk_take(dv, m, rs, ws, vs, qs, rbits, m + 1, true, dtg);
+              ll = m;
             }
             if (dv > 0.0) {
               if (topHead) {
                 qs[ll] += dv / dtg;
               } else {
-                while (ll + 1 < nz && dv > 0.0) {
-                  ++ll;
-                  walk_deposit(dv, ll, rs, ws, vs, qs, ll, -1.0, dtg);
+                while (dv > 0.0) {
+                  const int m = bits_lowest(rbits, ll + 1, nz - 1);
+                  if (m < 0) break;
+                  walk_take(dv, m, rs, ws, vs, qs, rbits, m, false, dtg);
+                  ll = m;
                 }
                 lost -= dv;
               }
             }
           }
-          dv = dn;
+          dv = dnv;
           if (dv > 0.0) {
             int ll = kk;
-            while (ll + 1 < nz && dv > 0.0) {
-              ++ll;
-              walk_deposit(dv, ll, rs, ws, vs, qs, ll, -1.0, dtg);
+            while (dv > 0.0) {
+              const int m = bits_lowest(rbits, ll + 1, nz - 1);
+              if (m < 0) break;
+              walk_take(dv, m, rs, ws, vs, qs, rbits, m, false, dtg);
+              ll = m;
             }
             lost -= dv;
           }
@@ -963,14 +1066,15 @@ void launch_flux(const Device& D, const double* wcn, double dtg) {
 
 void launch_update_wc(const Device& D, const double* hn, const double* wcn, double dtg) {
   k_update_wc<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.hp, hn, wcn, D.qx, D.qy, D.qzf,
-                                                      dtg, D.wcu, D.partial + kPSs * D.nblk);
+                                                      dtg, D.wcu, D.satf, D.partial + kPSs * D.nblk);
   ++D.launches;
 }
 
 void launch_classify(const Device& D, double* wc_out, double* h_out) {
   cudaMemsetAsync(D.colflag, 0, sizeof(int) * D.d.ncol, D.stream);
   k_classify<<<cells_grid(D), kBlock, 0, D.stream>>>(
-      D.d, D.f, D.kx, D.ky, D.kzf, D.wcu, D.hp, wc_out, h_out, D.room, D.sup, D.sdn, D.colflag,
+      D.d, D.f, D.kx, D.ky, D.kzf, D.wcu, D.hp, D.satf, wc_out, h_out, D.room, D.sup, D.sdn,
+      D.colflag,
       D.partial + kPAdj * D.nblk, D.partial + kPDrop * D.nblk);
   ++D.launches;
 }
