@@ -29,9 +29,32 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-ALG_BYTES_PER_CG_ITER = 128  # FP64 Jacobi-PCG iteration, bytes per active cell
-ALG_BYTES_FIXED = 536        # FP64 step outside the solve, bytes per active cell
+# Algorithmic bytes per active cell (interior cells, each array read or
+# written once per pass).
+ALG_BYTES_PER_CG_ITER = 128   # FP64 Jacobi-PCG iteration: 16 words
+ALG_BYTES_MIXED_INNER = 68    # FP32 inner iteration: stencil pass 8 words, update +
+                              # line solve 9 words (d, p, r, w, dinv, l in; d, r, z out)
+ALG_BYTES_MIXED_SWEEP = 80    # FP64 outer residual sweep: x, b, 4 coefficients, d, l,
+                              # dinv in; x, r, z, p out
+ALG_BYTES_MIXED_OUTER = 4     # d reset after each outer sweep that continues
+ALG_BYTES_MIXED_INIT = 12     # x = 0, d = 0 at entry
+ALG_BYTES_FIXED = 536         # FP64 step outside the solve
 METRIC = "cell-steps/s at 512x512x128"
+# DRAM bytes (read + write) per algorithmic byte of k_cg_mixed, from the ncu
+# capture summarised in profiles/ (256x256x128 slab, one steady-state launch);
+# scaled to the timed launches by their algorithmic bytes.
+MIXED_TRAFFIC_PER_ALG_BYTE = 1.029
+# Bytes frehg_gw_step reads back per step: the device step record (nine FP64
+# audit and controller terms and the solver's exit state).
+STEP_RECORD_BYTES = 112
+
+
+def mixed_alg_bytes(cells, inner, outer, launches):
+    """Algorithmic bytes of `launches` k_cg_mixed launches that ran `inner`
+    inner iterations and `outer` outer corrections in total."""
+    sweeps = outer + launches
+    return cells * (ALG_BYTES_MIXED_INNER * inner + ALG_BYTES_MIXED_SWEEP * sweeps +
+                    ALG_BYTES_MIXED_OUTER * outer + ALG_BYTES_MIXED_INIT * launches)
 
 
 def parse():
@@ -43,7 +66,7 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
                    help="form of the headline value; the other form is timed too")
     p.add_argument("--size", default="512,512,128")
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-sample", default="64,64,128")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -217,23 +240,23 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
                solve_ms=solve_ms, launches=launches, clocks=clocks.summary(), active=active,
                e2e=None)
     if e2e_steps:
-        # End to end through the C ABI with host buffers: boundary values in,
-        # head and moisture back to host memory, every step.
+        # End to end through the public API, as a driver calls it each step:
+        # that step's boundary values uploaded from host memory (the handle's
+        # page-locked staging), the step, and its audit record read back.  The
+        # fields stay on the device, as the reference keeps them in its views.
         ras = rasterize(cfg)
         vals = (ras.top_value, ras.bot_value, ras.xm_value, ras.xp_value, ras.ym_value,
                 ras.yp_value)
-        h2d = sum(v.nbytes for v in vals)
-        d2h = 2 * active * 8
+        h2d = 6 * (nx + 2) * (ny + 2) * 8
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             gw.setBoundaryValues(*vals)
             gw.advance()
-            gw.head()
-            gw.waterContent()
         e2e_s = time.perf_counter() - t0
         out["e2e"] = {"value": total_cells * e2e_steps / e2e_s, "unit": "cell-steps/s",
-                      "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+                      "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": STEP_RECORD_BYTES,
+                      "steps": e2e_steps}
     gw.close()
     return out
 
@@ -264,25 +287,40 @@ def main():
     mixed = res if args.precision == "mixed" else res_other
 
     peak, peak_kind = peaks()
-    # Roofline of the dominant kernel of the plain FP64 form: its Jacobi-PCG
-    # solve (one cooperative launch per step), 128 B per active cell and
-    # iteration.
-    achieved = (ALG_BYTES_PER_CG_ITER * fp64["active"] * fp64["iters"] /
+    # Roofline of the dominant kernel of each form: its predictor solve, one
+    # launch per step, timed by the handle's CUDA events around that launch.
+    fp64_ach = (ALG_BYTES_PER_CG_ITER * fp64["active"] * fp64["iters"] /
                 (fp64["solve_ms"] / 1e3) / 1e9) if fp64["solve_ms"] else 0.0
-    roof = {"bound": "hbm", "kernel": "k_cg64v (FP64 Jacobi-PCG solve, one launch per step)",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": peak_kind, "traffic": None,
-            "alg_bytes_per_cell_iter": ALG_BYTES_PER_CG_ITER,
-            "cg_iterations_per_step": fp64["iters"] / args.steps,
-            "solve_share_of_step": fp64["solve_ms"] / fp64["ms"] if fp64["ms"] else None}
+    mixed_ach = (mixed_alg_bytes(mixed["active"], mixed["iters"], mixed["outer"], args.steps) /
+                 (mixed["solve_ms"] / 1e3) / 1e9) if mixed["solve_ms"] else 0.0
+    roof_fp64 = {"bound": "hbm", "kernel": "k_cg64v (FP64 Jacobi-PCG, one launch per step)",
+                 "achieved": fp64_ach, "peak": peak, "unit": "GB/s", "frac": fp64_ach / peak,
+                 "peak_source": peak_kind, "alg_bytes_per_cell_iter": ALG_BYTES_PER_CG_ITER,
+                 "cg_iterations_per_step": fp64["iters"] / args.steps,
+                 "solve_share_of_step": fp64["solve_ms"] / fp64["ms"] if fp64["ms"] else None}
+    mixed_traffic = None
+    if MIXED_TRAFFIC_PER_ALG_BYTE is not None:
+        mixed_traffic = MIXED_TRAFFIC_PER_ALG_BYTE * mixed_alg_bytes(
+            mixed["active"], mixed["iters"], mixed["outer"], args.steps) / args.steps
+    roof_mixed = {"bound": "hbm",
+                  "kernel": "k_cg_mixed (FP32 line-PCG inside FP64 defect correction, one "
+                            "cooperative launch per step)",
+                  "achieved": mixed_ach, "peak": peak, "unit": "GB/s", "frac": mixed_ach / peak,
+                  "peak_source": peak_kind, "traffic": mixed_traffic,
+                  "alg_bytes_per_cell": {"inner_iteration": ALG_BYTES_MIXED_INNER,
+                                         "outer_sweep": ALG_BYTES_MIXED_SWEEP},
+                  "inner_iterations_per_step": mixed["iters"] / args.steps,
+                  "outer_sweeps_per_step": mixed["outer"] / args.steps,
+                  "solve_share_of_step": mixed["solve_ms"] / mixed["ms"] if mixed["ms"] else None}
+    roof = roof_mixed if args.precision == "mixed" else dict(roof_fp64, traffic=None)
     forms = {
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms"] / args.steps,
                  "cg_iterations_per_step": fp64["iters"] / args.steps,
-                 "solve_ms_per_step": fp64["solve_ms"] / args.steps},
+                 "solve_ms_per_step": fp64["solve_ms"] / args.steps, "roofline": roof_fp64},
         "mixed": {"value": mixed["value"], "ms_per_step": mixed["ms"] / args.steps,
                   "inner_iterations_per_step": mixed["iters"] / args.steps,
                   "outer_sweeps_per_step": mixed["outer"] / args.steps,
-                  "solve_ms_per_step": mixed["solve_ms"] / args.steps},
+                  "solve_ms_per_step": mixed["solve_ms"] / args.steps, "roofline": roof_mixed},
         "mixed_over_fp64": mixed["value"] / fp64["value"] if fp64["value"] else None,
     }
     if rank != 0:

@@ -23,6 +23,7 @@ struct frehg_gw_handle {
   double* bath_dev = nullptr;
   std::vector<int> codes;      // host copy, 6 x ncol
   std::vector<double> values;  // host staging, 6 x ncol
+  bool values_pinned = false;  // staging page-locked with cudaHostRegister
   double rtol = 1e-8, atol = 1e-14, outer_rtol = 1e-10;
   int maxit = 1000, max_outer = 30, precision = 0;
   double dt_min = 0, dt_max = 0, dq_grow = 0.01, dq_shrink = 0.02, co_max = 2.0;
@@ -251,6 +252,11 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     hnd->nactive = H.nactive;
     hnd->codes = H.codes;
     hnd->values.assign(6 * static_cast<size_t>(d.ncol), 0.0);
+    // Page-lock the boundary-value staging so each step's upload is a direct
+    // DMA; without it (registration refused) the copy still works, staged.
+    hnd->values_pinned = cudaHostRegister(hnd->values.data(), hnd->values.size() * sizeof(double),
+                                          cudaHostRegisterDefault) == cudaSuccess;
+    if (!hnd->values_pinned) cudaGetLastError();
     hnd->rtol = desc->rtol;
     hnd->atol = desc->atol;
     hnd->maxit = desc->max_iterations;
@@ -276,6 +282,7 @@ int frehg_gw_destroy(frehg_gw_handle* h) {
   cudaStreamSynchronize(h->D.stream);
   for (cudaEvent_t& e : h->ev)
     if (e) cudaEventDestroy(e);
+  if (h->values_pinned) cudaHostUnregister(h->values.data());
   free_device(h->D);
   delete h;
   return FREHG_GW_OK;
@@ -404,8 +411,12 @@ int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* 
   fgw::launch_ghosts(D, hn, wcn);
   fgw::launch_closure_pred(D, hn);
   fgw::launch_assemble(D, hn, wcn, dtg);
-  mark(1);
   cudaError_t e;
+  if (h->precision == FREHG_GW_PRECISION_MIXED) {
+    e = fgw::launch_line_factor(D);
+    if (e != cudaSuccess) return cuda_fail(e, "line factor launch");
+  }
+  mark(1);
   if (h->precision == FREHG_GW_PRECISION_MIXED) {
     e = fgw::launch_cg_mixed(D, h->rtol, h->atol, h->maxit, h->outer_rtol, h->max_outer);
   } else {

@@ -651,14 +651,27 @@ int cg32_grid(int sm_count, long long ncell) {
   return sm_count;  // refined per domain in launch_cg_mixed (depends on nz)
 }
 
+cudaError_t launch_line_factor(Device& D) {
+  const int nz = D.d.nz;
+  const size_t fsm = factor_smem(nz);
+  cudaFuncSetAttribute(k_line_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(fsm));
+  const int tc = host_tile_cols(nz);
+  const long long ntiles = (D.d.ncol + tc - 1) / tc;
+  const int fgrid = static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));
+  k_line_factor<<<fgrid, kFactorBlock, fsm, D.stream>>>(D.d, D.diag, D.gxp, D.gyp, D.gzp,
+                                                        D.diag32, D.gxp32, D.gyp32, D.gzp32,
+                                                        D.dinv32, D.l32, tc);
+  ++D.launches;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, double outer_rtol,
                             int max_outer) {
   (void)rtol;
   const int nz = D.d.nz;
   if (host_tile_cols(nz) * nz > kTileCells && nz > kTileCells) return cudaErrorInvalidValue;
-  const size_t fsm = factor_smem(nz), msm = mixed_smem(nz);
-  cudaFuncSetAttribute(k_line_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(fsm));
+  const size_t msm = mixed_smem(nz);
   const bool vec = (nz % 4 == 0);
   const bool wcol = nz <= 32 * kMaxE;
   const int ecol = !wcol ? 0 : nz <= 32 ? 1 : nz <= 64 ? 2 : nz <= 128 ? 4 : 8;
@@ -673,11 +686,6 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm));
   const int tc = host_tile_cols(nz);
   const long long ntiles = (D.d.ncol + tc - 1) / tc;
-  const int fgrid = static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));
-  k_line_factor<<<fgrid, kFactorBlock, fsm, D.stream>>>(D.d, D.diag, D.gxp, D.gyp, D.gzp,
-                                                        D.diag32, D.gxp32, D.gyp32, D.gzp32,
-                                                        D.dinv32, D.l32, tc);
-  ++D.launches;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCgBlock, ksm);
   if (per_sm < 1) return cudaErrorInvalidConfiguration;

@@ -271,4 +271,56 @@ __device__ inline double face_kz(const Dims& d, const Fields& f, const PassK& p,
   return 0.5 * (p.kcz[up] + p.kcz[lo]);
 }
 
+
+// ---------------------------------------------------------------- face rules on loaded values
+// The rules of face_kx / face_ky / face_kz, evaluated on values the caller
+// has already loaded, so a kernel can issue every load of a cell before its
+// first branch on loaded data.
+struct Flank {
+  double kc, ks;  // K(h, Ks) of the pass and Ks along the face normal
+  double w, ws;   // the pass moisture and theta_s (use_full3d test)
+  int8_t act;
+};
+
+// Lateral face between flank a (lower index) and flank b.  lo_edge / hi_edge:
+// the face is the domain's low / high boundary face in this direction, whose
+// BC code is `code`.
+__device__ inline double face_lat(const Dims& d, const Flank& a, const Flank& b, bool lo_edge,
+                                  bool hi_edge, int code) {
+  double kf = d.harm ? face_harm(a.kc, a.ks, 1.0, b.kc, b.ks, 1.0) : 0.5 * (a.kc + b.kc);
+  if (lo_edge) {
+    if (code == kNoFlux) kf = 0.0;
+    else if (is_head(code)) kf = b.kc;
+  } else if (hi_edge) {
+    if (code == kNoFlux) kf = 0.0;
+    else if (is_head(code)) kf = a.kc;
+  }
+  if (!d.full3d) {
+    if ((a.act && a.w < a.ws) || (b.act && b.w < b.ws)) kf = 0.0;
+  }
+  if ((!lo_edge && !a.act) || (!hi_edge && !b.act)) kf = 0.0;
+  return kf;
+}
+
+struct ZFlank {
+  double kc, ks, dz;
+  int8_t act;
+};
+
+// z face plane k of a column: u = cell k-1 (above), l = cell k (below).
+__device__ inline double face_z(const Dims& d, const ZFlank& u, const ZFlank& l, int k, int topc,
+                                int botc) {
+  const bool below = (k < d.nz) && l.act;
+  const bool above = (k >= 1) && u.act;
+  if ((k < d.nz && !below) || (k >= 1 && !above)) return 0.0;
+  if (k == 0) {
+    if (topc == kHead) return l.ks;
+    if (topc == kNoFlux) return 0.0;
+    return l.kc;
+  }
+  if (k == d.nz) return (botc == kNoFlux) ? 0.0 : u.kc;
+  if (d.harm) return face_harm(u.kc, u.ks, u.dz, l.kc, l.ks, l.dz);
+  return 0.5 * (u.kc + l.kc);
+}
+
 }  // namespace fgw

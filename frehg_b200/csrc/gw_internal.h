@@ -118,6 +118,9 @@ void launch_init_state(const Device& D, int form, double constant, const double*
 // FP64 Jacobi-PCG (PETSc KSPCG semantics); returns a CUDA error code.
 cudaError_t launch_cg64(Device& D, double rtol, double atol, int maxit);
 // FP32-inner / FP64-outer defect correction.
+// FP32 casts of the coefficients and the per-column LDL^T factors of the
+// mixed solve's line preconditioner (one launch before launch_cg_mixed).
+cudaError_t launch_line_factor(Device& D);
 cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, double outer_rtol,
                             int max_outer);
 int cg64_grid(int sm_count, long long ncell);

@@ -101,17 +101,22 @@ __global__ void k_ghosts(Dims d, Fields f, double* h, double* wc) {
 // them for both flanks of every face).
 // The same pass also evaluates C(h^n), the capacity of the storage term
 // (Predictor.cpp:445-452), from the same powers.
-__global__ void k_closure_pred(Dims d, Fields f, const double* __restrict__ h, double* kcx,
-                               double* kcy, double* kcz, double* ch) {
+__global__ void __launch_bounds__(kBlock) k_closure_pred(Dims d, Fields f,
+                                                         const double* __restrict__ h,
+                                                         double* __restrict__ kcx,
+                                                         double* __restrict__ kcy,
+                                                         double* __restrict__ kcz,
+                                                         double* __restrict__ ch) {
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const Soil so = soil_at(f, c);
     const double hc = h[c];
+    const Soil so = soil_at(f, c);
+    const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
     const VgParts v = vg_parts(so, hc);
     const KrParts p = vg_kr_from(v, hc);
-    kcx[c] = vg_k_from(p, f.ksx[c]);
-    kcy[c] = vg_k_from(p, f.ksy[c]);
-    kcz[c] = vg_k_from(p, f.ksz[c]);
+    kcx[c] = vg_k_from(p, ksx);
+    kcy[c] = vg_k_from(p, ksy);
+    kcz[c] = vg_k_from(p, ksz);
     ch[c] = vg_capacity_from(so, v, hc);
   }
 }
@@ -120,35 +125,47 @@ __global__ void k_closure_pred(Dims d, Fields f, const double* __restrict__ h, d
 // Predictor.cpp:745-754), re-impose the ghost heads (enforceHeadBc after the
 // solve, RichardsSolver.cpp:762) and evaluate the per-cell conductivities of
 // the predicted head (the corrector's computeFaceConductivity, :768).
-__global__ void k_closure_corr(Dims d, Fields f, const double* __restrict__ x,
-                               const double* __restrict__ hn, double* hp, double* kcx,
-                               double* kcy, double* kcz) {
+__global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
+                                                         const double* __restrict__ x,
+                                                         const double* __restrict__ hn,
+                                                         double* __restrict__ hp,
+                                                         double* __restrict__ kcx,
+                                                         double* __restrict__ kcy,
+                                                         double* __restrict__ kcz) {
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     const bool jin = j >= 1 && j <= d.ny, iin = i >= 1 && i <= d.nx;
+    const Soil so = soil_at(f, c);
+    const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
     double hv = 0.0;
     if (jin && iin) {
-      hv = f.act[c] ? x[c] : hn[c];
+      const int8_t ac = f.act[c];
+      const double xc = x[c], hc = hn[c];
+      hv = ac ? xc : hc;
     } else if (jin && (i == 0 || i == d.nx + 1)) {
       const long long ci = (i == 0) ? c + d.sx : c - d.sx;
       const long long cc = col2(d, j, i == 0 ? 1 : d.nx);
-      const double hi = f.act[ci] ? x[ci] : hn[ci];
-      hv = ghost_head(i == 0 ? f.xmc[cc] : f.xpc[cc], i == 0 ? f.xmv[cc] : f.xpv[cc], hi,
-                      f.bot[ci] + 0.5 * f.dz[ci]);
+      const int8_t ai = f.act[ci];
+      const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
+      const int code = i == 0 ? f.xmc[cc] : f.xpc[cc];
+      const double val = i == 0 ? f.xmv[cc] : f.xpv[cc];
+      hv = ghost_head(code, val, ai ? xi : hi0, zc);
     } else if (iin && (j == 0 || j == d.ny + 1)) {
       const long long ci = (j == 0) ? c + d.sy : c - d.sy;
       const long long cc = col2(d, j == 0 ? 1 : d.ny, i);
-      const double hi = f.act[ci] ? x[ci] : hn[ci];
-      hv = ghost_head(j == 0 ? f.ymc[cc] : f.ypc[cc], j == 0 ? f.ymv[cc] : f.ypv[cc], hi,
-                      f.bot[ci] + 0.5 * f.dz[ci]);
+      const int8_t ai = f.act[ci];
+      const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
+      const int code = j == 0 ? f.ymc[cc] : f.ypc[cc];
+      const double val = j == 0 ? f.ymv[cc] : f.ypv[cc];
+      hv = ghost_head(code, val, ai ? xi : hi0, zc);
     }
+    const KrParts p = vg_kr_parts(so, hv);
     hp[c] = hv;
-    const KrParts p = vg_kr_parts(soil_at(f, c), hv);
-    kcx[c] = vg_k_from(p, f.ksx[c]);
-    kcy[c] = vg_k_from(p, f.ksy[c]);
-    kcz[c] = vg_k_from(p, f.ksz[c]);
+    kcx[c] = vg_k_from(p, ksx);
+    kcy[c] = vg_k_from(p, ksy);
+    kcz[c] = vg_k_from(p, ksz);
   }
 }
 
@@ -162,17 +179,52 @@ __global__ void k_closure_corr(Dims d, Fields f, const double* __restrict__ x,
 // (the same expression on the same data, so the stored matrix is the
 // reference's up to the rounding of its z legs).  Legs toward an inactive
 // cell or out of the domain are stored as 0 (PETSc ignores column -1).
-__global__ void __launch_bounds__(kBlock, 3)
+__global__ void __launch_bounds__(kBlock, 2)
     k_assemble(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
                const double* __restrict__ wcn, const double* __restrict__ ch, double dtg,
-               double* diag, double* gxps, double* gyps, double* gzps, double* rhs) {
+               double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
+               double* __restrict__ gzps, double* __restrict__ rhs) {
   const double dx = d.dx, dy = d.dy;
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     if (j < 1 || j > d.ny || i < 1 || i > d.nx) continue;
-    if (!f.act[c]) {
+    const long long cw = c - d.sx, ce = c + d.sx, cs = c - d.sy, cn = c + d.sy;
+    const long long cu = (k >= 1) ? c - 1 : c, cl = (k + 1 < d.nz) ? c + 1 : c;
+    const long long col = col2(d, j, i);
+    // Gather: the six faces' flanks, the cell's metrics, heads and BC data.
+    const Flank xw{pk.kcx[cw], f.ksx[cw], wcn[cw], f.wcs[cw], f.act[cw]};
+    const Flank xc{pk.kcx[c], f.ksx[c], wcn[c], f.wcs[c], f.act[c]};
+    const Flank xe{pk.kcx[ce], f.ksx[ce], wcn[ce], f.wcs[ce], f.act[ce]};
+    const Flank ys{pk.kcy[cs], f.ksy[cs], wcn[cs], f.wcs[cs], f.act[cs]};
+    const Flank yc{pk.kcy[c], f.ksy[c], xc.w, xc.ws, xc.act};
+    const Flank yn{pk.kcy[cn], f.ksy[cn], wcn[cn], f.wcs[cn], f.act[cn]};
+    const ZFlank zu{pk.kcz[cu], f.ksz[cu], f.dz[cu], (k >= 1) ? f.act[cu] : int8_t(0)};
+    const ZFlank zc{pk.kcz[c], f.ksz[c], f.dz[c], xc.act};
+    const ZFlank zl{pk.kcz[cl], f.ksz[cl], f.dz[cl], (k + 1 < d.nz) ? f.act[cl] : int8_t(0)};
+    const double cosxc = f.cosx[c], cosxw = f.cosx[cw], axc = f.ax[c], axw = f.ax[cw];
+    const double cosyc = f.cosy[c], cosys = f.cosy[cs], ayc = f.ay[c], ays = f.ay[cs];
+    const double chc = ch[c], hnc = hn[c], hne = hn[ce], hnw = hn[cw], hnn = hn[cn],
+                 hns = hn[cs];
+    const int cxp = f.xpc[col], cxm = f.xmc[col], cyp = f.ypc[col], cym = f.ymc[col];
+    const int botc = f.botc[col], topc = f.topc[col];
+    const double vxp = f.xpv[col], vxm = f.xmv[col], vyp = f.ypv[col], vym = f.ymv[col];
+    const double vbot = f.botv[col], vtop = f.topv[col];
+    double botc_ = 0.0, bote = 0.0, botw = 0.0, botn = 0.0, bots = 0.0;
+    double sinxc = 0.0, sinxw = 0.0, sinyc = 0.0, sinys = 0.0;
+    if (d.terrain) {
+      botc_ = f.bot[c];
+      bote = f.bot[ce];
+      botw = f.bot[cw];
+      botn = f.bot[cn];
+      bots = f.bot[cs];
+      sinxc = f.sinx[c];
+      sinxw = f.sinx[cw];
+      sinyc = f.siny[c];
+      sinys = f.siny[cs];
+    }
+    if (!xc.act) {
       diag[c] = 1.0;
       gxps[c] = 0.0;
       gyps[c] = 0.0;
@@ -180,80 +232,79 @@ __global__ void __launch_bounds__(kBlock, 3)
       rhs[c] = 0.0;
       continue;
     }
-    const long long cw = c - d.sx, ce = c + d.sx, cs = c - d.sy, cn = c + d.sy;
-    const long long col = col2(d, j, i);
     const bool east = i == d.nx, west = i == 1, north = j == d.ny, south = j == 1;
-    const bool top = (k == 0) || !f.act[c - 1];
-    const double dzc = f.dz[c];
+    const bool top = (k == 0) || !zu.act;
+    const double dzc = zc.dz;
     const double volume = d.az * dzc;
-    const double kxp = face_kx(d, f, pk, j, i, k), kxm = face_kx(d, f, pk, j, i - 1, k);
-    const double kyp = face_ky(d, f, pk, j, i, k), kym = face_ky(d, f, pk, j - 1, i, k);
-    const double kzm = face_kz(d, f, pk, j, i, k), kzp = face_kz(d, f, pk, j, i, k + 1);
-    double gxp = -kxp * dtg * f.cosx[c] / (dx * dx) * (f.ax[c] * dx);
-    double gxm = -kxm * dtg * f.cosx[cw] / (dx * dx) * (f.ax[cw] * dx);
-    double gyp = -kyp * dtg * f.cosy[c] / (dy * dy) * (f.ay[c] * dy);
-    double gym = -kym * dtg * f.cosy[cs] / (dy * dy) * (f.ay[cs] * dy);
-    const int cxp = f.xpc[col], cxm = f.xmc[col], cyp = f.ypc[col], cym = f.ymc[col];
+    const double kxp = face_lat(d, xc, xe, false, east, cxp);
+    const double kxm = face_lat(d, xw, xc, west, false, cxm);
+    const double kyp = face_lat(d, yc, yn, false, north, cyp);
+    const double kym = face_lat(d, ys, yc, south, false, cym);
+    const double kzm = face_z(d, zu, zc, k, topc, botc);
+    const double kzp = face_z(d, zc, zl, k + 1, topc, botc);
+    double gxp = -kxp * dtg * cosxc / (dx * dx) * (axc * dx);
+    double gxm = -kxm * dtg * cosxw / (dx * dx) * (axw * dx);
+    double gyp = -kyp * dtg * cosyc / (dy * dy) * (ayc * dy);
+    double gym = -kym * dtg * cosys / (dy * dy) * (ays * dy);
     if (east && is_head(cxp)) gxp *= 2.0;
     if (west && is_head(cxm)) gxm *= 2.0;
     if (north && is_head(cyp)) gyp *= 2.0;
     if (south && is_head(cym)) gym *= 2.0;
-    double dzf = (k == d.nz - 1) ? 0.5 * dzc : 0.5 * (dzc + f.dz[c + 1]);
+    double dzf = (k == d.nz - 1) ? 0.5 * dzc : 0.5 * (dzc + zl.dz);
     const double gzp = -kzp * dtg / (dzc * dzf) * volume;
-    dzf = top ? 0.5 * dzc : 0.5 * (dzc + f.dz[c - 1]);
+    dzf = top ? 0.5 * dzc : 0.5 * (dzc + zu.dz);
     const double gzm = -kzm * dtg / (dzc * dzf) * volume;
 
-    const double storage = ch[c] + d.ss * wcn[c] / f.wcs[c];
+    const double storage = chc + d.ss * xc.w / xc.ws;
     double gct = storage * volume - (gxp + gxm + gyp + gym);
     if (east && cxp == kFlux) gct += gxp;
     if (west && cxm == kFlux) gct += gxm;
     if (north && cyp == kFlux) gct += gyp;
     if (south && cym == kFlux) gct += gym;
-    const int botc = f.botc[col], topc = f.topc[col];
     if (!(k == d.nz - 1 && botc != kHead)) gct -= gzp;
     if (!top || topc == kHead) gct -= gzm;
 
-    double b = storage * hn[c] * volume;
+    double b = storage * hnc * volume;
     b -= dtg * volume * kzp / dzc;
     b += dtg * volume * kzm / dzc;
     if (d.terrain) {
-      double sg = (f.bot[ce] > f.bot[c]) ? 1.0 : -1.0;
-      b += sg * dtg * f.ax[c] * kxp * f.sinx[c];
-      sg = (f.bot[c] > f.bot[cw]) ? -1.0 : 1.0;
-      b += sg * dtg * f.ax[cw] * kxm * f.sinx[cw];
-      sg = (f.bot[cn] > f.bot[c]) ? 1.0 : -1.0;
-      b += sg * dtg * f.ay[c] * kyp * f.siny[c];
-      sg = (f.bot[c] > f.bot[cs]) ? -1.0 : 1.0;
-      b += sg * dtg * f.ay[cs] * kym * f.siny[cs];
+      double sg = (bote > botc_) ? 1.0 : -1.0;
+      b += sg * dtg * axc * kxp * sinxc;
+      sg = (botc_ > botw) ? -1.0 : 1.0;
+      b += sg * dtg * axw * kxm * sinxw;
+      sg = (botn > botc_) ? 1.0 : -1.0;
+      b += sg * dtg * ayc * kyp * sinyc;
+      sg = (botc_ > bots) ? -1.0 : 1.0;
+      b += sg * dtg * ays * kym * sinys;
     }
     if (east) {
-      if (cxp == kFlux) b += f.ax[c] * f.xpv[col] * dtg;
-      else b -= gxp * hn[ce];
+      if (cxp == kFlux) b += axc * vxp * dtg;
+      else b -= gxp * hne;
     }
     if (west) {
-      if (cxm == kFlux) b += f.ax[cw] * f.xmv[col] * dtg;
-      else b -= gxm * hn[cw];
+      if (cxm == kFlux) b += axw * vxm * dtg;
+      else b -= gxm * hnw;
     }
     if (north) {
-      if (cyp == kFlux) b += f.ay[c] * f.ypv[col] * dtg;
-      else b -= gyp * hn[cn];
+      if (cyp == kFlux) b += ayc * vyp * dtg;
+      else b -= gyp * hnn;
     }
     if (south) {
-      if (cym == kFlux) b += f.ay[cs] * f.ymv[col] * dtg;
-      else b -= gym * hn[cs];
+      if (cym == kFlux) b += ays * vym * dtg;
+      else b -= gym * hns;
     }
     if (k == d.nz - 1) {
-      if (botc == kFlux) b += dtg * volume * (f.botv[col] + kzp) / dzc;
-      else if (botc == kHead) b -= gzp * f.botv[col];
+      if (botc == kFlux) b += dtg * volume * (vbot + kzp) / dzc;
+      else if (botc == kHead) b -= gzp * vbot;
     }
     if (top) {
-      if (topc == kHead) b -= gzm * f.topv[col];
-      else if (topc == kFlux) b += -dtg * volume * (f.topv[col] + kzm) / dzc;
+      if (topc == kHead) b -= gzm * vtop;
+      else if (topc == kFlux) b += -dtg * volume * (vtop + kzm) / dzc;
     }
     diag[c] = gct;
-    gxps[c] = (!east && f.act[ce]) ? gxp : 0.0;
-    gyps[c] = (!north && f.act[cn]) ? gyp : 0.0;
-    gzps[c] = (k + 1 < d.nz && f.act[c + 1]) ? gzp : 0.0;
+    gxps[c] = (!east && xe.act) ? gxp : 0.0;
+    gyps[c] = (!north && yn.act) ? gyp : 0.0;
+    gzps[c] = (k + 1 < d.nz && zl.act) ? gzp : 0.0;
     rhs[c] = b;
   }
 }
@@ -263,147 +314,159 @@ __global__ void __launch_bounds__(kBlock, 3)
 // head, Predictor.cpp:105-386, and computeFluxesImpl<PC, HARM>,
 // Corrector.cpp:135-527, uncoupled).  Thread c owns the x+ and y+ faces of
 // its cell and the z face above it (plus the bottom face for k = nz-1).
-__device__ inline double flux_x(const Dims& d, const Fields& f, const PassK& pk,
-                                const double* hp, const double* wcn, int j, int i, int k) {
-  const long long c = cidx(d, j, i, k);
-  const double faceA = f.ax[c];
+// Darcy flux of a lateral face from loaded values (computeFluxesImpl's x / y
+// branches): a = the face's lower-index flank, b = its upper one; lo_edge /
+// hi_edge mark the domain's boundary faces, whose BC code and value apply.
+struct LatFlux {
+  double kca, kcb, ksa, ksb, hpa, hpb, wa, wb, wsa, wsb, bota, botb;
+  double area, cosv, sinv;
+  int8_t acta, actb;
+};
+
+__device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux& v, double h,
+                                  bool lo_edge, bool hi_edge, int code, double value, long long b,
+                                  const double* __restrict__ hp) {
   double q;
-  if (i == 0) {
-    const long long ci = c + d.sx;
-    q = faceA * pk.kcx[ci] * f.cosx[c] * (hp[ci] - hp[c]) / (0.5 * d.dx);
-    const int code = f.xmc[col2(d, j, 1)];
+  if (lo_edge) {
+    q = v.area * v.kcb * v.cosv * (v.hpb - v.hpa) / (0.5 * h);
     if (code == kNoFlux) q = 0.0;
-    else if (code == kFlux) q = -f.xmv[col2(d, j, 1)] * faceA;
+    else if (code == kFlux) q = -value * v.area;
     return q;
   }
-  const long long e = c + d.sx;
-  double kf, delta = d.dx;
-  const double sg = (f.bot[e] > f.bot[c]) ? 1.0 : -1.0;
-  if (i == d.nx) {
-    kf = pk.kcx[c];
-    delta = 0.5 * d.dx;
+  double kf, delta = h;
+  const double sg = (v.botb > v.bota) ? 1.0 : -1.0;
+  if (hi_edge) {
+    kf = v.kca;
+    delta = 0.5 * h;
   } else {
     if (d.pc) {
-      kf = d.harm ? face_harm(pk.kcx[c], f.ksx[c], 1.0, pk.kcx[e], f.ksx[e], 1.0)
-                  : 0.5 * (pk.kcx[c] + pk.kcx[e]);
+      kf = d.harm ? face_harm(v.kca, v.ksa, 1.0, v.kcb, v.ksb, 1.0) : 0.5 * (v.kca + v.kcb);
     } else {
-      kf = 0.5 * (pk.kcx[c] + vg_k(soil_at(f, e), hp[e], f.ksx[c]));
+      kf = 0.5 * (v.kca + vg_k(soil_at(f, b), hp[b], v.ksa));
     }
-    if (!f.act[c] || !f.act[e]) kf = 0.0;
+    if (!v.acta || !v.actb) kf = 0.0;
   }
-  q = faceA * (kf * f.cosx[c] * (hp[e] - hp[c]) / delta + sg * kf * f.sinx[c]);
-  if (!d.full3d && ((f.act[c] && wcn[c] < f.wcs[c]) || (f.act[e] && wcn[e] < f.wcs[e]))) q = 0.0;
-  if (i == d.nx) {
-    const int code = f.xpc[col2(d, j, d.nx)];
+  q = v.area * (kf * v.cosv * (v.hpb - v.hpa) / delta + sg * kf * v.sinv);
+  if (!d.full3d && ((v.acta && v.wa < v.wsa) || (v.actb && v.wb < v.wsb))) q = 0.0;
+  if (hi_edge) {
     if (code == kNoFlux) q = 0.0;
-    else if (code == kFlux) q = f.xpv[col2(d, j, d.nx)] * faceA;
+    else if (code == kFlux) q = value * v.area;
   }
   return q;
 }
 
-__device__ inline double flux_y(const Dims& d, const Fields& f, const PassK& pk,
-                                const double* hp, const double* wcn, int j, int i, int k) {
-  const long long c = cidx(d, j, i, k);
-  const double faceA = f.ay[c];
-  double q;
-  if (j == 0) {
-    const long long ci = c + d.sy;
-    q = faceA * pk.kcy[ci] * f.cosy[c] * (hp[ci] - hp[c]) / (0.5 * d.dy);
-    const int code = f.ymc[col2(d, 1, i)];
-    if (code == kNoFlux) q = 0.0;
-    else if (code == kFlux) q = -f.ymv[col2(d, 1, i)] * faceA;
-    return q;
-  }
-  const long long n = c + d.sy;
-  double kf, delta = d.dy;
-  const double sg = (f.bot[n] > f.bot[c]) ? 1.0 : -1.0;
-  if (j == d.ny) {
-    kf = pk.kcy[c];
-    delta = 0.5 * d.dy;
-  } else {
-    if (d.pc) {
-      kf = d.harm ? face_harm(pk.kcy[c], f.ksy[c], 1.0, pk.kcy[n], f.ksy[n], 1.0)
-                  : 0.5 * (pk.kcy[c] + pk.kcy[n]);
-    } else {
-      kf = 0.5 * (pk.kcy[c] + vg_k(soil_at(f, n), hp[n], f.ksy[c]));
-    }
-    if (!f.act[c] || !f.act[n]) kf = 0.0;
-  }
-  q = faceA * (kf * f.cosy[c] * (hp[n] - hp[c]) / delta + sg * kf * f.siny[c]);
-  if (!d.full3d && ((f.act[c] && wcn[c] < f.wcs[c]) || (f.act[n] && wcn[n] < f.wcs[n]))) q = 0.0;
-  if (j == d.ny) {
-    const int code = f.ypc[col2(d, d.ny, i)];
-    if (code == kNoFlux) q = 0.0;
-    else if (code == kFlux) q = f.ypv[col2(d, d.ny, i)] * faceA;
-  }
-  return q;
-}
-
-__device__ inline double flux_z(const Dims& d, const Fields& f, const PassK& pk,
-                                const double* hp, int j, int i, int k) {
-  const long long base = cidx(d, j, i, 0), col = col2(d, j, i);
-  const bool below = (k < d.nz) && f.act[base + k];
-  const bool above = (k >= 1) && f.act[base + k - 1];
+// Darcy flux of z-face plane k from loaded values (computeFluxesImpl's z
+// branch): u = cell k-1, l = cell k.
+__device__ inline double flux_zv(const Dims& d, const Fields& f, const ZFlank& u, const ZFlank& l,
+                                 double hpu, double hpl, int k, int topc, double topv, int botc,
+                                 double botv, long long cu, const double* __restrict__ hp) {
+  const bool below = (k < d.nz) && l.act;
+  const bool above = (k >= 1) && u.act;
   if (below && !above) {  // face above a column's top cell
-    const long long c = base + k;
-    const int code = f.topc[col];
-    if (code == kFlux) return f.topv[col] * d.az;
-    if (code == kHead) {
-      const double delta = 0.5 * f.dz[c];
-      return d.az * f.ksz[c] * ((hp[c] - f.topv[col]) / delta - 1.0);
+    if (topc == kFlux) return topv * d.az;
+    if (topc == kHead) {
+      const double delta = 0.5 * l.dz;
+      return d.az * l.ks * ((hpl - topv) / delta - 1.0);
     }
     return 0.0;
   }
   if (k == d.nz && above) {  // bottom boundary face
-    const long long c = base + d.nz - 1;
-    const int code = f.botc[col];
-    const double kf = pk.kcz[c];
-    if (code == kFlux) return f.botv[col] * d.az;
-    if (code == kGravity) return -kf * d.az;
-    if (code == kHead) {
-      const double delta = 0.5 * f.dz[c];
-      return d.az * kf * ((f.botv[col] - hp[c]) / delta - 1.0);
+    const double kf = u.kc;
+    if (botc == kFlux) return botv * d.az;
+    if (botc == kGravity) return -kf * d.az;
+    if (botc == kHead) {
+      const double delta = 0.5 * u.dz;
+      return d.az * kf * ((botv - hpu) / delta - 1.0);
     }
     return 0.0;
   }
   if (above && below) {
-    const long long up = base + k - 1, lo = base + k;
     double kf;
     if (d.pc) {
-      kf = d.harm ? face_harm(pk.kcz[up], f.ksz[up], f.dz[up], pk.kcz[lo], f.ksz[lo], f.dz[lo])
-                  : 0.5 * (pk.kcz[up] + pk.kcz[lo]);
+      kf = d.harm ? face_harm(u.kc, u.ks, u.dz, l.kc, l.ks, l.dz) : 0.5 * (u.kc + l.kc);
     } else {
-      kf = 0.5 * (vg_k(soil_at(f, up), hp[up], f.ksz[lo]) + pk.kcz[lo]);
+      kf = 0.5 * (vg_k(soil_at(f, cu), hp[cu], l.ks) + l.kc);
     }
-    const double delta = 0.5 * (f.dz[up] + f.dz[lo]);
-    return d.az * kf * ((hp[lo] - hp[up]) / delta - 1.0);
+    const double delta = 0.5 * (u.dz + l.dz);
+    return d.az * kf * ((hpl - hpu) / delta - 1.0);
   }
   return 0.0;
 }
 
-__global__ void k_flux(Dims d, Fields f, PassK pk, const double* __restrict__ hp,
-                       const double* __restrict__ wcn, double* kx, double* ky, double* kzf,
-                       double* qx, double* qy, double* qzf) {
+// Thread c owns the x+ and y+ faces of its cell (the domain's west and south
+// boundary faces through the ghost cells i = 0, j = 0) and the z face above
+// it (plus the bottom face for k = nz-1).  Each face's loads are issued
+// before its rules run.
+__global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
+                                                    const double* __restrict__ hp,
+                                                    const double* __restrict__ wcn,
+                                                    double* __restrict__ kx,
+                                                    double* __restrict__ ky,
+                                                    double* __restrict__ kzf,
+                                                    double* __restrict__ qx,
+                                                    double* __restrict__ qy,
+                                                    double* __restrict__ qzf) {
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     const bool jin = j >= 1 && j <= d.ny, iin = i >= 1 && i <= d.nx;
-    if (jin && i <= d.nx) {
-      kx[c] = face_kx(d, f, pk, j, i, k);
-      qx[c] = flux_x(d, f, pk, hp, wcn, j, i, k);
+    const bool doX = jin && i <= d.nx, doY = iin && j <= d.ny, doZ = jin && iin;
+    LatFlux vx{}, vy{};
+    int codex = 0, codey = 0;
+    double valx = 0.0, valy = 0.0;
+    const long long e = c + d.sx, n = c + d.sy;
+    if (doX) {
+      const long long ec = col2(d, j, i == 0 ? 1 : d.nx);
+      vx = LatFlux{pk.kcx[c], pk.kcx[e], f.ksx[c], f.ksx[e], hp[c], hp[e], wcn[c], wcn[e],
+                   f.wcs[c], f.wcs[e], f.bot[c], f.bot[e], f.ax[c], f.cosx[c], f.sinx[c],
+                   f.act[c], f.act[e]};
+      codex = (i == 0) ? f.xmc[ec] : f.xpc[ec];
+      valx = (i == 0) ? f.xmv[ec] : f.xpv[ec];
     }
-    if (iin && j <= d.ny) {
-      ky[c] = face_ky(d, f, pk, j, i, k);
-      qy[c] = flux_y(d, f, pk, hp, wcn, j, i, k);
+    if (doY) {
+      const long long ec = col2(d, j == 0 ? 1 : d.ny, i);
+      vy = LatFlux{pk.kcy[c], pk.kcy[n], f.ksy[c], f.ksy[n], hp[c], hp[n], wcn[c], wcn[n],
+                   f.wcs[c], f.wcs[n], f.bot[c], f.bot[n], f.ay[c], f.cosy[c], f.siny[c],
+                   f.act[c], f.act[n]};
+      codey = (j == 0) ? f.ymc[ec] : f.ypc[ec];
+      valy = (j == 0) ? f.ymv[ec] : f.ypv[ec];
     }
-    if (jin && iin) {
+    ZFlank zu{}, zc{};
+    double hpu = 0.0, hpc = 0.0, topv = 0.0, botv = 0.0;
+    int topc = 0, botc = 0;
+    const long long cu = (k >= 1) ? c - 1 : c;
+    if (doZ) {
+      const long long col = col2(d, j, i);
+      zu = ZFlank{pk.kcz[cu], f.ksz[cu], f.dz[cu], (k >= 1) ? f.act[cu] : int8_t(0)};
+      zc = ZFlank{pk.kcz[c], f.ksz[c], f.dz[c], f.act[c]};
+      hpu = hp[cu];
+      hpc = hp[c];
+      topc = f.topc[col];
+      botc = f.botc[col];
+      topv = f.topv[col];
+      botv = f.botv[col];
+    }
+    if (doX) {
+      const Flank a{vx.kca, vx.ksa, vx.wa, vx.wsa, vx.acta};
+      const Flank b{vx.kcb, vx.ksb, vx.wb, vx.wsb, vx.actb};
+      kx[c] = face_lat(d, a, b, i == 0, i == d.nx, codex);
+      qx[c] = flux_lat(d, f, vx, d.dx, i == 0, i == d.nx, codex, valx, e, hp);
+    }
+    if (doY) {
+      const Flank a{vy.kca, vy.ksa, vy.wa, vy.wsa, vy.acta};
+      const Flank b{vy.kcb, vy.ksb, vy.wb, vy.wsb, vy.actb};
+      ky[c] = face_lat(d, a, b, j == 0, j == d.ny, codey);
+      qy[c] = flux_lat(d, f, vy, d.dy, j == 0, j == d.ny, codey, valy, n, hp);
+    }
+    if (doZ) {
       const long long fz = fidx(d, j, i, k);
-      kzf[fz] = face_kz(d, f, pk, j, i, k);
-      qzf[fz] = flux_z(d, f, pk, hp, j, i, k);
+      kzf[fz] = face_z(d, zu, zc, k, topc, botc);
+      qzf[fz] = flux_zv(d, f, zu, zc, hpu, hpc, k, topc, topv, botc, botv, cu, hp);
       if (k == d.nz - 1) {
-        kzf[fz + 1] = face_kz(d, f, pk, j, i, d.nz);
-        qzf[fz + 1] = flux_z(d, f, pk, hp, j, i, d.nz);
+        const ZFlank none{0.0, 0.0, 0.0, 0};
+        kzf[fz + 1] = face_z(d, zc, none, d.nz, topc, botc);
+        qzf[fz + 1] = flux_zv(d, f, zc, none, hpc, 0.0, d.nz, topc, topv, botc, botv, c, hp);
       }
     }
   }
@@ -419,7 +482,7 @@ __global__ void k_flux(Dims d, Fields f, PassK pk, const double* __restrict__ hp
 // the post-allocation classification tests on the six neighbours of a cell.
 // All loads of a cell are issued before its first store and before any
 // branch on loaded data, so one memory round trip serves the cell.
-__global__ void __launch_bounds__(kBlock) k_update_wc(
+__global__ void __launch_bounds__(kBlock, 4) k_update_wc(
     Dims d, Fields f, const double* __restrict__ hp, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ qx, const double* __restrict__ qy,
     const double* __restrict__ qzf, double dtg, double* __restrict__ wcu,
@@ -872,48 +935,62 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
 // finalizeWaterContent (Corrector.cpp:758-792), accumulateBoundaryFlux
 // (RichardsSolver.cpp:961-1006), the adaptTimeStep inputs (AdaptiveStep.cpp:
 // 58-98) and the owned volume (RichardsSolver.cpp:892-912), in one sweep.
-__global__ void __launch_bounds__(kBlock, 3) k_finalize(Dims d, Fields f, double* wc, double* vloss,
-                           const double* __restrict__ qx, const double* __restrict__ qy,
-                           const double* __restrict__ qzf, double dtg, double co_max,
-                           double* partial, int nblk) {
+__global__ void __launch_bounds__(kBlock, 3) k_finalize(Dims d, Fields f, double* __restrict__ wc,
+                                                        double* __restrict__ vloss,
+                                                        const double* __restrict__ qx,
+                                                        const double* __restrict__ qy,
+                                                        const double* __restrict__ qzf,
+                                                        double dtg, double co_max,
+                                                        double* partial, int nblk) {
   double vl = 0.0, inflow = 0.0, dqmax = -DBL_MAX, dtco = DBL_MAX, vol = 0.0;
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
-    if (j < 1 || j > d.ny || i < 1 || i > d.nx || !f.act[c]) continue;
-    const double volume = d.az * f.dz[c];
-    double w = wc[c];
-    if (w > f.wcs[c]) {
-      const double ex = (w - f.wcs[c]) * volume;
+    if (j < 1 || j > d.ny || i < 1 || i > d.nx) continue;
+    const long long fz = fidx(d, j, i, k);
+    const long long cu = (k >= 1) ? c - 1 : c;
+    const int8_t ac = f.act[c];
+    const int8_t au = (k >= 1) ? f.act[cu] : int8_t(0);
+    const double dzc = f.dz[c], ts = f.wcs[c], tr = f.wcr[c];
+    const double w0 = wc[c];
+    const double qxp = qx[c], qxm = qx[c - d.sx], qyp = qy[c], qym = qy[c - d.sy];
+    const double qzt = qzf[fz], qzb = qzf[fz + 1];
+    const double axc = f.ax[c], ayc = f.ay[c];
+    const double vga = f.vga[c], vgn = f.vgn[c], ksz = f.ksz[c];
+    if (!ac) continue;
+    const double volume = d.az * dzc;
+    double w = w0;
+    if (w > ts) {
+      const double ex = (w - ts) * volume;
       vloss[c] += ex;
       vl += ex;
-      w = f.wcs[c];
+      w = ts;
       wc[c] = w;
-    } else if (w < f.wcr[c]) {
-      const double de = (f.wcr[c] - w) * volume;
+    } else if (w < tr) {
+      const double de = (tr - w) * volume;
       vloss[c] -= de;
       vl -= de;
-      w = f.wcr[c];
+      w = tr;
       wc[c] = w;
     }
-    vol += w * d.az * f.dz[c];
-    const long long fz = fidx(d, j, i, k);
-    const bool top = (k == 0) || !f.act[c - 1];
-    if (top) inflow -= qzf[fz] * dtg;
-    if (k == d.nz - 1) inflow += qzf[fz + 1] * dtg;
-    if (i == 1) inflow -= qx[c - d.sx] * dtg;
-    if (i == d.nx) inflow += qx[c] * dtg;
-    if (j == 1) inflow -= qy[c - d.sy] * dtg;
-    if (j == d.ny) inflow += qy[c] * dtg;
+    vol += w * d.az * dzc;
+    const bool top = (k == 0) || !au;
+    if (top) inflow -= qzt * dtg;
+    if (k == d.nz - 1) inflow += qzb * dtg;
+    if (i == 1) inflow -= qxm * dtg;
+    if (i == d.nx) inflow += qxp * dtg;
+    if (j == 1) inflow -= qym * dtg;
+    if (j == d.ny) inflow += qyp * dtg;
     if (!top) {
-      const double qin = qx[c] / f.ax[c] + qy[c] / f.ay[c] + qzf[fz + 1] / d.az;
-      const double qou = qx[c - d.sx] / f.ax[c] + qy[c - d.sy] / f.ay[c] + qzf[fz] / d.az;
-      const double dq = fabs(qin - qou) * dtg / f.dz[c];
+      const double qin = qxp / axc + qyp / ayc + qzb / d.az;
+      const double qou = qxm / axc + qym / ayc + qzt / d.az;
+      const double dq = fabs(qin - qou) * dtg / dzc;
       if (dq > dqmax) dqmax = dq;
-      if (w < f.wcs[c]) {
-        const double dk = vg_dkdtheta(soil_at(f, c), w, f.ksz[c]);
-        const double t = co_max * f.dz[c] / dk;
+      if (w < ts) {
+        const Soil so{vga, vgn, ts, tr, 0.0};
+        const double dk = vg_dkdtheta(so, w, ksz);
+        const double t = co_max * dzc / dk;
         if (t < dtco) dtco = t;
       }
     }

@@ -214,7 +214,8 @@ long long frehg_gw_active_cells(const frehg_gw_handle* h);
 /* Tracing (no counterpart in the reference, whose Timer sections do not
  * fence the device): with profiling on, each step records CUDA events around
  * its phases; frehg_gw_phase_times returns the last step's device times in
- * ms: [0] step-start refresh + predictor assembly, [1] predictor solve,
+ * ms: [0] step-start refresh + predictor assembly (and, in the mixed form,
+ * the FP32 cast and line factorization), [1] the predictor solve kernel,
  * [2] corrector, [3] post-allocation, [4] clamp, audit and controller. */
 int frehg_gw_set_profiling(frehg_gw_handle* h, int on);
 int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5);
