@@ -16,28 +16,13 @@
 #include "gw_internal.h"
 #include "gw_setup.h"
 
-struct frehg_gw_handle {
-  fgw::Device D;
-  double offset = 0.0;
-  long long nactive = 0;
-  double* bath_dev = nullptr;
-  std::vector<int> codes;      // host copy, 6 x ncol
-  std::vector<double> values;  // host staging, 6 x ncol
-  bool values_pinned = false;  // staging page-locked with cudaHostRegister
-  double rtol = 1e-8, atol = 1e-14, outer_rtol = 1e-10;
-  int maxit = 1000, max_outer = 30, precision = 0;
-  double dt_min = 0, dt_max = 0, dq_grow = 0.01, dq_shrink = 0.02, co_max = 2.0;
-  double next_dt = 0.0;
-  bool have_state = false;
-  int start_buf = 0;  // ping-pong index of the last step's theta^n
-  bool profiling = false;
-  cudaEvent_t ev[6] = {};
-  double phase_ms[5] = {0, 0, 0, 0, 0};
-};
+#include "gw_handle.h"
 
 namespace {
-
 thread_local std::string g_error;
+}  // namespace
+
+namespace fgw_api {
 
 int fail(int status, const std::string& msg) {
   g_error = msg;
@@ -47,6 +32,13 @@ int fail(int status, const std::string& msg) {
 int cuda_fail(cudaError_t e, const char* what) {
   return fail(FREHG_GW_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
+
+}  // namespace fgw_api
+
+namespace {
+
+using fgw_api::cuda_fail;
+using fgw_api::fail;
 
 #define CUDA_TRY(call, what)                    \
   do {                                          \
@@ -393,59 +385,45 @@ int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc)
   return FREHG_GW_OK;
 }
 
-int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* info) {
-  (void)t;  // boundary values arrive through frehg_gw_set_bc_values
-  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
-  if (!h->have_state) return fail(FREHG_GW_ESTATE, "frehg_gw_step before frehg_gw_init_state");
-  if (!(dtg > 0.0) || !std::isfinite(dtg)) return fail(FREHG_GW_EINVAL, "dtg must be positive");
+}  // extern "C"
+
+namespace fgw_api {
+
+cudaError_t enqueue_predictor(frehg_gw_handle* h) {
   fgw::Device& D = h->D;
-  const int cur = D.cur, nxt = 1 - cur;
-  double* hn = D.h[cur];
-  double* wcn = D.wc[cur];
-  const bool prof = h->profiling;
-  auto mark = [&](int n) {
-    if (prof) cudaEventRecord(h->ev[n], D.stream);
-  };
-  // Step-start refresh, predictor, solve.
-  mark(0);
+  double* hn = D.h[D.cur];
+  double* wcn = D.wc[D.cur];
   fgw::launch_ghosts(D, hn, wcn);
   fgw::launch_closure_pred(D, hn);
-  fgw::launch_assemble(D, hn, wcn, dtg);
-  cudaError_t e;
-  if (h->precision == FREHG_GW_PRECISION_MIXED) {
-    e = fgw::launch_line_factor(D);
-    if (e != cudaSuccess) return cuda_fail(e, "line factor launch");
-  }
-  mark(1);
-  if (h->precision == FREHG_GW_PRECISION_MIXED) {
-    e = fgw::launch_cg_mixed(D, h->rtol, h->atol, h->maxit, h->outer_rtol, h->max_outer);
-  } else {
-    e = fgw::launch_cg64(D, h->rtol, h->atol, h->maxit);
-  }
-  if (e != cudaSuccess) return cuda_fail(e, "predictor solve launch");
-  mark(2);
-  // Corrector, post-allocation, clamp, audit, controller.
+  fgw::launch_assemble(D, hn, wcn);
+  if (h->precision == FREHG_GW_PRECISION_MIXED) return fgw::launch_line_factor(D);
+  return cudaGetLastError();
+}
+
+void enqueue_corrector(frehg_gw_handle* h) {
+  fgw::Device& D = h->D;
+  const int nxt = 1 - D.cur;
+  double* hn = D.h[D.cur];
+  double* wcn = D.wc[D.cur];
   fgw::launch_closure_corr(D, hn);
-  fgw::launch_flux(D, wcn, dtg);
-  fgw::launch_update_wc(D, hn, wcn, dtg);
-  mark(3);
+  fgw::launch_flux(D, wcn);
+  fgw::launch_update_wc(D, hn, wcn);
+  if (h->profiling) cudaEventRecord(h->ev[3], D.stream);
   fgw::launch_classify(D, D.wc[nxt], D.h[nxt]);
-  fgw::launch_walk(D, D.wc[nxt], dtg);
-  mark(4);
-  fgw::launch_finalize(D, D.wc[nxt], dtg, h->co_max);
-  fgw::launch_step_info(D, dtg, h->dq_grow, h->dq_shrink, h->dt_min, h->dt_max);
-  mark(5);
-  CUDA_TRY(cudaMemcpyAsync(D.out_host, D.out, sizeof(fgw::StepOut), cudaMemcpyDeviceToHost,
-                           D.stream), "step readback");
-  CUDA_TRY(cudaStreamSynchronize(D.stream), "step");
-  CUDA_TRY(cudaGetLastError(), "step kernels");
-  if (prof) {
-    for (int n = 0; n < 5; ++n) {
-      float ms = 0.0f;
-      cudaEventElapsedTime(&ms, h->ev[n], h->ev[n + 1]);
-      h->phase_ms[n] = ms;
-    }
-  }
+  fgw::launch_walk(D, D.wc[nxt]);
+  if (h->profiling) cudaEventRecord(h->ev[4], D.stream);
+  fgw::launch_finalize(D, D.wc[nxt], h->co_max);
+  fgw::launch_step_info(D, h->dq_grow, h->dq_shrink, h->dt_min, h->dt_max);
+}
+
+cudaError_t upload_next_dt(frehg_gw_handle* h) {
+  h->D.out_host->next_dt = h->next_dt;
+  return cudaMemcpyAsync(&h->D.out->next_dt, &h->D.out_host->next_dt, sizeof(double),
+                         cudaMemcpyHostToDevice, h->D.stream);
+}
+
+int finish_step(frehg_gw_handle* h, frehg_gw_step_info* info) {
+  fgw::Device& D = h->D;
   const fgw::StepOut& o = *D.out_host;
   frehg_gw_step_info s{};
   s.cg_iterations = o.cg.its;
@@ -470,10 +448,56 @@ int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* 
   s.status = status;
   if (info) *info = s;
   if (status != FREHG_GW_OK) return status;
-  h->start_buf = cur;
-  D.cur = nxt;
+  h->start_buf = D.cur;
+  D.cur = 1 - D.cur;
   h->next_dt = o.next_dt;
   return FREHG_GW_OK;
+}
+
+}  // namespace fgw_api
+
+extern "C" {
+
+int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* info) {
+  (void)t;  // boundary values arrive through frehg_gw_set_bc_values
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  if (!h->have_state) return fail(FREHG_GW_ESTATE, "frehg_gw_step before frehg_gw_init_state");
+  if (!(dtg > 0.0) || !std::isfinite(dtg)) return fail(FREHG_GW_EINVAL, "dtg must be positive");
+  fgw::Device& D = h->D;
+  const bool prof = h->profiling;
+  auto mark = [&](int n) {
+    if (prof) cudaEventRecord(h->ev[n], D.stream);
+  };
+  // The step's dtg goes into the device step record, where every kernel of
+  // the step reads it.
+  D.out_host->next_dt = dtg;
+  CUDA_TRY(cudaMemcpyAsync(&D.out->next_dt, &D.out_host->next_dt, sizeof(double),
+                           cudaMemcpyHostToDevice, D.stream), "step dtg");
+  mark(0);
+  cudaError_t e = fgw_api::enqueue_predictor(h);
+  if (e != cudaSuccess) return cuda_fail(e, "predictor launch");
+  mark(1);
+  if (h->precision == FREHG_GW_PRECISION_MIXED) {
+    e = fgw::launch_cg_mixed(D, h->rtol, h->atol, h->maxit, h->outer_rtol, h->max_outer);
+  } else {
+    e = fgw::launch_cg64(D, h->rtol, h->atol, h->maxit);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "predictor solve launch");
+  mark(2);
+  fgw_api::enqueue_corrector(h);
+  mark(5);
+  CUDA_TRY(cudaMemcpyAsync(D.out_host, D.out, sizeof(fgw::StepOut), cudaMemcpyDeviceToHost,
+                           D.stream), "step readback");
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "step");
+  CUDA_TRY(cudaGetLastError(), "step kernels");
+  if (prof) {
+    for (int n = 0; n < 5; ++n) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, h->ev[n], h->ev[n + 1]);
+      h->phase_ms[n] = ms;
+    }
+  }
+  return fgw_api::finish_step(h, info);
 }
 
 int frehg_gw_next_dt(frehg_gw_handle* h, double* out) {

@@ -26,6 +26,7 @@
 // instead of hanging.
 #include <cfloat>
 #include <cstdio>
+#include <cstring>
 
 #include "gw_coop.cuh"
 #include "gw_internal.h"
@@ -48,11 +49,10 @@ struct Cg64Args {
 
 __device__ inline int sgn(double v) { return (v > 0.0) - (v < 0.0); }
 
-__global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
+__device__ __forceinline__ void cg64_body(const Cg64Args& a, const int bid, const int G) {
   const long long N = a.d.ncell, sx = a.d.sx, sy = a.d.sy;
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  const int G = gridDim.x;
+  const long long stride = static_cast<long long>(G) * blockDim.x;
+  const long long t0 = bid * static_cast<long long>(blockDim.x) + threadIdx.x;
   double* const pzz = a.part;
   double* const pzr = a.part + G;
   double* const ppw = a.part + 2 * G;
@@ -71,9 +71,9 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
     zr += z * rc;
   }
   double s = block_sum_all(zz);
-  if (threadIdx.x == 0) pzz[blockIdx.x] = s;
+  if (threadIdx.x == 0) pzz[bid] = s;
   s = block_sum_all(zr);
-  if (threadIdx.x == 0) pzr[blockIdx.x] = s;
+  if (threadIdx.x == 0) pzr[bid] = s;
   if (!grid_sync(a.st, G)) return;
   double dp = sqrt(reduce_partials(pzz, G));
   double beta = reduce_partials(pzr, G);
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
       pw += pc * wv;
     }
     s = block_sum_all(pw);
-    if (threadIdx.x == 0) ppw[blockIdx.x] = s;
+    if (threadIdx.x == 0) ppw[bid] = s;
     if (!grid_sync(a.st, G)) return;
     dpiold = dpi;
     dpi = reduce_partials(ppw, G);
@@ -147,9 +147,9 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
       zr += z * rc;
     }
     s = block_sum_all(zz);
-    if (threadIdx.x == 0) pzz[blockIdx.x] = s;
+    if (threadIdx.x == 0) pzz[bid] = s;
     s = block_sum_all(zr);
-    if (threadIdx.x == 0) pzr[blockIdx.x] = s;
+    if (threadIdx.x == 0) pzr[bid] = s;
     if (!grid_sync(a.st, G)) return;
     dp = sqrt(reduce_partials(pzz, G));
     test(dp);
@@ -161,13 +161,33 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
       break;
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bid == 0 && threadIdx.x == 0) {
     a.st->dp = dp;
     a.st->rnorm0 = rnorm0;
     a.st->its = its;
     a.st->reason = reason;
     a.st->outer = 1;
   }
+}
+
+__global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
+  cg64_body(a, blockIdx.x, gridDim.x);
+}
+
+// One cooperative launch over several domains: instance i owns blocks
+// [first[i], first[i+1]) and runs its own solve on them.
+__global__ void __launch_bounds__(kCgBlock, 3)
+    k_cg64_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n) {
+  __shared__ Cg64Args sa;
+  __shared__ int sb, sg;
+  if (threadIdx.x == 0) {
+    const int i = instance_of(first, n, blockIdx.x);
+    sa = tab[i];
+    sb = blockIdx.x - first[i];
+    sg = first[i + 1] - first[i];
+  }
+  __syncthreads();
+  cg64_body(sa, sb, sg);
 }
 
 
@@ -180,11 +200,10 @@ __device__ inline void st2(double* p, double a, double b) {
   *reinterpret_cast<double2*>(p) = make_double2(a, b);
 }
 
-__global__ void __launch_bounds__(kCgBlock, 3) k_cg64v(Cg64Args a) {
+__device__ __forceinline__ void cg64v_body(const Cg64Args& a, const int bid, const int G) {
   const long long N2 = a.d.ncell / 2, sx = a.d.sx, sy = a.d.sy;
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  const int G = gridDim.x;
+  const long long stride = static_cast<long long>(G) * blockDim.x;
+  const long long t0 = bid * static_cast<long long>(blockDim.x) + threadIdx.x;
   double* const pzz = a.part;
   double* const pzr = a.part + G;
   double* const ppw = a.part + 2 * G;
@@ -206,9 +225,9 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64v(Cg64Args a) {
     zr += z1 * rc.y;
   }
   double s = block_sum_all(zz);
-  if (threadIdx.x == 0) pzz[blockIdx.x] = s;
+  if (threadIdx.x == 0) pzz[bid] = s;
   s = block_sum_all(zr);
-  if (threadIdx.x == 0) pzr[blockIdx.x] = s;
+  if (threadIdx.x == 0) pzr[bid] = s;
   if (!grid_sync(a.st, G)) return;
   double dp = sqrt(reduce_partials(pzz, G));
   double beta = reduce_partials(pzr, G);
@@ -277,7 +296,7 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64v(Cg64Args a) {
       pw += P1 * w1;
     }
     s = block_sum_all(pw);
-    if (threadIdx.x == 0) ppw[blockIdx.x] = s;
+    if (threadIdx.x == 0) ppw[bid] = s;
     if (!grid_sync(a.st, G)) return;
     dpiold = dpi;
     dpi = reduce_partials(ppw, G);
@@ -304,9 +323,9 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64v(Cg64Args a) {
       zr += z1 * r1;
     }
     s = block_sum_all(zz);
-    if (threadIdx.x == 0) pzz[blockIdx.x] = s;
+    if (threadIdx.x == 0) pzz[bid] = s;
     s = block_sum_all(zr);
-    if (threadIdx.x == 0) pzr[blockIdx.x] = s;
+    if (threadIdx.x == 0) pzr[bid] = s;
     if (!grid_sync(a.st, G)) return;
     dp = sqrt(reduce_partials(pzz, G));
     test(dp);
@@ -318,13 +337,33 @@ __global__ void __launch_bounds__(kCgBlock, 3) k_cg64v(Cg64Args a) {
       break;
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bid == 0 && threadIdx.x == 0) {
     a.st->dp = dp;
     a.st->rnorm0 = rnorm0;
     a.st->its = its;
     a.st->reason = reason;
     a.st->outer = 1;
   }
+}
+
+__global__ void __launch_bounds__(kCgBlock, 3) k_cg64v(Cg64Args a) {
+  cg64v_body(a, blockIdx.x, gridDim.x);
+}
+
+// One cooperative launch over several domains: instance i owns blocks
+// [first[i], first[i+1]) and runs its own solve on them.
+__global__ void __launch_bounds__(kCgBlock, 3)
+    k_cg64v_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n) {
+  __shared__ Cg64Args sa;
+  __shared__ int sb, sg;
+  if (threadIdx.x == 0) {
+    const int i = instance_of(first, n, blockIdx.x);
+    sa = tab[i];
+    sb = blockIdx.x - first[i];
+    sg = first[i + 1] - first[i];
+  }
+  __syncthreads();
+  cg64v_body(sa, sb, sg);
 }
 
 }  // namespace
@@ -342,8 +381,9 @@ int cg64_grid(int sm_count, long long ncell) {
   return static_cast<int>(g < 1 ? 1 : g);
 }
 
-cudaError_t launch_cg64(Device& D, double rtol, double atol, int maxit) {
-  cudaMemsetAsync(&D.out->cg, 0, sizeof(CgState), D.stream);
+namespace {
+
+Cg64Args make_cg64_args(const Device& D, double rtol, double atol, int maxit) {
   Cg64Args a;
   a.d = D.d;
   a.diag = D.diag;
@@ -362,11 +402,31 @@ cudaError_t launch_cg64(Device& D, double rtol, double atol, int maxit) {
   a.rtol = rtol;
   a.atol = atol;
   a.maxit = maxit;
+  return a;
+}
+
+}  // namespace
+
+cudaError_t launch_cg64(Device& D, double rtol, double atol, int maxit) {
+  cudaMemsetAsync(&D.out->cg, 0, sizeof(CgState), D.stream);
+  Cg64Args a = make_cg64_args(D, rtol, atol, maxit);
   void* args[] = {&a};
   ++D.launches;
   const void* kern = (D.d.nz % 2 == 0) ? reinterpret_cast<const void*>(k_cg64v)
                                        : reinterpret_cast<const void*>(k_cg64);
   return cudaLaunchCooperativeKernel(kern, dim3(D.cg_grid), dim3(kCgBlock), args, 0, D.stream);
+}
+
+size_t cg64_args_bytes() { return sizeof(Cg64Args); }
+
+void cg64_fill_args(const Device& D, const SolveParams& p, void* dst) {
+  const Cg64Args a = make_cg64_args(D, p.rtol, p.atol, p.maxit);
+  std::memcpy(dst, &a, sizeof(a));
+}
+
+const void* cg64_batch_kernel(int variant) {
+  return variant ? reinterpret_cast<const void*>(k_cg64v_batch)
+                 : reinterpret_cast<const void*>(k_cg64_batch);
 }
 
 }  // namespace fgw

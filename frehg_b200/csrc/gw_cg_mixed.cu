@@ -30,6 +30,7 @@
 // (z, p_old, diag, gxp, gyp, gzp in; p_new, w out), phase B 9 words (d, p, r,
 // w, dinv, l in; d, r, z out) -> 68 B.
 #include <cfloat>
+#include <cstring>
 
 #include "gw_coop.cuh"
 #include "gw_internal.h"
@@ -360,20 +361,19 @@ __device__ inline double phase_a(const MixedArgs& a, float bc, const float* __re
 // E = 0: shared-memory tiled line solve; E > 0: warp-per-column solve with E
 // cells per lane.
 template <int V, int E>
-__global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
+__device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid, const int G) {
   extern __shared__ float msm[];
   const Dims& d = a.d;
   const int nz = d.nz, nzp = nz + 1, tc = a.tc;
   float* s_r = msm;
   float* s_z = msm + tc * nzp;
   const long long N = d.ncell, sx = d.sx, sy = d.sy;
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  const long long stride = static_cast<long long>(G) * blockDim.x;
+  const long long t0 = bid * static_cast<long long>(blockDim.x) + threadIdx.x;
   const long long ntiles = (d.ncol + tc - 1) / tc;
-  const int G = gridDim.x;
   const int lane = threadIdx.x & 31;
   const bool vec = (E > 0) && (nz % (E > 0 ? E : 1) == 0);
-  const long long gwarp = blockIdx.x * static_cast<long long>(kCgBlock / 32) + (threadIdx.x >> 5);
+  const long long gwarp = bid * static_cast<long long>(kCgBlock / 32) + (threadIdx.x >> 5);
   const long long nwarp = static_cast<long long>(G) * (kCgBlock / 32);
   double* const q0 = a.part;
   double* const q1 = a.part + G;
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
         st_col<E>(a.p0, cb, lane, nz, vec, lk);
       }
     } else {
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (long long t = bid; t < ntiles; t += G) {
       const long long base = t * tc * nz;
       const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
       const int ncells = ncols * nz;
@@ -469,11 +469,11 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
     }
     }
     double s = block_sum_all(rn2);
-    if (threadIdx.x == 0) q0[blockIdx.x] = s;
+    if (threadIdx.x == 0) q0[bid] = s;
     s = block_sum_all(zz);
-    if (threadIdx.x == 0) q1[blockIdx.x] = s;
+    if (threadIdx.x == 0) q1[bid] = s;
     s = block_sum_all(zr);
-    if (threadIdx.x == 0) q2[blockIdx.x] = s;
+    if (threadIdx.x == 0) q2[bid] = s;
     if (!grid_sync(a.st, G)) return;
     rnorm = sqrt(reduce_partials(q0, G));
     const double zn0 = sqrt(reduce_partials(q1, G));
@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
       float* __restrict__ pnew = (i & 1) ? a.p0 : a.p1;
       const double pw = phase_a<V>(a, bc, pold, pnew, t0, stride);
       s = block_sum_all(pw);
-      if (threadIdx.x == 0) q0[blockIdx.x] = s;
+      if (threadIdx.x == 0) q0[bid] = s;
       if (!grid_sync(a.st, G)) return;
       const double dpi = reduce_partials(q0, G);
       if (!(dpi > 0.0)) break;  // inner breakdown: keep d, let the FP64 sweep judge
@@ -542,7 +542,7 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
           }
         }
       } else {
-      for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      for (long long t = bid; t < ntiles; t += G) {
         const long long base = t * tc * nz;
         const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
         const int ncells = ncols * nz;
@@ -612,9 +612,9 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
       }
       }
       s = block_sum_all(zz);
-      if (threadIdx.x == 0) q1[blockIdx.x] = s;
+      if (threadIdx.x == 0) q1[bid] = s;
       s = block_sum_all(zr);
-      if (threadIdx.x == 0) q2[blockIdx.x] = s;
+      if (threadIdx.x == 0) q2[bid] = s;
       if (!grid_sync(a.st, G)) return;
       const double zn = sqrt(reduce_partials(q1, G));
       if (zn <= itol) break;
@@ -625,13 +625,35 @@ __global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
   if (final_buf == 1) {
     for (long long c = t0; c < N; c += stride) a.x0[c] = a.x1[c];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bid == 0 && threadIdx.x == 0) {
     a.st->dp = rnorm;
     a.st->rnorm0 = bnorm;
     a.st->its = total;
     a.st->reason = reason;
     a.st->outer = outer;
   }
+}
+
+template <int V, int E>
+__global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
+  cg_mixed_body<V, E>(a, blockIdx.x, gridDim.x);
+}
+
+// One cooperative launch over several domains of the same (V, E) class:
+// instance i owns blocks [first[i], first[i+1]) and runs its own solve.
+template <int V, int E>
+__global__ void __launch_bounds__(kCgBlock, 4)
+    k_cg_mixed_batch(const MixedArgs* __restrict__ tab, const int* __restrict__ first, int n) {
+  __shared__ MixedArgs sa;
+  __shared__ int sb, sg;
+  if (threadIdx.x == 0) {
+    const int i = instance_of(first, n, blockIdx.x);
+    sa = tab[i];
+    sb = blockIdx.x - first[i];
+    sg = first[i + 1] - first[i];
+  }
+  __syncthreads();
+  cg_mixed_body<V, E>(sa, sb, sg);
 }
 
 int host_tile_cols(int nz) {
@@ -643,6 +665,42 @@ int host_tile_cols(int nz) {
 
 size_t mixed_smem(int nz) { return 2 * sizeof(float) * host_tile_cols(nz) * (nz + 1); }
 size_t factor_smem(int nz) { return 2 * sizeof(double) * host_tile_cols(nz) * (nz + 1); }
+
+MixedArgs make_mixed_args(const Device& D, double atol, int maxit, double outer_rtol,
+                          int max_outer) {
+  const int tc = host_tile_cols(D.d.nz);
+  MixedArgs a;
+  a.d = D.d;
+  a.diag = D.diag;
+  a.gxp = D.gxp;
+  a.gyp = D.gyp;
+  a.gzp = D.gzp;
+  a.b = D.rhs;
+  a.x0 = D.x;
+  a.x1 = D.xalt;
+  a.diag32 = D.diag32;
+  a.gxp32 = D.gxp32;
+  a.gyp32 = D.gyp32;
+  a.gzp32 = D.gzp32;
+  a.dinv32 = D.dinv32;
+  a.l32 = D.l32;
+  a.r32 = D.r32;
+  a.z32 = D.z32;
+  a.p0 = D.p032;
+  a.p1 = D.p132;
+  a.w32 = D.w32;
+  a.d32 = D.d32;
+  a.part = D.cgpart;
+  a.st = &D.out->cg;
+  a.outer_rtol = outer_rtol;
+  a.inner_rtol = 1.0e-5;
+  a.atol = atol;
+  a.max_inner = maxit;
+  a.max_outer = max_outer;
+  a.max_total = maxit;
+  a.tc = tc;
+  return a;
+}
 
 }  // namespace
 
@@ -695,40 +753,52 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
   if (!wcol && g > ntiles) g = ntiles;
   if (g < 1) g = 1;
   cudaMemsetAsync(&D.out->cg, 0, sizeof(CgState), D.stream);
-  MixedArgs a;
-  a.d = D.d;
-  a.diag = D.diag;
-  a.gxp = D.gxp;
-  a.gyp = D.gyp;
-  a.gzp = D.gzp;
-  a.b = D.rhs;
-  a.x0 = D.x;
-  a.x1 = D.xalt;
-  a.diag32 = D.diag32;
-  a.gxp32 = D.gxp32;
-  a.gyp32 = D.gyp32;
-  a.gzp32 = D.gzp32;
-  a.dinv32 = D.dinv32;
-  a.l32 = D.l32;
-  a.r32 = D.r32;
-  a.z32 = D.z32;
-  a.p0 = D.p032;
-  a.p1 = D.p132;
-  a.w32 = D.w32;
-  a.d32 = D.d32;
-  a.part = D.cgpart;
-  a.st = &D.out->cg;
-  a.outer_rtol = outer_rtol;
-  a.inner_rtol = 1.0e-5;
-  a.atol = atol;
-  a.max_inner = maxit;
-  a.max_outer = max_outer;
-  a.max_total = maxit;
-  a.tc = tc;
+  MixedArgs a = make_mixed_args(D, atol, maxit, outer_rtol, max_outer);
   void* args[] = {&a};
   ++D.launches;
   D.cg_grid32 = static_cast<int>(g);
   return cudaLaunchCooperativeKernel(kern, dim3(g), dim3(kCgBlock), args, ksm, D.stream);
+}
+
+
+// ---------------------------------------------------------------- batched solves
+namespace {
+
+// Line-solve layout of a column depth: E cells per lane (warp per column,
+// nz <= 32 E) or 0 (shared-memory tiles).
+int line_e(int nz, bool tiled) {
+  if (tiled || nz > 32 * kMaxE) return 0;
+  return nz <= 32 ? 1 : nz <= 64 ? 2 : nz <= 128 ? 4 : 8;
+}
+
+}  // namespace
+
+int mixed_variant(const Device& D, bool tiled) {
+  const int v = (D.d.nz % 4 == 0) ? 4 : 1;
+  return v * 16 + line_e(D.d.nz, tiled);
+}
+
+size_t mixed_args_bytes() { return sizeof(MixedArgs); }
+
+void mixed_fill_args(const Device& D, const SolveParams& p, void* dst) {
+  const MixedArgs a = make_mixed_args(D, p.atol, p.maxit, p.outer_rtol, p.max_outer);
+  std::memcpy(dst, &a, sizeof(a));
+}
+
+size_t mixed_batch_smem(const Device& D, int variant) {
+  return (variant % 16 == 0) ? mixed_smem(D.d.nz) : 0;
+}
+
+const void* mixed_batch_kernel(int variant) {
+  using Kern = void (*)(const MixedArgs*, const int*, int);
+  static const Kern table[2][5] = {
+      {k_cg_mixed_batch<1, 0>, k_cg_mixed_batch<1, 1>, k_cg_mixed_batch<1, 2>,
+       k_cg_mixed_batch<1, 4>, k_cg_mixed_batch<1, 8>},
+      {k_cg_mixed_batch<4, 0>, k_cg_mixed_batch<4, 1>, k_cg_mixed_batch<4, 2>,
+       k_cg_mixed_batch<4, 4>, k_cg_mixed_batch<4, 8>}};
+  const int v = variant / 16, e = variant % 16;
+  const int slot = e == 0 ? 0 : e == 1 ? 1 : e == 2 ? 2 : e == 4 ? 3 : 4;
+  return reinterpret_cast<const void*>(table[v == 4 ? 1 : 0][slot]);
 }
 
 }  // namespace fgw

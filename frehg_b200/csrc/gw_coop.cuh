@@ -89,5 +89,17 @@ __device__ inline double reduce_partials(const double* part, int G) {
   return block_sum_all(v);
 }
 
+// The member of a batched launch whose block range [first[i], first[i+1])
+// holds block b (first has n + 1 ascending entries).
+__device__ inline int instance_of(const int* first, int n, int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 }  // namespace coop
 }  // namespace fgw

@@ -1,0 +1,49 @@
+// Internal: the handle behind the C ABI and the step phases shared by the
+// single-domain step (gw_api.cu) and the batched step (gw_batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/frehg_gw.h"
+#include "gw_internal.h"
+
+struct frehg_gw_handle {
+  fgw::Device D;
+  double offset = 0.0;
+  long long nactive = 0;
+  double* bath_dev = nullptr;
+  std::vector<int> codes;      // host copy, 6 x ncol
+  std::vector<double> values;  // host staging, 6 x ncol
+  bool values_pinned = false;  // staging page-locked with cudaHostRegister
+  double rtol = 1e-8, atol = 1e-14, outer_rtol = 1e-10;
+  int maxit = 1000, max_outer = 30, precision = 0;
+  double dt_min = 0, dt_max = 0, dq_grow = 0.01, dq_shrink = 0.02, co_max = 2.0;
+  double next_dt = 0.0;
+  bool have_state = false;
+  int start_buf = 0;  // ping-pong index of the last step's theta^n
+  bool profiling = false;
+  cudaEvent_t ev[6] = {};
+  double phase_ms[5] = {0, 0, 0, 0, 0};
+};
+
+namespace fgw_api {
+
+// Records `msg` as the calling thread's last error and returns `status`.
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+// The kernels of one step before and after the predictor solve, on the
+// handle's stream; every kernel reads the step's dtg from the device step
+// record.
+cudaError_t enqueue_predictor(frehg_gw_handle* h);
+void enqueue_corrector(frehg_gw_handle* h);
+// Interprets the step record read back into D.out_host: fills *info (may be
+// null) and, on success, flips the state buffers and takes the next dt.
+int finish_step(frehg_gw_handle* h, frehg_gw_step_info* info);
+// Writes the host's next dt into the device step record.
+cudaError_t upload_next_dt(frehg_gw_handle* h);
+
+}  // namespace fgw_api

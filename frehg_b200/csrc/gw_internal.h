@@ -103,15 +103,15 @@ struct Device {
 // ---------------------------------------------------------------- launchers
 void launch_ghosts(const Device& D, double* h, double* wc);
 void launch_closure_pred(const Device& D, const double* h);
-void launch_assemble(const Device& D, const double* hn, const double* wcn, double dtg);
+void launch_assemble(const Device& D, const double* hn, const double* wcn);
 void launch_closure_corr(const Device& D, const double* hn);
-void launch_flux(const Device& D, const double* wcn, double dtg);
-void launch_update_wc(const Device& D, const double* hn, const double* wcn, double dtg);
+void launch_flux(const Device& D, const double* wcn);
+void launch_update_wc(const Device& D, const double* hn, const double* wcn);
 void launch_classify(const Device& D, double* wc_out, double* h_out);
-void launch_walk(const Device& D, double* wc_out, double dtg);
-void launch_finalize(const Device& D, double* wc_out, double dtg, double co_max);
-void launch_step_info(const Device& D, double dtg, double dq_grow, double dq_shrink,
-                      double dt_min, double dt_max);
+void launch_walk(const Device& D, double* wc_out);
+void launch_finalize(const Device& D, double* wc_out, double co_max);
+void launch_step_info(const Device& D, double dq_grow, double dq_shrink, double dt_min,
+                      double dt_max);
 void launch_volume(const Device& D, const double* wc);
 void launch_init_state(const Device& D, int form, double constant, const double* field,
                        const double* bath, double offset);
@@ -124,5 +124,51 @@ cudaError_t launch_line_factor(Device& D);
 cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, double outer_rtol,
                             int max_outer);
 int cg64_grid(int sm_count, long long ncell);
+
+// ---------------------------------------------------------------- batched solves
+// Several domains' predictor solves in one cooperative launch: member i runs
+// its own solve (own CG state, reductions and barrier) on the block range
+// [first[i], first[i+1]); its blocks leave as soon as its solve ends.
+struct SolveParams {
+  double rtol, atol, outer_rtol;
+  int maxit, max_outer;
+};
+
+// Kernel variant of a domain's solve: FP64 (kind 0; variant 1 = two cells a
+// thread, nz even) or mixed (kind 1; variant = V * 16 + E, see gw_cg_mixed.cu).
+struct SolveClass {
+  int kind, variant;
+  bool operator==(const SolveClass& o) const { return kind == o.kind && variant == o.variant; }
+};
+SolveClass solve_class(const Device& D, int precision, bool tiled_line_solve);
+// Blocks of that variant one SM holds (the cooperative limit per SM).
+int solve_blocks_per_sm(const SolveClass& c, size_t smem);
+// Largest block count a member may take (its reduction buffer's capacity).
+int solve_max_blocks(const Device& D, const SolveClass& c);
+
+struct SolveGroup {
+  SolveClass cls{0, 0};
+  int n = 0, grid = 0;
+  size_t smem = 0;
+  void* tab = nullptr;           // device table of per-member kernel arguments
+  int* first = nullptr;          // device block offsets, n + 1
+  CgState** states = nullptr;    // device array of the members' CG states
+};
+// Builds a group over `ds` with `nb[i]` blocks each (all of class `c`).
+cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
+                              const std::vector<int>& nb, const std::vector<SolveParams>& p);
+// Zeroes the members' CG states and launches the group on `s`.
+cudaError_t solve_group_launch(const SolveGroup& g, cudaStream_t s);
+void solve_group_free(SolveGroup& g);
+
+// Per-kind pieces of the batched solves (gw_cg.cu, gw_cg_mixed.cu).
+size_t cg64_args_bytes();
+void cg64_fill_args(const Device& D, const SolveParams& p, void* dst);
+const void* cg64_batch_kernel(int variant);
+int mixed_variant(const Device& D, bool tiled);
+size_t mixed_args_bytes();
+void mixed_fill_args(const Device& D, const SolveParams& p, void* dst);
+size_t mixed_batch_smem(const Device& D, int variant);
+const void* mixed_batch_kernel(int variant);
 
 }  // namespace fgw

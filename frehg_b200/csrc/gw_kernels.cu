@@ -181,10 +181,11 @@ __global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
 // cell or out of the domain are stored as 0 (PETSc ignores column -1).
 __global__ void __launch_bounds__(kBlock, 2)
     k_assemble(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
-               const double* __restrict__ wcn, const double* __restrict__ ch, double dtg,
-               double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
+               const double* __restrict__ wcn, const double* __restrict__ ch,
+               const double* __restrict__ dtgp, double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
                double* __restrict__ gzps, double* __restrict__ rhs) {
   const double dx = d.dx, dy = d.dy;
+  const double dtg = *dtgp;
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
     int j, i, k;
@@ -485,8 +486,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
 __global__ void __launch_bounds__(kBlock, 4) k_update_wc(
     Dims d, Fields f, const double* __restrict__ hp, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ qx, const double* __restrict__ qy,
-    const double* __restrict__ qzf, double dtg, double* __restrict__ wcu,
+    const double* __restrict__ qzf, const double* __restrict__ dtgp, double* __restrict__ wcu,
     uint8_t* __restrict__ satf, double* partial) {
+  const double dtg = *dtgp;
   double acc = 0.0;
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -686,7 +688,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_classify(
 // ascending (Reallocate.cpp:410-540, uncoupled, no transport window).
 __global__ void k_walk_thread(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
                        const double* __restrict__ sdn, double* qzf, const int* __restrict__ colflag,
-                       double dtg, double* partial) {
+                       const double* __restrict__ dtgp, double* partial) {
+  const double dtg = *dtgp;
   double lost = 0.0;
   const long long ncolint = static_cast<long long>(d.nx) * d.ny;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < ncolint;
@@ -821,9 +824,11 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ room,
                                                  const double* __restrict__ sup,
                                                  const double* __restrict__ sdn, double* qzf,
-                                                 const int* __restrict__ colflag, double dtg,
+                                                 const int* __restrict__ colflag,
+                                                 const double* __restrict__ dtgp,
                                                  double* partial) {
   extern __shared__ __align__(16) unsigned char walk_smem[];
+  const double dtg = *dtgp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nz = d.nz, nw = walk_words(nz);
   double* rs = reinterpret_cast<double*>(walk_smem + warp * walk_warp_bytes(nz));
@@ -940,8 +945,9 @@ __global__ void __launch_bounds__(kBlock, 3) k_finalize(Dims d, Fields f, double
                                                         const double* __restrict__ qx,
                                                         const double* __restrict__ qy,
                                                         const double* __restrict__ qzf,
-                                                        double dtg, double co_max,
-                                                        double* partial, int nblk) {
+                                                        const double* __restrict__ dtgp,
+                                                        double co_max, double* partial, int nblk) {
+  const double dtg = *dtgp;
   double vl = 0.0, inflow = 0.0, dqmax = -DBL_MAX, dtco = DBL_MAX, vol = 0.0;
   for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -1069,7 +1075,9 @@ __device__ double reduce_slot(const double* p, int n, Op op, double identity) {
 // One block: combine the partials in block order into the step record and run
 // the controller (adaptTimeStep, AdaptiveStep.cpp:100-117; grow 1.25, shrink
 // 0.75, Courant cap, [dt_min, dt_max] clamp).
-__global__ void k_step_info(const double* partial, int nblk, int off, double dtg, double dq_grow,
+// The step's dtg is read from out->next_dt, where the step found it, and the
+// controller's next dt replaces it there.
+__global__ void k_step_info(const double* partial, int nblk, int off, double dq_grow,
                             double dq_shrink, double dt_min, double dt_max, StepOut* out) {
   const double ss = reduce_slot(partial + kPSs * nblk, nblk, SumOp(), 0.0);
   const double adj = reduce_slot(partial + kPAdj * nblk, nblk, SumOp(), 0.0);
@@ -1089,6 +1097,7 @@ __global__ void k_step_info(const double* partial, int nblk, int off, double dtg
     out->dqmax = dqmax;
     out->dtco = dtco;
     out->volume = vol;
+    const double dtg = out->next_dt;
     double next = dtg;
     if (dqmax > dq_shrink) next = dtg * 0.75;
     else if (dqmax < dq_grow) next = dtg * 1.25;
@@ -1107,6 +1116,11 @@ __global__ void k_volume_final(const double* partial, int nblk, StepOut* out) {
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
+// Kernels that need the step's dtg read it on the device from the step record
+// (see k_step_info), so a captured step replays with the dt the previous step
+// chose.
+inline const double* dtg_slot(const Device& D) { return &D.out->next_dt; }
+
 void launch_ghosts(const Device& D, double* h, double* wc) {
   const long long n = 2LL * (D.d.nx + D.d.ny) * D.d.nz;
   const int g = static_cast<int>(std::min<long long>((n + kBlock - 1) / kBlock, 4096));
@@ -1120,9 +1134,9 @@ void launch_closure_pred(const Device& D, const double* h) {
   ++D.launches;
 }
 
-void launch_assemble(const Device& D, const double* hn, const double* wcn, double dtg) {
+void launch_assemble(const Device& D, const double* hn, const double* wcn) {
   PassK pk{D.kcx, D.kcy, D.kcz, wcn};
-  k_assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, hn, wcn, D.ch, dtg, D.diag,
+  k_assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, hn, wcn, D.ch, dtg_slot(D), D.diag,
                                                      D.gxp, D.gyp, D.gzp, D.rhs);
   ++D.launches;
 }
@@ -1133,17 +1147,16 @@ void launch_closure_corr(const Device& D, const double* hn) {
   ++D.launches;
 }
 
-void launch_flux(const Device& D, const double* wcn, double dtg) {
-  (void)dtg;
+void launch_flux(const Device& D, const double* wcn) {
   PassK pk{D.kcx, D.kcy, D.kcz, wcn};
   k_flux<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.hp, wcn, D.kx, D.ky, D.kzf, D.qx,
                                                  D.qy, D.qzf);
   ++D.launches;
 }
 
-void launch_update_wc(const Device& D, const double* hn, const double* wcn, double dtg) {
+void launch_update_wc(const Device& D, const double* hn, const double* wcn) {
   k_update_wc<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.hp, hn, wcn, D.qx, D.qy, D.qzf,
-                                                      dtg, D.wcu, D.satf, D.partial + kPSs * D.nblk);
+                                                      dtg_slot(D), D.wcu, D.satf, D.partial + kPSs * D.nblk);
   ++D.launches;
 }
 
@@ -1159,30 +1172,30 @@ void launch_classify(const Device& D, double* wc_out, double* h_out) {
 // Columns deeper than the shared-memory staging allows take the per-thread walk.
 constexpr size_t kWalkSmemMax = 48 * 1024;
 
-void launch_walk(const Device& D, double* wc_out, double dtg) {
+void launch_walk(const Device& D, double* wc_out) {
   const size_t smem = kWalkWarps * walk_warp_bytes(D.d.nz);
   if (smem <= kWalkSmemMax) {
     k_walk<<<cells_grid(D), kBlock, smem, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
-                                                      D.qzf, D.colflag, dtg,
+                                                      D.qzf, D.colflag, dtg_slot(D),
                                                       D.partial + kPLost * D.nblk);
   } else {
     k_walk_thread<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
-                                                          D.qzf, D.colflag, dtg,
+                                                          D.qzf, D.colflag, dtg_slot(D),
                                                           D.partial + kPLost * D.nblk);
   }
   ++D.launches;
 }
 
-void launch_finalize(const Device& D, double* wc_out, double dtg, double co_max) {
+void launch_finalize(const Device& D, double* wc_out, double co_max) {
   k_finalize<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, wc_out, D.vloss, D.qx, D.qy,
-                                                     D.qzf, dtg, co_max, D.partial, D.nblk);
+                                                     D.qzf, dtg_slot(D), co_max, D.partial, D.nblk);
   ++D.launches;
 }
 
-void launch_step_info(const Device& D, double dtg, double dq_grow, double dq_shrink,
+void launch_step_info(const Device& D, double dq_grow, double dq_shrink,
                       double dt_min, double dt_max) {
-  k_step_info<<<1, kBlock, 0, D.stream>>>(D.partial, D.nblk, D.d.off, dtg, dq_grow, dq_shrink,
-                                          dt_min, dt_max, D.out);
+  k_step_info<<<1, kBlock, 0, D.stream>>>(D.partial, D.nblk, D.d.off, dq_grow, dq_shrink, dt_min,
+                                          dt_max, D.out);
   ++D.launches;
 }
 

@@ -12,6 +12,10 @@ workloads the step is measured on.
   lnKs Gaussian random field, per-cell van Genuchten parameters, water
   table 2 m below the surface, top flux 1e-6 m/s downward, dt0 = 60 s.
   Smaller sizes give parity crops of the same construction.
+* :func:`ensemble` — many independent homogeneous boxes of uneven size
+  (nx, ny ~ U{16..128}, nz ~ U{32..200}), per-member van Genuchten
+  parameters, lnKs ~ N(ln 1e-5, 1), initial head ~ U[-3, -0.2] m, ponded
+  head or flux 1e-6 m/s on top by a seeded coin, free drainage below.
 
 Choices the case descriptions leave open are fixed here and documented in
 the docstrings (dt_min / dt_max, bottom condition, theta_s / theta_r / Ss of
@@ -124,3 +128,49 @@ def hillslope(nx: int = 512, ny: int = 512, nz: int = 128, seed: int = 20261203,
         cell_soil=cfg_soil,
     )
     return cfg
+
+
+def ensemble_member(rng: np.random.Generator, precision: str = "fp64",
+                    nx_range=(16, 128), nz_range=(32, 200)) -> GwConfig:
+    """One member of :func:`ensemble` drawn from ``rng``.
+
+    Sizes nx, ny ~ U{16..128}, nz ~ U{32..200}; dx = dy = 1 m, dz = 0.02 m
+    (the box case's grid).  Soil: alpha ~ U[0.5, 3] 1/m, n ~ U[1.4, 2.5],
+    theta_s = 0.40, theta_r = 0.05 (the box case's), lnKs ~ N(ln 1e-5, 1)
+    with Ksx = Ksy = Ksz, Ss = 1e-5 1/m.  Initial head uniform in the member,
+    drawn from U[-3, -0.2] m.  Top: ponded head 0.01 m or flux 1e-6 m/s
+    downward by a fair coin; bottom free drainage; sides no-flux.  dt0 = 10 s,
+    dt_min = 1e-3 s, dt_max = 600 s.
+    """
+    nx = int(rng.integers(nx_range[0], nx_range[1] + 1))
+    ny = int(rng.integers(nx_range[0], nx_range[1] + 1))
+    nz = int(rng.integers(nz_range[0], nz_range[1] + 1))
+    ks = float(np.exp(np.log(1e-5) + rng.standard_normal()))
+    alpha = float(rng.uniform(0.5, 3.0))
+    vgn = float(rng.uniform(1.4, 2.5))
+    h0 = float(rng.uniform(-3.0, -0.2))
+    ponded = bool(rng.integers(0, 2))
+    soil = SoilType("member", ks, ks, ks, 0.40, 0.05, alpha, vgn, 0.0)
+    fp = whole_footprint(nx, ny)
+    top = (BoundaryCondition("ponded-top", fp, "groundwater_top", "head", "constant", 0.01)
+           if ponded else
+           BoundaryCondition("recharge-top", fp, "groundwater_top", "flux", "constant", -1e-6))
+    return GwConfig(
+        domain=Domain(nx=nx, ny=ny, nz=nz, dx=1.0, dy=1.0, dz=0.02, bottom_elevation=0.0),
+        soil_types=[soil],
+        groundwater=Groundwater(timestep=Timestep(dt_init=10.0, dt_min=1e-3, dt_max=600.0),
+                                specific_storage=1e-5),
+        initial=InitialCondition("head", h0),
+        solver=Solver(precision=precision),
+        boundary_conditions=[
+            top,
+            BoundaryCondition("free-drainage", fp, "groundwater_bottom", "flux", "gravity"),
+        ],
+    )
+
+
+def ensemble(n: int = 256, seed: int = 20261204, precision: str = "fp64",
+             nx_range=(16, 128), nz_range=(32, 200)) -> list:
+    """``n`` independent members (see :func:`ensemble_member`), seeded."""
+    rng = np.random.default_rng(seed)
+    return [ensemble_member(rng, precision, nx_range, nz_range) for _ in range(n)]

@@ -223,6 +223,65 @@ int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5);
 /* Kernels this handle has launched since creation. */
 long long frehg_gw_kernel_launches(const frehg_gw_handle* h);
 
+/* ---------------------------------------------------------------- batches
+ * Many independent domains stepped together: ensemble members, soil-parameter
+ * sweeps, hillslopes of uneven size.  No counterpart in the reference, whose
+ * driver steps one domain per rank; each member's step is exactly
+ * frehg_gw_step's, with the member's own dt.
+ *
+ * A batch is a view over existing handles (it neither owns nor destroys
+ * them).  One batch step runs the non-solve phases of all members on
+ * concurrent streams and their predictor solves in one cooperative launch per
+ * kernel class, each member on its own block range with its own CG state and
+ * barrier (a member's blocks leave when its solve converges).  The step is
+ * captured once as a CUDA graph per pattern of the members' state parities
+ * and replayed.  A member's block counts depend on its own size and the
+ * options only, so its results do not depend on the other members.  Member
+ * handles stay usable between batch steps (boundary values, fields, state);
+ * a batch must not step while its members are stepped on their own. */
+typedef struct frehg_gw_batch frehg_gw_batch;
+
+typedef struct {
+  int cells_per_block;  /* active cells per solve block of a member; 0 = 65536 */
+  int tiled_line_solve; /* mixed form: 1 = shared-memory tiled line solve at every depth */
+  int use_graph;        /* 1 = replay each step as a CUDA graph, 0 = launch directly */
+  int streams;          /* concurrent streams for the non-solve phases; 0 = 32 */
+} frehg_gw_batch_opts;
+
+typedef struct {
+  int members;
+  int solve_launches;       /* cooperative solve launches per step */
+  int solve_blocks;         /* their blocks in total */
+  int graphs;               /* captured step graphs */
+  int uses_graph;           /* 0 once a capture failed (steps then launch directly) */
+  long long steps;          /* batch steps since creation or the last autotune */
+  long long kernel_launches;/* kernels those steps ran */
+  long long kernels_per_step;
+  int cells_per_block;
+  int tiled_line_solve;
+} frehg_gw_batch_stats_t;
+
+/* Batch over n members (each initialised); opts may be NULL (defaults,
+ * graphs on). */
+int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
+                          const frehg_gw_batch_opts* opts, frehg_gw_batch** out);
+int frehg_gw_batch_destroy(frehg_gw_batch* b);
+/* One step of every member with its own next dt (frehg_gw_next_dt, or the
+ * value set by frehg_gw_batch_set_dt); infos receives n step records.  A
+ * failing member does not advance; the first failure is returned. */
+int frehg_gw_batch_step(frehg_gw_batch* b, frehg_gw_step_info* infos);
+/* Overrides member i's dt for the next batch step (e.g. to end on a time). */
+int frehg_gw_batch_set_dt(frehg_gw_batch* b, int i, double dtg);
+/* Times candidate decompositions (solve blocks per member, and for the mixed
+ * form the column or tiled line solve) on trial steps from a snapshot of the
+ * members' state, restores that state and keeps the fastest; results are
+ * cached per batch shape for the process.  best_ms is -1 on a cache hit. */
+int frehg_gw_batch_autotune(frehg_gw_batch* b, int trials, frehg_gw_batch_opts* chosen,
+                            double* best_ms);
+int frehg_gw_batch_stats(const frehg_gw_batch* b, frehg_gw_batch_stats_t* out);
+/* Solve blocks of each member (n ints). */
+int frehg_gw_batch_solve_blocks(const frehg_gw_batch* b, int* nb);
+
 #ifdef __cplusplus
 }
 #endif

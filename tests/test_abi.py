@@ -60,3 +60,15 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert lib.frehg_gw_create(None, None) == 1  # FREHG_GW_EINVAL
     lib.frehg_gw_last_error.restype = ctypes.c_char_p
     assert b"null" in lib.frehg_gw_last_error()
+
+
+def test_batch_create_rejects_bad_arguments_without_a_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("libfrehg_gw.so not built")
+    lib = ctypes.CDLL(LIB)
+    lib.frehg_gw_batch_create.restype = ctypes.c_int
+    out = ctypes.c_void_p()
+    assert lib.frehg_gw_batch_create(None, 0, None, ctypes.byref(out)) == 1  # FREHG_GW_EINVAL
+    members = (ctypes.c_void_p * 1)(None)
+    assert lib.frehg_gw_batch_create(members, 1, None, ctypes.byref(out)) == 1
+    assert out.value is None
