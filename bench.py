@@ -69,6 +69,12 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-sample", default="64,64,128")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="slab", choices=["slab", "ensemble"],
+                   help="slab: the 512x512x128 headline; ensemble: many uneven domains "
+                        "stepped as one batch (prints its own line)")
+    p.add_argument("--members", type=int, default=256)
+    p.add_argument("--seq-steps", type=int, default=3,
+                   help="ensemble: steps of the member-by-member comparison loop")
     return p.parse_args()
 
 
@@ -261,6 +267,86 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
     return out
 
 
+def run_ensemble(args, rank, world):
+    """Many uneven domains stepped as one batch (frehg_gw_batch_*), each form.
+
+    The members (``workloads.ensemble``: nx, ny ~ U{16..128}, nz ~ U{32..200},
+    per-member soil, seeded) are stepped with their own adaptive dt; the batch
+    is autotuned first (trial steps from a snapshot, state restored), then
+    ``--warmup`` steps, then ``--steps`` timed steps, each ending with the
+    batch's host synchronisation, so wall time is device time plus the host's
+    step records.  For comparison the same members are then stepped one after
+    another through frehg_gw_step for ``--seq-steps`` steps.  Under torchrun
+    every rank steps its own ensemble (seed + rank); no collective.
+    """
+    import torch
+
+    from frehg_b200 import workloads
+    from frehg_b200.batch import RichardsBatch
+    from frehg_b200.gw import RichardsSolver
+
+    forms = {}
+    for prec in ("mixed", "fp64"):
+        cfgs = workloads.ensemble(args.members, seed=20261204 + rank, precision=prec)
+        solvers = [RichardsSolver(c) for c in cfgs]
+        cells = float(sum(s.activeCells() for s in solvers))
+        batch = RichardsBatch(solvers)
+        tuned, tune_ms = batch.autotune(trials=1)
+        for _ in range(args.warmup):
+            batch.step()
+        st0 = batch.stats()
+        torch.cuda.synchronize()
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+            t0 = time.perf_counter()
+            iters = 0
+            for _ in range(args.steps):
+                infos = batch.step()
+                iters += sum(i["cg_iterations"] for i in infos)
+            sec = time.perf_counter() - t0
+        st = batch.stats()
+        batch.close()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(args.seq_steps):
+            for s in solvers:
+                s.advance()
+        seq_sec = time.perf_counter() - t1
+        for s in solvers:
+            s.close()
+        forms[prec] = {
+            "value": cells * args.steps / sec, "ms_per_step": 1e3 * sec / args.steps,
+            "members": len(cfgs), "active_cells": cells,
+            "solve_iterations_per_member_step": iters / (args.steps * len(cfgs)),
+            "kernels_per_step": st["kernels_per_step"],
+            "kernel_launches": st["kernel_launches"] - st0["kernel_launches"],
+            "solve_launches_per_step": st["solve_launches"], "solve_blocks": st["solve_blocks"],
+            "graph_replay": bool(st["uses_graph"]), "autotuned": tuned,
+            "autotune_best_step_ms": tune_ms, "clocks": clocks.summary(),
+            "member_by_member": {"value": cells * args.seq_steps / seq_sec,
+                                 "ms_per_step": 1e3 * seq_sec / args.seq_steps,
+                                 "steps": args.seq_steps},
+            "batch_over_member_by_member": (cells * args.steps / sec) /
+                                           (cells * args.seq_steps / seq_sec),
+        }
+    if rank != 0:
+        return
+    line = {
+        "metric": "cell-steps/s, ensemble of uneven domains stepped as one batch",
+        "value": forms["mixed"]["value"], "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": forms["mixed"]["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32-inner/f64", "data": "synthetic",
+        "config": {"workload": f"{args.members} independent boxes, nx,ny U{{16..128}}, "
+                               "nz U{32..200}, per-member van Genuchten + lnKs ~ N(ln 1e-5, 1), "
+                               "head0 U[-3,-0.2], ponded head or 1e-6 m/s flux top, "
+                               "own adaptive dt each",
+                   "parallelism": f"replicas x{world}"},
+        "forms": forms,
+        "mixed_over_fp64": forms["mixed"]["value"] / forms["fp64"]["value"],
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -273,6 +359,9 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
+    if args.workload == "ensemble":
+        run_ensemble(args, rank, world)
+        return
     dist = None
     if world > 1:
         import datetime

@@ -76,8 +76,7 @@ SolveClass solve_class(const Device& D, int precision, bool tiled_line_solve) {
 
 int solve_blocks_per_sm(const SolveClass& c, size_t smem) {
   const void* k = batch_kernel(c);
-  if (smem > 0) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem));
+  if (smem > 0) raise_smem_limit(k, smem);
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, coop::kCgBlock, smem) !=
       cudaSuccess)
@@ -119,8 +118,7 @@ cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vec
   if (e == cudaSuccess)
     e = cudaMemcpy(g.states, st.data(), st.size() * sizeof(CgState*), cudaMemcpyHostToDevice);
   if (e == cudaSuccess && g.smem > 0)
-    e = cudaFuncSetAttribute(batch_kernel(c), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(g.smem));
+    e = raise_smem_limit(batch_kernel(c), g.smem);
   return e;
 }
 

@@ -712,8 +712,8 @@ int cg32_grid(int sm_count, long long ncell) {
 cudaError_t launch_line_factor(Device& D) {
   const int nz = D.d.nz;
   const size_t fsm = factor_smem(nz);
-  cudaFuncSetAttribute(k_line_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(fsm));
+  const cudaError_t ea = raise_smem_limit(reinterpret_cast<const void*>(k_line_factor), fsm);
+  if (ea != cudaSuccess) return ea;
   const int tc = host_tile_cols(nz);
   const long long ntiles = (D.d.ncol + tc - 1) / tc;
   const int fgrid = static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));
@@ -741,7 +741,7 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
   const void* kern = reinterpret_cast<const void*>(table[vec ? 1 : 0][slot]);
   const size_t ksm = wcol ? 0 : msm;
   if (!wcol)
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(msm));
+    raise_smem_limit(kern, msm);
   const int tc = host_tile_cols(nz);
   const long long ntiles = (D.d.ncol + tc - 1) / tc;
   int per_sm = 0;

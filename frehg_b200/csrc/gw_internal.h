@@ -125,6 +125,11 @@ cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, doub
                             int max_outer);
 int cg64_grid(int sm_count, long long ncell);
 
+// Raises (never lowers) a kernel's opt-in dynamic shared-memory limit to
+// `bytes`.  Only raising keeps every launch recorded earlier (in a captured
+// graph, or by another domain) within the limit.
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
+
 // ---------------------------------------------------------------- batched solves
 // Several domains' predictor solves in one cooperative launch: member i runs
 // its own solve (own CG state, reductions and barrier) on the block range

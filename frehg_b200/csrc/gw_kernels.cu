@@ -13,6 +13,8 @@
 // k_step_info combines the partials in block order, so a step's audit is
 // bit-reproducible run to run.
 #include <cfloat>
+#include <map>
+#include <mutex>
 
 #include "gw_internal.h"
 
@@ -1116,6 +1118,18 @@ __global__ void k_volume_final(const double* partial, int nblk, StepOut* out) {
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<const void*, size_t> limit;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limit[kernel];
+  if (bytes <= cur) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(bytes));
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
+
 // Kernels that need the step's dtg read it on the device from the step record
 // (see k_step_info), so a captured step replays with the dt the previous step
 // chose.
@@ -1169,12 +1183,15 @@ void launch_classify(const Device& D, double* wc_out, double* h_out) {
   ++D.launches;
 }
 
-// Columns deeper than the shared-memory staging allows take the per-thread walk.
-constexpr size_t kWalkSmemMax = 48 * 1024;
+// Columns up to kWalkMaxNz cells take the warp walk (dynamic shared memory
+// opted in up to kWalkSmemMax); deeper columns take the per-thread walk.
+constexpr int kWalkMaxNz = 256;
+constexpr size_t kWalkSmemMax = 96 * 1024;
 
 void launch_walk(const Device& D, double* wc_out) {
   const size_t smem = kWalkWarps * walk_warp_bytes(D.d.nz);
-  if (smem <= kWalkSmemMax) {
+  if (D.d.nz <= kWalkMaxNz && smem <= kWalkSmemMax &&
+      raise_smem_limit(reinterpret_cast<const void*>(k_walk), smem) == cudaSuccess) {
     k_walk<<<cells_grid(D), kBlock, smem, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
                                                       D.qzf, D.colflag, dtg_slot(D),
                                                       D.partial + kPLost * D.nblk);

@@ -30,7 +30,7 @@ def rel_linf(a, b):
 
 def mix_configs():
     """Members of uneven size, both precisions, odd and even depths,
-    column-solve depths 20..130 and the tiled depth 300."""
+    column-solve depths 20..190 and the tiled depth 300."""
     out = []
     c = workloads.column_32x32x50(nx=6, ny=5, nz=20)
     out.append(c)
@@ -43,6 +43,7 @@ def mix_configs():
     out.append(c)
     c = cases.SCENARIOS["sand_clay_redistribute"]()
     out.append(c)
+    out.append(workloads.column_32x32x50(nx=3, ny=3, nz=190, precision="mixed"))
     return out
 
 

@@ -95,6 +95,13 @@ def test_hillslope_crop_parity():
     compare(workloads.hillslope(24, 20, 32), 4)
 
 
+def test_deep_columns_parity():
+    # 190 cells: the deepest column whose warp walk needs more than the
+    # default 48 KB of shared memory per block; 257: the per-thread walk.
+    compare(workloads.column_32x32x50(nx=3, ny=2, nz=190), 3)
+    compare(workloads.column_32x32x50(nx=2, ny=2, nz=257), 2)
+
+
 def test_step_is_deterministic():
     cfg = cases.mixed_box()
     runs = []
