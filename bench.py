@@ -26,6 +26,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -69,9 +71,12 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--cpu-sample", default="64,64,128")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="slab", choices=["slab", "ensemble"],
+    p.add_argument("--workload", default="slab", choices=["slab", "ensemble", "serve"],
                    help="slab: the 512x512x128 headline; ensemble: many uneven domains "
-                        "stepped as one batch (prints its own line)")
+                        "stepped as one batch; serve: a Poisson stream of mixed-size "
+                        "requests through the serving loop (each prints its own line)")
+    p.add_argument("--rates", default="10,100,1000", help="serve: arrival rates, req/s")
+    p.add_argument("--requests", type=int, default=64, help="serve: requests per rate")
     p.add_argument("--members", type=int, default=256)
     p.add_argument("--seq-steps", type=int, default=3,
                    help="ensemble: steps of the member-by-member comparison loop")
@@ -347,6 +352,66 @@ def run_ensemble(args, rank, world):
     print(json.dumps(line))
 
 
+def serve_requests(n, seed):
+    """``n`` requests: cells log-uniform in [1e4, 1e7], nz ~ U{32..200},
+    nx = ny from the cell count, soil and top condition drawn as for the
+    ensemble members, steps ~ U{20..200}; mixed precision."""
+    from frehg_b200 import workloads
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        cells = float(np.exp(rng.uniform(np.log(1e4), np.log(1e7))))
+        nz = int(rng.integers(32, 201))
+        side = max(2, int(round(np.sqrt(cells / nz))))
+        cfg = workloads.ensemble_member(rng, "mixed", (side, side), (nz, nz))
+        out.append((cfg, int(rng.integers(20, 201))))
+    return out
+
+
+def run_serve(args, rank, world):
+    """A Poisson stream of mixed-size requests through frehg_gw_server_*.
+
+    For each arrival rate, ``--requests`` requests (see serve_requests) are
+    prepared on the host first, then submitted at seeded exponential
+    inter-arrival times while the server ticks (admit by free device memory
+    and slots, one batch step of everything admitted, retire); latency is
+    submission to completion.  Under torchrun every rank serves its own
+    stream; no collective.
+    """
+    from frehg_b200.serve import PreparedRequest, RichardsServer, run_stream
+
+    rates = [float(r) for r in args.rates.split(",")]
+    reqs = [PreparedRequest(c, n) for c, n in serve_requests(args.requests, 20261205 + rank)]
+    work = sum(r.nx * r.ny * r.nz * r.steps for r in reqs)
+    per_rate = {}
+    for rate in rates:
+        rng = np.random.default_rng(7 + rank)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+            with RichardsServer() as srv:
+                res = run_stream(srv, reqs, arrivals)
+        res["clocks"] = clocks.summary()
+        res["arrival_span_s"] = float(arrivals[-1])
+        per_rate[str(int(rate) if rate.is_integer() else rate)] = res
+    if rank != 0:
+        return
+    best = max(per_rate.values(), key=lambda r: r["cell_steps_per_s"])
+    line = {
+        "metric": "served stream: cell-steps/s with p50/p99 request latency",
+        "value": best["cell_steps_per_s"], "unit": "cell-steps/s", "n_gpus": world,
+        "steps": None, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-inner/f64", "data": "synthetic",
+        "config": {"workload": f"{args.requests} requests per rate, cells log-uniform 1e4-1e7, "
+                               "nz U{32..200}, 20-200 adaptive steps each, mixed precision, "
+                               "Poisson arrivals",
+                   "rates_req_per_s": rates, "requested_cell_steps": int(work),
+                   "parallelism": f"replicas x{world}"},
+        "per_rate": per_rate,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -361,6 +426,9 @@ def main():
     torch.cuda.set_device(local)
     if args.workload == "ensemble":
         run_ensemble(args, rank, world)
+        return
+    if args.workload == "serve":
+        run_serve(args, rank, world)
         return
     dist = None
     if world > 1:

@@ -46,15 +46,23 @@ using fgw_api::fail;
     if (e_ != cudaSuccess) return cuda_fail(e_, what); \
   } while (0)
 
+// Every device array of a domain is a 256-byte-aligned slice of one arena
+// allocation: create runs its allocation sequence twice, first to size the
+// arena (plan), then to hand out the slices.  One allocation avoids the
+// page rounding of many mid-sized ones and makes the footprint
+// frehg_gw_device_bytes reports exact up to that alignment.
 template <class T>
 cudaError_t dalloc(fgw::Device& D, T** p, size_t n) {
-  void* raw = nullptr;
-  cudaError_t e = cudaMalloc(&raw, (n ? n : 1) * sizeof(T));
-  if (e != cudaSuccess) return e;
-  D.allocs.push_back(raw);
-  e = cudaMemset(raw, 0, (n ? n : 1) * sizeof(T));
-  *p = static_cast<T*>(raw);
-  return e;
+  const size_t bytes = ((n ? n : 1) * sizeof(T) + 255) & ~static_cast<size_t>(255);
+  if (D.arena_plan) {
+    D.arena_bytes += bytes;
+    *p = nullptr;
+    return cudaSuccess;
+  }
+  if (!D.arena || D.arena_off + bytes > D.arena_bytes) return cudaErrorMemoryAllocation;
+  *p = reinterpret_cast<T*>(D.arena + D.arena_off);
+  D.arena_off += bytes;
+  return cudaSuccess;
 }
 
 // Solver arrays carry a zero margin of one j-row on both ends.
@@ -62,7 +70,7 @@ template <class T>
 cudaError_t dalloc_margin(fgw::Device& D, T** p, long long ncell, long long margin) {
   T* base = nullptr;
   cudaError_t e = dalloc(D, &base, static_cast<size_t>(ncell + 2 * margin));
-  *p = base + margin;
+  *p = base ? base + margin : nullptr;
   return e;
 }
 
@@ -128,85 +136,93 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     d.redistribute = desc->surplus_redistribute ? 1 : 0;
     d.terrain = desc->follow_terrain ? 1 : 0;
 
-    const long long n3 = d.ncell, nf = d.ncol * (d.nz + 1), m = d.sy;
-    auto up = [&](double** p, const std::vector<double>& v) -> cudaError_t {
-      cudaError_t e = dalloc(D, p, v.size());
-      if (e != cudaSuccess) return e;
-      return cudaMemcpy(*p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
-    };
-    cudaError_t e = cudaSuccess;
-    double** soil[8] = {&D.ksx, &D.ksy, &D.ksz, &D.vga, &D.vgn, &D.wcs, &D.wcr, &D.aev};
-    for (int f = 0; f < 8 && e == cudaSuccess; ++f) e = up(soil[f], H.soil[f]);
-    if (e == cudaSuccess) e = up(&D.dz, H.dz);
-    if (e == cudaSuccess) e = up(&D.bot, H.bot);
-    if (e == cudaSuccess) e = up(&D.ax, H.ax);
-    if (e == cudaSuccess) e = up(&D.ay, H.ay);
-    if (e == cudaSuccess) e = up(&D.sinx, H.sinx);
-    if (e == cudaSuccess) e = up(&D.cosx, H.cosx);
-    if (e == cudaSuccess) e = up(&D.siny, H.siny);
-    if (e == cudaSuccess) e = up(&D.cosy, H.cosy);
-    if (e == cudaSuccess) e = up(&hnd->bath_dev, H.bath);
-    if (e == cudaSuccess) e = dalloc(D, &D.act, static_cast<size_t>(n3));
-    if (e == cudaSuccess)
-      e = cudaMemcpy(D.act, H.act.data(), static_cast<size_t>(n3), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = dalloc(D, &D.codes, 6 * static_cast<size_t>(d.ncol));
-    if (e == cudaSuccess)
-      e = cudaMemcpy(D.codes, H.codes.data(), H.codes.size() * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = dalloc(D, &D.values, 6 * static_cast<size_t>(d.ncol));
-    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-      e = dalloc(D, &D.h[b], n3);
-      if (e == cudaSuccess) e = dalloc(D, &D.wc[b], n3);
-    }
-    double** cellf[] = {&D.hp, &D.wcu, &D.ch, &D.kcx, &D.kcy, &D.kcz, &D.kx, &D.ky, &D.qx, &D.qy,
-                        &D.vloss, &D.room, &D.sup, &D.sdn};
-    for (double** p : cellf)
-      if (e == cudaSuccess) e = dalloc(D, p, n3);
-    if (e == cudaSuccess) e = dalloc(D, &D.kzf, nf);
-    if (e == cudaSuccess) e = dalloc(D, &D.qzf, nf);
-    if (e == cudaSuccess) e = dalloc(D, &D.colflag, d.ncol);
-    if (e == cudaSuccess) e = dalloc(D, &D.satf, n3);
-    double** solv[] = {&D.diag, &D.gxp, &D.gyp, &D.gzp, &D.rhs, &D.x, &D.r, &D.z, &D.p0, &D.p1, &D.w};
-    for (double** p : solv)
-      if (e == cudaSuccess) e = dalloc_margin(D, p, n3, m);
-    if (desc->precision == FREHG_GW_PRECISION_MIXED) {
-      float** solv32[] = {&D.diag32, &D.gxp32, &D.gyp32, &D.gzp32, &D.dinv32, &D.l32,
-                          &D.r32,    &D.z32,   &D.d32,   &D.p032,  &D.p132, &D.w32};
-      for (float** p : solv32)
+    // Allocation sequence, run twice (see dalloc): plan, then slices.
+    auto allocate = [&]() -> cudaError_t {
+      const long long n3 = d.ncell, nf = d.ncol * (d.nz + 1), m = d.sy;
+      auto up = [&](double** p, const std::vector<double>& v) -> cudaError_t {
+        cudaError_t e = dalloc(D, p, v.size());
+        if (e != cudaSuccess || D.arena_plan) return e;
+        return cudaMemcpy(*p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
+      };
+      cudaError_t e = cudaSuccess;
+      double** soil[8] = {&D.ksx, &D.ksy, &D.ksz, &D.vga, &D.vgn, &D.wcs, &D.wcr, &D.aev};
+      for (int f = 0; f < 8 && e == cudaSuccess; ++f) e = up(soil[f], H.soil[f]);
+      if (e == cudaSuccess) e = up(&D.dz, H.dz);
+      if (e == cudaSuccess) e = up(&D.bot, H.bot);
+      if (e == cudaSuccess) e = up(&D.ax, H.ax);
+      if (e == cudaSuccess) e = up(&D.ay, H.ay);
+      if (e == cudaSuccess) e = up(&D.sinx, H.sinx);
+      if (e == cudaSuccess) e = up(&D.cosx, H.cosx);
+      if (e == cudaSuccess) e = up(&D.siny, H.siny);
+      if (e == cudaSuccess) e = up(&D.cosy, H.cosy);
+      if (e == cudaSuccess) e = up(&hnd->bath_dev, H.bath);
+      if (e == cudaSuccess) e = dalloc(D, &D.act, static_cast<size_t>(n3));
+      if (e == cudaSuccess && !D.arena_plan)
+        e = cudaMemcpy(D.act, H.act.data(), static_cast<size_t>(n3), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = dalloc(D, &D.codes, 6 * static_cast<size_t>(d.ncol));
+      if (e == cudaSuccess && !D.arena_plan)
+        e = cudaMemcpy(D.codes, H.codes.data(), H.codes.size() * sizeof(int), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = dalloc(D, &D.values, 6 * static_cast<size_t>(d.ncol));
+      for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+        e = dalloc(D, &D.h[b], n3);
+        if (e == cudaSuccess) e = dalloc(D, &D.wc[b], n3);
+      }
+      double** cellf[] = {&D.hp, &D.wcu, &D.ch, &D.kcx, &D.kcy, &D.kcz, &D.kx, &D.ky, &D.qx, &D.qy,
+                          &D.vloss, &D.room, &D.sup, &D.sdn};
+      for (double** p : cellf)
+        if (e == cudaSuccess) e = dalloc(D, p, n3);
+      if (e == cudaSuccess) e = dalloc(D, &D.kzf, nf);
+      if (e == cudaSuccess) e = dalloc(D, &D.qzf, nf);
+      if (e == cudaSuccess) e = dalloc(D, &D.colflag, d.ncol);
+      if (e == cudaSuccess) e = dalloc(D, &D.satf, n3);
+      double** solv[] = {&D.diag, &D.gxp, &D.gyp, &D.gzp, &D.rhs, &D.x, &D.r, &D.z, &D.p0, &D.p1, &D.w};
+      for (double** p : solv)
         if (e == cudaSuccess) e = dalloc_margin(D, p, n3, m);
-      if (e == cudaSuccess) e = dalloc_margin(D, &D.xalt, n3, m);
+      if (desc->precision == FREHG_GW_PRECISION_MIXED) {
+        float** solv32[] = {&D.diag32, &D.gxp32, &D.gyp32, &D.gzp32, &D.dinv32, &D.l32,
+                            &D.r32,    &D.z32,   &D.d32,   &D.p032,  &D.p132, &D.w32};
+        for (float** p : solv32)
+          if (e == cudaSuccess) e = dalloc_margin(D, p, n3, m);
+        if (e == cudaSuccess) e = dalloc_margin(D, &D.xalt, n3, m);
+      }
+      // Diagonal 1 everywhere outside the active rows (ghosts, margins), so the
+      // Jacobi scaling of those always-zero entries stays finite.
+      if (e == cudaSuccess && !D.arena_plan) {
+        std::vector<double> ones(static_cast<size_t>(n3 + 2 * m), 1.0);
+        e = cudaMemcpy(D.diag - m, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && D.diag32) {
+          std::vector<float> onesf(ones.size(), 1.0f);
+          e = cudaMemcpy(D.diag32 - m, onesf.data(), onesf.size() * sizeof(float),
+                         cudaMemcpyHostToDevice);
+        }
+      }
+      D.nblk = static_cast<int>(std::min<long long>((n3 + fgw::kBlock - 1) / fgw::kBlock,
+                                                    static_cast<long long>(D.sm_count) * 8));
+      if (D.nblk < 1) D.nblk = 1;
+      D.cg_grid = fgw::cg64_grid(D.sm_count, n3);
+      D.cg_grid32 = D.sm_count * 4;
+      if (e == cudaSuccess)
+        e = dalloc(D, &D.partial, static_cast<size_t>(fgw::kPSlots) * D.nblk);
+      if (e == cudaSuccess)
+        e = dalloc(D, &D.cgpart, 4 * static_cast<size_t>(std::max(D.cg_grid, D.cg_grid32)));
+      if (e == cudaSuccess) e = dalloc(D, &D.out, 1);
+      return e;
+    };
+    D.arena_plan = true;
+    cudaError_t e = allocate();
+    D.arena_plan = false;
+    if (e == cudaSuccess) e = cudaMalloc(&D.arena, D.arena_bytes);
+    if (e == cudaSuccess) {
+      D.allocs.push_back(D.arena);
+      e = cudaMemset(D.arena, 0, D.arena_bytes);
     }
+    if (e == cudaSuccess) e = allocate();
+    if (e == cudaSuccess) e = cudaMallocHost(&D.out_host, sizeof(fgw::StepOut));
     if (e != cudaSuccess) {
       free_device(D);
       delete hnd;
       return fail(e == cudaErrorMemoryAllocation ? FREHG_GW_ENOMEM : FREHG_GW_ECUDA,
                   std::string("frehg_gw_create: ") + cudaGetErrorString(e));
-    }
-    // Diagonal 1 everywhere outside the active rows (ghosts, margins), so the
-    // Jacobi scaling of those always-zero entries stays finite.
-    {
-      std::vector<double> ones(static_cast<size_t>(n3 + 2 * m), 1.0);
-      e = cudaMemcpy(D.diag - m, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice);
-      if (e == cudaSuccess && D.diag32) {
-        std::vector<float> onesf(ones.size(), 1.0f);
-        e = cudaMemcpy(D.diag32 - m, onesf.data(), onesf.size() * sizeof(float),
-                       cudaMemcpyHostToDevice);
-      }
-    }
-    D.nblk = static_cast<int>(std::min<long long>((n3 + fgw::kBlock - 1) / fgw::kBlock,
-                                                  static_cast<long long>(D.sm_count) * 8));
-    if (D.nblk < 1) D.nblk = 1;
-    D.cg_grid = fgw::cg64_grid(D.sm_count, n3);
-    D.cg_grid32 = D.sm_count * 4;
-    if (e == cudaSuccess)
-      e = dalloc(D, &D.partial, static_cast<size_t>(fgw::kPSlots) * D.nblk);
-    if (e == cudaSuccess)
-      e = dalloc(D, &D.cgpart, 4 * static_cast<size_t>(std::max(D.cg_grid, D.cg_grid32)));
-    if (e == cudaSuccess) e = dalloc(D, &D.out, 1);
-    if (e == cudaSuccess) e = cudaMallocHost(&D.out_host, sizeof(fgw::StepOut));
-    if (e != cudaSuccess) {
-      free_device(D);
-      delete hnd;
-      return fail(FREHG_GW_ECUDA, std::string("frehg_gw_create: ") + cudaGetErrorString(e));
     }
 
     fgw::Fields& f = D.f;

@@ -94,6 +94,9 @@ struct Device {
   StepOut* out = nullptr;      // device
   StepOut* out_host = nullptr; // pinned
   std::vector<void*> allocs;   // everything to cudaFree
+  char* arena = nullptr;       // the one allocation every device array slices
+  size_t arena_bytes = 0, arena_off = 0;
+  bool arena_plan = false;     // sizing pass of the allocation sequence
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int sm_count = 0;

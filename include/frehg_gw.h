@@ -282,6 +282,80 @@ int frehg_gw_batch_stats(const frehg_gw_batch* b, frehg_gw_batch_stats_t* out);
 /* Solve blocks of each member (n ints). */
 int frehg_gw_batch_solve_blocks(const frehg_gw_batch* b, int* nb);
 
+/* Device memory frehg_gw_create allocates for this descriptor (an upper
+ * estimate including allocation rounding); no counterpart in the reference. */
+size_t frehg_gw_device_bytes(const frehg_gw_desc* desc);
+
+/* ---------------------------------------------------------------- serving
+ * A request loop for Richards solves of mixed sizes (no counterpart in the
+ * reference).  Requests are copied at submission and queued; each tick
+ * admits queued requests in arrival order while the device-memory budget and
+ * the slot count allow (their fields and solver state then stay on the
+ * device), steps every admitted request once as one batch (each with its own
+ * adaptive dt; their work overlaps on the device), and retires finished
+ * requests (head and theta kept on the host, device state freed).  A
+ * request's result depends on its own inputs and the server options only, so
+ * it is the same alone and among others.  One host thread drives a server. */
+typedef struct frehg_gw_server frehg_gw_server;
+
+typedef struct {
+  size_t hbm_budget_bytes; /* device memory the server may hold; 0 = 90% of free memory */
+  int max_active;          /* slots: requests stepping at once; 0 = 64 */
+  int cells_per_block;     /* batch option (frehg_gw_batch_opts) */
+  int use_graph;           /* batch option; graphs are re-captured when the set changes */
+  int streams;             /* batch option */
+} frehg_gw_server_opts;
+
+typedef struct {
+  const frehg_gw_desc* desc;   /* the domain, as for frehg_gw_create */
+  int ic_form;                 /* FREHG_GW_IC_* */
+  double ic_constant;
+  const double* ic_field;      /* as for frehg_gw_init_state; NULL = the constant */
+  const double *bc_top, *bc_bottom, *bc_xm, *bc_xp, *bc_ym, *bc_yp; /* NULL = 0 */
+  int steps;                   /* adaptive steps to run */
+} frehg_gw_request;
+
+enum {
+  FREHG_GW_REQ_QUEUED = 0,
+  FREHG_GW_REQ_RUNNING = 1,
+  FREHG_GW_REQ_DONE = 2,
+  FREHG_GW_REQ_FAILED = 3
+};
+
+typedef struct {
+  int state;               /* FREHG_GW_REQ_* */
+  int status;              /* frehg_gw_status of a finished request */
+  int steps, steps_done;
+  long long cells;         /* active cells (0 until admitted) */
+  double sim_time;         /* simulated time reached */
+  double submit_s;         /* submission time, s since the server's creation */
+  double queue_s;          /* submission to admission, -1 while queued */
+  double latency_s;        /* submission to completion, -1 until finished */
+  frehg_gw_step_info last; /* the request's last step record */
+} frehg_gw_request_status;
+
+typedef struct {
+  int active, queued;
+  long long completed, ticks, cell_steps;
+  size_t device_bytes_used, device_bytes_budget;
+  double busy_s;           /* time spent inside frehg_gw_server_tick */
+  double now_s;            /* time since the server's creation */
+} frehg_gw_server_stats_t;
+
+int frehg_gw_server_create(const frehg_gw_server_opts* opts, frehg_gw_server** out);
+int frehg_gw_server_destroy(frehg_gw_server* s);
+/* Copies the request and queues it; *id identifies it from then on.
+ * FREHG_GW_ENOMEM when it can never fit the budget. */
+int frehg_gw_server_submit(frehg_gw_server* s, const frehg_gw_request* req, long long* id);
+/* Admit, step, retire (see above); returns the counts left running/queued. */
+int frehg_gw_server_tick(frehg_gw_server* s, int* active, int* queued);
+int frehg_gw_server_poll(frehg_gw_server* s, long long id, frehg_gw_request_status* st);
+/* A finished request's head or water content (FREHG_GW_FIELD_HEAD / _WC). */
+int frehg_gw_server_fetch(frehg_gw_server* s, long long id, int field, double* host_out);
+/* Forgets a finished request. */
+int frehg_gw_server_release(frehg_gw_server* s, long long id);
+int frehg_gw_server_stats(const frehg_gw_server* s, frehg_gw_server_stats_t* st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,3 +72,23 @@ def test_batch_create_rejects_bad_arguments_without_a_gpu():
     members = (ctypes.c_void_p * 1)(None)
     assert lib.frehg_gw_batch_create(members, 1, None, ctypes.byref(out)) == 1
     assert out.value is None
+
+
+def test_server_queues_and_rejects_oversized_requests_without_a_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("libfrehg_gw.so not built")
+    from frehg_b200 import workloads
+    from frehg_b200.gw import FatalError
+    from frehg_b200.serve import QUEUED, PreparedRequest, RichardsServer
+    req = PreparedRequest(workloads.column_32x32x50(nx=4, ny=4, nz=20), 3)
+    need = req.device_bytes()
+    assert need > 6 * 6 * 20 * 8 * 40  # at least 40 doubles per halo cell
+    with RichardsServer(hbm_budget_bytes=need - 1) as srv:
+        with pytest.raises(FatalError) as e:
+            srv.submit(req)
+        assert e.value.status == 3  # FREHG_GW_ENOMEM
+    with RichardsServer(hbm_budget_bytes=need * 4) as srv:
+        rid = srv.submit(req)
+        st = srv.poll(rid)
+        assert st["state"] == QUEUED and st["steps"] == 3 and st["queue_s"] == -1.0
+        assert srv.stats()["queued"] == 1
