@@ -2,11 +2,12 @@
 
 ``RichardsBatch`` is a view over existing :class:`frehg_b200.gw.RichardsSolver`
 objects: each batch step advances every member by its own adaptive dt, the
-way ``RichardsSolver.advance`` does, with the non-solve phases of all members
-on concurrent streams, their predictor solves in one cooperative launch per
-kernel class and the whole step replayed from a CUDA graph.  Members remain
-ordinary solvers between steps (boundary values, fields, state).  The
-reference has no counterpart: its driver steps one domain per rank.
+way ``RichardsSolver.advance`` does: each non-solve phase is one launch for
+all members (or, with ``per_member_phases``, member by member on concurrent
+streams), their predictor solves one cooperative launch per kernel class, and
+the whole step is replayed from a CUDA graph.  Members remain ordinary solvers
+between steps (boundary values, fields, state).  The reference has no
+counterpart: its driver steps one domain per rank.
 """
 from __future__ import annotations
 
@@ -19,14 +20,15 @@ from .gw import FatalError, RichardsSolver, load_library
 
 class BatchOpts(C.Structure):
     _fields_ = [("cells_per_block", C.c_int), ("tiled_line_solve", C.c_int),
-                ("use_graph", C.c_int), ("streams", C.c_int)]
+                ("use_graph", C.c_int), ("streams", C.c_int), ("per_member_phases", C.c_int)]
 
 
 class BatchStats(C.Structure):
     _fields_ = [("members", C.c_int), ("solve_launches", C.c_int), ("solve_blocks", C.c_int),
                 ("graphs", C.c_int), ("uses_graph", C.c_int), ("steps", C.c_longlong),
                 ("kernel_launches", C.c_longlong), ("kernels_per_step", C.c_longlong),
-                ("cells_per_block", C.c_int), ("tiled_line_solve", C.c_int)]
+                ("cells_per_block", C.c_int), ("tiled_line_solve", C.c_int),
+                ("phase_ms", C.c_double * 3)]
 
 
 def _declare(lib):
@@ -60,13 +62,14 @@ class RichardsBatch:
     """Steps the given solvers together; see the module docstring."""
 
     def __init__(self, solvers: Iterable[RichardsSolver], cells_per_block: int = 0,
-                 tiled_line_solve: bool = False, use_graph: bool = True, streams: int = 0):
+                 tiled_line_solve: bool = False, use_graph: bool = True, streams: int = 0,
+                 per_member_phases: bool = False):
         self.lib = _declare(load_library())
         self.members: List[RichardsSolver] = list(solvers)
         n = len(self.members)
         arr = (C.c_void_p * n)(*[s.h.value for s in self.members])
         opts = BatchOpts(int(cells_per_block), int(bool(tiled_line_solve)), int(bool(use_graph)),
-                         int(streams))
+                         int(streams), int(bool(per_member_phases)))
         b = C.c_void_p()
         _check(self.lib, self.lib.frehg_gw_batch_create(arr, n, C.byref(opts), C.byref(b)))
         self.b = b
@@ -120,7 +123,9 @@ class RichardsBatch:
     def stats(self) -> dict:
         st = BatchStats()
         _check(self.lib, self.lib.frehg_gw_batch_stats(self.b, C.byref(st)))
-        return {name: getattr(st, name) for name, _ in st._fields_}
+        out = {name: getattr(st, name) for name, _ in st._fields_}
+        out["phase_ms"] = list(st.phase_ms)
+        return out
 
     def solve_blocks(self) -> List[int]:
         n = len(self.members)

@@ -3,21 +3,25 @@
 // A batch is a view over existing handles.  One batch step runs every
 // member's step with the member's own dt:
 //
-//   fork:  per member, on a pool of streams, the dt upload, step-start ghost
-//          refresh, closure and assembly (and the mixed form's FP32 cast and
-//          line factorisation)
-//   join:  the predictor solves of all members in one cooperative launch per
+//   1.     the predictor phases of all members -- step-start ghost refresh,
+//          closure, assembly (and the mixed form's FP32 cast and line
+//          factorisation) -- one launch per phase, each member on its
+//          single-domain block count
+
+//   2.     the predictor solves of all members in one cooperative launch per
 //          kernel class (FP64 / mixed, column layout), each member on its own
 //          block range with its own CG state, reductions and barrier; a
 //          member's blocks leave as soon as its solve has converged
-//   fork:  per member, corrector, post-allocation, clamp, audit, controller
-//          and the read-back of its step record
-//   join:  one synchronisation for the whole batch
+//   3.     corrector, post-allocation, clamp, audit and controller of all
+//          members, one launch per phase, and one read-back of all step
+//          records; one synchronisation for the whole batch
 //
-// Every kernel takes its dt from the member's device step record, so the
-// whole step is captured once as a CUDA graph (per pattern of the members'
-// state-buffer parities) and replayed; the host only writes each member's dt
-// into pinned memory before a replay and reads the step records after it.
+// Each phase launch reads every member's arguments (state buffers of its
+// current parity, dt) from a table the host refreshes in pinned memory before
+// the step, so the whole step is captured once as a CUDA graph and replayed.
+// With per_member_phases the non-solve kernels are instead launched member by
+// member on a pool of streams (the members' dt then travels through their
+// device step records, and one graph is captured per pattern of parities).
 //
 // A member's block counts depend on its own size and the batch options only,
 // never on the other members, so a member's arithmetic (including the order
@@ -158,11 +162,14 @@ struct frehg_gw_batch {
   long long launches_per_step = 0;  // of the last step
   long long steps = 0;
   std::string graph_error;          // why graphs were given up, if they were
+  fgw::PhaseTables phases;          // batched non-solve phases
+  cudaEvent_t ev[4] = {};           // step start, after predictor, after solves, end
+  double phase_ms[3] = {0, 0, 0};   // of the last step
 };
 
 namespace {
 
-constexpr int kDefaultCellsPerBlock = 65536;
+constexpr int kDefaultCellsPerBlock = 16384;
 constexpr int kDefaultStreams = 32;
 
 void free_groups(frehg_gw_batch* b) {
@@ -242,9 +249,35 @@ int build_groups(frehg_gw_batch* b) {
   return FREHG_GW_OK;
 }
 
-// Enqueues one batch step on b->stream (under capture or not).  Counts the
-// kernels it launches into *kernels.
-cudaError_t enqueue_batch_step(frehg_gw_batch* b, long long* kernels) {
+// Enqueues one batch step with batched phases on b->stream (under capture
+// or not); the member records must be filled.  Counts kernels into *kernels.
+cudaError_t enqueue_batched_phases(frehg_gw_batch* b, long long* kernels) {
+  const fgw::PhaseTables& t = b->phases;
+  // Phase timing events only on direct launches (a graph replay does not
+  // time captured events).
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(b->stream, &cap);
+  const bool timed = cap == cudaStreamCaptureStatusNone;
+  auto mark = [&](int k) { return timed ? cudaEventRecord(b->ev[k], b->stream) : cudaSuccess; };
+  cudaError_t e = mark(0);
+  if (e == cudaSuccess) e = fgw::batch_predictor(t, b->stream);
+  if (e == cudaSuccess) e = mark(1);
+  long long k = 3 + (t.grid_factor > 0 ? 1 : 0);
+  for (const auto& g : b->groups) {
+    if (e != cudaSuccess) break;
+    e = fgw::solve_group_launch(g, b->stream);
+    k += 2;
+  }
+  if (e == cudaSuccess) e = mark(2);
+  if (e == cudaSuccess) e = fgw::batch_corrector(t, b->stream);
+  if (e == cudaSuccess) e = mark(3);
+  *kernels = k + 8;
+  return e;
+}
+
+// Enqueues one batch step, member by member, on b->stream and its pool
+// (under capture or not).  Counts the kernels it launches into *kernels.
+cudaError_t enqueue_member_phases(frehg_gw_batch* b, long long* kernels) {
   const int n = static_cast<int>(b->m.size());
   const int P = static_cast<int>(b->pool.size());
   long long before = 0;
@@ -291,6 +324,7 @@ cudaError_t enqueue_batch_step(frehg_gw_batch* b, long long* kernels) {
 }
 
 std::vector<unsigned char> parities(const frehg_gw_batch* b) {
+  if (!b->opts.per_member_phases) return {};  // one graph serves every parity pattern
   std::vector<unsigned char> k(b->m.size());
   for (size_t i = 0; i < b->m.size(); ++i) k[i] = static_cast<unsigned char>(b->m[i]->D.cur);
   return k;
@@ -298,7 +332,17 @@ std::vector<unsigned char> parities(const frehg_gw_batch* b) {
 
 // Runs one batch step (graph replay when possible) and waits for it.
 int run_step(frehg_gw_batch* b) {
-  for (auto* h : b->m) h->D.out_host->next_dt = h->next_dt;
+  const bool batched = !b->opts.per_member_phases;
+  auto enqueue = batched ? enqueue_batched_phases : enqueue_member_phases;
+  if (batched) {
+    for (size_t i = 0; i < b->m.size(); ++i) {
+      const frehg_gw_handle* h = b->m[i];
+      fgw::fill_step_args(h->D, h->precision == FREHG_GW_PRECISION_MIXED, h->next_dt, h->co_max,
+                          h->dq_grow, h->dq_shrink, h->dt_min, h->dt_max, b->phases.tab_host[i]);
+    }
+  } else {
+    for (auto* h : b->m) h->D.out_host->next_dt = h->next_dt;
+  }
   long long kernels = 0;
   cudaError_t e = cudaSuccess;
   bool ran = false;
@@ -310,7 +354,7 @@ int run_step(frehg_gw_batch* b) {
       cudaGraphExec_t exec = nullptr;
       e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
-        const cudaError_t ee = enqueue_batch_step(b, &kernels);
+        const cudaError_t ee = enqueue(b, &kernels);
         e = cudaStreamEndCapture(b->stream, &graph);
         if (ee != cudaSuccess) e = ee;
       }
@@ -334,7 +378,7 @@ int run_step(frehg_gw_batch* b) {
     }
   }
   if (!ran) {
-    e = enqueue_batch_step(b, &kernels);
+    e = enqueue(b, &kernels);
     if (e != cudaSuccess) return cuda_fail(e, "batch step");
     b->launches_per_step = kernels;
   }
@@ -342,6 +386,16 @@ int run_step(frehg_gw_batch* b) {
   if (e != cudaSuccess) return cuda_fail(e, "batch step");
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batch step kernels");
+  if (batched) {
+    for (size_t i = 0; i < b->m.size(); ++i) *b->m[i]->D.out_host = b->phases.outs_host[i];
+    if (!ran) {
+      for (int p = 0; p < 3; ++p) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, b->ev[p], b->ev[p + 1]) == cudaSuccess) b->phase_ms[p] = ms;
+        else cudaGetLastError();
+      }
+    }
+  }
   b->launches += kernels;
   ++b->steps;
   return FREHG_GW_OK;
@@ -438,10 +492,21 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join1[p], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join2[p], cudaEventDisableTiming);
   }
+  for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreate(&b->ev[k]);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork1, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork2, cudaEventDisableTiming);
   int rc = (e == cudaSuccess) ? FREHG_GW_OK : cuda_fail(e, "batch: streams");
   if (rc == FREHG_GW_OK) rc = build_groups(b);
+  if (rc == FREHG_GW_OK) {
+    std::vector<const fgw::Device*> ds;
+    std::vector<int> mixed;
+    for (auto* h : b->m) {
+      ds.push_back(&h->D);
+      mixed.push_back(h->precision == FREHG_GW_PRECISION_MIXED ? 1 : 0);
+    }
+    const cudaError_t ep = fgw::phase_tables_build(b->phases, ds, mixed);
+    if (ep != cudaSuccess) rc = cuda_fail(ep, "batch: phase tables");
+  }
   if (rc != FREHG_GW_OK) {
     frehg_gw_batch_destroy(b);
     return rc;
@@ -455,9 +520,11 @@ int frehg_gw_batch_destroy(frehg_gw_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graphs(b);
   free_groups(b);
+  fgw::phase_tables_free(b->phases);
   for (auto s : b->pool) if (s) cudaStreamDestroy(s);
   for (auto ev : b->join1) if (ev) cudaEventDestroy(ev);
   for (auto ev : b->join2) if (ev) cudaEventDestroy(ev);
+  for (auto ev : b->ev) if (ev) cudaEventDestroy(ev);
   if (b->fork1) cudaEventDestroy(b->fork1);
   if (b->fork2) cudaEventDestroy(b->fork2);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -513,7 +580,7 @@ int frehg_gw_batch_autotune(frehg_gw_batch* b, int trials, frehg_gw_batch_opts* 
   bool any_mixed_columns = false;
   for (auto* h : b->m)
     if (h->precision == FREHG_GW_PRECISION_MIXED && h->D.d.nz <= 256) any_mixed_columns = true;
-  const int cpbs[] = {16384, 32768, 65536, 131072, 262144};
+  const int cpbs[] = {4096, 8192, 16384, 32768, 65536, 131072};
   Snapshot snap;
   int rc = snapshot_take(b, snap);
   const frehg_gw_batch_opts start = b->opts;
@@ -573,6 +640,7 @@ int frehg_gw_batch_stats(const frehg_gw_batch* b, frehg_gw_batch_stats_t* out) {
   out->cells_per_block = b->opts.cells_per_block > 0 ? b->opts.cells_per_block
                                                      : kDefaultCellsPerBlock;
   out->tiled_line_solve = b->opts.tiled_line_solve;
+  for (int p = 0; p < 3; ++p) out->phase_ms[p] = b->phase_ms[p];
   return FREHG_GW_OK;
 }
 

@@ -46,19 +46,19 @@ constexpr int kTileCells = 4096;  // tc * nz <= kTileCells (2 x 16 KB of FP32 st
 
 // Cast the FP64 coefficients to FP32 and factor every column's tridiagonal
 // block T = LDL^T (pivots in FP64, stored as FP32 1/d_k and l_k).
-__global__ void __launch_bounds__(kFactorBlock) k_line_factor(Dims d, const double* __restrict__ diag,
+__device__ __forceinline__ void line_factor_body(Dims d, const double* __restrict__ diag,
                                                               const double* __restrict__ gxp,
                                                               const double* __restrict__ gyp,
                                                               const double* __restrict__ gzp,
                                                               float* diag32, float* gxp32,
                                                               float* gyp32, float* gzp32,
-                                                              float* dinv32, float* l32, int tc) {
+                                                              float* dinv32, float* l32, int tc, const int bid, const int G) {
   extern __shared__ double fsm[];
   const int nz = d.nz, nzp = nz + 1;
   double* s_a = fsm;
   double* s_e = fsm + static_cast<long long>(tc) * nzp;
   const long long ntiles = (d.ncol + tc - 1) / tc;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (long long t = bid; t < ntiles; t += G) {
     const long long base = t * tc * nz;
     const int ncols = static_cast<int>((d.ncol - t * tc) < tc ? (d.ncol - t * tc) : tc);
     const int ncells = ncols * nz;
@@ -98,6 +98,16 @@ __global__ void __launch_bounds__(kFactorBlock) k_line_factor(Dims d, const doub
     }
     __syncthreads();
   }
+}
+
+__global__ void __launch_bounds__(kFactorBlock) k_line_factor(Dims d, const double* __restrict__ diag,
+                                                              const double* __restrict__ gxp,
+                                                              const double* __restrict__ gyp,
+                                                              const double* __restrict__ gzp,
+                                                              float* diag32, float* gxp32,
+                                                              float* gyp32, float* gzp32,
+                                                              float* dinv32, float* l32, int tc) {
+  line_factor_body(d, diag, gxp, gyp, gzp, diag32, gxp32, gyp32, gzp32, dinv32, l32, tc, blockIdx.x, gridDim.x);
 }
 
 struct MixedArgs {
@@ -715,8 +725,7 @@ cudaError_t launch_line_factor(Device& D) {
   const cudaError_t ea = raise_smem_limit(reinterpret_cast<const void*>(k_line_factor), fsm);
   if (ea != cudaSuccess) return ea;
   const int tc = host_tile_cols(nz);
-  const long long ntiles = (D.d.ncol + tc - 1) / tc;
-  const int fgrid = static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));
+  const int fgrid = line_factor_blocks(D);
   k_line_factor<<<fgrid, kFactorBlock, fsm, D.stream>>>(D.d, D.diag, D.gxp, D.gyp, D.gzp,
                                                         D.diag32, D.gxp32, D.gyp32, D.gzp32,
                                                         D.dinv32, D.l32, tc);
@@ -799,6 +808,46 @@ const void* mixed_batch_kernel(int variant) {
   const int v = variant / 16, e = variant % 16;
   const int slot = e == 0 ? 0 : e == 1 ? 1 : e == 2 ? 2 : e == 4 ? 3 : 4;
   return reinterpret_cast<const void*>(table[v == 4 ? 1 : 0][slot]);
+}
+
+// ---------------------------------------------------------------- batched line factor
+namespace {
+
+__global__ void __launch_bounds__(kFactorBlock) k_line_factor_batch(const StepArgs* tab,
+                                                                    const int* first, int n) {
+  __shared__ StepArgs sa;
+  __shared__ int si;
+  if (threadIdx.x == 0) si = instance_of(first, n, blockIdx.x);
+  __syncthreads();
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(tab + si);
+  unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sa);
+  for (int w = threadIdx.x; w < static_cast<int>(sizeof(StepArgs) / 8); w += blockDim.x)
+    dst[w] = src[w];
+  const int bid = blockIdx.x - first[si], G = first[si + 1] - first[si];
+  __syncthreads();
+  line_factor_body(sa.d, sa.diag, sa.gxp, sa.gyp, sa.gzp, sa.diag32, sa.gxp32, sa.gyp32,
+                   sa.gzp32, sa.dinv32, sa.l32, sa.tc, bid, G);
+}
+
+}  // namespace
+
+int line_tile_cols(int nz) { return host_tile_cols(nz); }
+
+int line_factor_blocks(const Device& D) {
+  const int tc = host_tile_cols(D.d.nz);
+  const long long ntiles = (D.d.ncol + tc - 1) / tc;
+  return static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));
+}
+
+size_t line_factor_smem(int nz) { return factor_smem(nz); }
+
+cudaError_t launch_line_factor_batch(const PhaseTables& t, cudaStream_t s) {
+  const cudaError_t e =
+      raise_smem_limit(reinterpret_cast<const void*>(k_line_factor_batch), t.factor_smem);
+  if (e != cudaSuccess) return e;
+  k_line_factor_batch<<<t.grid_factor, kFactorBlock, t.factor_smem, s>>>(t.tab, t.first_factor,
+                                                                        t.n);
+  return cudaGetLastError();
 }
 
 }  // namespace fgw

@@ -133,6 +133,57 @@ int cg64_grid(int sm_count, long long ncell);
 // graph, or by another domain) within the limit.
 cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
 
+// ---------------------------------------------------------------- batched phases
+// One member's arguments for the batched non-solve phases: its geometry and
+// fields, the state buffers of its current parity, its dt and controller
+// constants, and its per-kernel block counts (the single-domain launch's, so
+// a member's arithmetic in a batch is the single-domain step's bit for bit).
+// The host refreshes the records before every batched step.
+struct alignas(16) StepArgs {
+  Dims d;
+  Fields f;
+  double *hn, *wcn, *h_out, *wc_out;
+  double *hp, *wcu, *ch, *kcx, *kcy, *kcz, *kx, *ky, *kzf, *qx, *qy, *qzf;
+  double *vloss, *room, *sup, *sdn;
+  double *diag, *gxp, *gyp, *gzp, *rhs, *x;
+  float *diag32, *gxp32, *gyp32, *gzp32, *dinv32, *l32;
+  uint8_t* satf;
+  int* colflag;
+  double* partial;
+  StepOut* out;
+  double dtg, co_max, dq_grow, dq_shrink, dt_min, dt_max;
+  int nblk, tc, mixed, warp_walk;
+};
+
+// Device tables of a batch's members for the batched phases.
+struct PhaseTables {
+  int n = 0;
+  StepArgs* tab = nullptr;       // device, n records
+  StepArgs* tab_host = nullptr;  // pinned, refreshed before each step
+  int *first_cells = nullptr, *first_ghost = nullptr, *first_factor = nullptr;  // device, n + 1
+  int grid_cells = 0, grid_ghost = 0, grid_factor = 0;
+  size_t walk_smem = 0, factor_smem = 0;
+  StepOut* outs = nullptr;       // device, n step records gathered
+  StepOut* outs_host = nullptr;  // pinned
+};
+cudaError_t phase_tables_build(PhaseTables& t, const std::vector<const Device*>& ds,
+                               const std::vector<int>& mixed);
+void phase_tables_free(PhaseTables& t);
+void fill_step_args(const Device& D, bool mixed, double dtg, double co_max, double dq_grow,
+                    double dq_shrink, double dt_min, double dt_max, StepArgs& a);
+// Enqueue on s: the records' upload and the predictor phases of every member
+// (ghosts, closure, assembly, and the line factor of the mixed members) ...
+cudaError_t batch_predictor(const PhaseTables& t, cudaStream_t s);
+// ... and, after the solves, every member's corrector, post-allocation,
+// clamp, audit and controller, and the read-back of the step records.
+cudaError_t batch_corrector(const PhaseTables& t, cudaStream_t s);
+// Launch geometry shared by the single-domain and batched launches.
+int ghost_blocks(const Device& D);
+int line_tile_cols(int nz);
+int line_factor_blocks(const Device& D);
+size_t line_factor_smem(int nz);
+cudaError_t launch_line_factor_batch(const PhaseTables& t, cudaStream_t s);
+
 // ---------------------------------------------------------------- batched solves
 // Several domains' predictor solves in one cooperative launch: member i runs
 // its own solve (own CG state, reductions and barrier) on the block range

@@ -12,10 +12,13 @@
 // the same grid of D.nblk blocks, writes one partial per block, and
 // k_step_info combines the partials in block order, so a step's audit is
 // bit-reproducible run to run.
+#include <algorithm>
 #include <cfloat>
+#include <cstring>
 #include <map>
 #include <mutex>
 
+#include "gw_coop.cuh"
 #include "gw_internal.h"
 
 namespace fgw {
@@ -63,10 +66,10 @@ inline dim3 cells_grid(const Device& D) { return dim3(static_cast<unsigned>(D.nb
 // ---------------------------------------------------------------- ghosts
 // Domain-edge ghost heads and moisture (enforceHeadBc, Predictor.cpp:757-817;
 // enforceMoistureBc, Corrector.cpp:709-756).  Either pointer may be null.
-__global__ void k_ghosts(Dims d, Fields f, double* h, double* wc) {
+__device__ __forceinline__ void ghosts_body(Dims d, Fields f, double* h, double* wc, const int bid, const int G) {
   const long long nxg = 2LL * d.ny * d.nz, nyg = 2LL * d.nx * d.nz;
-  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < nxg + nyg;
-       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long t = bid * static_cast<long long>(blockDim.x) + threadIdx.x; t < nxg + nyg;
+       t += static_cast<long long>(G) * blockDim.x) {
     long long g, c;
     int code;
     double val;
@@ -97,20 +100,24 @@ __global__ void k_ghosts(Dims d, Fields f, double* h, double* wc) {
   }
 }
 
+__global__ void k_ghosts(Dims d, Fields f, double* h, double* wc) {
+  ghosts_body(d, f, h, wc, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------- closures
 // Per-cell directional conductivities K(h, Ksx|Ksy|Ksz) of the predictor pass
 // from the step-start head (ghosts included; Predictor.cpp:127-232 evaluates
 // them for both flanks of every face).
 // The same pass also evaluates C(h^n), the capacity of the storage term
 // (Predictor.cpp:445-452), from the same powers.
-__global__ void __launch_bounds__(kBlock) k_closure_pred(Dims d, Fields f,
+__device__ __forceinline__ void closure_pred_body(Dims d, Fields f,
                                                          const double* __restrict__ h,
                                                          double* __restrict__ kcx,
                                                          double* __restrict__ kcy,
                                                          double* __restrict__ kcz,
-                                                         double* __restrict__ ch) {
-  for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
-       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+                                                         double* __restrict__ ch, const int bid, const int G) {
+  for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
+       c += static_cast<long long>(G) * blockDim.x) {
     const double hc = h[c];
     const Soil so = soil_at(f, c);
     const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
@@ -123,19 +130,28 @@ __global__ void __launch_bounds__(kBlock) k_closure_pred(Dims d, Fields f,
   }
 }
 
+__global__ void __launch_bounds__(kBlock) k_closure_pred(Dims d, Fields f,
+                                                         const double* __restrict__ h,
+                                                         double* __restrict__ kcx,
+                                                         double* __restrict__ kcy,
+                                                         double* __restrict__ kcz,
+                                                         double* __restrict__ ch) {
+  closure_pred_body(d, f, h, kcx, kcy, kcz, ch, blockIdx.x, gridDim.x);
+}
+
 // Corrector pass: scatter the solved heads (fillAndSolve's gw_scatter_head,
 // Predictor.cpp:745-754), re-impose the ghost heads (enforceHeadBc after the
 // solve, RichardsSolver.cpp:762) and evaluate the per-cell conductivities of
 // the predicted head (the corrector's computeFaceConductivity, :768).
-__global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
+__device__ __forceinline__ void closure_corr_body(Dims d, Fields f,
                                                          const double* __restrict__ x,
                                                          const double* __restrict__ hn,
                                                          double* __restrict__ hp,
                                                          double* __restrict__ kcx,
                                                          double* __restrict__ kcy,
-                                                         double* __restrict__ kcz) {
-  for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
-       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+                                                         double* __restrict__ kcz, const int bid, const int G) {
+  for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
+       c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     const bool jin = j >= 1 && j <= d.ny, iin = i >= 1 && i <= d.nx;
@@ -171,6 +187,16 @@ __global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
   }
 }
 
+__global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
+                                                         const double* __restrict__ x,
+                                                         const double* __restrict__ hn,
+                                                         double* __restrict__ hp,
+                                                         double* __restrict__ kcx,
+                                                         double* __restrict__ kcy,
+                                                         double* __restrict__ kcz) {
+  closure_corr_body(d, f, x, hn, hp, kcx, kcy, kcz, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------- assembly
 // The 7-point head system of one active cell (assembleSystemImpl,
 // Predictor.cpp:400-698, uncoupled, density ratios 1): storage
@@ -181,15 +207,14 @@ __global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
 // (the same expression on the same data, so the stored matrix is the
 // reference's up to the rounding of its z legs).  Legs toward an inactive
 // cell or out of the domain are stored as 0 (PETSc ignores column -1).
-__global__ void __launch_bounds__(kBlock, 2)
-    k_assemble(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
+__device__ __forceinline__ void assemble_body(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
                const double* __restrict__ wcn, const double* __restrict__ ch,
                const double* __restrict__ dtgp, double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
-               double* __restrict__ gzps, double* __restrict__ rhs) {
+               double* __restrict__ gzps, double* __restrict__ rhs, const int bid, const int G) {
   const double dx = d.dx, dy = d.dy;
   const double dtg = *dtgp;
-  for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
-       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
+       c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     if (j < 1 || j > d.ny || i < 1 || i > d.nx) continue;
@@ -312,6 +337,13 @@ __global__ void __launch_bounds__(kBlock, 2)
   }
 }
 
+__global__ void __launch_bounds__(kBlock, 2) k_assemble(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
+               const double* __restrict__ wcn, const double* __restrict__ ch,
+               const double* __restrict__ dtgp, double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
+               double* __restrict__ gzps, double* __restrict__ rhs) {
+  assemble_body(d, f, pk, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------- fluxes
 // Corrector faces and Darcy fluxes (computeFaceConductivity from the predicted
 // head, Predictor.cpp:105-386, and computeFluxesImpl<PC, HARM>,
@@ -400,7 +432,7 @@ __device__ inline double flux_zv(const Dims& d, const Fields& f, const ZFlank& u
 // boundary faces through the ghost cells i = 0, j = 0) and the z face above
 // it (plus the bottom face for k = nz-1).  Each face's loads are issued
 // before its rules run.
-__global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
+__device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
                                                     const double* __restrict__ hp,
                                                     const double* __restrict__ wcn,
                                                     double* __restrict__ kx,
@@ -408,9 +440,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
                                                     double* __restrict__ kzf,
                                                     double* __restrict__ qx,
                                                     double* __restrict__ qy,
-                                                    double* __restrict__ qzf) {
-  for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
-       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+                                                    double* __restrict__ qzf, const int bid, const int G) {
+  for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
+       c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     const bool jin = j >= 1 && j <= d.ny, iin = i >= 1 && i <= d.nx;
@@ -475,6 +507,18 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
   }
 }
 
+__global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
+                                                    const double* __restrict__ hp,
+                                                    const double* __restrict__ wcn,
+                                                    double* __restrict__ kx,
+                                                    double* __restrict__ ky,
+                                                    double* __restrict__ kzf,
+                                                    double* __restrict__ qx,
+                                                    double* __restrict__ qy,
+                                                    double* __restrict__ qzf) {
+  flux_body(d, f, pk, hp, wcn, kx, ky, kzf, qx, qy, qzf, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------- theta update
 // theta from the flux divergence with the Ss factor, and the Ss audit term
 // (updateWaterContent, Corrector.cpp:629-672).  Cells outside the update keep
@@ -482,18 +526,20 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
 //
 // The same pass writes the saturation flag of every cell (theta >= theta_s or
 // h > h_ae on the corrected theta and predicted head, ghosts included) that
-// the post-allocation classification tests on the six neighbours of a cell.
+// the post-allocation classification tests on the six neighbours of a cell,
+// and clears the column flags the classification then sets.
 // All loads of a cell are issued before its first store and before any
 // branch on loaded data, so one memory round trip serves the cell.
-__global__ void __launch_bounds__(kBlock, 4) k_update_wc(
+__device__ __forceinline__ void update_wc_body(
     Dims d, Fields f, const double* __restrict__ hp, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ qx, const double* __restrict__ qy,
     const double* __restrict__ qzf, const double* __restrict__ dtgp, double* __restrict__ wcu,
-    uint8_t* __restrict__ satf, double* partial) {
+    uint8_t* __restrict__ satf, int* __restrict__ colflag, double* partial, const int bid,
+    const int G) {
   const double dtg = *dtgp;
   double acc = 0.0;
-  for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
-       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
+       c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     const bool in = j >= 1 && j <= d.ny && i >= 1 && i <= d.nx;
@@ -518,9 +564,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_update_wc(
     }
     wcu[c] = upd;
     satf[c] = (upd >= ts || hpc > aev) ? 1 : 0;
+    if (k == 0) colflag[col2(d, j, i)] = 0;  // the walk's column flags start clear
   }
   const double s = block_reduce(acc, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  if (threadIdx.x == 0) partial[bid] = s;
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_update_wc(
+    Dims d, Fields f, const double* __restrict__ hp, const double* __restrict__ hn,
+    const double* __restrict__ wcn, const double* __restrict__ qx, const double* __restrict__ qy,
+    const double* __restrict__ qzf, const double* __restrict__ dtgp, double* __restrict__ wcu,
+    uint8_t* __restrict__ satf, int* __restrict__ colflag, double* partial) {
+  update_wc_body(d, f, hp, hn, wcn, qx, qy, qzf, dtgp, wcu, satf, colflag, partial, blockIdx.x,
+                 gridDim.x);
 }
 
 // ---------------------------------------------------------------- post-allocation
@@ -587,15 +643,15 @@ __device__ inline Split gradient_split(const Dims& d, const SplitIn& n, int k) {
 // neighbour-saturation tests read the flags k_update_wc wrote from the same
 // snapshot.  Every load of an interior cell, its neighbours included, is
 // issued before the first branch on loaded data.
-__global__ void __launch_bounds__(kBlock, 3) k_classify(
+__device__ __forceinline__ void classify_body(
     Dims d, Fields f, const double* __restrict__ kx, const double* __restrict__ ky,
     const double* __restrict__ kzf, const double* __restrict__ wcR,
     const double* __restrict__ hR, const uint8_t* __restrict__ satf, double* __restrict__ wc_out,
     double* __restrict__ h_out, double* __restrict__ room, double* __restrict__ sup,
-    double* __restrict__ sdn, int* colflag, double* part_adj, double* part_drop) {
+    double* __restrict__ sdn, int* colflag, double* part_adj, double* part_drop, const int bid, const int G) {
   double adj = 0.0, drop = 0.0;
-  for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
-       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
+       c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     const double before = wcR[c];
@@ -681,21 +737,30 @@ __global__ void __launch_bounds__(kBlock, 3) k_classify(
     sdn[c] = dn;
   }
   const double s1 = block_reduce(adj, SumOp(), 0.0);
-  if (threadIdx.x == 0) part_adj[blockIdx.x] = s1;
+  if (threadIdx.x == 0) part_adj[bid] = s1;
   const double s2 = block_reduce(drop, SumOp(), 0.0);
-  if (threadIdx.x == 0) part_drop[blockIdx.x] = s2;
+  if (threadIdx.x == 0) part_drop[bid] = s2;
+}
+
+__global__ void __launch_bounds__(kBlock, 3) k_classify(
+    Dims d, Fields f, const double* __restrict__ kx, const double* __restrict__ ky,
+    const double* __restrict__ kzf, const double* __restrict__ wcR,
+    const double* __restrict__ hR, const uint8_t* __restrict__ satf, double* __restrict__ wc_out,
+    double* __restrict__ h_out, double* __restrict__ room, double* __restrict__ sup,
+    double* __restrict__ sdn, int* colflag, double* part_adj, double* part_drop) {
+  classify_body(d, f, kx, ky, kzf, wcR, hR, satf, wc_out, h_out, room, sup, sdn, colflag, part_adj, part_drop, blockIdx.x, gridDim.x);
 }
 
 // Phase 2: the vertical send walks, one thread per flagged column, k
 // ascending (Reallocate.cpp:410-540, uncoupled, no transport window).
-__global__ void k_walk_thread(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
+__device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
                        const double* __restrict__ sdn, double* qzf, const int* __restrict__ colflag,
-                       const double* __restrict__ dtgp, double* partial) {
+                       const double* __restrict__ dtgp, double* partial, const int bid, const int G) {
   const double dtg = *dtgp;
   double lost = 0.0;
   const long long ncolint = static_cast<long long>(d.nx) * d.ny;
-  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < ncolint;
-       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long t = bid * static_cast<long long>(blockDim.x) + threadIdx.x; t < ncolint;
+       t += static_cast<long long>(G) * blockDim.x) {
     const int j = static_cast<int>(t / d.nx) + 1, i = static_cast<int>(t % d.nx) + 1;
     const long long col = col2(d, j, i);
     if (!colflag[col]) continue;
@@ -755,7 +820,13 @@ __global__ void k_walk_thread(Dims d, Fields f, double* wc, double* room, const 
     }
   }
   const double s = block_reduce(lost, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  if (threadIdx.x == 0) partial[bid] = s;
+}
+
+__global__ void k_walk_thread(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
+                       const double* __restrict__ sdn, double* qzf, const int* __restrict__ colflag,
+                       const double* __restrict__ dtgp, double* partial) {
+  walk_thread_body(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, blockIdx.x, gridDim.x);
 }
 
 // The same walk with one warp per flagged column.  The column's room, theta,
@@ -822,13 +893,13 @@ __device__ inline void walk_take(double& dv, int m, double* rs, double* ws, cons
   if (!(rs[m] > 0.0)) rbits[m >> 5] &= ~(1u << (m & 31));
 }
 
-__global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
+__device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ room,
                                                  const double* __restrict__ sup,
                                                  const double* __restrict__ sdn, double* qzf,
                                                  const int* __restrict__ colflag,
                                                  const double* __restrict__ dtgp,
-                                                 double* partial) {
+                                                 double* partial, const int bid, const int G) {
   extern __shared__ __align__(16) unsigned char walk_smem[];
   const double dtg = *dtgp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -841,8 +912,8 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
   unsigned* ibits = rbits + nw;  // inactive cells
   double lost = 0.0;
   const long long ncolint = static_cast<long long>(d.nx) * d.ny;
-  const long long nwarps = static_cast<long long>(gridDim.x) * kWalkWarps;
-  for (long long t = blockIdx.x * static_cast<long long>(kWalkWarps) + warp; t < ncolint;
+  const long long nwarps = static_cast<long long>(G) * kWalkWarps;
+  for (long long t = bid * static_cast<long long>(kWalkWarps) + warp; t < ncolint;
        t += nwarps) {
     const int j = static_cast<int>(t / d.nx) + 1, i = static_cast<int>(t % d.nx) + 1;
     const long long col = col2(d, j, i);
@@ -935,24 +1006,34 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
     __syncwarp();
   }
   const double s = block_reduce(lost, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  if (threadIdx.x == 0) partial[bid] = s;
+}
+
+__global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
+                                                 const double* __restrict__ room,
+                                                 const double* __restrict__ sup,
+                                                 const double* __restrict__ sdn, double* qzf,
+                                                 const int* __restrict__ colflag,
+                                                 const double* __restrict__ dtgp,
+                                                 double* partial) {
+  walk_body(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- clamp, audit, controller
 // finalizeWaterContent (Corrector.cpp:758-792), accumulateBoundaryFlux
 // (RichardsSolver.cpp:961-1006), the adaptTimeStep inputs (AdaptiveStep.cpp:
 // 58-98) and the owned volume (RichardsSolver.cpp:892-912), in one sweep.
-__global__ void __launch_bounds__(kBlock, 3) k_finalize(Dims d, Fields f, double* __restrict__ wc,
+__device__ __forceinline__ void finalize_body(Dims d, Fields f, double* __restrict__ wc,
                                                         double* __restrict__ vloss,
                                                         const double* __restrict__ qx,
                                                         const double* __restrict__ qy,
                                                         const double* __restrict__ qzf,
                                                         const double* __restrict__ dtgp,
-                                                        double co_max, double* partial, int nblk) {
+                                                        double co_max, double* partial, int nblk, const int bid, const int G) {
   const double dtg = *dtgp;
   double vl = 0.0, inflow = 0.0, dqmax = -DBL_MAX, dtco = DBL_MAX, vol = 0.0;
-  for (long long c = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
-       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+  for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
+       c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
     if (j < 1 || j > d.ny || i < 1 || i > d.nx) continue;
@@ -1004,15 +1085,25 @@ __global__ void __launch_bounds__(kBlock, 3) k_finalize(Dims d, Fields f, double
     }
   }
   double s = block_reduce(vl, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[kPVloss * nblk + blockIdx.x] = s;
+  if (threadIdx.x == 0) partial[kPVloss * nblk + bid] = s;
   s = block_reduce(inflow, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[kPInflow * nblk + blockIdx.x] = s;
+  if (threadIdx.x == 0) partial[kPInflow * nblk + bid] = s;
   s = block_reduce(dqmax, MaxOp(), -DBL_MAX);
-  if (threadIdx.x == 0) partial[kPDqmax * nblk + blockIdx.x] = s;
+  if (threadIdx.x == 0) partial[kPDqmax * nblk + bid] = s;
   s = block_reduce(dtco, MinOp(), DBL_MAX);
-  if (threadIdx.x == 0) partial[kPDtco * nblk + blockIdx.x] = s;
+  if (threadIdx.x == 0) partial[kPDtco * nblk + bid] = s;
   s = block_reduce(vol, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[kPVol * nblk + blockIdx.x] = s;
+  if (threadIdx.x == 0) partial[kPVol * nblk + bid] = s;
+}
+
+__global__ void __launch_bounds__(kBlock, 3) k_finalize(Dims d, Fields f, double* __restrict__ wc,
+                                                        double* __restrict__ vloss,
+                                                        const double* __restrict__ qx,
+                                                        const double* __restrict__ qy,
+                                                        const double* __restrict__ qzf,
+                                                        const double* __restrict__ dtgp,
+                                                        double co_max, double* partial, int nblk) {
+  finalize_body(d, f, wc, vloss, qx, qy, qzf, dtgp, co_max, partial, nblk, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_volume(Dims d, Fields f, const double* __restrict__ wc, double* partial) {
@@ -1079,8 +1170,9 @@ __device__ double reduce_slot(const double* p, int n, Op op, double identity) {
 // 0.75, Courant cap, [dt_min, dt_max] clamp).
 // The step's dtg is read from out->next_dt, where the step found it, and the
 // controller's next dt replaces it there.
-__global__ void k_step_info(const double* partial, int nblk, int off, double dq_grow,
-                            double dq_shrink, double dt_min, double dt_max, StepOut* out) {
+__device__ __forceinline__ void step_info_body(const double* partial, int nblk, int off,
+                                               double dq_grow, double dq_shrink, double dt_min,
+                                               double dt_max, double dtg, StepOut* out) {
   const double ss = reduce_slot(partial + kPSs * nblk, nblk, SumOp(), 0.0);
   const double adj = reduce_slot(partial + kPAdj * nblk, nblk, SumOp(), 0.0);
   const double drop = reduce_slot(partial + kPDrop * nblk, nblk, SumOp(), 0.0);
@@ -1099,7 +1191,6 @@ __global__ void k_step_info(const double* partial, int nblk, int off, double dq_
     out->dqmax = dqmax;
     out->dtco = dtco;
     out->volume = vol;
-    const double dtg = out->next_dt;
     double next = dtg;
     if (dqmax > dq_shrink) next = dtg * 0.75;
     else if (dqmax < dq_grow) next = dtg * 1.25;
@@ -1110,9 +1201,143 @@ __global__ void k_step_info(const double* partial, int nblk, int off, double dq_
   }
 }
 
+__global__ void k_step_info(const double* partial, int nblk, int off, double dq_grow,
+                            double dq_shrink, double dt_min, double dt_max, StepOut* out) {
+  const double dtg = out->next_dt;  // read by every thread before thread 0 replaces it
+  step_info_body(partial, nblk, off, dq_grow, dq_shrink, dt_min, dt_max, dtg, out);
+}
+
 __global__ void k_volume_final(const double* partial, int nblk, StepOut* out) {
   const double vol = reduce_slot(partial, nblk, SumOp(), 0.0);
   if (threadIdx.x == 0) out->volume = vol;
+}
+
+// ---------------------------------------------------------------- batched phases
+// One launch runs a phase for every member of a batch: block b belongs to the
+// member whose range [first[i], first[i+1]) holds it, loads that member's
+// record into shared memory and runs the phase's body on its own blocks.
+
+__device__ inline void load_member(const StepArgs* tab, const int* first, int n, StepArgs& sa,
+                                   int& bid, int& G) {
+  __shared__ int si;
+  if (threadIdx.x == 0) si = coop::instance_of(first, n, blockIdx.x);
+  __syncthreads();
+  const int i = si;
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(tab + i);
+  unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sa);
+  for (int w = threadIdx.x; w < static_cast<int>(sizeof(StepArgs) / 8); w += blockDim.x)
+    dst[w] = src[w];
+  bid = blockIdx.x - first[i];
+  G = first[i + 1] - first[i];
+  __syncthreads();
+}
+
+static_assert(sizeof(StepArgs) % 8 == 0, "StepArgs is copied in 8-byte words");
+
+__global__ void k_ghosts_batch(const StepArgs* tab, const int* first, int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  ghosts_body(sa.d, sa.f, sa.hn, sa.wcn, bid, G);
+}
+
+__global__ void __launch_bounds__(kBlock) k_closure_pred_batch(const StepArgs* tab,
+                                                               const int* first, int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  closure_pred_body(sa.d, sa.f, sa.hn, sa.kcx, sa.kcy, sa.kcz, sa.ch, bid, G);
+}
+
+__global__ void __launch_bounds__(kBlock, 2) k_assemble_batch(const StepArgs* tab,
+                                                              const int* first, int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  const PassK pk{sa.kcx, sa.kcy, sa.kcz, sa.wcn};
+  assemble_body(sa.d, sa.f, pk, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp, sa.gyp, sa.gzp,
+                sa.rhs, bid, G);
+}
+
+__global__ void __launch_bounds__(kBlock) k_closure_corr_batch(const StepArgs* tab,
+                                                               const int* first, int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  closure_corr_body(sa.d, sa.f, sa.x, sa.hn, sa.hp, sa.kcx, sa.kcy, sa.kcz, bid, G);
+}
+
+__global__ void __launch_bounds__(kBlock, 2) k_flux_batch(const StepArgs* tab, const int* first,
+                                                          int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  const PassK pk{sa.kcx, sa.kcy, sa.kcz, sa.wcn};
+  flux_body(sa.d, sa.f, pk, sa.hp, sa.wcn, sa.kx, sa.ky, sa.kzf, sa.qx, sa.qy, sa.qzf, bid, G);
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_update_wc_batch(const StepArgs* tab,
+                                                               const int* first, int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  update_wc_body(sa.d, sa.f, sa.hp, sa.hn, sa.wcn, sa.qx, sa.qy, sa.qzf, &sa.dtg, sa.wcu, sa.satf,
+                 sa.colflag, sa.partial + kPSs * sa.nblk, bid, G);
+}
+
+__global__ void __launch_bounds__(kBlock, 3) k_classify_batch(const StepArgs* tab,
+                                                              const int* first, int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  classify_body(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.wcu, sa.hp, sa.satf, sa.wc_out, sa.h_out,
+                sa.room, sa.sup, sa.sdn, sa.colflag, sa.partial + kPAdj * sa.nblk,
+                sa.partial + kPDrop * sa.nblk, bid, G);
+}
+
+__global__ void __launch_bounds__(kBlock) k_walk_batch(const StepArgs* tab, const int* first,
+                                                       int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  if (sa.warp_walk) {
+    walk_body(sa.d, sa.f, sa.wc_out, sa.room, sa.sup, sa.sdn, sa.qzf, sa.colflag, &sa.dtg,
+              sa.partial + kPLost * sa.nblk, bid, G);
+  } else {
+    walk_thread_body(sa.d, sa.f, sa.wc_out, sa.room, sa.sup, sa.sdn, sa.qzf, sa.colflag, &sa.dtg,
+                     sa.partial + kPLost * sa.nblk, bid, G);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock, 3) k_finalize_batch(const StepArgs* tab,
+                                                              const int* first, int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
+  finalize_body(sa.d, sa.f, sa.wc_out, sa.vloss, sa.qx, sa.qy, sa.qzf, &sa.dtg, sa.co_max,
+                sa.partial, sa.nblk, bid, G);
+}
+
+// One block per member.
+__global__ void k_step_info_batch(const StepArgs* tab) {
+  __shared__ StepArgs sa;
+  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(tab + blockIdx.x);
+  unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sa);
+  for (int w = threadIdx.x; w < static_cast<int>(sizeof(StepArgs) / 8); w += blockDim.x)
+    dst[w] = src[w];
+  __syncthreads();
+  step_info_body(sa.partial, sa.nblk, sa.d.off, sa.dq_grow, sa.dq_shrink, sa.dt_min, sa.dt_max,
+                 sa.dtg, sa.out);
+}
+
+// The members' step records into one array, for a single read-back.
+__global__ void k_gather_outs(const StepArgs* tab, StepOut* outs, int n) {
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const unsigned* src = reinterpret_cast<const unsigned*>(tab[i].out);
+    unsigned* dst = reinterpret_cast<unsigned*>(outs + i);
+    for (int w = threadIdx.x; w < static_cast<int>(sizeof(StepOut) / 4); w += blockDim.x)
+      dst[w] = src[w];
+  }
 }
 
 }  // namespace
@@ -1135,10 +1360,13 @@ cudaError_t raise_smem_limit(const void* kernel, size_t bytes) {
 // chose.
 inline const double* dtg_slot(const Device& D) { return &D.out->next_dt; }
 
-void launch_ghosts(const Device& D, double* h, double* wc) {
+int ghost_blocks(const Device& D) {
   const long long n = 2LL * (D.d.nx + D.d.ny) * D.d.nz;
-  const int g = static_cast<int>(std::min<long long>((n + kBlock - 1) / kBlock, 4096));
-  k_ghosts<<<g, kBlock, 0, D.stream>>>(D.d, D.f, h, wc);
+  return static_cast<int>(std::min<long long>((n + kBlock - 1) / kBlock, 4096));
+}
+
+void launch_ghosts(const Device& D, double* h, double* wc) {
+  k_ghosts<<<ghost_blocks(D), kBlock, 0, D.stream>>>(D.d, D.f, h, wc);
   ++D.launches;
 }
 
@@ -1170,12 +1398,12 @@ void launch_flux(const Device& D, const double* wcn) {
 
 void launch_update_wc(const Device& D, const double* hn, const double* wcn) {
   k_update_wc<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.hp, hn, wcn, D.qx, D.qy, D.qzf,
-                                                      dtg_slot(D), D.wcu, D.satf, D.partial + kPSs * D.nblk);
+                                                      dtg_slot(D), D.wcu, D.satf, D.colflag,
+                                                      D.partial + kPSs * D.nblk);
   ++D.launches;
 }
 
 void launch_classify(const Device& D, double* wc_out, double* h_out) {
-  cudaMemsetAsync(D.colflag, 0, sizeof(int) * D.d.ncol, D.stream);
   k_classify<<<cells_grid(D), kBlock, 0, D.stream>>>(
       D.d, D.f, D.kx, D.ky, D.kzf, D.wcu, D.hp, D.satf, wc_out, h_out, D.room, D.sup, D.sdn,
       D.colflag,
@@ -1228,6 +1456,137 @@ void launch_volume(const Device& D, const double* wc) {
   ++D.launches;
   k_volume_final<<<1, kBlock, 0, D.stream>>>(D.partial + kPVol * D.nblk, D.nblk, D.out);
   ++D.launches;
+}
+
+// ---------------------------------------------------------------- batched phases (host)
+void fill_step_args(const Device& D, bool mixed, double dtg, double co_max, double dq_grow,
+                    double dq_shrink, double dt_min, double dt_max, StepArgs& a) {
+  std::memset(&a, 0, sizeof(a));
+  const int cur = D.cur, nxt = 1 - D.cur;
+  a.d = D.d;
+  a.f = D.f;
+  a.hn = D.h[cur];
+  a.wcn = D.wc[cur];
+  a.h_out = D.h[nxt];
+  a.wc_out = D.wc[nxt];
+  a.hp = D.hp;
+  a.wcu = D.wcu;
+  a.ch = D.ch;
+  a.kcx = D.kcx;
+  a.kcy = D.kcy;
+  a.kcz = D.kcz;
+  a.kx = D.kx;
+  a.ky = D.ky;
+  a.kzf = D.kzf;
+  a.qx = D.qx;
+  a.qy = D.qy;
+  a.qzf = D.qzf;
+  a.vloss = D.vloss;
+  a.room = D.room;
+  a.sup = D.sup;
+  a.sdn = D.sdn;
+  a.diag = D.diag;
+  a.gxp = D.gxp;
+  a.gyp = D.gyp;
+  a.gzp = D.gzp;
+  a.rhs = D.rhs;
+  a.x = D.x;
+  a.diag32 = D.diag32;
+  a.gxp32 = D.gxp32;
+  a.gyp32 = D.gyp32;
+  a.gzp32 = D.gzp32;
+  a.dinv32 = D.dinv32;
+  a.l32 = D.l32;
+  a.satf = D.satf;
+  a.colflag = D.colflag;
+  a.partial = D.partial;
+  a.out = D.out;
+  a.dtg = dtg;
+  a.co_max = co_max;
+  a.dq_grow = dq_grow;
+  a.dq_shrink = dq_shrink;
+  a.dt_min = dt_min;
+  a.dt_max = dt_max;
+  a.nblk = D.nblk;
+  a.tc = line_tile_cols(D.d.nz);
+  a.mixed = mixed ? 1 : 0;
+  const size_t smem = kWalkWarps * walk_warp_bytes(D.d.nz);
+  a.warp_walk = (D.d.nz <= kWalkMaxNz && smem <= kWalkSmemMax) ? 1 : 0;
+}
+
+cudaError_t phase_tables_build(PhaseTables& t, const std::vector<const Device*>& ds,
+                               const std::vector<int>& mixed) {
+  t.n = static_cast<int>(ds.size());
+  std::vector<int> fc(t.n + 1, 0), fg(t.n + 1, 0), ff(t.n + 1, 0);
+  t.walk_smem = 0;
+  t.factor_smem = 0;
+  for (int i = 0; i < t.n; ++i) {
+    const Device& D = *ds[i];
+    fc[i + 1] = fc[i] + D.nblk;
+    fg[i + 1] = fg[i] + ghost_blocks(D);
+    ff[i + 1] = ff[i] + (mixed[i] ? line_factor_blocks(D) : 0);
+    const size_t ws = kWalkWarps * walk_warp_bytes(D.d.nz);
+    if (D.d.nz <= kWalkMaxNz && ws <= kWalkSmemMax) t.walk_smem = std::max(t.walk_smem, ws);
+    if (mixed[i]) t.factor_smem = std::max(t.factor_smem, line_factor_smem(D.d.nz));
+  }
+  t.grid_cells = fc.back();
+  t.grid_ghost = fg.back();
+  t.grid_factor = ff.back();
+  cudaError_t e = cudaMalloc(&t.tab, sizeof(StepArgs) * t.n);
+  if (e == cudaSuccess) e = cudaMallocHost(&t.tab_host, sizeof(StepArgs) * t.n);
+  if (e == cudaSuccess) e = cudaMalloc(&t.first_cells, sizeof(int) * (t.n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&t.first_ghost, sizeof(int) * (t.n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&t.first_factor, sizeof(int) * (t.n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&t.outs, sizeof(StepOut) * t.n);
+  if (e == cudaSuccess) e = cudaMallocHost(&t.outs_host, sizeof(StepOut) * t.n);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t.first_cells, fc.data(), sizeof(int) * fc.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t.first_ghost, fg.data(), sizeof(int) * fg.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t.first_factor, ff.data(), sizeof(int) * ff.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && t.walk_smem > 0)
+    e = raise_smem_limit(reinterpret_cast<const void*>(k_walk_batch), t.walk_smem);
+  return e;
+}
+
+void phase_tables_free(PhaseTables& t) {
+  if (t.tab) cudaFree(t.tab);
+  if (t.tab_host) cudaFreeHost(t.tab_host);
+  if (t.first_cells) cudaFree(t.first_cells);
+  if (t.first_ghost) cudaFree(t.first_ghost);
+  if (t.first_factor) cudaFree(t.first_factor);
+  if (t.outs) cudaFree(t.outs);
+  if (t.outs_host) cudaFreeHost(t.outs_host);
+  t = PhaseTables{};
+}
+
+cudaError_t batch_predictor(const PhaseTables& t, cudaStream_t s) {
+  cudaError_t e = cudaMemcpyAsync(t.tab, t.tab_host, sizeof(StepArgs) * t.n,
+                                  cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  k_ghosts_batch<<<t.grid_ghost, kBlock, 0, s>>>(t.tab, t.first_ghost, t.n);
+  k_closure_pred_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
+  k_assemble_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
+  if (t.grid_factor > 0) {
+    e = launch_line_factor_batch(t, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t batch_corrector(const PhaseTables& t, cudaStream_t s) {
+  k_closure_corr_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
+  k_flux_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
+  k_update_wc_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
+  k_classify_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
+  k_walk_batch<<<t.grid_cells, kBlock, t.walk_smem, s>>>(t.tab, t.first_cells, t.n);
+  k_finalize_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
+  k_step_info_batch<<<t.n, kBlock, 0, s>>>(t.tab);
+  k_gather_outs<<<std::min(t.n, 1024), 32, 0, s>>>(t.tab, t.outs, t.n);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyAsync(t.outs_host, t.outs, sizeof(StepOut) * t.n, cudaMemcpyDeviceToHost, s);
 }
 
 }  // namespace fgw

@@ -242,10 +242,12 @@ long long frehg_gw_kernel_launches(const frehg_gw_handle* h);
 typedef struct frehg_gw_batch frehg_gw_batch;
 
 typedef struct {
-  int cells_per_block;  /* active cells per solve block of a member; 0 = 65536 */
+  int cells_per_block;  /* active cells per solve block of a member; 0 = 16384 */
   int tiled_line_solve; /* mixed form: 1 = shared-memory tiled line solve at every depth */
   int use_graph;        /* 1 = replay each step as a CUDA graph, 0 = launch directly */
-  int streams;          /* concurrent streams for the non-solve phases; 0 = 32 */
+  int streams;          /* per_member_phases: concurrent member streams; 0 = 32 */
+  int per_member_phases;/* 1 = launch each member's non-solve kernels on its own (streams);
+                           0 = one launch per phase for all members (default) */
 } frehg_gw_batch_opts;
 
 typedef struct {
@@ -259,6 +261,8 @@ typedef struct {
   long long kernels_per_step;
   int cells_per_block;
   int tiled_line_solve;
+  double phase_ms[3];       /* last directly launched step (batched phases, use_graph = 0):
+                               predictor, solves, corrector ms */
 } frehg_gw_batch_stats_t;
 
 /* Batch over n members (each initialised); opts may be NULL (defaults,
@@ -275,7 +279,8 @@ int frehg_gw_batch_set_dt(frehg_gw_batch* b, int i, double dtg);
 /* Times candidate decompositions (solve blocks per member, and for the mixed
  * form the column or tiled line solve) on trial steps from a snapshot of the
  * members' state, restores that state and keeps the fastest; results are
- * cached per batch shape for the process.  best_ms is -1 on a cache hit. */
+ * cached per batch shape for the process.  best_ms is -1 on a cache hit.
+ * Candidates: 4096..131072 cells per block. */
 int frehg_gw_batch_autotune(frehg_gw_batch* b, int trials, frehg_gw_batch_opts* chosen,
                             double* best_ms);
 int frehg_gw_batch_stats(const frehg_gw_batch* b, frehg_gw_batch_stats_t* out);
