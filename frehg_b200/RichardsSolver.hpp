@@ -39,6 +39,13 @@ struct GwStepAudit {
   double vloss = 0.0;
 };
 
+/// The groundwater state of a checkpoint (Simulation::checkpointFields3 and
+/// the "dtg" scalar, driver/Simulation.cpp:707-722, 1211-1216).
+struct GwCheckpoint {
+  double t = 0.0, dtg = 0.0;
+  std::vector<double> h, wc, vloss;
+};
+
 /// The reference's SolveStats of the predictor solve.
 struct SolveStats {
   int iterations = 0;
@@ -92,6 +99,17 @@ class RichardsSolver {
   std::vector<double> faceConductivityX() const { return field(FREHG_GW_FIELD_KX); }
   std::vector<double> faceConductivityY() const { return field(FREHG_GW_FIELD_KY); }
   std::vector<double> faceConductivityZFace() const { return field(FREHG_GW_FIELD_KZ); }
+
+  /// The state a checkpoint stores, at time t.
+  GwCheckpoint checkpoint(double t) const {
+    return GwCheckpoint{t, nextDt(), head(), waterContent(), field(FREHG_GW_FIELD_VLOSS)};
+  }
+
+  /// Simulation::restoreFromCheckpoint for the groundwater step (:756-792).
+  void restore(const GwCheckpoint& ck) {
+    check(frehg_gw_restore(h_, ck.h.data(), ck.wc.data(),
+                           ck.vloss.empty() ? nullptr : ck.vloss.data(), ck.dtg));
+  }
 
   /// Restart read + refreshDerivedState (interior arrays).
   void setState(const double* head, const double* wc) { check(frehg_gw_set_state(h_, head, wc)); }

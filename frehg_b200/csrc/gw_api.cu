@@ -401,6 +401,28 @@ int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc)
   return FREHG_GW_OK;
 }
 
+int frehg_gw_restore(frehg_gw_handle* h, const double* head, const double* wc,
+                     const double* vloss, double dtg) {
+  if (!h || !head || !wc) return fail(FREHG_GW_EINVAL, "null argument");
+  if (!(dtg > 0.0) || !std::isfinite(dtg)) return fail(FREHG_GW_EINVAL, "dtg must be positive");
+  const int rc = frehg_gw_set_state(h, head, wc);
+  if (rc != FREHG_GW_OK) return rc;
+  fgw::Device& D = h->D;
+  const fgw::Dims& d = D.d;
+  if (vloss) {
+    std::vector<double> v(static_cast<size_t>(d.ncell), 0.0);
+    for (int j = 1; j <= d.ny; ++j)
+      for (int i = 1; i <= d.nx; ++i)
+        for (int k = 0; k < d.nz; ++k)
+          v[fgw::cidx(d, j, i, k)] =
+              vloss[(static_cast<long long>(j - 1) * d.nx + (i - 1)) * d.nz + k];
+    CUDA_TRY(cudaMemcpy(D.vloss, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice),
+             "restore");
+  }
+  h->next_dt = dtg;
+  return FREHG_GW_OK;
+}
+
 }  // extern "C"
 
 namespace fgw_api {

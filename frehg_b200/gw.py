@@ -51,6 +51,7 @@ def load_library(path: str = LIB_PATH):
     lib.frehg_gw_set_bc_values.argtypes = [H] + [_dp] * 6
     lib.frehg_gw_init_state.argtypes = [H, C.c_int, C.c_double, _dp]
     lib.frehg_gw_set_state.argtypes = [H, _dp, _dp]
+    lib.frehg_gw_restore.argtypes = [H, _dp, _dp, _dp, C.c_double]
     lib.frehg_gw_step.argtypes = [H, C.c_double, C.c_double, C.POINTER(StepInfo)]
     lib.frehg_gw_next_dt.argtypes = [H, _dp]
     lib.frehg_gw_get_field.argtypes = [H, C.c_int, _dp]
@@ -67,7 +68,7 @@ def load_library(path: str = LIB_PATH):
     lib.frehg_gw_kernel_launches.restype = C.c_longlong
     for name in ("frehg_gw_create", "frehg_gw_destroy", "frehg_gw_set_stream",
                  "frehg_gw_set_bc_values", "frehg_gw_init_state", "frehg_gw_set_state",
-                 "frehg_gw_step", "frehg_gw_next_dt", "frehg_gw_get_field",
+                 "frehg_gw_step", "frehg_gw_next_dt", "frehg_gw_get_field", "frehg_gw_restore",
                  "frehg_gw_owned_volume"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -157,6 +158,41 @@ class RichardsSolver:
                 for v in (top, bottom, xm, xp, ym, yp)]
         _check(self.lib, self.lib.frehg_gw_set_bc_values(
             self.h, *[None if a is None else a.ctypes.data_as(_dp) for a in arrs]))
+
+    # -- checkpoint / restart --------------------------------------------------
+    def checkpoint(self) -> dict:
+        """The groundwater state the reference's checkpoint stores
+        (``Simulation::checkpointFields3`` and the ``dtg`` scalar,
+        driver/Simulation.cpp:707-722, 1211-1216): interior h, wc, the
+        cumulative clamp loss, the next dt, and the time reached."""
+        return {"t": self.t, "dtg": self.nextDt(), "h": self.field("h"),
+                "wc": self.field("wc"), "vloss": self.field("vloss")}
+
+    def restore(self, ck: dict) -> None:
+        """``Simulation::restoreFromCheckpoint`` for the groundwater step
+        (:756-792): state, clamp-loss field and dt; the solver continues as the
+        uninterrupted run would."""
+        hh = np.ascontiguousarray(ck["h"], np.float64)
+        ww = np.ascontiguousarray(ck["wc"], np.float64)
+        vl = ck.get("vloss")
+        vv = None if vl is None else np.ascontiguousarray(vl, np.float64)
+        _check(self.lib, self.lib.frehg_gw_restore(
+            self.h, hh.ctypes.data_as(_dp), ww.ctypes.data_as(_dp),
+            None if vv is None else vv.ctypes.data_as(_dp), float(ck["dtg"])))
+        self.t = float(ck["t"])
+
+    def save_checkpoint(self, path: str) -> None:
+        """Writes :meth:`checkpoint` to ``path`` (numpy .npz, exact values)."""
+        ck = self.checkpoint()
+        np.savez(path, t=ck["t"], dtg=ck["dtg"], h=ck["h"], wc=ck["wc"], vloss=ck["vloss"],
+                 shape=np.array([self.nx, self.ny, self.nz]))
+
+    def load_checkpoint(self, path: str) -> None:
+        with np.load(path) as z:
+            if tuple(z["shape"]) != (self.nx, self.ny, self.nz):
+                raise FatalError(1, f"checkpoint {path} is for a {tuple(z['shape'])} domain")
+            self.restore({"t": float(z["t"]), "dtg": float(z["dtg"]), "h": z["h"],
+                          "wc": z["wc"], "vloss": z["vloss"]})
 
     def setState(self, head: np.ndarray, wc: np.ndarray) -> None:
         """Restart read + ``refreshDerivedState``."""

@@ -14,6 +14,9 @@
  *   frehg_gw_init_state    RichardsSolver::applyInitialConditions (:331-427)
  *   frehg_gw_set_state     a restart read + RichardsSolver::refreshDerivedState
  *                          (RichardsSolver.hpp:336, RichardsSolver.cpp:880-890)
+ *   frehg_gw_restore       the groundwater part of Simulation::restoreFromCheckpoint
+ *                          (driver/Simulation.cpp:707-792, io/Checkpoint.hpp):
+ *                          h, wc, vloss_cum and the adaptive-step scalar dtg
  *   frehg_gw_set_bc_values RichardsSolver::updateBoundaryValues (:526-566);
  *                          the caller evaluates BoundaryCondition::value(t)
  *   frehg_gw_step          RichardsSolver::step(t, dtg) (RichardsSolver.hpp:257,
@@ -192,6 +195,13 @@ int frehg_gw_init_state_static(frehg_gw_handle* h, int form, double constant,
 
 /* Overwrite the interior head and moisture (host, ny*nx*nz each). */
 int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc);
+
+/* Restart from a checkpoint: interior head, moisture and (optionally, NULL
+ * keeps it) the cumulative clamp-loss field, ny*nx*nz each, and the dt of the
+ * next step.  A checkpoint is frehg_gw_get_field of HEAD, WC and VLOSS plus
+ * frehg_gw_next_dt; stepping on from a restore equals the uninterrupted run. */
+int frehg_gw_restore(frehg_gw_handle* h, const double* head, const double* wc,
+                     const double* vloss, double dtg);
 
 /* One groundwater step of size dtg ending at time t. */
 int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* info);

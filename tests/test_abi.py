@@ -92,3 +92,12 @@ def test_server_queues_and_rejects_oversized_requests_without_a_gpu():
         st = srv.poll(rid)
         assert st["state"] == QUEUED and st["steps"] == 3 and st["queue_s"] == -1.0
         assert srv.stats()["queued"] == 1
+
+
+def test_restore_rejects_bad_arguments_without_a_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("libfrehg_gw.so not built")
+    lib = ctypes.CDLL(LIB)
+    lib.frehg_gw_restore.restype = ctypes.c_int
+    lib.frehg_gw_restore.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_double]
+    assert lib.frehg_gw_restore(None, None, None, None, 1.0) == 1  # FREHG_GW_EINVAL
