@@ -262,7 +262,7 @@ cudaError_t enqueue_batched_phases(frehg_gw_batch* b, long long* kernels) {
   cudaError_t e = mark(0);
   if (e == cudaSuccess) e = fgw::batch_predictor(t, b->stream);
   if (e == cudaSuccess) e = mark(1);
-  long long k = 3 + (t.grid_factor > 0 ? 1 : 0);
+  long long k = 4 + (t.grid_factor > 0 ? 1 : 0);
   for (const auto& g : b->groups) {
     if (e != cudaSuccess) break;
     e = fgw::solve_group_launch(g, b->stream);

@@ -207,10 +207,12 @@ __global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
 // (the same expression on the same data, so the stored matrix is the
 // reference's up to the rounding of its z legs).  Legs toward an inactive
 // cell or out of the domain are stored as 0 (PETSc ignores column -1).
-__device__ __forceinline__ void assemble_body(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
-               const double* __restrict__ wcn, const double* __restrict__ ch,
-               const double* __restrict__ dtgp, double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
-               double* __restrict__ gzps, double* __restrict__ rhs, const int bid, const int G) {
+__device__ __forceinline__ void assemble_body(
+    Dims d, Fields f, const double* __restrict__ kxf, const double* __restrict__ kyf,
+    const double* __restrict__ kzff, const double* __restrict__ hn,
+    const double* __restrict__ wcn, const double* __restrict__ ch, const double* __restrict__ dtgp,
+    double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
+    double* __restrict__ gzps, double* __restrict__ rhs, const int bid, const int G) {
   const double dx = d.dx, dy = d.dy;
   const double dtg = *dtgp;
   for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
@@ -221,16 +223,15 @@ __device__ __forceinline__ void assemble_body(Dims d, Fields f, PassK pk, const 
     const long long cw = c - d.sx, ce = c + d.sx, cs = c - d.sy, cn = c + d.sy;
     const long long cu = (k >= 1) ? c - 1 : c, cl = (k + 1 < d.nz) ? c + 1 : c;
     const long long col = col2(d, j, i);
-    // Gather: the six faces' flanks, the cell's metrics, heads and BC data.
-    const Flank xw{pk.kcx[cw], f.ksx[cw], wcn[cw], f.wcs[cw], f.act[cw]};
-    const Flank xc{pk.kcx[c], f.ksx[c], wcn[c], f.wcs[c], f.act[c]};
-    const Flank xe{pk.kcx[ce], f.ksx[ce], wcn[ce], f.wcs[ce], f.act[ce]};
-    const Flank ys{pk.kcy[cs], f.ksy[cs], wcn[cs], f.wcs[cs], f.act[cs]};
-    const Flank yc{pk.kcy[c], f.ksy[c], xc.w, xc.ws, xc.act};
-    const Flank yn{pk.kcy[cn], f.ksy[cn], wcn[cn], f.wcs[cn], f.act[cn]};
-    const ZFlank zu{pk.kcz[cu], f.ksz[cu], f.dz[cu], (k >= 1) ? f.act[cu] : int8_t(0)};
-    const ZFlank zc{pk.kcz[c], f.ksz[c], f.dz[c], xc.act};
-    const ZFlank zl{pk.kcz[cl], f.ksz[cl], f.dz[cl], (k + 1 < d.nz) ? f.act[cl] : int8_t(0)};
+    // Gather: the six face conductivities (k_faces), the cell's metrics,
+    // heads and BC data.
+    const long long fz = fidx(d, j, i, k);
+    const double kxp = kxf[c], kxm = kxf[cw], kyp = kyf[c], kym = kyf[cs];
+    const double kzm = kzff[fz], kzp = kzff[fz + 1];
+    const int8_t ac = f.act[c], ae = f.act[ce], an = f.act[cn];
+    const int8_t au = (k >= 1) ? f.act[cu] : int8_t(0), al = (k + 1 < d.nz) ? f.act[cl] : int8_t(0);
+    const double dzc = f.dz[c], dzu = f.dz[cu], dzl = f.dz[cl];
+    const double wcnc = wcn[c], wcsc = f.wcs[c];
     const double cosxc = f.cosx[c], cosxw = f.cosx[cw], axc = f.ax[c], axw = f.ax[cw];
     const double cosyc = f.cosy[c], cosys = f.cosy[cs], ayc = f.ay[c], ays = f.ay[cs];
     const double chc = ch[c], hnc = hn[c], hne = hn[ce], hnw = hn[cw], hnn = hn[cn],
@@ -252,7 +253,7 @@ __device__ __forceinline__ void assemble_body(Dims d, Fields f, PassK pk, const 
       sinyc = f.siny[c];
       sinys = f.siny[cs];
     }
-    if (!xc.act) {
+    if (!ac) {
       diag[c] = 1.0;
       gxps[c] = 0.0;
       gyps[c] = 0.0;
@@ -261,15 +262,8 @@ __device__ __forceinline__ void assemble_body(Dims d, Fields f, PassK pk, const 
       continue;
     }
     const bool east = i == d.nx, west = i == 1, north = j == d.ny, south = j == 1;
-    const bool top = (k == 0) || !zu.act;
-    const double dzc = zc.dz;
+    const bool top = (k == 0) || !au;
     const double volume = d.az * dzc;
-    const double kxp = face_lat(d, xc, xe, false, east, cxp);
-    const double kxm = face_lat(d, xw, xc, west, false, cxm);
-    const double kyp = face_lat(d, yc, yn, false, north, cyp);
-    const double kym = face_lat(d, ys, yc, south, false, cym);
-    const double kzm = face_z(d, zu, zc, k, topc, botc);
-    const double kzp = face_z(d, zc, zl, k + 1, topc, botc);
     double gxp = -kxp * dtg * cosxc / (dx * dx) * (axc * dx);
     double gxm = -kxm * dtg * cosxw / (dx * dx) * (axw * dx);
     double gyp = -kyp * dtg * cosyc / (dy * dy) * (ayc * dy);
@@ -278,12 +272,12 @@ __device__ __forceinline__ void assemble_body(Dims d, Fields f, PassK pk, const 
     if (west && is_head(cxm)) gxm *= 2.0;
     if (north && is_head(cyp)) gyp *= 2.0;
     if (south && is_head(cym)) gym *= 2.0;
-    double dzf = (k == d.nz - 1) ? 0.5 * dzc : 0.5 * (dzc + zl.dz);
+    double dzf = (k == d.nz - 1) ? 0.5 * dzc : 0.5 * (dzc + dzl);
     const double gzp = -kzp * dtg / (dzc * dzf) * volume;
-    dzf = top ? 0.5 * dzc : 0.5 * (dzc + zu.dz);
+    dzf = top ? 0.5 * dzc : 0.5 * (dzc + dzu);
     const double gzm = -kzm * dtg / (dzc * dzf) * volume;
 
-    const double storage = chc + d.ss * xc.w / xc.ws;
+    const double storage = chc + d.ss * wcnc / wcsc;
     double gct = storage * volume - (gxp + gxm + gyp + gym);
     if (east && cxp == kFlux) gct += gxp;
     if (west && cxm == kFlux) gct += gxm;
@@ -330,18 +324,70 @@ __device__ __forceinline__ void assemble_body(Dims d, Fields f, PassK pk, const 
       else if (topc == kFlux) b += -dtg * volume * (vtop + kzm) / dzc;
     }
     diag[c] = gct;
-    gxps[c] = (!east && xe.act) ? gxp : 0.0;
-    gyps[c] = (!north && yn.act) ? gyp : 0.0;
-    gzps[c] = (k + 1 < d.nz && zl.act) ? gzp : 0.0;
+    gxps[c] = (!east && ae) ? gxp : 0.0;
+    gyps[c] = (!north && an) ? gyp : 0.0;
+    gzps[c] = (k + 1 < d.nz && al) ? gzp : 0.0;
     rhs[c] = b;
   }
 }
 
-__global__ void __launch_bounds__(kBlock, 2) k_assemble(Dims d, Fields f, PassK pk, const double* __restrict__ hn,
-               const double* __restrict__ wcn, const double* __restrict__ ch,
-               const double* __restrict__ dtgp, double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
-               double* __restrict__ gzps, double* __restrict__ rhs) {
-  assemble_body(d, f, pk, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs, blockIdx.x, gridDim.x);
+__global__ void __launch_bounds__(kBlock, 2) k_assemble(
+    Dims d, Fields f, const double* __restrict__ kxf, const double* __restrict__ kyf,
+    const double* __restrict__ kzff, const double* __restrict__ hn,
+    const double* __restrict__ wcn, const double* __restrict__ ch, const double* __restrict__ dtgp,
+    double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
+    double* __restrict__ gzps, double* __restrict__ rhs) {
+  assemble_body(d, f, kxf, kyf, kzff, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs, blockIdx.x,
+                gridDim.x);
+}
+
+// ---------------------------------------------------------------- predictor faces
+// Face conductivities of the predictor pass (computeFaceConductivity from
+// h^n, Predictor.cpp:105-386): thread c writes its cell's x+ and y+ faces
+// (the domain's west and south boundary faces through the ghost cells i = 0,
+// j = 0) and the z face above it (plus the bottom face for k = nz-1), into
+// the face arrays the corrector's k_flux overwrites later in the step.  A
+// separate pass keeps the assembly's loads to six face values.
+__device__ __forceinline__ void faces_body(Dims d, Fields f, PassK pk, double* __restrict__ kx,
+                                           double* __restrict__ ky, double* __restrict__ kzf,
+                                           const int bid, const int G) {
+  for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
+       c += static_cast<long long>(G) * blockDim.x) {
+    int j, i, k;
+    unflatten(d, c, j, i, k);
+    const bool jin = j >= 1 && j <= d.ny, iin = i >= 1 && i <= d.nx;
+    if (jin && i <= d.nx) {
+      const long long e = c + d.sx;
+      const Flank a{pk.kcx[c], f.ksx[c], pk.wc[c], f.wcs[c], f.act[c]};
+      const Flank b{pk.kcx[e], f.ksx[e], pk.wc[e], f.wcs[e], f.act[e]};
+      const int code = (i == 0) ? f.xmc[col2(d, j, 1)] : f.xpc[col2(d, j, d.nx)];
+      kx[c] = face_lat(d, a, b, i == 0, i == d.nx, code);
+    }
+    if (iin && j <= d.ny) {
+      const long long n = c + d.sy;
+      const Flank a{pk.kcy[c], f.ksy[c], pk.wc[c], f.wcs[c], f.act[c]};
+      const Flank b{pk.kcy[n], f.ksy[n], pk.wc[n], f.wcs[n], f.act[n]};
+      const int code = (j == 0) ? f.ymc[col2(d, 1, i)] : f.ypc[col2(d, d.ny, i)];
+      ky[c] = face_lat(d, a, b, j == 0, j == d.ny, code);
+    }
+    if (jin && iin) {
+      const long long col = col2(d, j, i), fz = fidx(d, j, i, k);
+      const long long cu = (k >= 1) ? c - 1 : c;
+      const ZFlank zu{pk.kcz[cu], f.ksz[cu], f.dz[cu], (k >= 1) ? f.act[cu] : int8_t(0)};
+      const ZFlank zc{pk.kcz[c], f.ksz[c], f.dz[c], f.act[c]};
+      const int topc = f.topc[col], botc = f.botc[col];
+      kzf[fz] = face_z(d, zu, zc, k, topc, botc);
+      if (k == d.nz - 1) {
+        const ZFlank none{0.0, 0.0, 0.0, 0};
+        kzf[fz + 1] = face_z(d, zc, none, d.nz, topc, botc);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_faces(Dims d, Fields f, PassK pk, double* kx,
+                                                     double* ky, double* kzf) {
+  faces_body(d, f, pk, kx, ky, kzf, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- fluxes
@@ -643,98 +689,115 @@ __device__ inline Split gradient_split(const Dims& d, const SplitIn& n, int k) {
 // neighbour-saturation tests read the flags k_update_wc wrote from the same
 // snapshot.  Every load of an interior cell, its neighbours included, is
 // issued before the first branch on loaded data.
+// Classification of interior cell c (Reallocate.cpp:181-391) from the
+// pre-sweep snapshot wcR, hR: the restored theta and head, the fresh room
+// and the surplus sent up and down; accumulates the audit terms.
+struct CellPost {
+  double wout, hout, rm, up, dn;
+};
+
+__device__ __forceinline__ CellPost classify_cell(
+    const Dims& d, const Fields& f, const double* __restrict__ kx, const double* __restrict__ ky,
+    const double* __restrict__ kzf, const double* __restrict__ wcR,
+    const double* __restrict__ hR, const uint8_t* __restrict__ satf, long long c, int j, int i,
+    int k, double& adj, double& drop) {
+  const double before = wcR[c];
+  double wout = before, hout = hR[c], rm = 0.0, up = 0.0, dn = 0.0;
+  const long long col = col2(d, j, i), fz = fidx(d, j, i, k);
+  const long long cp = (k + 1 < d.nz) ? c + 1 : c, cm = (k >= 1) ? c - 1 : c;
+  SplitIn n;
+  n.hc = hout;
+  n.hxp = hR[c + d.sx];
+  n.hxm = hR[c - d.sx];
+  n.hyp = hR[c + d.sy];
+  n.hym = hR[c - d.sy];
+  n.hzp = hR[cp];
+  n.hzm = hR[cm];
+  n.kxp = kx[c];
+  n.kxm = kx[c - d.sx];
+  n.kyp = ky[c];
+  n.kym = ky[c - d.sy];
+  n.kzt = kzf[fz];
+  n.kzb = kzf[fz + 1];
+  n.dzc = f.dz[c];
+  n.dzp = f.dz[cp];
+  n.dzm = f.dz[cm];
+  n.axp = f.act[c + d.sx];
+  n.axm = f.act[c - d.sx];
+  n.ayp = f.act[c + d.sy];
+  n.aym = f.act[c - d.sy];
+  n.azp = (k + 1 < d.nz) ? f.act[cp] : 0;
+  n.azm = (k >= 1) ? f.act[cm] : 0;
+  const int8_t ac = f.act[c];
+  const uint8_t sxp = satf[c + d.sx], sxm = satf[c - d.sx], syp = satf[c + d.sy],
+                sym = satf[c - d.sy], szp = satf[cp], szm = satf[cm];
+  const int topc = f.topc[col];
+  const double topv = f.topv[col];
+  const Soil so = soil_at(f, c);
+  if (ac) {
+    const double volume = d.az * n.dzc;
+    if (before >= so.ts) {
+      if (!d.off) {
+        const double excess = (before - so.ts) * volume;
+        const Split sp = gradient_split(d, n, k);
+        up = excess * sp.up;
+        dn = excess * sp.down;
+        adj -= excess - up - dn;
+        drop += excess - up - dn;
+        wout = so.ts;
+      }
+    } else {
+      rm = (so.ts - before) * volume;
+      const bool top = (k == 0) || !n.azm;
+      const bool adjsat = (n.azp && szp) || (n.kxp != 0.0 && sxp) ||
+                          (n.kxm != 0.0 && sxm) || (n.kyp != 0.0 && syp) ||
+                          (n.kym != 0.0 && sym) ||
+                          (top ? (topc == kHead && topv >= 0.0) : (szm != 0));
+      if (!adjsat) {
+        if (before < 0.9999 * so.ts) hout = vg_head(so, before);
+      } else if (!d.off) {
+        const double after = vg_theta(so, hout);
+        wout = after;
+        rm = (so.ts - after) * volume;
+        if (d.redistribute && after < before) {
+          const double surplus = (before - after) * volume;
+          const Split sp = gradient_split(d, n, k);
+          up = surplus * sp.up;
+          dn = surplus * sp.down;
+          adj -= surplus - up - dn;
+          drop += surplus - up - dn;
+        } else {
+          adj += (after - before) * volume;
+          if (after < before) drop += (before - after) * volume;
+        }
+      }
+    }
+  }
+  return CellPost{wout, hout, rm, up, dn};
+}
+
 __device__ __forceinline__ void classify_body(
     Dims d, Fields f, const double* __restrict__ kx, const double* __restrict__ ky,
     const double* __restrict__ kzf, const double* __restrict__ wcR,
     const double* __restrict__ hR, const uint8_t* __restrict__ satf, double* __restrict__ wc_out,
     double* __restrict__ h_out, double* __restrict__ room, double* __restrict__ sup,
-    double* __restrict__ sdn, int* colflag, double* part_adj, double* part_drop, const int bid, const int G) {
+    double* __restrict__ sdn, int* colflag, double* part_adj, double* part_drop, const int bid,
+    const int G) {
   double adj = 0.0, drop = 0.0;
   for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
-    const double before = wcR[c];
-    double wout = before, hout = hR[c], rm = 0.0, up = 0.0, dn = 0.0;
-    const bool in = j >= 1 && j <= d.ny && i >= 1 && i <= d.nx;
-    if (in) {
-      const long long col = col2(d, j, i), fz = fidx(d, j, i, k);
-      const long long cp = (k + 1 < d.nz) ? c + 1 : c, cm = (k >= 1) ? c - 1 : c;
-      SplitIn n;
-      n.hc = hout;
-      n.hxp = hR[c + d.sx];
-      n.hxm = hR[c - d.sx];
-      n.hyp = hR[c + d.sy];
-      n.hym = hR[c - d.sy];
-      n.hzp = hR[cp];
-      n.hzm = hR[cm];
-      n.kxp = kx[c];
-      n.kxm = kx[c - d.sx];
-      n.kyp = ky[c];
-      n.kym = ky[c - d.sy];
-      n.kzt = kzf[fz];
-      n.kzb = kzf[fz + 1];
-      n.dzc = f.dz[c];
-      n.dzp = f.dz[cp];
-      n.dzm = f.dz[cm];
-      n.axp = f.act[c + d.sx];
-      n.axm = f.act[c - d.sx];
-      n.ayp = f.act[c + d.sy];
-      n.aym = f.act[c - d.sy];
-      n.azp = (k + 1 < d.nz) ? f.act[cp] : 0;
-      n.azm = (k >= 1) ? f.act[cm] : 0;
-      const int8_t ac = f.act[c];
-      const uint8_t sxp = satf[c + d.sx], sxm = satf[c - d.sx], syp = satf[c + d.sy],
-                    sym = satf[c - d.sy], szp = satf[cp], szm = satf[cm];
-      const int topc = f.topc[col];
-      const double topv = f.topv[col];
-      const Soil so = soil_at(f, c);
-      if (ac) {
-        const double volume = d.az * n.dzc;
-        if (before >= so.ts) {
-          if (!d.off) {
-            const double excess = (before - so.ts) * volume;
-            const Split sp = gradient_split(d, n, k);
-            up = excess * sp.up;
-            dn = excess * sp.down;
-            adj -= excess - up - dn;
-            drop += excess - up - dn;
-            wout = so.ts;
-          }
-        } else {
-          rm = (so.ts - before) * volume;
-          const bool top = (k == 0) || !n.azm;
-          const bool adjsat = (n.azp && szp) || (n.kxp != 0.0 && sxp) ||
-                              (n.kxm != 0.0 && sxm) || (n.kyp != 0.0 && syp) ||
-                              (n.kym != 0.0 && sym) ||
-                              (top ? (topc == kHead && topv >= 0.0) : (szm != 0));
-          if (!adjsat) {
-            if (before < 0.9999 * so.ts) hout = vg_head(so, before);
-          } else if (!d.off) {
-            const double after = vg_theta(so, hout);
-            wout = after;
-            rm = (so.ts - after) * volume;
-            if (d.redistribute && after < before) {
-              const double surplus = (before - after) * volume;
-              const Split sp = gradient_split(d, n, k);
-              up = surplus * sp.up;
-              dn = surplus * sp.down;
-              adj -= surplus - up - dn;
-              drop += surplus - up - dn;
-            } else {
-              adj += (after - before) * volume;
-              if (after < before) drop += (before - after) * volume;
-            }
-          }
-        }
-        if (up > 0.0 || dn > 0.0) colflag[col] = 1;
-      }
+    CellPost r{wcR[c], hR[c], 0.0, 0.0, 0.0};
+    if (j >= 1 && j <= d.ny && i >= 1 && i <= d.nx) {
+      r = classify_cell(d, f, kx, ky, kzf, wcR, hR, satf, c, j, i, k, adj, drop);
+      if (r.up > 0.0 || r.dn > 0.0) colflag[col2(d, j, i)] = 1;
     }
-    wc_out[c] = wout;
-    h_out[c] = hout;
-    room[c] = rm;
-    sup[c] = up;
-    sdn[c] = dn;
+    wc_out[c] = r.wout;
+    h_out[c] = r.hout;
+    room[c] = r.rm;
+    sup[c] = r.up;
+    sdn[c] = r.dn;
   }
   const double s1 = block_reduce(adj, SumOp(), 0.0);
   if (threadIdx.x == 0) part_adj[bid] = s1;
@@ -893,6 +956,55 @@ __device__ inline void walk_take(double& dv, int m, double* rs, double* ws, cons
   if (!(rs[m] > 0.0)) rbits[m >> 5] &= ~(1u << (m & 31));
 }
 
+// Lane 0's send walks of surplus cell kk (sent up upv, sent down dnv) on a
+// staged column (Reallocate.cpp:410-540): upward through the cells with room
+// up to the first inactive cell above or the surface, then out through a
+// head top or back down; downward to the bottom; what finds no room is lost.
+__device__ inline void walk_cell(int kk, double upv, double dnv, int nz, bool topHead, double* rs,
+                                 double* ws, const double* vs, double* qs, unsigned* rbits,
+                                 const unsigned* ibits, double dtg, double& lost) {
+  double dv = upv;
+  if (dv > 0.0) {
+    // Upward: cells kk-1, kk-2, ... up to the first inactive cell above
+    // kk (exclusive) or the surface.
+    const int lim = bits_highest(ibits, 0, kk - 1) + 1;
+    int ll = kk;
+    while (dv > 0.0) {
+      const int m = bits_highest(rbits, lim, ll - 1);
+      if (m < 0) {
+        ll = lim;
+        break;
+      }
+      walk_take(dv, m, rs, ws, vs, qs, rbits, m + 1, true, dtg);
+      ll = m;
+    }
+    if (dv > 0.0) {
+      if (topHead) {
+        qs[ll] += dv / dtg;
+      } else {
+        while (dv > 0.0) {
+          const int m = bits_lowest(rbits, ll + 1, nz - 1);
+          if (m < 0) break;
+          walk_take(dv, m, rs, ws, vs, qs, rbits, m, false, dtg);
+          ll = m;
+        }
+        lost -= dv;
+      }
+    }
+  }
+  dv = dnv;
+  if (dv > 0.0) {
+    int ll = kk;
+    while (dv > 0.0) {
+      const int m = bits_lowest(rbits, ll + 1, nz - 1);
+      if (m < 0) break;
+      walk_take(dv, m, rs, ws, vs, qs, rbits, m, false, dtg);
+      ll = m;
+    }
+    lost -= dv;
+  }
+}
+
 __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ room,
                                                  const double* __restrict__ sup,
@@ -955,49 +1067,8 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
         mask &= mask - 1;
         const double upv = __shfl_sync(0xffffffffu, su, b);
         const double dnv = __shfl_sync(0xffffffffu, sd, b);
-        if (lane == 0) {
-          const int kk = k0 + b;
-          double dv = upv;
-          if (dv > 0.0) {
-            // Upward: cells kk-1, kk-2, ... up to the first inactive cell above
-            // kk (exclusive) or the surface.
-            const int lim = bits_highest(ibits, 0, kk - 1) + 1;
-            int ll = kk;
-            while (dv > 0.0) {
-              const int m = bits_highest(rbits, lim, ll - 1);
-              if (m < 0) {
-                ll = lim;
-                break;
-              }
-              walk_take(dv, m, rs, ws, vs, qs, rbits, m + 1, true, dtg);
-              ll = m;
-            }
-            if (dv > 0.0) {
-              if (topHead) {
-                qs[ll] += dv / dtg;
-              } else {
-                while (dv > 0.0) {
-                  const int m = bits_lowest(rbits, ll + 1, nz - 1);
-                  if (m < 0) break;
-                  walk_take(dv, m, rs, ws, vs, qs, rbits, m, false, dtg);
-                  ll = m;
-                }
-                lost -= dv;
-              }
-            }
-          }
-          dv = dnv;
-          if (dv > 0.0) {
-            int ll = kk;
-            while (dv > 0.0) {
-              const int m = bits_lowest(rbits, ll + 1, nz - 1);
-              if (m < 0) break;
-              walk_take(dv, m, rs, ws, vs, qs, rbits, m, false, dtg);
-              ll = m;
-            }
-            lost -= dv;
-          }
-        }
+        if (lane == 0) walk_cell(k0 + b, upv, dnv, nz, topHead, rs, ws, vs, qs, rbits, ibits, dtg,
+                                 lost);
         __syncwarp();
       }
     }
@@ -1023,15 +1094,83 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
 // finalizeWaterContent (Corrector.cpp:758-792), accumulateBoundaryFlux
 // (RichardsSolver.cpp:961-1006), the adaptTimeStep inputs (AdaptiveStep.cpp:
 // 58-98) and the owned volume (RichardsSolver.cpp:892-912), in one sweep.
-__device__ __forceinline__ void finalize_body(Dims d, Fields f, double* __restrict__ wc,
-                                                        double* __restrict__ vloss,
-                                                        const double* __restrict__ qx,
-                                                        const double* __restrict__ qy,
-                                                        const double* __restrict__ qzf,
-                                                        const double* __restrict__ dtgp,
-                                                        double co_max, double* partial, int nblk, const int bid, const int G) {
-  const double dtg = *dtgp;
+// Clamp, clamp loss, boundary inflow and controller inputs of active interior
+// cell c (finalizeWaterContent, Corrector.cpp:758-792; accumulateBoundaryFlux,
+// RichardsSolver.cpp:961-1006; adaptTimeStep's dq and Courant terms,
+// AdaptiveStep.cpp:58-98; ownedVolume) from its values loaded by the caller;
+// returns the clamped moisture.
+struct FinIn {
+  double w0, dzc, ts, tr, qxp, qxm, qyp, qym, qzt, qzb, axc, ayc, vga, vgn, ksz;
+  bool top;
+};
+
+struct FinAcc {
   double vl = 0.0, inflow = 0.0, dqmax = -DBL_MAX, dtco = DBL_MAX, vol = 0.0;
+};
+
+__device__ __forceinline__ double finalize_cell(const Dims& d, const FinIn& v, long long c, int j,
+                                                int i, int k, double dtg, double co_max,
+                                                double* __restrict__ vloss, FinAcc& acc) {
+  const double volume = d.az * v.dzc;
+  double w = v.w0;
+  if (w > v.ts) {
+    const double ex = (w - v.ts) * volume;
+    vloss[c] += ex;
+    acc.vl += ex;
+    w = v.ts;
+  } else if (w < v.tr) {
+    const double de = (v.tr - w) * volume;
+    vloss[c] -= de;
+    acc.vl -= de;
+    w = v.tr;
+  }
+  acc.vol += w * d.az * v.dzc;
+  if (v.top) acc.inflow -= v.qzt * dtg;
+  if (k == d.nz - 1) acc.inflow += v.qzb * dtg;
+  if (i == 1) acc.inflow -= v.qxm * dtg;
+  if (i == d.nx) acc.inflow += v.qxp * dtg;
+  if (j == 1) acc.inflow -= v.qym * dtg;
+  if (j == d.ny) acc.inflow += v.qyp * dtg;
+  if (!v.top) {
+    const double qin = v.qxp / v.axc + v.qyp / v.ayc + v.qzb / d.az;
+    const double qou = v.qxm / v.axc + v.qym / v.ayc + v.qzt / d.az;
+    const double dq = fabs(qin - qou) * dtg / v.dzc;
+    if (dq > acc.dqmax) acc.dqmax = dq;
+    if (w < v.ts) {
+      const Soil so{v.vga, v.vgn, v.ts, v.tr, 0.0};
+      const double dk = vg_dkdtheta(so, w, v.ksz);
+      const double t = co_max * v.dzc / dk;
+      if (t < acc.dtco) acc.dtco = t;
+    }
+  }
+  return w;
+}
+
+// The finalize reductions of a block into the partial slots.
+__device__ __forceinline__ void finalize_reduce(const FinAcc& acc, double* partial, int nblk,
+                                                int bid) {
+  double s = block_reduce(acc.vl, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[kPVloss * nblk + bid] = s;
+  s = block_reduce(acc.inflow, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[kPInflow * nblk + bid] = s;
+  s = block_reduce(acc.dqmax, MaxOp(), -DBL_MAX);
+  if (threadIdx.x == 0) partial[kPDqmax * nblk + bid] = s;
+  s = block_reduce(acc.dtco, MinOp(), DBL_MAX);
+  if (threadIdx.x == 0) partial[kPDtco * nblk + bid] = s;
+  s = block_reduce(acc.vol, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[kPVol * nblk + bid] = s;
+}
+
+__device__ __forceinline__ void finalize_body(Dims d, Fields f, double* __restrict__ wc,
+                                              double* __restrict__ vloss,
+                                              const double* __restrict__ qx,
+                                              const double* __restrict__ qy,
+                                              const double* __restrict__ qzf,
+                                              const double* __restrict__ dtgp, double co_max,
+                                              double* partial, int nblk, const int bid,
+                                              const int G) {
+  const double dtg = *dtgp;
+  FinAcc acc;
   for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
@@ -1041,59 +1180,28 @@ __device__ __forceinline__ void finalize_body(Dims d, Fields f, double* __restri
     const long long cu = (k >= 1) ? c - 1 : c;
     const int8_t ac = f.act[c];
     const int8_t au = (k >= 1) ? f.act[cu] : int8_t(0);
-    const double dzc = f.dz[c], ts = f.wcs[c], tr = f.wcr[c];
-    const double w0 = wc[c];
-    const double qxp = qx[c], qxm = qx[c - d.sx], qyp = qy[c], qym = qy[c - d.sy];
-    const double qzt = qzf[fz], qzb = qzf[fz + 1];
-    const double axc = f.ax[c], ayc = f.ay[c];
-    const double vga = f.vga[c], vgn = f.vgn[c], ksz = f.ksz[c];
+    FinIn v;
+    v.w0 = wc[c];
+    v.dzc = f.dz[c];
+    v.ts = f.wcs[c];
+    v.tr = f.wcr[c];
+    v.qxp = qx[c];
+    v.qxm = qx[c - d.sx];
+    v.qyp = qy[c];
+    v.qym = qy[c - d.sy];
+    v.qzt = qzf[fz];
+    v.qzb = qzf[fz + 1];
+    v.axc = f.ax[c];
+    v.ayc = f.ay[c];
+    v.vga = f.vga[c];
+    v.vgn = f.vgn[c];
+    v.ksz = f.ksz[c];
+    v.top = (k == 0) || !au;
     if (!ac) continue;
-    const double volume = d.az * dzc;
-    double w = w0;
-    if (w > ts) {
-      const double ex = (w - ts) * volume;
-      vloss[c] += ex;
-      vl += ex;
-      w = ts;
-      wc[c] = w;
-    } else if (w < tr) {
-      const double de = (tr - w) * volume;
-      vloss[c] -= de;
-      vl -= de;
-      w = tr;
-      wc[c] = w;
-    }
-    vol += w * d.az * dzc;
-    const bool top = (k == 0) || !au;
-    if (top) inflow -= qzt * dtg;
-    if (k == d.nz - 1) inflow += qzb * dtg;
-    if (i == 1) inflow -= qxm * dtg;
-    if (i == d.nx) inflow += qxp * dtg;
-    if (j == 1) inflow -= qym * dtg;
-    if (j == d.ny) inflow += qyp * dtg;
-    if (!top) {
-      const double qin = qxp / axc + qyp / ayc + qzb / d.az;
-      const double qou = qxm / axc + qym / ayc + qzt / d.az;
-      const double dq = fabs(qin - qou) * dtg / dzc;
-      if (dq > dqmax) dqmax = dq;
-      if (w < ts) {
-        const Soil so{vga, vgn, ts, tr, 0.0};
-        const double dk = vg_dkdtheta(so, w, ksz);
-        const double t = co_max * dzc / dk;
-        if (t < dtco) dtco = t;
-      }
-    }
+    const double w = finalize_cell(d, v, c, j, i, k, dtg, co_max, vloss, acc);
+    if (w != v.w0) wc[c] = w;
   }
-  double s = block_reduce(vl, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[kPVloss * nblk + bid] = s;
-  s = block_reduce(inflow, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[kPInflow * nblk + bid] = s;
-  s = block_reduce(dqmax, MaxOp(), -DBL_MAX);
-  if (threadIdx.x == 0) partial[kPDqmax * nblk + bid] = s;
-  s = block_reduce(dtco, MinOp(), DBL_MAX);
-  if (threadIdx.x == 0) partial[kPDtco * nblk + bid] = s;
-  s = block_reduce(vol, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[kPVol * nblk + bid] = s;
+  finalize_reduce(acc, partial, nblk, bid);
 }
 
 __global__ void __launch_bounds__(kBlock, 3) k_finalize(Dims d, Fields f, double* __restrict__ wc,
@@ -1254,9 +1362,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_assemble_batch(const StepArgs* ta
   __shared__ StepArgs sa;
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
+  assemble_body(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp,
+                sa.gyp, sa.gzp, sa.rhs, bid, G);
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_faces_batch(const StepArgs* tab, const int* first,
+                                                           int n) {
+  __shared__ StepArgs sa;
+  int bid, G;
+  load_member(tab, first, n, sa, bid, G);
   const PassK pk{sa.kcx, sa.kcy, sa.kcz, sa.wcn};
-  assemble_body(sa.d, sa.f, pk, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp, sa.gyp, sa.gzp,
-                sa.rhs, bid, G);
+  faces_body(sa.d, sa.f, pk, sa.kx, sa.ky, sa.kzf, bid, G);
 }
 
 __global__ void __launch_bounds__(kBlock) k_closure_corr_batch(const StepArgs* tab,
@@ -1376,11 +1492,14 @@ void launch_closure_pred(const Device& D, const double* h) {
   ++D.launches;
 }
 
+// The predictor's faces go through D.kx, D.ky, D.kzf (free until k_flux).
 void launch_assemble(const Device& D, const double* hn, const double* wcn) {
-  PassK pk{D.kcx, D.kcy, D.kcz, wcn};
-  k_assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, hn, wcn, D.ch, dtg_slot(D), D.diag,
-                                                     D.gxp, D.gyp, D.gzp, D.rhs);
-  ++D.launches;
+  const PassK pk{D.kcx, D.kcy, D.kcz, wcn};
+  k_faces<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.kx, D.ky, D.kzf);
+  k_assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.kx, D.ky, D.kzf, hn, wcn, D.ch,
+                                                     dtg_slot(D), D.diag, D.gxp, D.gyp, D.gzp,
+                                                     D.rhs);
+  D.launches += 2;
 }
 
 void launch_closure_corr(const Device& D, const double* hn) {
@@ -1567,6 +1686,7 @@ cudaError_t batch_predictor(const PhaseTables& t, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   k_ghosts_batch<<<t.grid_ghost, kBlock, 0, s>>>(t.tab, t.first_ghost, t.n);
   k_closure_pred_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
+  k_faces_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
   k_assemble_batch<<<t.grid_cells, kBlock, 0, s>>>(t.tab, t.first_cells, t.n);
   if (t.grid_factor > 0) {
     e = launch_line_factor_batch(t, s);
