@@ -44,9 +44,10 @@ def _declare(lib):
                                             C.POINTER(C.c_double)]
     lib.frehg_gw_batch_stats.argtypes = [B, C.POINTER(BatchStats)]
     lib.frehg_gw_batch_solve_blocks.argtypes = [B, C.POINTER(C.c_int)]
+    lib.frehg_gw_batch_set_members.argtypes = [B, C.POINTER(C.c_void_p), C.c_int]
     for name in ("frehg_gw_batch_create", "frehg_gw_batch_destroy", "frehg_gw_batch_step",
                  "frehg_gw_batch_set_dt", "frehg_gw_batch_autotune", "frehg_gw_batch_stats",
-                 "frehg_gw_batch_solve_blocks"):
+                 "frehg_gw_batch_solve_blocks", "frehg_gw_batch_set_members"):
         getattr(lib, name).restype = C.c_int
     del H
     lib._batch_declared = True
@@ -107,6 +108,13 @@ class RichardsBatch:
                 s._info = info
         _check(self.lib, rc)
         return out
+
+    def set_members(self, solvers: Iterable[RichardsSolver]) -> None:
+        """Rebinds the batch to a new member list, reusing its buffers."""
+        self.members = list(solvers)
+        n = len(self.members)
+        arr = (C.c_void_p * n)(*[s.h.value for s in self.members])
+        _check(self.lib, self.lib.frehg_gw_batch_set_members(self.b, arr, n))
 
     def set_dt(self, i: int, dtg: float) -> None:
         _check(self.lib, self.lib.frehg_gw_batch_set_dt(self.b, i, dtg))

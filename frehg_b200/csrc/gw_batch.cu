@@ -96,8 +96,14 @@ int solve_max_blocks(const Device& D, const SolveClass& c) {
   return std::max(1, cap);
 }
 
+size_t solve_group_bytes(const SolveClass& c, int n) {
+  auto r = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  return r(args_bytes(c) * n) + r(sizeof(int) * (n + 1)) + r(sizeof(CgState*) * n);
+}
+
 cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
-                              const std::vector<int>& nb, const std::vector<SolveParams>& p) {
+                              const std::vector<int>& nb, const std::vector<SolveParams>& p,
+                              void* mem) {
   g.cls = c;
   g.n = static_cast<int>(ds.size());
   const size_t ab = args_bytes(c);
@@ -113,10 +119,12 @@ cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vec
     if (c.kind == 1) g.smem = std::max(g.smem, mixed_batch_smem(*ds[i], c.variant));
   }
   g.grid = first.back();
-  cudaError_t e = cudaMalloc(&g.tab, tab.size());
-  if (e == cudaSuccess) e = cudaMalloc(&g.first, first.size() * sizeof(int));
-  if (e == cudaSuccess) e = cudaMalloc(&g.states, st.size() * sizeof(CgState*));
-  if (e == cudaSuccess) e = cudaMemcpy(g.tab, tab.data(), tab.size(), cudaMemcpyHostToDevice);
+  auto r = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  char* base = static_cast<char*>(mem);
+  g.tab = base;
+  g.first = reinterpret_cast<int*>(base + r(tab.size()));
+  g.states = reinterpret_cast<CgState**>(base + r(tab.size()) + r(first.size() * sizeof(int)));
+  cudaError_t e = cudaMemcpy(g.tab, tab.data(), tab.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(g.first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
@@ -136,14 +144,6 @@ cudaError_t solve_group_launch(const SolveGroup& g, cudaStream_t s) {
                                      g.smem, s);
 }
 
-void solve_group_free(SolveGroup& g) {
-  if (g.tab) cudaFree(g.tab);
-  if (g.first) cudaFree(g.first);
-  if (g.states) cudaFree(g.states);
-  g.tab = nullptr;
-  g.first = nullptr;
-  g.states = nullptr;
-}
 
 }  // namespace fgw
 
@@ -163,6 +163,8 @@ struct frehg_gw_batch {
   long long steps = 0;
   std::string graph_error;          // why graphs were given up, if they were
   fgw::PhaseTables phases;          // batched non-solve phases
+  void* group_mem = nullptr;        // the solve groups' tables
+  size_t group_cap = 0;
   cudaEvent_t ev[4] = {};           // step start, after predictor, after solves, end
   double phase_ms[3] = {0, 0, 0};   // of the last step
 };
@@ -172,10 +174,7 @@ namespace {
 constexpr int kDefaultCellsPerBlock = 16384;
 constexpr int kDefaultStreams = 32;
 
-void free_groups(frehg_gw_batch* b) {
-  for (auto& g : b->groups) fgw::solve_group_free(g);
-  b->groups.clear();
-}
+void free_groups(frehg_gw_batch* b) { b->groups.clear(); }
 
 void drop_graphs(frehg_gw_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
@@ -201,6 +200,13 @@ int build_groups(frehg_gw_batch* b) {
   }
   // Members of one class share a launch while their blocks fit the device
   // co-resident; a class that needs more takes several launches in turn.
+  struct Spec {
+    fgw::SolveClass c;
+    std::vector<fgw::Device*> ds;
+    std::vector<int> nbs;
+    std::vector<fgw::SolveParams> ps;
+  };
+  std::vector<Spec> specs;
   std::vector<bool> done(n, false);
   for (int i = 0; i < n; ++i) {
     if (done[i]) continue;
@@ -212,39 +218,46 @@ int build_groups(frehg_gw_batch* b) {
     const int per_sm = fgw::solve_blocks_per_sm(c, smem);
     if (per_sm < 1) return fail(FREHG_GW_ECUDA, "batch: solve kernel cannot be resident");
     const int cap = per_sm * b->m[i]->D.sm_count;
-    std::vector<fgw::Device*> ds;
-    std::vector<int> nbs;
-    std::vector<fgw::SolveParams> ps;
+    Spec cur{c, {}, {}, {}};
     int used = 0;
-    auto flush = [&]() -> int {
-      if (ds.empty()) return FREHG_GW_OK;
-      fgw::SolveGroup g;
-      const cudaError_t e = fgw::solve_group_build(g, c, ds, nbs, ps);
-      b->groups.push_back(g);
-      if (e != cudaSuccess) return cuda_fail(e, "batch: solve group");
-      ds.clear();
-      nbs.clear();
-      ps.clear();
-      used = 0;
-      return FREHG_GW_OK;
-    };
     for (int j = i; j < n; ++j) {
       if (done[j] || !(cls[j] == c)) continue;
       const int take = std::min(b->nb[j], cap);
       b->nb[j] = take;
       if (used + take > cap) {
-        const int rc = flush();
-        if (rc != FREHG_GW_OK) return rc;
+        specs.push_back(cur);
+        cur = Spec{c, {}, {}, {}};
+        used = 0;
       }
       frehg_gw_handle* h = b->m[j];
-      ds.push_back(&h->D);
-      nbs.push_back(take);
-      ps.push_back(fgw::SolveParams{h->rtol, h->atol, h->outer_rtol, h->maxit, h->max_outer});
+      cur.ds.push_back(&h->D);
+      cur.nbs.push_back(take);
+      cur.ps.push_back(fgw::SolveParams{h->rtol, h->atol, h->outer_rtol, h->maxit, h->max_outer});
       used += take;
       done[j] = true;
     }
-    const int rc = flush();
-    if (rc != FREHG_GW_OK) return rc;
+    if (!cur.ds.empty()) specs.push_back(cur);
+  }
+  // One device allocation for every group's tables, kept while it fits.
+  size_t need = 0;
+  for (const auto& sp : specs) need += fgw::solve_group_bytes(sp.c, static_cast<int>(sp.ds.size()));
+  if (need > b->group_cap) {
+    const size_t cap = std::max(need, 2 * b->group_cap);
+    if (b->group_mem) cudaFree(b->group_mem);
+    b->group_mem = nullptr;
+    b->group_cap = 0;
+    const cudaError_t e = cudaMalloc(&b->group_mem, cap);
+    if (e != cudaSuccess) return cuda_fail(e, "batch: solve tables");
+    b->group_cap = cap;
+  }
+  size_t off = 0;
+  for (const auto& sp : specs) {
+    fgw::SolveGroup g;
+    const cudaError_t e = fgw::solve_group_build(g, sp.c, sp.ds, sp.nbs, sp.ps,
+                                                 static_cast<char*>(b->group_mem) + off);
+    if (e != cudaSuccess) return cuda_fail(e, "batch: solve group");
+    off += fgw::solve_group_bytes(sp.c, static_cast<int>(sp.ds.size()));
+    b->groups.push_back(g);
   }
   return FREHG_GW_OK;
 }
@@ -321,6 +334,20 @@ cudaError_t enqueue_member_phases(frehg_gw_batch* b, long long* kernels) {
   for (auto* h : b->m) after += h->D.launches;
   *kernels = (after - before) + solves;
   return e;
+}
+
+// The solve groups and the phase tables of the current members.
+int build_member_tables(frehg_gw_batch* b) {
+  int rc = build_groups(b);
+  if (rc != FREHG_GW_OK) return rc;
+  std::vector<const fgw::Device*> ds;
+  std::vector<int> mixed;
+  for (auto* h : b->m) {
+    ds.push_back(&h->D);
+    mixed.push_back(h->precision == FREHG_GW_PRECISION_MIXED ? 1 : 0);
+  }
+  const cudaError_t ep = fgw::phase_tables_build(b->phases, ds, mixed);
+  return ep == cudaSuccess ? FREHG_GW_OK : cuda_fail(ep, "batch: phase tables");
 }
 
 std::vector<unsigned char> parities(const frehg_gw_batch* b) {
@@ -482,7 +509,11 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
   b->m.assign(members, members + n);
   if (opts) b->opts = *opts;
   else b->opts.use_graph = 1;
-  const int P = std::max(1, std::min(n, b->opts.streams > 0 ? b->opts.streams : kDefaultStreams));
+  // The stream pool serves the member-by-member path only.
+  const int P = b->opts.per_member_phases
+                    ? std::max(1, std::min(n, b->opts.streams > 0 ? b->opts.streams
+                                                                  : kDefaultStreams))
+                    : 0;
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   b->pool.resize(P, nullptr);
   b->join1.resize(P, nullptr);
@@ -496,17 +527,7 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork1, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork2, cudaEventDisableTiming);
   int rc = (e == cudaSuccess) ? FREHG_GW_OK : cuda_fail(e, "batch: streams");
-  if (rc == FREHG_GW_OK) rc = build_groups(b);
-  if (rc == FREHG_GW_OK) {
-    std::vector<const fgw::Device*> ds;
-    std::vector<int> mixed;
-    for (auto* h : b->m) {
-      ds.push_back(&h->D);
-      mixed.push_back(h->precision == FREHG_GW_PRECISION_MIXED ? 1 : 0);
-    }
-    const cudaError_t ep = fgw::phase_tables_build(b->phases, ds, mixed);
-    if (ep != cudaSuccess) rc = cuda_fail(ep, "batch: phase tables");
-  }
+  if (rc == FREHG_GW_OK) rc = build_member_tables(b);
   if (rc != FREHG_GW_OK) {
     frehg_gw_batch_destroy(b);
     return rc;
@@ -515,11 +536,24 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
   return FREHG_GW_OK;
 }
 
+int frehg_gw_batch_set_members(frehg_gw_batch* b, frehg_gw_handle* const* members, int n) {
+  if (!b || !members || n < 1) return fail(FREHG_GW_EINVAL, "batch: null argument or n < 1");
+  for (int i = 0; i < n; ++i) {
+    if (!members[i]) return fail(FREHG_GW_EINVAL, "batch: null member");
+    if (!members[i]->have_state) return fail(FREHG_GW_ESTATE, "batch: member without state");
+  }
+  const cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "batch: set members");
+  b->m.assign(members, members + n);
+  return build_member_tables(b);
+}
+
 int frehg_gw_batch_destroy(frehg_gw_batch* b) {
   if (!b) return FREHG_GW_OK;
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graphs(b);
   free_groups(b);
+  if (b->group_mem) cudaFree(b->group_mem);
   fgw::phase_tables_free(b->phases);
   for (auto s : b->pool) if (s) cudaStreamDestroy(s);
   for (auto ev : b->join1) if (ev) cudaEventDestroy(ev);

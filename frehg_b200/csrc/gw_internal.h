@@ -165,7 +165,9 @@ struct PhaseTables {
   size_t walk_smem = 0, factor_smem = 0;
   StepOut* outs = nullptr;       // device, n step records gathered
   StepOut* outs_host = nullptr;  // pinned
+  int cap = 0;                   // members the buffers hold (reused while n <= cap)
 };
+// (Re)builds the tables for the members `ds`, reusing the buffers while they fit.
 cudaError_t phase_tables_build(PhaseTables& t, const std::vector<const Device*>& ds,
                                const std::vector<int>& mixed);
 void phase_tables_free(PhaseTables& t);
@@ -213,12 +215,15 @@ struct SolveGroup {
   int* first = nullptr;          // device block offsets, n + 1
   CgState** states = nullptr;    // device array of the members' CG states
 };
-// Builds a group over `ds` with `nb[i]` blocks each (all of class `c`).
+// Device bytes a group of n members of class c needs for its tables.
+size_t solve_group_bytes(const SolveClass& c, int n);
+// Builds a group over `ds` with `nb[i]` blocks each (all of class `c`), its
+// tables placed in `mem` (solve_group_bytes of device memory the caller owns).
 cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
-                              const std::vector<int>& nb, const std::vector<SolveParams>& p);
+                              const std::vector<int>& nb, const std::vector<SolveParams>& p,
+                              void* mem);
 // Zeroes the members' CG states and launches the group on `s`.
 cudaError_t solve_group_launch(const SolveGroup& g, cudaStream_t s);
-void solve_group_free(SolveGroup& g);
 
 // Per-kind pieces of the batched solves (gw_cg.cu, gw_cg_mixed.cu).
 size_t cg64_args_bytes();

@@ -1636,6 +1636,21 @@ void fill_step_args(const Device& D, bool mixed, double dtg, double co_max, doub
 cudaError_t phase_tables_build(PhaseTables& t, const std::vector<const Device*>& ds,
                                const std::vector<int>& mixed) {
   t.n = static_cast<int>(ds.size());
+  cudaError_t e = cudaSuccess;
+  if (t.n > t.cap) {
+    // Grow (sizes first: freeing resets the record).
+    const int n = t.n, cap = std::max(t.n, 2 * t.cap);
+    phase_tables_free(t);
+    t.n = n;
+    t.cap = cap;
+    e = cudaMalloc(&t.tab, sizeof(StepArgs) * cap);
+    if (e == cudaSuccess) e = cudaMallocHost(&t.tab_host, sizeof(StepArgs) * cap);
+    if (e == cudaSuccess) e = cudaMalloc(&t.first_cells, sizeof(int) * (cap + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&t.first_ghost, sizeof(int) * (cap + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&t.first_factor, sizeof(int) * (cap + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&t.outs, sizeof(StepOut) * cap);
+    if (e == cudaSuccess) e = cudaMallocHost(&t.outs_host, sizeof(StepOut) * cap);
+  }
   std::vector<int> fc(t.n + 1, 0), fg(t.n + 1, 0), ff(t.n + 1, 0);
   t.walk_smem = 0;
   t.factor_smem = 0;
@@ -1651,13 +1666,6 @@ cudaError_t phase_tables_build(PhaseTables& t, const std::vector<const Device*>&
   t.grid_cells = fc.back();
   t.grid_ghost = fg.back();
   t.grid_factor = ff.back();
-  cudaError_t e = cudaMalloc(&t.tab, sizeof(StepArgs) * t.n);
-  if (e == cudaSuccess) e = cudaMallocHost(&t.tab_host, sizeof(StepArgs) * t.n);
-  if (e == cudaSuccess) e = cudaMalloc(&t.first_cells, sizeof(int) * (t.n + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&t.first_ghost, sizeof(int) * (t.n + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&t.first_factor, sizeof(int) * (t.n + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&t.outs, sizeof(StepOut) * t.n);
-  if (e == cudaSuccess) e = cudaMallocHost(&t.outs_host, sizeof(StepOut) * t.n);
   if (e == cudaSuccess)
     e = cudaMemcpy(t.first_cells, fc.data(), sizeof(int) * fc.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)

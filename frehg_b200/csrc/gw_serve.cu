@@ -2,16 +2,19 @@
 //
 // Requests arrive with their whole input (domain, soil, boundary codes and
 // values, initial state, step count) and are copied at submission, so the
-// caller's buffers can be reused at once.  Each tick:
+// caller's buffers can be reused at once.  A worker thread admits queued
+// requests in arrival order while the device-memory budget and the slot count
+// allow (it builds each request's handle and state on the device, where the
+// state stays until the request finishes) and retires finished ones (head and
+// theta copied to host memory, device state freed, latency recorded), so that
+// host-side set-up and read-back overlap the device work.  Each tick of the
+// caller's thread:
 //
-//   1. admits queued requests in arrival order while the device-memory budget
-//      and the slot count allow: creates the request's handle and state on
-//      the device, where it stays until the request finishes;
-//   2. steps every admitted request once, each with its own adaptive dt, as
-//      one batch (frehg_gw_batch_*): the requests' work overlaps on the device
-//      and their solves share cooperative launches;
-//   3. retires finished requests: copies head and theta to host memory, frees
-//      the device state and records the request's latency.
+//   1. takes the requests the worker has made ready into the running set;
+//   2. steps every running request once, each with its own adaptive dt, as one
+//      batch (frehg_gw_batch_*): the requests' work overlaps on the device and
+//      their solves share cooperative launches;
+//   3. hands the requests that have taken all their steps to the worker.
 //
 // A request's arithmetic depends on its own inputs and the server options
 // only: its solve's block count comes from its own size, and its dt sequence
@@ -21,10 +24,13 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gw_handle.h"
@@ -71,16 +77,31 @@ void copy_in(std::vector<T>& dst, const T* src, size_t n) {
 
 struct frehg_gw_server {
   frehg_gw_server_opts opts{};
-  size_t budget = 0, used = 0;
+  size_t budget = 0;
+  int slots = 64;
+  int device = 0;
   Clock::time_point t0;
+  // Shared with the worker (under mu).
+  std::mutex mu;
+  std::condition_variable cv;   // wakes the worker
+  std::condition_variable done; // wakes a tick waiting for the worker
+  bool stop = false;
   long long next_id = 1;
-  std::deque<std::unique_ptr<Request>> queue;
-  std::vector<std::unique_ptr<Request>> active;
+  size_t used = 0;              // device memory held by admitted requests
+  int held = 0;                 // requests being admitted, ready or running
+  int busy = 0;                 // requests the worker is admitting or retiring
+  std::deque<std::unique_ptr<Request>> queue, retiring;
+  std::vector<std::unique_ptr<Request>> ready;
   std::map<long long, std::unique_ptr<Request>> finished;
+  long long completed = 0;
+  double admit_s = 0.0, retire_s = 0.0;
+  // The ticking thread's own.
+  std::vector<std::unique_ptr<Request>> active;
   frehg_gw_batch* batch = nullptr;
   bool dirty = true;
-  long long ticks = 0, cell_steps = 0, completed = 0;
-  double busy_s = 0.0;
+  long long ticks = 0, cell_steps = 0;
+  double busy_s = 0.0, rebatch_s = 0.0, step_s = 0.0;
+  std::thread worker;
 };
 
 namespace {
@@ -90,8 +111,8 @@ double now_s(const frehg_gw_server* s) {
 }
 
 // Finishes request r (success or failure): keeps head and theta on the host,
-// frees its device state.
-void retire(frehg_gw_server* s, Request* r, int status, const std::string& err) {
+// frees its device state.  Worker thread, outside the lock.
+void finish(Request* r, int status, const std::string& err) {
   r->status = status;
   r->error = err;
   if (status == FREHG_GW_OK && r->h) {
@@ -107,15 +128,12 @@ void retire(frehg_gw_server* s, Request* r, int status, const std::string& err) 
   if (r->h) {
     frehg_gw_destroy(r->h);
     r->h = nullptr;
-    s->used -= std::min(s->used, r->bytes);
   }
   r->state = (r->status == FREHG_GW_OK) ? FREHG_GW_REQ_DONE : FREHG_GW_REQ_FAILED;
-  r->t_done = now_s(s);
-  ++s->completed;
-  s->dirty = true;
 }
 
-// Creates the device state of a queued request; returns a status.
+// Creates the device state of a queued request; returns a status.  Worker
+// thread, outside the lock.
 int admit(Request* r) {
   frehg_gw_handle* h = nullptr;
   int rc = frehg_gw_create(&r->desc, &h);
@@ -135,12 +153,84 @@ int admit(Request* r) {
   return FREHG_GW_OK;
 }
 
+// The worker: retirements first (they free memory and slots), then
+// admissions in arrival order while the budget and the slots allow.
+void worker_loop(frehg_gw_server* s) {
+  cudaSetDevice(s->device);  // the device of the thread that created the server
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop) {
+    if (!s->retiring.empty()) {
+      std::unique_ptr<Request> r = std::move(s->retiring.front());
+      s->retiring.pop_front();
+      ++s->busy;
+      lk.unlock();
+      const auto t = Clock::now();
+      finish(r.get(), r->status, r->error);
+      const double dt = std::chrono::duration<double>(Clock::now() - t).count();
+      lk.lock();
+      --s->busy;
+      s->retire_s += dt;
+      s->used -= std::min(s->used, r->bytes);
+      r->t_done = now_s(s);
+      ++s->completed;
+      const long long id = r->id;
+      s->finished[id] = std::move(r);
+      s->done.notify_all();
+      continue;
+    }
+    if (!s->queue.empty() && s->held < s->slots && s->used + s->queue.front()->bytes <= s->budget) {
+      std::unique_ptr<Request> r = std::move(s->queue.front());
+      s->queue.pop_front();
+      s->used += r->bytes;
+      ++s->held;
+      ++s->busy;
+      lk.unlock();
+      const auto t = Clock::now();
+      const int rc = admit(r.get());
+      const std::string err = rc == FREHG_GW_OK ? "" : frehg_gw_last_error();
+      const double dt = std::chrono::duration<double>(Clock::now() - t).count();
+      lk.lock();
+      --s->busy;
+      s->admit_s += dt;
+      if (rc == FREHG_GW_ENOMEM && s->held > 1) {
+        // Out of device memory despite the budget: wait for a retirement.
+        s->used -= std::min(s->used, r->bytes);
+        --s->held;
+        s->queue.push_front(std::move(r));
+        s->cv.wait(lk, [&] { return s->stop || !s->retiring.empty(); });
+        continue;
+      }
+      r->t_admit = now_s(s);
+      if (rc != FREHG_GW_OK) {
+        s->used -= std::min(s->used, r->bytes);
+        --s->held;
+        r->status = rc;
+        r->error = err;
+        r->state = FREHG_GW_REQ_FAILED;
+        r->t_done = r->t_admit;
+        ++s->completed;
+        const long long id = r->id;
+        s->finished[id] = std::move(r);
+      } else {
+        s->ready.push_back(std::move(r));
+      }
+      s->done.notify_all();
+      continue;
+    }
+    s->cv.wait(lk);
+  }
+}
+
 Request* find(frehg_gw_server* s, long long id) {
   auto it = s->finished.find(id);
   if (it != s->finished.end()) return it->second.get();
   for (auto& r : s->active)
     if (r->id == id) return r.get();
+  for (auto& r : s->ready)
+    if (r->id == id) return r.get();
   for (auto& r : s->queue)
+    if (r->id == id) return r.get();
+  for (auto& r : s->retiring)
     if (r->id == id) return r.get();
   return nullptr;
 }
@@ -181,6 +271,7 @@ int frehg_gw_server_create(const frehg_gw_server_opts* opts, frehg_gw_server** o
   auto* s = new frehg_gw_server;
   if (opts) s->opts = *opts;
   s->budget = s->opts.hbm_budget_bytes;
+  s->slots = s->opts.max_active > 0 ? s->opts.max_active : 64;
   if (s->budget == 0) {
     size_t free_b = 0, total_b = 0;
     const cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
@@ -190,15 +281,32 @@ int frehg_gw_server_create(const frehg_gw_server_opts* opts, frehg_gw_server** o
     }
     s->budget = free_b / 10 * 9;
   }
+  if (cudaGetDevice(&s->device) != cudaSuccess) {
+    // No device to query (submission and queueing still work; admission
+    // reports the device error per request).
+    s->device = 0;
+    cudaGetLastError();
+  }
   s->t0 = Clock::now();
+  s->worker = std::thread(worker_loop, s);
   *out = s;
   return FREHG_GW_OK;
 }
 
 int frehg_gw_server_destroy(frehg_gw_server* s) {
   if (!s) return FREHG_GW_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv.notify_all();
+  if (s->worker.joinable()) s->worker.join();
   if (s->batch) frehg_gw_batch_destroy(s->batch);
   for (auto& r : s->active)
+    if (r->h) frehg_gw_destroy(r->h);
+  for (auto& r : s->ready)
+    if (r->h) frehg_gw_destroy(r->h);
+  for (auto& r : s->retiring)
     if (r->h) frehg_gw_destroy(r->h);
   delete s;
   return FREHG_GW_OK;
@@ -255,62 +363,68 @@ int frehg_gw_server_submit(frehg_gw_server* s, const frehg_gw_request* q, long l
     return fail(FREHG_GW_ENOMEM, "server: request needs " + std::to_string(r->bytes) +
                                      " bytes of device memory; the budget is " +
                                      std::to_string(s->budget));
-  r->id = s->next_id++;
-  r->t_submit = now_s(s);
-  *id = r->id;
-  s->queue.push_back(std::move(r));
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->id = s->next_id++;
+    r->t_submit = now_s(s);
+    *id = r->id;
+    s->queue.push_back(std::move(r));
+  }
+  s->cv.notify_all();
   return FREHG_GW_OK;
 }
 
 int frehg_gw_server_tick(frehg_gw_server* s, int* active, int* queued) {
   if (!s) return fail(FREHG_GW_EINVAL, "null server");
   const auto tick0 = Clock::now();
-  const int slots = s->opts.max_active > 0 ? s->opts.max_active : 64;
-  // 1. Admission, in arrival order.
-  while (!s->queue.empty() && static_cast<int>(s->active.size()) < slots &&
-         s->used + s->queue.front()->bytes <= s->budget) {
-    std::unique_ptr<Request> r = std::move(s->queue.front());
-    s->queue.pop_front();
-    const int rc = admit(r.get());
-    if (rc == FREHG_GW_ENOMEM && !s->active.empty()) {
-      s->queue.push_front(std::move(r));  // retry once memory frees up
-      break;
+  auto lap = [](Clock::time_point& t) {
+    const auto now = Clock::now();
+    const double d = std::chrono::duration<double>(now - t).count();
+    t = now;
+    return d;
+  };
+  auto t = tick0;
+  // 1. Take in what the worker has made ready; with nothing to step, wait
+  // briefly for the worker instead of spinning.
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->active.empty() && s->ready.empty() && (s->busy > 0 || !s->queue.empty()))
+      s->done.wait_for(lk, std::chrono::milliseconds(2));
+    for (auto& r : s->ready) {
+      r->state = FREHG_GW_REQ_RUNNING;
+      s->active.push_back(std::move(r));
+      s->dirty = true;
     }
-    r->t_admit = now_s(s);
-    if (rc != FREHG_GW_OK) {
-      const long long id = r->id;
-      retire(s, r.get(), rc, frehg_gw_last_error());
-      s->finished[id] = std::move(r);
-      continue;
-    }
-    r->state = FREHG_GW_REQ_RUNNING;
-    s->used += r->bytes;
-    s->active.push_back(std::move(r));
-    s->dirty = true;
+    s->ready.clear();
   }
-  // 2. One step of every admitted request, as one batch.
+  // 2. One step of every running request, as one batch.
   int status = FREHG_GW_OK;
   if (!s->active.empty()) {
     if (s->dirty) {
-      if (s->batch) frehg_gw_batch_destroy(s->batch);
-      s->batch = nullptr;
       std::vector<frehg_gw_handle*> hs;
       for (auto& r : s->active) hs.push_back(r->h);
-      frehg_gw_batch_opts bo{};
-      bo.cells_per_block = s->opts.cells_per_block;
-      bo.use_graph = s->opts.use_graph;
-      bo.streams = s->opts.streams;
-      const int rc = frehg_gw_batch_create(hs.data(), static_cast<int>(hs.size()), &bo, &s->batch);
+      int rc;
+      if (s->batch) {
+        rc = frehg_gw_batch_set_members(s->batch, hs.data(), static_cast<int>(hs.size()));
+      } else {
+        frehg_gw_batch_opts bo{};
+        bo.cells_per_block = s->opts.cells_per_block;
+        bo.use_graph = s->opts.use_graph;
+        bo.streams = s->opts.streams;
+        rc = frehg_gw_batch_create(hs.data(), static_cast<int>(hs.size()), &bo, &s->batch);
+      }
       if (rc != FREHG_GW_OK) return rc;
       s->dirty = false;
     }
+    s->rebatch_s += lap(t);
     std::vector<frehg_gw_step_info> infos(s->active.size());
     std::vector<double> dts(s->active.size());
     for (size_t i = 0; i < s->active.size(); ++i) dts[i] = s->active[i]->h->next_dt;
     const int rc = frehg_gw_batch_step(s->batch, infos.data());
     if (rc == FREHG_GW_ECUDA) status = rc;  // device trouble: report, keep state
-    // 3. Progress and retirement.
-    std::vector<std::unique_ptr<Request>> keep;
+    s->step_s += lap(t);
+    // 3. Progress; requests done (or failed) go to the worker for retirement.
+    std::vector<std::unique_ptr<Request>> keep, out;
     for (size_t i = 0; i < s->active.size(); ++i) {
       std::unique_ptr<Request>& r = s->active[i];
       if (infos[i].status == FREHG_GW_OK) {
@@ -320,26 +434,37 @@ int frehg_gw_server_tick(frehg_gw_server* s, int* active, int* queued) {
         s->cell_steps += r->cells;
       }
       if (infos[i].status != FREHG_GW_OK || r->done_steps >= r->steps) {
-        const long long id = r->id;
-        retire(s, r.get(), infos[i].status,
-               infos[i].status == FREHG_GW_OK ? "" : "step failed (status " +
-                                                         std::to_string(infos[i].status) + ")");
-        s->finished[id] = std::move(r);
+        r->status = infos[i].status;
+        if (r->status != FREHG_GW_OK)
+          r->error = "step failed (status " + std::to_string(r->status) + ")";
+        out.push_back(std::move(r));
       } else {
         keep.push_back(std::move(r));
       }
     }
     s->active.swap(keep);
+    if (!out.empty()) {
+      s->dirty = true;
+      std::lock_guard<std::mutex> lk(s->mu);
+      for (auto& r : out) {
+        s->retiring.push_back(std::move(r));
+        --s->held;
+      }
+    }
+    s->cv.notify_all();
     ++s->ticks;
   }
   s->busy_s += std::chrono::duration<double>(Clock::now() - tick0).count();
-  if (active) *active = static_cast<int>(s->active.size());
-  if (queued) *queued = static_cast<int>(s->queue.size());
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (active) *active = static_cast<int>(s->active.size() + s->ready.size());
+  if (queued)
+    *queued = static_cast<int>(s->queue.size() + s->retiring.size()) + s->busy;
   return status;
 }
 
 int frehg_gw_server_poll(frehg_gw_server* s, long long id, frehg_gw_request_status* st) {
   if (!s || !st) return fail(FREHG_GW_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
   Request* r = find(s, id);
   if (!r) return fail(FREHG_GW_EINVAL, "server: unknown or released request");
   st->state = r->state;
@@ -357,6 +482,7 @@ int frehg_gw_server_poll(frehg_gw_server* s, long long id, frehg_gw_request_stat
 
 int frehg_gw_server_fetch(frehg_gw_server* s, long long id, int field, double* out) {
   if (!s || !out) return fail(FREHG_GW_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
   Request* r = find(s, id);
   if (!r || r->state != FREHG_GW_REQ_DONE)
     return fail(FREHG_GW_ESTATE, "server: request not finished");
@@ -370,6 +496,7 @@ int frehg_gw_server_fetch(frehg_gw_server* s, long long id, int field, double* o
 
 int frehg_gw_server_release(frehg_gw_server* s, long long id) {
   if (!s) return fail(FREHG_GW_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->finished.find(id);
   if (it == s->finished.end()) return fail(FREHG_GW_ESTATE, "server: request not finished");
   s->finished.erase(it);
@@ -378,7 +505,9 @@ int frehg_gw_server_release(frehg_gw_server* s, long long id) {
 
 int frehg_gw_server_stats(const frehg_gw_server* s, frehg_gw_server_stats_t* st) {
   if (!s || !st) return fail(FREHG_GW_EINVAL, "null argument");
-  st->active = static_cast<int>(s->active.size());
+  auto* m = const_cast<frehg_gw_server*>(s);
+  std::lock_guard<std::mutex> lk(m->mu);
+  st->active = static_cast<int>(s->active.size() + s->ready.size());
   st->queued = static_cast<int>(s->queue.size());
   st->completed = s->completed;
   st->ticks = s->ticks;
@@ -386,6 +515,10 @@ int frehg_gw_server_stats(const frehg_gw_server* s, frehg_gw_server_stats_t* st)
   st->device_bytes_used = s->used;
   st->device_bytes_budget = s->budget;
   st->busy_s = s->busy_s;
+  st->admit_s = s->admit_s;
+  st->rebatch_s = s->rebatch_s;
+  st->step_s = s->step_s;
+  st->retire_s = s->retire_s;
   st->now_s = now_s(s);
   return FREHG_GW_OK;
 }

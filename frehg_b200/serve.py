@@ -47,7 +47,8 @@ class ServerStats(C.Structure):
     _fields_ = [("active", C.c_int), ("queued", C.c_int), ("completed", C.c_longlong),
                 ("ticks", C.c_longlong), ("cell_steps", C.c_longlong),
                 ("device_bytes_used", C.c_size_t), ("device_bytes_budget", C.c_size_t),
-                ("busy_s", C.c_double), ("now_s", C.c_double)]
+                ("busy_s", C.c_double), ("now_s", C.c_double), ("admit_s", C.c_double),
+                ("rebatch_s", C.c_double), ("step_s", C.c_double), ("retire_s", C.c_double)]
 
 
 def _declare(lib):
@@ -225,4 +226,5 @@ def run_stream(server: RichardsServer, requests: Sequence[PreparedRequest],
             "latency_p99_s": float(np.percentile(lat, 99)),
             "latency_max_s": float(lat.max()),
             "queue_p50_s": float(np.percentile(np.asarray(queue), 50)),
-            "ticks": st["ticks"] - st0["ticks"]}
+            "ticks": st["ticks"] - st0["ticks"],
+            "tick_s": {k: st[k] - st0[k] for k in ("admit_s", "rebatch_s", "step_s", "retire_s")}}

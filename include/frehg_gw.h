@@ -280,6 +280,10 @@ typedef struct {
 int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
                           const frehg_gw_batch_opts* opts, frehg_gw_batch** out);
 int frehg_gw_batch_destroy(frehg_gw_batch* b);
+/* Rebinds the batch to a new member list (same options), reusing its streams
+ * and buffers while they fit; for callers whose set of domains changes often
+ * (continuous batching).  Captured graphs are dropped. */
+int frehg_gw_batch_set_members(frehg_gw_batch* b, frehg_gw_handle* const* members, int n);
 /* One step of every member with its own next dt (frehg_gw_next_dt, or the
  * value set by frehg_gw_batch_set_dt); infos receives n step records.  A
  * failing member does not advance; the first failure is returned. */
@@ -355,6 +359,8 @@ typedef struct {
   size_t device_bytes_used, device_bytes_budget;
   double busy_s;           /* time spent inside frehg_gw_server_tick */
   double now_s;            /* time since the server's creation */
+  double admit_s, rebatch_s, step_s, retire_s; /* busy_s by part: admission (device
+                              state creation), batch rebuilds, batch steps, retirement */
 } frehg_gw_server_stats_t;
 
 int frehg_gw_server_create(const frehg_gw_server_opts* opts, frehg_gw_server** out);

@@ -129,6 +129,30 @@ def test_member_alone_equals_member_in_mix():
         np.testing.assert_array_equal(u, v)
 
 
+def test_set_members_keeps_every_member_exact():
+    # Rebinding the batch mid-run (a member joins, another leaves) changes no
+    # member's arithmetic: each ends as it would stepping in a batch alone.
+    cfgs = mix_configs()[:3]
+    ref, _ = run_batch([cfgs[0]], 4, cells_per_block=4096)
+    ref2, _ = run_batch([cfgs[2]], 2, cells_per_block=4096)
+    mem = [RichardsSolver(copy.deepcopy(c)) for c in cfgs]
+    batch = RichardsBatch(mem[:2], cells_per_block=4096)
+    try:
+        batch.step()
+        batch.step()
+        batch.set_members([mem[0], mem[2]])    # member 1 leaves, member 2 joins
+        batch.step()
+        batch.step()
+        for u, v in zip(ref[0], (mem[0].field("h"), mem[0].field("wc"), mem[0].field("qz"))):
+            np.testing.assert_array_equal(v, u)
+        for u, v in zip(ref2[0], (mem[2].field("h"), mem[2].field("wc"), mem[2].field("qz"))):
+            np.testing.assert_array_equal(v, u)
+    finally:
+        batch.close()
+        for m in mem:
+            m.close()
+
+
 def test_autotune_keeps_state_and_picks_options():
     cfgs = mix_configs()[:4]
     mem = [RichardsSolver(copy.deepcopy(c)) for c in cfgs]
