@@ -61,6 +61,42 @@ class StepInfo(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+# Coupled top (include/frehg_gw.h, FREHG_GW_SURF_*).
+SURF = {"eta": 0, "dept": 1, "seep_accum": 2, "avail": 3, "gain": 4, "bounce": 5, "qss": 6,
+        "bottom": 7, "mode": 8}
+
+
+class CoupledAudit(C.Structure):
+    _fields_ = [("exchanged", C.c_double), ("bounce", C.c_double), ("vent", C.c_double),
+                ("vent_thin", C.c_double), ("evap", C.c_double),
+                ("pc_clamp_volume", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Coupling(C.Structure):
+    _fields_ = [("min_depth", C.c_double), ("vent_all", C.c_int), ("book_bounce", C.c_int),
+                ("field", C.c_void_p * 8)]
+
+
+class CouplerOpts(C.Structure):
+    _fields_ = [("sync", C.c_int), ("dt", C.c_double), ("dt_init", C.c_double),
+                ("t_start", C.c_double)]
+
+
+class WindowAudit(C.Structure):
+    _fields_ = [("gw", StepInfo), ("cpl", CoupledAudit), ("applied", C.c_double),
+                ("discarded", C.c_double), ("surface_gain", C.c_double),
+                ("accum_volume", C.c_double), ("substeps", C.c_long)]
+
+    def as_dict(self) -> dict:
+        out = {"gw": self.gw.as_dict(), "cpl": self.cpl.as_dict()}
+        for name in ("applied", "discarded", "surface_gain", "accum_volume", "substeps"):
+            out[name] = getattr(self, name)
+        return out
+
+
 def dptr(a: np.ndarray):
     return a.ctypes.data_as(_dp)
 

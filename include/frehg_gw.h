@@ -377,6 +377,108 @@ int frehg_gw_server_fetch(frehg_gw_server* s, long long id, int field, double* h
 int frehg_gw_server_release(frehg_gw_server* s, long long id);
 int frehg_gw_server_stats(const frehg_gw_server* s, frehg_gw_server_stats_t* st);
 
+/* ---------------------------------------------------------------- coupled top
+ * The surface-subsurface exchange of coupled runs.
+ *
+ *   frehg_gw_attach_coupling  RichardsSolver::attachCoupling with the
+ *                             GwCoupling views (src/gw/RichardsSolver.hpp:
+ *                             132-186); the step then runs the coupled
+ *                             branches of classifyCoupledTop (Corrector.cpp:
+ *                             47-115), the top face K (Predictor.cpp:278-310),
+ *                             assembly (:527-547, :627-674), the top flux
+ *                             (Corrector.cpp:388-465),
+ *                             applyCoupledTopBookkeeping (:539-627), the
+ *                             reallocation's wet-top contact and surface vent
+ *                             (Reallocate.cpp:323-333, :463-490) and the
+ *                             hydrostatic edge ghost (Predictor.cpp:66-87)
+ *   frehg_gw_coupled_audit    the GwStepAudit cpl* terms and pcClampVolume
+ *                             (RichardsSolver.hpp:96-128, :384)
+ *   frehg_gw_coupler_*        coupling::Coupler (src/coupling/Coupler.hpp,
+ *                             Coupler.cpp:13-131, Exchange.cpp:21-127): the
+ *                             sync / subcycled substep window, the seepage
+ *                             application and the coupled audit
+ *
+ * Surface fields are (ny+2)*(nx+2) doubles in the halo layout (index
+ * j * (nx+2) + i), elevations in the mesh's offset frame
+ * (frehg_gw_elevation_offset).  The groundwater step reads the depth, debits
+ * the window's infiltration budget and deposits bounce-backs and vents onto
+ * eta and depth exactly where the reference does; the surface solve itself
+ * (its free-surface and velocity phases and the depth refresh) stays with the
+ * caller.  Evapotranspiration, the transport window and the paired salt
+ * store are outside this drop-in. */
+enum {
+  FREHG_GW_SURF_ETA = 0,        /* free surface, offset frame */
+  FREHG_GW_SURF_DEPTH = 1,      /* surface depth */
+  FREHG_GW_SURF_SEEP_ACCUM = 2, /* exchanged, not yet applied depth */
+  FREHG_GW_SURF_AVAIL = 3,      /* the window's remaining infiltrable depth */
+  FREHG_GW_SURF_GAIN = 4,       /* this surface step's coupled deposits */
+  FREHG_GW_SURF_BOUNCE = 5,     /* the bounce-back share of gain (when booked) */
+  FREHG_GW_SURF_QSS = 6,        /* applied seepage rate of the last window */
+  FREHG_GW_SURF_BOTTOM = 7,     /* surface bed elevation, offset frame */
+  FREHG_GW_SURF_MODE = 8,       /* exchange mode of the last step (read only) */
+  FREHG_GW_SURF_COUNT = 9
+};
+
+typedef struct frehg_gw_coupling {
+  double min_depth;  /* surfaceWater.min_depth */
+  int vent_all;      /* every vent deposits (the paired store's rule) */
+  int book_bounce;   /* keep the bounce-back share of gain */
+  /* Device arrays, (ny+2)*(nx+2) each, indexed by FREHG_GW_SURF_* (MODE
+   * excluded); NULL = the handle allocates and zeroes its own. */
+  double* field[8];
+} frehg_gw_coupling;
+
+/* The cpl* terms of the last step [m^3] and the cumulative clamp volume of
+ * the consistent form's pressurized seepage faces. */
+typedef struct frehg_gw_coupled_audit {
+  double exchanged; /* net upward volume through the coupled top faces */
+  double bounce;    /* returned to a dry surface by a full top cell */
+  double vent;      /* vented onto the surface by the send walk */
+  double vent_thin; /* the part of vent the legacy rule would have discarded */
+  double evap;      /* evaporative top flux taken off the seepage accumulator */
+  double pc_clamp_volume;
+} frehg_gw_coupled_audit;
+
+int frehg_gw_attach_coupling(frehg_gw_handle* h, const frehg_gw_coupling* c);
+/* Host copies of a surface field (FREHG_GW_SURF_*). */
+int frehg_gw_get_surface(frehg_gw_handle* h, int which, double* host_out);
+int frehg_gw_set_surface(frehg_gw_handle* h, int which, const double* host_in);
+/* Device address of a surface field (for a caller's own surface kernels). */
+int frehg_gw_surface_ptr(frehg_gw_handle* h, int which, double** dev_out);
+int frehg_gw_coupled_audit_get(frehg_gw_handle* h, frehg_gw_coupled_audit* out);
+/* Mesh elevation offset: offset-frame elevation = datum elevation + offset. */
+double frehg_gw_elevation_offset(const frehg_gw_handle* h);
+
+typedef struct frehg_gw_coupler_opts {
+  int sync;       /* coupling.mode: 1 sync (lockstep), 0 subcycled */
+  double dt;      /* time.dt, the surface step */
+  double dt_init; /* groundwater dt_init (subcycled start) */
+  double t_start; /* time.t_start */
+} frehg_gw_coupler_opts;
+
+/* One surface step's coupled budget (CouplingAudit, Coupler.hpp:59-66). */
+typedef struct frehg_gw_window_audit {
+  frehg_gw_step_info gw;      /* audit terms and CG iterations summed over the
+                                 substeps; next_dt = the subsurface dtg after */
+  frehg_gw_coupled_audit cpl; /* summed; pc_clamp_volume cumulative */
+  double applied;      /* net volume the seepage application added to eta */
+  double discarded;    /* infiltration remainder cut by the eta >= bottom clamp */
+  double surface_gain; /* all coupled surface deposits of the step */
+  double accum_volume; /* held seepage at the end of the step */
+  long substeps;
+} frehg_gw_window_audit;
+
+int frehg_gw_coupler_init(frehg_gw_handle* h, const frehg_gw_coupler_opts* o);
+/* The subsurface part of Coupler::step(t, dt) on a surface the caller has
+ * already advanced to t (depth refreshed): open the window, take the sync
+ * step or the subcycled steps that fit, apply the seepage, reduce the audit. */
+int frehg_gw_coupler_step(frehg_gw_handle* h, double t, double dt, frehg_gw_window_audit* out);
+/* Coupler::nextDt, currentDtg, gwLag(t). */
+int frehg_gw_coupler_state(frehg_gw_handle* h, double t, double* next_dt, double* dtg,
+                           double* lag);
+/* Coupler::restore(t, dtg, lag) after a checkpoint read. */
+int frehg_gw_coupler_restore(frehg_gw_handle* h, double t, double dtg, double lag);
+
 #ifdef __cplusplus
 }
 #endif

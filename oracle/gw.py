@@ -13,7 +13,8 @@ import os
 
 import numpy as np
 
-from frehg_b200.abi import FIELD, GwDesc, StepInfo, field_shape, make_desc
+from frehg_b200.abi import (FIELD, SURF, CoupledAudit, CouplerOpts, GwDesc, StepInfo,
+                            WindowAudit, field_shape, make_desc)
 from frehg_b200.config import IC_FORMS, GwConfig, rasterize
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -64,6 +65,13 @@ def load():
     lib.oracle_gw_last_system.argtypes = [C.c_void_p, _dp, _lp, _dp]
     lib.oracle_cg7.restype = C.c_int
     lib.oracle_cg7.argtypes = [C.c_long, _dp, _lp, _dp, _dp, C.c_double, C.c_double, C.c_int, _dp]
+    lib.oracle_gw_attach_coupling.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
+    lib.oracle_gw_surface.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+    lib.oracle_gw_coupled_audit.argtypes = [C.c_void_p, C.POINTER(CoupledAudit)]
+    lib.oracle_gw_coupler_init.argtypes = [C.c_void_p, C.POINTER(CouplerOpts)]
+    lib.oracle_gw_coupler_step.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp,
+                                           C.POINTER(WindowAudit)]
+    lib.oracle_gw_coupler_state.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp]
     _lib = lib
     return lib
 
@@ -155,6 +163,47 @@ class OracleSolver:
 
     def elevation_offset(self) -> float:
         return self.lib.oracle_gw_elevation_offset(self.h)
+
+    # ------------------------------------------------------------ coupled top
+    def attach_coupling(self, min_depth: float, vent_all: bool = False,
+                        book_bounce: bool = False) -> None:
+        self._check(self.lib.oracle_gw_attach_coupling(self.h, min_depth, int(vent_all),
+                                                       int(book_bounce)))
+
+    def surface(self, name: str) -> np.ndarray:
+        out = np.empty((self.ny + 2, self.nx + 2))
+        self._check(self.lib.oracle_gw_surface(self.h, SURF[name], out.ctypes.data_as(_dp),
+                                               None))
+        return out
+
+    def set_surface(self, name: str, value) -> None:
+        v = np.ascontiguousarray(np.broadcast_to(value, (self.ny + 2, self.nx + 2)), np.float64)
+        self._check(self.lib.oracle_gw_surface(self.h, SURF[name], None, v.ctypes.data_as(_dp)))
+
+    def coupled_audit(self) -> dict:
+        a = CoupledAudit()
+        self.lib.oracle_gw_coupled_audit(self.h, C.byref(a))
+        return a.as_dict()
+
+    def coupler_init(self, sync: bool, dt: float, dt_init: float, t_start: float = 0.0) -> None:
+        o = CouplerOpts(int(sync), dt, dt_init, t_start)
+        self._check(self.lib.oracle_gw_coupler_init(self.h, C.byref(o)))
+
+    def coupler_step(self, t: float, dt: float, bottom: np.ndarray) -> dict:
+        b = np.ascontiguousarray(bottom, np.float64)
+        a = WindowAudit()
+        self._check(self.lib.oracle_gw_coupler_step(self.h, t, dt, b.ctypes.data_as(_dp),
+                                                    C.byref(a)))
+        return a.as_dict()
+
+    def coupler_state(self, t: float) -> tuple:
+        v = [C.c_double(), C.c_double(), C.c_double()]
+        self.lib.oracle_gw_coupler_state(self.h, t, *[C.byref(x) for x in v])
+        return tuple(x.value for x in v)
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise RuntimeError("oracle: " + self.lib.oracle_gw_last_error().decode())
 
     def gid(self):
         gid = np.empty((self.ny + 2, self.nx + 2, self.nz), np.int32)

@@ -55,6 +55,17 @@ struct oracle_gw {
   double *rhs, *sol;
   int have_state;
   frehg_gw_step_info last;
+  /* coupled top (GwCoupling, src/gw/RichardsSolver.hpp:132-175): surface
+   * fields (ny+2)(nx+2), the per-column exchange mode and the step's books */
+  int cpl, vent_all, book_bounce;
+  double min_depth;
+  double *eta, *dept, *seep, *avail, *gain, *bounce, *qss;
+  int* cmode;
+  double cpl_exch, cpl_bounce, cpl_vent, cpl_thin, cpl_evap, pc_clamp;
+  /* coupler (src/coupling/Coupler.hpp): sync flag, surface dt, adaptive
+   * subsurface dt and clock */
+  int csync;
+  double cdt, cdtg, ctsub, clast_dt;
 };
 
 #define I2(s, j, i) ((size_t)(j) * (size_t)((s)->nx + 2) + (size_t)(i))
@@ -173,7 +184,8 @@ void oracle_gw_destroy(oracle_gw* s) {
                     &s->aev, &s->h, &s->hn, &s->wc, &s->wcn, &s->ch, &s->kx, &s->ky, &s->kz,
                     &s->qx, &s->qy, &s->qz, &s->vloss, &s->room, &s->sup, &s->sdown,
                     &s->wcsnap, &s->hsnap, &s->topv, &s->botv, &s->xmv, &s->xpv, &s->ymv,
-                    &s->ypv, &s->vals7, &s->rhs, &s->sol};
+                    &s->ypv, &s->vals7, &s->rhs, &s->sol, &s->eta, &s->dept, &s->seep,
+                    &s->avail, &s->gain, &s->bounce, &s->qss};
   for (size_t n = 0; n < sizeof dbl / sizeof dbl[0]; ++n) free(*dbl[n]);
   free(s->ktop);
   free(s->gid);
@@ -184,6 +196,7 @@ void oracle_gw_destroy(oracle_gw* s) {
   free(s->ymc);
   free(s->ypc);
   free(s->cols7);
+  free(s->cmode);
   free(s);
 }
 
@@ -502,10 +515,19 @@ int oracle_gw_set_bc_values(oracle_gw* s, const double* top, const double* bot,
 }
 
 /* ------------------------------------------------------------------ ghosts */
-/* enforceHeadBc + ghostHead, uncoupled (Predictor.cpp:66-87, 757-817). */
-static double ghost_head(int code, double value, double interior, double zc) {
+/* enforceHeadBc + ghostHead (Predictor.cpp:66-87, 757-817), density ratio 1.
+ * In a coupled run a hydrostatic stage above the edge column's bed follows
+ * the live surface there: (bed - zc) + depth. */
+static double ghost_head(const oracle_gw* s, int code, double value, double interior, double zc,
+                         size_t col) {
   if (code == HEAD) return value;
-  if (code == HYDRO) return (value - zc);
+  if (code == HYDRO) {
+    if (s->cpl && value > s->bath[col]) {
+      const double hydro = (s->bath[col] - zc);
+      return hydro + s->dept[col];
+    }
+    return (value - zc);
+  }
   return interior;
 }
 
@@ -515,21 +537,23 @@ static void enforce_head_bc(oracle_gw* s) {
     for (int k = 0; k < nz; ++k) {
       size_t c = I3(s, j, 1, k);
       double zc = s->bot[c] + 0.5 * s->dz[c];
-      s->h[I3(s, j, 0, k)] = ghost_head(s->xmc[I2(s, j, 1)], s->xmv[I2(s, j, 1)], s->h[c], zc);
+      s->h[I3(s, j, 0, k)] =
+          ghost_head(s, s->xmc[I2(s, j, 1)], s->xmv[I2(s, j, 1)], s->h[c], zc, I2(s, j, 1));
       c = I3(s, j, nx, k);
       zc = s->bot[c] + 0.5 * s->dz[c];
       s->h[I3(s, j, nx + 1, k)] =
-          ghost_head(s->xpc[I2(s, j, nx)], s->xpv[I2(s, j, nx)], s->h[c], zc);
+          ghost_head(s, s->xpc[I2(s, j, nx)], s->xpv[I2(s, j, nx)], s->h[c], zc, I2(s, j, nx));
     }
   for (int i = 1; i <= nx; ++i)
     for (int k = 0; k < nz; ++k) {
       size_t c = I3(s, 1, i, k);
       double zc = s->bot[c] + 0.5 * s->dz[c];
-      s->h[I3(s, 0, i, k)] = ghost_head(s->ymc[I2(s, 1, i)], s->ymv[I2(s, 1, i)], s->h[c], zc);
+      s->h[I3(s, 0, i, k)] =
+          ghost_head(s, s->ymc[I2(s, 1, i)], s->ymv[I2(s, 1, i)], s->h[c], zc, I2(s, 1, i));
       c = I3(s, ny, i, k);
       zc = s->bot[c] + 0.5 * s->dz[c];
       s->h[I3(s, ny + 1, i, k)] =
-          ghost_head(s->ypc[I2(s, ny, i)], s->ypv[I2(s, ny, i)], s->h[c], zc);
+          ghost_head(s, s->ypc[I2(s, ny, i)], s->ypv[I2(s, ny, i)], s->h[c], zc, I2(s, ny, i));
     }
 }
 
@@ -611,6 +635,34 @@ int oracle_gw_set_state(oracle_gw* s, const double* head, const double* wc) {
 
 /* ------------------------------------------------------------------ predictor */
 /* computeFaceConductivityImpl<PC, HARM> (Predictor.cpp:105-386). */
+/* classifyCoupledTopImpl<PC> (Corrector.cpp:55-115): per column, 1 = a wet
+ * surface whose saturated demand the window's water funds (Dirichlet top),
+ * 2 = a wet surface it cannot fund (supply-limited flux), 3 = (consistent
+ * form) a dry surface over a top cell pressurized past dz/2, 0 = dry. */
+static void classify_coupled_top(oracle_gw* s, double dtg) {
+  for (int j = 1; j <= s->ny; ++j)
+    for (int i = 1; i <= s->nx; ++i) {
+      const size_t col = I2(s, j, i);
+      int kt = s->ktop[(size_t)(j - 1) * s->nx + (i - 1)];
+      if (kt >= s->nz) kt = -1;
+      if (kt < 0 || s->dept[col] <= 0.0) {
+        if (s->pc && kt >= 0) {
+          const size_t c = I3(s, j, i, kt);
+          if (s->h[c] > 0.5 * s->dz[c]) {
+            s->cmode[col] = 3;
+            continue;
+          }
+        }
+        s->cmode[col] = 0;
+        continue;
+      }
+      const size_t c = I3(s, j, i, kt);
+      const double ks = s->ksz[c];
+      const double qEst = 2.0 * ks * (s->h[c] - s->dept[col]) / s->dz[c] - ks;
+      s->cmode[col] = (qEst < 0.0 && -qEst * dtg > s->avail[col]) ? 2 : 1;
+    }
+}
+
 static void face_conductivity(oracle_gw* s) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   for (int j = 1; j <= ny; ++j) /* gw_face_k_x */
@@ -697,7 +749,9 @@ static void face_conductivity(oracle_gw* s) {
           else if (is_head(code)) s->ky[c] = vg_k(soil_at(s, c), s->h[c], s->ksy[c]);
         }
       }
-  /* gw_face_k_top (uncoupled): head -> Ksz, no-flux -> 0, otherwise K(h). */
+  /* gw_face_k_top (Predictor.cpp:278-310): uncoupled, head -> Ksz, no-flux
+   * -> 0, otherwise K(h); coupled, a wet surface gives Ksz (consistent) or
+   * the mean of Ksz and K(h) (legacy), a dry one K(h). */
   for (int j = 1; j <= ny; ++j)
     for (int i = 1; i <= nx; ++i)
       for (int k = 0; k < nz; ++k) {
@@ -705,6 +759,11 @@ static void face_conductivity(oracle_gw* s) {
         const int top = s->gid[c] >= 0 && (k == 0 || s->gid[c - 1] < 0);
         if (!top) continue;
         const double own = vg_k(soil_at(s, c), s->h[c], s->ksz[c]);
+        if (s->cpl) {
+          if (s->pc) s->kz[IF(s, j, i, k)] = (s->dept[I2(s, j, i)] > 0.0) ? s->ksz[c] : own;
+          else s->kz[IF(s, j, i, k)] = (s->dept[I2(s, j, i)] > 0.0) ? 0.5 * (s->ksz[c] + own) : own;
+          continue;
+        }
         const int code = s->topc[I2(s, j, i)];
         s->kz[IF(s, j, i, k)] = (code == HEAD) ? s->ksz[c] : (code == NOFLUX ? 0.0 : own);
       }
@@ -748,7 +807,8 @@ static void face_conductivity(oracle_gw* s) {
       }
 }
 
-/* assembleSystemImpl<PC> (Predictor.cpp:400-698), uncoupled, no ET. */
+/* assembleSystemImpl<PC> (Predictor.cpp:400-698), no ET; the coupled top's
+ * Dirichlet leg and RHS by exchange mode (:527-547, :627-674). */
 static void assemble(oracle_gw* s, double dtg) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   const double dx = s->dx, dy = s->dy, az = s->az, ss = s->ss;
@@ -791,7 +851,9 @@ static void assemble(oracle_gw* s, double dtg) {
         if (south && s->ymc[col] == FLUX) gct += gym;
         if (!(k == nz - 1 && s->botc[col] != HEAD)) gct -= gzp;
         if (top) {
-          if (s->topc[col] == HEAD) gct -= gzm;
+          int dirichlet = s->cpl ? (s->cmode[col] == 1) : (s->topc[col] == HEAD);
+          if (s->pc) dirichlet = dirichlet || (s->cpl && s->cmode[col] == 3);
+          if (dirichlet) gct -= gzm;
         } else {
           gct -= gzm;
         }
@@ -832,7 +894,26 @@ static void assemble(oracle_gw* s, double dtg) {
             b -= gzp * s->botv[col];
           }
         }
-        if (top) {
+        if (top && s->cpl) {
+          const int m = s->cmode[col];
+          if (m == 1) {
+            b -= gzm * s->dept[col];
+          } else if (s->pc && m == 3) {
+            /* the ghost head is 0: the leg is in the diagonal only */
+          } else if (m == 2) {
+            const double roomTop = fmax(0.0, (0.9999 * s->wcs[c] - s->wcn[c]) * s->dz[c]);
+            const double take = fmin(s->avail[col], roomTop);
+            const double qSupply = -take / dtg;
+            b += -dtg * volume * (qSupply + s->kz[IF(s, j, i, k)]) / s->dz[c];
+          } else {
+            double qtop = 0.0;
+            if (s->topc[col] == FLUX) {
+              const double v = s->topv[col];
+              if ((v > 0.0 && s->wcn[c] < s->wcs[c]) || (v < 0.0 && s->wcn[c] > s->wcr[c])) qtop = v;
+            }
+            b += -dtg * volume * (qtop + s->kz[IF(s, j, i, k)]) / s->dz[c];
+          }
+        } else if (top) {
           if (s->topc[col] == HEAD) {
             b -= gzm * s->topv[col];
           } else if (s->topc[col] == FLUX) {
@@ -953,7 +1034,6 @@ int oracle_cg7(long n, const double* v7, const long* c7, const double* bvec, dou
 /* ------------------------------------------------------------------ corrector */
 /* computeFluxesImpl<PC, HARM> (Corrector.cpp:135-533), uncoupled, no ET. */
 static void fluxes(oracle_gw* s, double dtg) {
-  (void)dtg;
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   const double dx = s->dx, dy = s->dy, az = s->az;
   for (int j = 1; j <= ny; ++j) /* gw_flux_x */
@@ -1055,7 +1135,47 @@ static void fluxes(oracle_gw* s, double dtg) {
         const int below = (k < nz) && s->gid[I3(s, j, i, k)] >= 0;
         const int above = (k >= 1) && s->gid[I3(s, j, i, k - 1)] >= 0;
         double q = 0.0;
-        if (below && !above) {
+        if (below && !above && s->cpl) {
+          /* coupled exchange face (Corrector.cpp:388-465): the ghost head is
+           * the surface depth; infiltration debits the window's budget */
+          const size_t c = I3(s, j, i, k);
+          const double ks = s->ksz[c], depth = s->dept[col];
+          const int m = s->cmode[col];
+          const double delta = 0.5 * s->dz[c];
+          if (m == 2) {
+            const double roomTop = fmax(0.0, (0.9999 * s->wcs[c] - s->wc[c]) * s->dz[c]);
+            const double take = fmin(s->avail[col], roomTop);
+            q = -take * az / dtg;
+            s->avail[col] -= take;
+          } else if (m == 1) {
+            q = az * ks * ((s->h[c] - depth) / delta - 1.0);
+            if (q < 0.0) {
+              const double need = -q * dtg / az;
+              if (need > s->avail[col]) {
+                q = -s->avail[col] * az / dtg;
+                s->avail[col] = 0.0;
+              } else {
+                s->avail[col] -= need;
+              }
+            }
+          } else if (s->pc && m == 3) {
+            q = az * ks * ((s->h[c] - depth) / delta - 1.0);
+            if (q <= 0.0) {
+              s->pc_clamp += -q * dtg;
+              q = 0.0;
+            }
+          } else {
+            const double kGhost = vg_k(soil_at(s, c), depth, ks);
+            const double kCell = vg_k(soil_at(s, c), s->h[c], ks);
+            const double kface = 0.5 * (kGhost + kCell);
+            q = az * kface * ((s->h[c] - depth) / delta - 1.0);
+            if (q <= 0.0) q = 0.0;
+            if (s->topc[col] == FLUX) {
+              const double v = s->topv[col];
+              if ((v > 0.0 && s->wc[c] > s->wcr[c]) || v < 0.0) q += v * az;
+            }
+          }
+        } else if (below && !above) {
           const size_t c = I3(s, j, i, k);
           const int code = s->topc[col];
           if (code == FLUX) {
@@ -1094,6 +1214,44 @@ static void fluxes(oracle_gw* s, double dtg) {
         }
         s->qz[IF(s, j, i, k)] = q;
       }
+}
+
+/* applyCoupledTopBookkeeping (Corrector.cpp:539-627), no ET: the exchanged
+ * volume, the saturation bounce-back onto a dry surface, the seepage
+ * accumulator and the evaporation correction. */
+static void coupled_top_bookkeeping(oracle_gw* s, double dtg) {
+  const double az = s->az;
+  double sumE = 0.0, sumB = 0.0, sumV = 0.0;
+  for (int j = 1; j <= s->ny; ++j)
+    for (int i = 1; i <= s->nx; ++i) {
+      const size_t col = I2(s, j, i);
+      const int kt = s->ktop[(size_t)(j - 1) * s->nx + (i - 1)];
+      if (kt < 0 || kt >= s->nz) continue;
+      const size_t c = I3(s, j, i, kt);
+      const double q = s->qz[IF(s, j, i, kt)];
+      sumE += q * dtg;
+      if (q < 0.0 && s->dept[col] <= s->min_depth) {
+        const double volume = az * s->dz[c];
+        if ((s->wcs[c] - s->wc[c]) < -q * dtg / volume) {
+          const double d = -q * dtg / az;
+          s->eta[col] += d;
+          s->dept[col] += d;
+          s->avail[col] += d;
+          s->gain[col] += d;
+          if (s->book_bounce) s->bounce[col] += d;
+          sumB += d * az;
+        }
+      }
+      s->seep[col] += q * dtg / az;
+      if (s->topc[col] == FLUX && s->topv[col] > 0.0 && s->wc[c] > s->wcr[c] &&
+          s->dept[col] <= s->min_depth) {
+        s->seep[col] -= s->topv[col] * dtg;
+        sumV += s->topv[col] * dtg * az;
+      }
+    }
+  s->cpl_exch = sumE;
+  s->cpl_bounce = sumB;
+  s->cpl_evap = sumV;
 }
 
 /* updateWaterContent (Corrector.cpp:629-672). */
@@ -1230,7 +1388,11 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
         else {
           const int top = (k == 0) || (s->gid[c - 1] < 0);
           if (top) {
-            if (s->topc[I2(s, j, i)] == HEAD && s->topv[I2(s, j, i)] >= 0.0) adj = 1;
+            if (s->cpl) {
+              if (s->dept[I2(s, j, i)] > 0.0) adj = 1;
+            } else if (s->topc[I2(s, j, i)] == HEAD && s->topv[I2(s, j, i)] >= 0.0) {
+              adj = 1;
+            }
           } else if (s->gid[c - 1] >= 0 && SAT(c - 1)) {
             adj = 1;
           }
@@ -1260,9 +1422,11 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
   if (s->off) {
     *adjust = 0.0;
     *dropped_out = 0.0;
+    s->cpl_vent = 0.0;
+    s->cpl_thin = 0.0;
     return;
   }
-  double lost = 0.0;
+  double lost = 0.0, vent = 0.0, thin = 0.0;
   for (int j = 1; j <= ny; ++j) /* gw_reallocate_send: k-sequential column walks */
     for (int i = 1; i <= nx; ++i) {
       const size_t col = I2(s, j, i);
@@ -1284,7 +1448,22 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
             }
           }
           if (dV > 0.0) {
-            if (top_head) {
+            if (s->cpl) {
+              /* coupled columns vent onto the surface (Reallocate.cpp:463-490) */
+              const double d = dV / az;
+              if (s->vent_all || s->dept[col] > 0.0 || d > s->min_depth) {
+                if (!(s->dept[col] > 0.0 || d > s->min_depth)) thin += dV;
+                s->eta[col] += d;
+                s->dept[col] += d;
+                s->avail[col] += d;
+                s->gain[col] += d;
+                s->qz[IF(s, j, i, ll)] += dV / dtg;
+                vent += dV;
+              } else {
+                lost -= dV;
+              }
+              dV = 0.0;
+            } else if (top_head) {
               s->qz[IF(s, j, i, ll)] += dV / dtg;
               dV = 0.0;
             } else {
@@ -1324,6 +1503,8 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
     }
   *adjust = sum + lost;
   *dropped_out = drop - lost;
+  s->cpl_vent = vent;
+  s->cpl_thin = thin;
 }
 
 /* finalizeWaterContent (Corrector.cpp:758-792). */
@@ -1412,7 +1593,8 @@ int oracle_gw_step(oracle_gw* s, double t, double dtg, frehg_gw_step_info* info)
   enforce_moisture_bc(s);
   memcpy(s->hn, s->h, s->n3 * sizeof(double));
   memcpy(s->wcn, s->wc, s->n3 * sizeof(double));
-  /* predictor (:759-763) */
+  /* predictor (:750-763) */
+  if (s->cpl) classify_coupled_top(s, dtg);
   face_conductivity(s);
   assemble(s, dtg);
   double resid = 0.0;
@@ -1428,6 +1610,7 @@ int oracle_gw_step(oracle_gw* s, double t, double dtg, frehg_gw_step_info* info)
   /* corrector (:768-774) */
   face_conductivity(s);
   fluxes(s, dtg);
+  if (s->cpl) coupled_top_bookkeeping(s, dtg);
   out.ss_storage = update_wc(s, dtg);
   /* post-allocation and the clamp (:784-787) */
   double adjust = 0.0, dropped = 0.0;
@@ -1515,4 +1698,177 @@ int oracle_gw_get_field(const oracle_gw* s, int field, double* out) {
     for (int i = i0; i <= nx; ++i)
       for (int k = 0; k < nz; ++k) out[q++] = src[I3(s, j, i, k)];
   return FREHG_GW_OK;
+}
+
+/* ------------------------------------------------------------------ coupled top
+ * RichardsSolver::attachCoupling (src/gw/RichardsSolver.hpp:180-186) with the
+ * surface fields owned here, zeroed. */
+int oracle_gw_attach_coupling(oracle_gw* s, double min_depth, int vent_all, int book_bounce) {
+  double** f[] = {&s->eta, &s->dept, &s->seep, &s->avail, &s->gain, &s->bounce, &s->qss};
+  for (size_t n = 0; n < sizeof f / sizeof f[0]; ++n) {
+    if (!*f[n]) *f[n] = xcalloc(s->n2, sizeof(double));
+    if (!*f[n]) {
+      set_err("oracle_gw_attach_coupling: out of memory");
+      return FREHG_GW_ENOMEM;
+    }
+  }
+  if (!s->cmode) s->cmode = xcalloc(s->n2, sizeof(int));
+  s->cpl = 1;
+  s->min_depth = min_depth;
+  s->vent_all = vent_all;
+  s->book_bounce = book_bounce;
+  return FREHG_GW_OK;
+}
+
+static double* surface_field(oracle_gw* s, int which) {
+  switch (which) {
+    case FREHG_GW_SURF_ETA: return s->eta;
+    case FREHG_GW_SURF_DEPTH: return s->dept;
+    case FREHG_GW_SURF_SEEP_ACCUM: return s->seep;
+    case FREHG_GW_SURF_AVAIL: return s->avail;
+    case FREHG_GW_SURF_GAIN: return s->gain;
+    case FREHG_GW_SURF_BOUNCE: return s->bounce;
+    case FREHG_GW_SURF_QSS: return s->qss;
+    default: return NULL;
+  }
+}
+
+/* Surface field `which` (FREHG_GW_SURF_*), (ny+2)(nx+2): copied out when out
+ * is given, then overwritten from in when in is given. */
+int oracle_gw_surface(oracle_gw* s, int which, double* out, const double* in) {
+  if (!s->cpl) {
+    set_err("oracle_gw_surface: no coupling attached");
+    return FREHG_GW_ESTATE;
+  }
+  if (which == FREHG_GW_SURF_MODE) {
+    if (out)
+      for (size_t n = 0; n < s->n2; ++n) out[n] = s->cmode[n];
+    return FREHG_GW_OK;
+  }
+  double* f = surface_field(s, which);
+  if (!f) {
+    set_err("oracle_gw_surface: unknown field");
+    return FREHG_GW_EINVAL;
+  }
+  if (out) memcpy(out, f, s->n2 * sizeof(double));
+  if (in) memcpy(f, in, s->n2 * sizeof(double));
+  return FREHG_GW_OK;
+}
+
+void oracle_gw_coupled_audit(const oracle_gw* s, frehg_gw_coupled_audit* out) {
+  out->exchanged = s->cpl_exch;
+  out->bounce = s->cpl_bounce;
+  out->vent = s->cpl_vent;
+  out->vent_thin = s->cpl_thin;
+  out->evap = s->cpl_evap;
+  out->pc_clamp_volume = s->pc_clamp;
+}
+
+/* Coupler::Coupler (src/coupling/Coupler.cpp:13-38): sync marches on the
+ * common dt, subcycled starts the subsurface at dt_init. */
+int oracle_gw_coupler_init(oracle_gw* s, const frehg_gw_coupler_opts* o) {
+  if (!s->cpl) {
+    set_err("oracle_gw_coupler_init: no coupling attached");
+    return FREHG_GW_ESTATE;
+  }
+  s->csync = o->sync != 0;
+  s->cdt = o->dt;
+  s->cdtg = s->csync ? o->dt : o->dt_init;
+  s->clast_dt = o->dt;
+  s->ctsub = o->t_start;
+  return FREHG_GW_OK;
+}
+
+/* The subsurface part of Coupler::step (Coupler.cpp:69-131) on a surface the
+ * caller has already advanced to t with its depth refreshed: beginWindow
+ * (Exchange.cpp:21-52), the sync or subcycled substeps, applySeepage
+ * (:54-107) against the bed `bottom` ((ny+2)(nx+2)) and reduceAudit
+ * (:109-127). */
+int oracle_gw_coupler_step(oracle_gw* s, double t, double dt, const double* bottom,
+                           frehg_gw_window_audit* out) {
+  frehg_gw_window_audit a;
+  memset(&a, 0, sizeof a);
+  s->clast_dt = dt;
+  for (int j = 1; j <= s->ny; ++j)
+    for (int i = 1; i <= s->nx; ++i) {
+      s->avail[I2(s, j, i)] = s->dept[I2(s, j, i)];
+      s->gain[I2(s, j, i)] = 0.0;
+    }
+  if (s->book_bounce)
+    for (size_t n = 0; n < s->n2; ++n) s->bounce[n] = 0.0;
+  for (;;) {
+    double tt, dtg;
+    if (s->csync) {
+      if (a.substeps > 0) break;
+      s->ctsub = t;
+      tt = t;
+      dtg = dt;
+    } else {
+      if (!(s->ctsub + s->cdtg <= t + 1.0e-9)) break;
+      s->ctsub += s->cdtg;
+      tt = s->ctsub;
+      dtg = s->cdtg;
+    }
+    frehg_gw_step_info info;
+    const int rc = oracle_gw_step(s, tt, dtg, &info);
+    if (rc != FREHG_GW_OK) return rc;
+    s->cdtg = s->dtg_next;
+    a.gw.boundary_in += info.boundary_in;
+    a.gw.ss_storage += info.ss_storage;
+    a.gw.realloc_adjust += info.realloc_adjust;
+    a.gw.realloc_dropped += info.realloc_dropped;
+    a.gw.vloss += info.vloss;
+    a.gw.cg_iterations += info.cg_iterations;
+    a.cpl.exchanged += s->cpl_exch;
+    a.cpl.bounce += s->cpl_bounce;
+    a.cpl.vent += s->cpl_vent;
+    a.cpl.vent_thin += s->cpl_thin;
+    a.cpl.evap += s->cpl_evap;
+    ++a.substeps;
+  }
+  a.cpl.pc_clamp_volume = s->pc_clamp;
+  a.gw.next_dt = s->cdtg;
+  double sumA = 0.0, sumD = 0.0;
+  for (int j = 1; j <= s->ny; ++j)
+    for (int i = 1; i <= s->nx; ++i) {
+      const size_t col = I2(s, j, i);
+      const double v = s->seep[col];
+      s->qss[col] = v / dt;
+      if (v < 0.0) {
+        const double before = s->eta[col];
+        s->eta[col] += v;
+        if (s->eta[col] < bottom[col]) s->eta[col] = bottom[col];
+        const double change = s->eta[col] - before;
+        s->gain[col] += change;
+        sumA += change;
+        sumD += change - v;
+        s->seep[col] = 0.0;
+      } else if (s->dept[col] > s->min_depth || v > s->min_depth) {
+        s->eta[col] += v;
+        s->gain[col] += v;
+        sumA += v;
+        s->seep[col] = 0.0;
+      }
+    }
+  const double cell = s->dx * s->dy;
+  a.applied = sumA * cell;
+  a.discarded = sumD * cell;
+  double sumG = 0.0, sumH = 0.0;
+  for (int j = 1; j <= s->ny; ++j)
+    for (int i = 1; i <= s->nx; ++i) {
+      sumG += s->gain[I2(s, j, i)];
+      sumH += s->seep[I2(s, j, i)];
+    }
+  a.surface_gain = sumG * cell;
+  a.accum_volume = sumH * cell;
+  if (out) *out = a;
+  return FREHG_GW_OK;
+}
+
+/* Coupler::nextDt / currentDtg / gwLag (Coupler.hpp:76-96). */
+void oracle_gw_coupler_state(const oracle_gw* s, double t, double* next_dt, double* dtg,
+                             double* lag) {
+  if (next_dt) *next_dt = s->csync ? s->cdtg : s->cdt;
+  if (dtg) *dtg = s->cdtg;
+  if (lag) *lag = s->csync ? 0.0 : (t - s->ctsub);
 }

@@ -41,6 +41,18 @@ double oracle_gw_elevation_offset(const oracle_gw* s);
 /* ktop per column (ny*nx) and gids in the halo layout ((ny+2)*(nx+2)*nz). */
 void oracle_gw_gid(const oracle_gw* s, int* gid, int* ktop);
 
+/* Coupled top (RichardsSolver::attachCoupling, src/gw/RichardsSolver.hpp:
+ * 132-186) with surface fields owned by the oracle, and the subsurface part
+ * of coupling::Coupler::step (src/coupling/Coupler.cpp:69-131). */
+int oracle_gw_attach_coupling(oracle_gw* s, double min_depth, int vent_all, int book_bounce);
+int oracle_gw_surface(oracle_gw* s, int which, double* out, const double* in);
+void oracle_gw_coupled_audit(const oracle_gw* s, frehg_gw_coupled_audit* out);
+int oracle_gw_coupler_init(oracle_gw* s, const frehg_gw_coupler_opts* o);
+int oracle_gw_coupler_step(oracle_gw* s, double t, double dt, const double* bottom,
+                           frehg_gw_window_audit* out);
+void oracle_gw_coupler_state(const oracle_gw* s, double t, double* next_dt, double* dtg,
+                             double* lag);
+
 /* Pointwise closures (src/gw/VanGenuchten.hpp:45-128), exported for the
  * golden-value tests. */
 double oracle_vg_theta(double vga, double vgn, double ts, double tr, double aev, double h);

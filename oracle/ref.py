@@ -79,6 +79,13 @@ def load(omp: bool = False):
     lib.ref_gid.argtypes = [C.c_void_p, _ip, _ip]
     lib.ref_bc_masks.argtypes = [C.c_void_p, C.c_double, _ip, _dp]
     lib.ref_reallocate_only.argtypes = [C.c_void_p]
+    lib.ref_attach_coupling.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
+    lib.ref_surface.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+    lib.ref_coupled_audit.argtypes = [C.c_void_p, _dp]
+    lib.ref_coupler_create.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_int]
+    lib.ref_coupler_step.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp]
+    lib.ref_coupler_state.argtypes = [C.c_void_p, C.c_double, _dp]
     _libs[path] = lib
     return lib
 
@@ -90,6 +97,11 @@ _IC = {"moisture": 0, "head": 1, "water_table": 2}
 
 AUDIT_KEYS = ("boundary_in", "ss_storage", "realloc_adjust", "realloc_dropped", "vloss",
               "cpl_vent", "pc_clamp_volume")
+CPL_KEYS = ("exchanged", "bounce", "vent", "vent_thin", "evap", "pc_clamp_volume")
+WINDOW_GW_KEYS = ("boundary_in", "ss_storage", "realloc_adjust", "realloc_dropped", "vloss")
+# ref_surface slots: the FREHG_GW_SURF_* numbering, plus the stand-in's rain.
+SURF = {"eta": 0, "dept": 1, "seep_accum": 2, "avail": 3, "gain": 4, "bounce": 5, "qss": 6,
+        "bottom": 7, "rain": 9}
 
 
 class RefSolver:
@@ -245,3 +257,47 @@ class RefSolver:
         hf[1:-1, 1:-1, :] = head
         wf[1:-1, 1:-1, :] = wc
         self.lib.ref_set_state(self.h, hf.ctypes.data_as(_dp), wf.ctypes.data_as(_dp))
+
+    # -- coupled top -------------------------------------------------------------
+    def attach_coupling(self, min_depth: float, vent_all: bool = False,
+                        book_bounce: bool = False) -> None:
+        """Harness-owned GwCoupling views, zeroed (Coupler.cpp:40-60)."""
+        self.lib.ref_attach_coupling(self.h, min_depth, int(vent_all), int(book_bounce))
+
+    def surface(self, name: str) -> np.ndarray:
+        out = np.empty((self.ny + 2, self.nx + 2))
+        if self.lib.ref_surface(self.h, SURF[name], out.ctypes.data_as(_dp), None) != 0:
+            raise KeyError(name)
+        return out
+
+    def set_surface(self, name: str, value) -> None:
+        v = np.ascontiguousarray(np.broadcast_to(value, (self.ny + 2, self.nx + 2)), np.float64)
+        if self.lib.ref_surface(self.h, SURF[name], None, v.ctypes.data_as(_dp)) != 0:
+            raise KeyError(name)
+
+    def coupled_audit(self) -> dict:
+        out = np.zeros(6)
+        self.lib.ref_coupled_audit(self.h, out.ctypes.data_as(_dp))
+        return dict(zip(CPL_KEYS, out.tolist()))
+
+    def coupler_create(self, sync: bool, dt: float, dt_init: float, t_start: float = 0.0,
+                       min_depth: float = 0.0, paired: bool = False) -> None:
+        """The reference's coupling::Coupler over the stand-in surface
+        (oracle/shim/include/swe/SurfaceSolver.hpp)."""
+        if self.lib.ref_coupler_create(self.h, int(sync), dt, dt_init, t_start, min_depth,
+                                       int(paired)) != 0:
+            raise RuntimeError("reference Coupler: " + self.lib.ref_last_error().decode())
+
+    def coupler_step(self, t: float, dt: float) -> dict:
+        out = np.zeros(15)
+        if self.lib.ref_coupler_step(self.h, t, dt, out.ctypes.data_as(_dp)) != 0:
+            raise RuntimeError("reference coupled step: " + self.lib.ref_last_error().decode())
+        v = out.tolist()
+        return {"gw": dict(zip(WINDOW_GW_KEYS, v[:5])), "cpl": dict(zip(CPL_KEYS[:5], v[5:10])),
+                "applied": v[10], "discarded": v[11], "surface_gain": v[12],
+                "accum_volume": v[13], "substeps": int(v[14])}
+
+    def coupler_state(self, t: float) -> tuple:
+        out = np.zeros(3)
+        self.lib.ref_coupler_state(self.h, t, out.ctypes.data_as(_dp))
+        return tuple(out.tolist())

@@ -9,6 +9,7 @@
 // with k fastest (src/core/Types.hpp:35-43).
 
 #include "bc/BoundarySet.hpp"
+#include "coupling/Coupler.hpp"
 #include "core/Config.hpp"
 #include "core/Grid.hpp"
 #include "core/HaloExchanger.hpp"
@@ -72,6 +73,11 @@ struct RefSim {
   std::unique_ptr<frehg::gw::TerrainMetric> mesh;
   std::unique_ptr<frehg::BoundarySet> boundaries;
   std::unique_ptr<frehg::gw::RichardsSolver> gw;
+  // coupled top: harness-owned GwCoupling views (ref_attach_coupling), or the
+  // reference's Coupler over the stand-in surface (ref_coupler_create)
+  frehg::gw::GwCoupling coupling;
+  std::unique_ptr<frehg::swe::SurfaceSolver> surface;
+  std::unique_ptr<frehg::coupling::Coupler> coupler;
 };
 
 std::string g_error;
@@ -355,5 +361,136 @@ void ref_bc_masks(void* h, double t, int* codes, double* values) {
 }
 
 void ref_reallocate_only(void* h) { static_cast<RefSim*>(h)->gw->reallocateWaterContent(); }
+
+/// Attach harness-owned coupled surface views (zeroed) to the solver, as the
+/// coupler's constructor does (src/coupling/Coupler.cpp:40-60).
+int ref_attach_coupling(void* h, double min_depth, int vent_all, int book_bounce) {
+  RefSim& s = *static_cast<RefSim*>(h);
+  const std::size_t ny2 = static_cast<std::size_t>(s.grid->nyLocal()) + 2;
+  const std::size_t nx2 = static_cast<std::size_t>(s.grid->nxLocal()) + 2;
+  frehg::gw::GwCoupling& c = s.coupling;
+  c.active = true;
+  c.minDepth = min_depth;
+  c.eta = frehg::Field2<double>("eta", ny2, nx2);
+  c.dept = frehg::Field2<double>("dept", ny2, nx2);
+  c.seepAccum = frehg::Field2<double>("seep", ny2, nx2);
+  c.avail = frehg::Field2<double>("avail", ny2, nx2);
+  c.gain = frehg::Field2<double>("gain", ny2, nx2);
+  if (book_bounce) c.bounce = frehg::Field2<double>("bounce", ny2, nx2);
+  c.ventAll = vent_all != 0;
+  s.gw->attachCoupling(c);
+  return 0;
+}
+
+namespace {
+frehg::Field2<double> surfaceView(RefSim& s, int which) {
+  if (s.coupler) {
+    switch (which) {
+      case 0: return s.surface->eta();
+      case 1: return s.surface->depth();
+      case 2: return s.coupler->seepAccum();
+      case 4: return s.coupler->gain();
+      case 5: return s.coupler->bounce();
+      case 6: return s.coupler->seepageRate();
+      case 7: return s.surface->bottom();
+      case 9: return s.surface->rain();
+      default: return frehg::Field2<double>();
+    }
+  }
+  switch (which) {
+    case 0: return s.coupling.eta;
+    case 1: return s.coupling.dept;
+    case 2: return s.coupling.seepAccum;
+    case 3: return s.coupling.avail;
+    case 4: return s.coupling.gain;
+    case 5: return s.coupling.bounce;
+    default: return frehg::Field2<double>();
+  }
+}
+}  // namespace
+
+/// Surface field `which` (0 eta, 1 depth, 2 seepAccum, 3 avail, 4 gain,
+/// 5 bounce, 6 qss, 7 bottom, 9 rain of the stand-in surface), (ny+2)*(nx+2):
+/// copied out when out is given, then overwritten from in when in is given.
+int ref_surface(void* h, int which, double* out, const double* in) {
+  RefSim& s = *static_cast<RefSim*>(h);
+  frehg::Field2<double> v = surfaceView(s, which);
+  if (!v.is_allocated()) {
+    g_error = "surface field not available";
+    return 1;
+  }
+  if (out) std::memcpy(out, v.data(), v.span() * sizeof(double));
+  if (in) std::memcpy(v.data(), in, v.span() * sizeof(double));
+  return 0;
+}
+
+/// cpl[0..4] = cplExchanged, cplBounce, cplVent, cplVentThin, cplEvap of the
+/// last step; cpl[5] = pcClampVolume (cumulative).
+void ref_coupled_audit(void* h, double* out) {
+  const auto& gw = *static_cast<RefSim*>(h)->gw;
+  const auto& a = gw.audit();
+  out[0] = a.cplExchanged;
+  out[1] = a.cplBounce;
+  out[2] = a.cplVent;
+  out[3] = a.cplVentThin;
+  out[4] = a.cplEvap;
+  out[5] = gw.pcClampVolume();
+}
+
+/// The reference's coupling::Coupler over the stand-in surface: sync or
+/// subcycled, surface dt, groundwater dt_init, start time, min_depth, the
+/// paired-store switch (every vent deposits).
+int ref_coupler_create(void* h, int sync, double dt, double dt_init, double t_start,
+                       double min_depth, int paired) {
+  try {
+    RefSim& s = *static_cast<RefSim*>(h);
+    frehg::FrehgConfig cfg = s.cfg;
+    cfg.coupling.mode = sync ? frehg::CouplingConfig::Mode::Sync
+                             : frehg::CouplingConfig::Mode::Subcycled;
+    cfg.time.dt = dt;
+    cfg.time.tStart = t_start;
+    cfg.groundwater.timestep.dtInit = dt_init;
+    cfg.surfaceWater.minDepth = min_depth;
+    cfg.modules.transport = false;
+    const std::size_t ny2 = static_cast<std::size_t>(s.grid->nyLocal()) + 2;
+    const std::size_t nx2 = static_cast<std::size_t>(s.grid->nxLocal()) + 2;
+    s.surface = std::make_unique<frehg::swe::SurfaceSolver>(ny2, nx2, min_depth);
+    s.surface->setPairedStore(paired != 0);
+    s.coupler = std::make_unique<frehg::coupling::Coupler>(*s.grid, cfg, *s.surface, *s.gw);
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+/// Coupler::step(t, dt).  out[0..] = the CouplingAudit: gw boundaryIn,
+/// ssStorage, reallocAdjust, reallocDropped, vloss, cplExchanged, cplBounce,
+/// cplVent, cplVentThin, cplEvap, applied, discarded, surfaceGain,
+/// accumVolume, substeps.
+int ref_coupler_step(void* h, double t, double dt, double* out) {
+  try {
+    RefSim& s = *static_cast<RefSim*>(h);
+    s.coupler->step(t, dt);
+    const frehg::coupling::CouplingAudit& a = s.coupler->audit();
+    const double v[] = {a.gw.boundaryIn, a.gw.ssStorage, a.gw.reallocAdjust, a.gw.reallocDropped,
+                        a.gw.vloss, a.gw.cplExchanged, a.gw.cplBounce, a.gw.cplVent,
+                        a.gw.cplVentThin, a.gw.cplEvap, a.applied, a.discarded, a.surfaceGain,
+                        a.accumVolume, static_cast<double>(a.substeps)};
+    std::memcpy(out, v, sizeof v);
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+/// Coupler::nextDt, currentDtg, gwLag(t).
+void ref_coupler_state(void* h, double t, double* out) {
+  const auto& c = *static_cast<RefSim*>(h)->coupler;
+  out[0] = c.nextDt();
+  out[1] = c.currentDtg();
+  out[2] = c.gwLag(t);
+}
 
 }  // extern "C"

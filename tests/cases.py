@@ -211,6 +211,61 @@ def mixed_box(seed: int = 7, nx: int = 6, ny: int = 5, nz: int = 12) -> GwConfig
     return cfg
 
 
+def coupled_box(pc: str = "consistent", seed: int = 11, nx: int = 7, ny: int = 6,
+                nz: int = 12) -> GwConfig:
+    """A small box for the coupled top: rough bed, two soils, Ss > 0, a head
+    IC that is saturated (positive, pressurized) in some columns, at the
+    retention curve's air-entry value near the top of others and dry
+    elsewhere; top flux conditions (infiltration on one half, evaporation on
+    a strip), a pushing head at part of the bottom, a hydrostatic west edge
+    whose stage stands above the bed, a masked column."""
+    rng = np.random.default_rng(seed)
+    cfg = base(nx, ny, nz, 0.05, 2.0)
+    cfg.groundwater.timestep = Timestep(dt_init=2.0, dt_min=0.01, dt_max=60.0)
+    cfg.groundwater.specific_storage = 1.0e-5
+    cfg.groundwater.predictor_corrector = pc
+    cfg.groundwater.reallocation_surplus = "redistribute"
+    bath = rng.uniform(-0.12, 0.0, size=(ny, nx))
+    bath[ny - 1, nx - 1] = -2.0  # fully masked column
+    cfg.domain.bottom_elevation = bath
+    cfg.soil_types = [test_soil(2e-5, "a"), SoilType("b", 5e-6, 5e-6, 2e-6, 0.42, 0.06, 2.0,
+                                                      1.8, 0.0)]
+    cfg.soil_map = rng.integers(0, 2, size=(ny, nx, nz))
+    head = rng.uniform(-1.2, -0.3, size=(ny, nx, nz))
+    z = (np.arange(nz) + 0.5) * 0.05
+    head[0:2, 0:3, :] = 0.15 + z                 # pressurized, saturated columns
+    head[2:4, 3:5, 0:3] = -0.01                  # wet top cells (h above the air-entry value)
+    cfg.initial = InitialCondition("head", head)
+    half = [(-0.1, -0.1), (nx / 2 + 0.01, -0.1), (nx / 2 + 0.01, ny + 0.1), (-0.1, ny + 0.1)]
+    strip = [(nx / 2 + 0.01, -0.1), (nx + 0.1, -0.1), (nx + 0.1, 1.5), (nx / 2 + 0.01, 1.5)]
+    cfg.boundary_conditions = [
+        BoundaryCondition("rain", half, "groundwater_top", "flux", "constant", -3e-6),
+        BoundaryCondition("evap", strip, "groundwater_top", "flux", "constant", 2e-7),
+        BoundaryCondition("push", [(-0.1, -0.1), (3.1, -0.1), (3.1, 2.1), (-0.1, 2.1)],
+                          "groundwater_bottom", "head", "constant", 0.9),
+        BoundaryCondition("drain", [(3.1, 2.1), (nx + 0.1, 2.1), (nx + 0.1, ny + 0.1),
+                                    (3.1, ny + 0.1)], "groundwater_bottom", "flux", "gravity"),
+        BoundaryCondition("west", [(-0.1, -0.1), (0.6, -0.1), (0.6, ny + 0.1), (-0.1, ny + 0.1)],
+                          "groundwater_side", "head", "hydrostatic", hydrostatic_eta=0.04),
+    ]
+    return cfg
+
+
+def coupled_surface(bath_halo: np.ndarray, seed: int = 5):
+    """Initial free surface and rain rate of the stand-in surface over a
+    coupled box: ponds of 5 cm, 1.2 mm (a thin supply-limited film) and
+    0.4 mm (below a 1 mm min_depth) on some columns, rain on a block."""
+    rng = np.random.default_rng(seed)
+    ny2, nx2 = bath_halo.shape
+    pond = np.zeros((ny2, nx2))
+    pond[3:5, 1:3] = 0.05
+    pond[5, 4:6] = 0.0012
+    pond[1, 5] = 0.0004
+    rain = np.zeros((ny2, nx2))
+    rain[4:7, 3:7] = rng.uniform(1e-6, 4e-6, size=rain[4:7, 3:7].shape)
+    return bath_halo + pond, rain
+
+
 SCENARIOS = {
     "closed_column": lambda: closed_column(),
     "closed_column_ss": lambda: closed_column(1.0e-4),
