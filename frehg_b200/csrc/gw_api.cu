@@ -432,6 +432,7 @@ cudaError_t enqueue_predictor(frehg_gw_handle* h) {
   double* hn = D.h[D.cur];
   double* wcn = D.wc[D.cur];
   fgw::launch_ghosts(D, hn, wcn);
+  if (D.f.cpl) fgw::launch_cpl_mode(D, hn);
   fgw::launch_closure_pred(D, hn);
   fgw::launch_assemble(D, hn, wcn);
   if (h->precision == FREHG_GW_PRECISION_MIXED) return fgw::launch_line_factor(D);
@@ -445,6 +446,7 @@ void enqueue_corrector(frehg_gw_handle* h) {
   double* wcn = D.wc[D.cur];
   fgw::launch_closure_corr(D, hn);
   fgw::launch_flux(D, wcn);
+  if (D.f.cpl) fgw::launch_cpl_book(D, wcn);
   fgw::launch_update_wc(D, hn, wcn);
   if (h->profiling) cudaEventRecord(h->ev[3], D.stream);
   fgw::launch_classify(D, D.wc[nxt], D.h[nxt]);
@@ -489,6 +491,11 @@ int finish_step(frehg_gw_handle* h, frehg_gw_step_info* info) {
   h->start_buf = D.cur;
   D.cur = 1 - D.cur;
   h->next_dt = o.next_dt;
+  if (D.f.cpl) {
+    h->pc_clamp_total += o.cpl[5];
+    h->cpl_last = frehg_gw_coupled_audit{o.cpl[0], o.cpl[1], o.cpl[2], o.cpl[3], o.cpl[4],
+                                         h->pc_clamp_total};
+  }
   return FREHG_GW_OK;
 }
 

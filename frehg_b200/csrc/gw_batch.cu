@@ -502,6 +502,8 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
   for (int i = 0; i < n; ++i) {
     if (!members[i]) return fail(FREHG_GW_EINVAL, "batch: null member");
     if (!members[i]->have_state) return fail(FREHG_GW_ESTATE, "batch: member without state");
+    if (members[i]->D.f.cpl)
+      return fail(FREHG_GW_EUNSUPPORTED, "batch: a coupled-top member steps on its own");
     for (int j = 0; j < i; ++j)
       if (members[j] == members[i]) return fail(FREHG_GW_EINVAL, "batch: member given twice");
   }
@@ -541,6 +543,8 @@ int frehg_gw_batch_set_members(frehg_gw_batch* b, frehg_gw_handle* const* member
   for (int i = 0; i < n; ++i) {
     if (!members[i]) return fail(FREHG_GW_EINVAL, "batch: null member");
     if (!members[i]->have_state) return fail(FREHG_GW_ESTATE, "batch: member without state");
+    if (members[i]->D.f.cpl)
+      return fail(FREHG_GW_EUNSUPPORTED, "batch: a coupled-top member steps on its own");
   }
   const cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return cuda_fail(e, "batch: set members");

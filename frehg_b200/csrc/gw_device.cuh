@@ -32,6 +32,19 @@ struct Dims {
   int full3d, pc, harm, off, redistribute, terrain;
 };
 
+// The coupled top's device state (GwCoupling), one per coupled domain: the
+// vent rule, min_depth, the mesh bed (offset frame) and the surface fields
+// the step reads and writes, (ny+2)(nx+2) each, and the per-column exchange
+// mode.  Kernels reach it through Fields::cpl, null in groundwater-only runs,
+// so those keep the kernels' parameter blocks of the uncoupled step.
+struct CplDev {
+  int vent_all, book_bounce;
+  double min_depth;
+  const double* bath;
+  double *eta, *dept, *seep, *avail, *gain, *bounce;
+  int8_t* cmode;
+};
+
 // Device pointers of one domain (see gw_internal.h for ownership).
 struct Fields {
   // soil (halo layout, mirrored ghosts)
@@ -42,6 +55,7 @@ struct Fields {
   // boundary markers, (ny+2)(nx+2); side codes live on the edge columns
   const int *topc, *botc, *xmc, *xpc, *ymc, *ypc;
   const double *topv, *botv, *xmv, *xpv, *ymv, *ypv;
+  const CplDev* cpl;  // coupled top, null when off
 };
 
 __host__ __device__ inline long long cidx(const Dims& d, int j, int i, int k) {
@@ -307,13 +321,19 @@ struct ZFlank {
   int8_t act;
 };
 
-// z face plane k of a column: u = cell k-1 (above), l = cell k (below).
+// z face plane k of a column: u = cell k-1 (above), l = cell k (below);
+// dep = the column's surface depth (coupled runs).
+template <bool CPL>
 __device__ inline double face_z(const Dims& d, const ZFlank& u, const ZFlank& l, int k, int topc,
-                                int botc) {
+                                int botc, double dep) {
   const bool below = (k < d.nz) && l.act;
   const bool above = (k >= 1) && u.act;
   if ((k < d.nz && !below) || (k >= 1 && !above)) return 0.0;
   if (k == 0) {
+    if (CPL) {  // coupled top (Predictor.cpp:293-302)
+      if (d.pc) return (dep > 0.0) ? l.ks : l.kc;
+      return (dep > 0.0) ? 0.5 * (l.ks + l.kc) : l.kc;
+    }
     if (topc == kHead) return l.ks;
     if (topc == kNoFlux) return 0.0;
     return l.kc;

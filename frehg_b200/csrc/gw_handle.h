@@ -27,6 +27,14 @@ struct frehg_gw_handle {
   bool profiling = false;
   cudaEvent_t ev[6] = {};
   double phase_ms[5] = {0, 0, 0, 0, 0};
+  // coupled top: the last step's books and the cumulative mode-3 clamp
+  frehg_gw_coupled_audit cpl_last{};
+  double pc_clamp_total = 0.0;
+  // coupler (coupling::Coupler state): sync flag, surface dt, subsurface dt
+  // and clock
+  bool coupler = false;
+  int csync = 1;
+  double cdt = 0.0, cdtg = 0.0, ctsub = 0.0;
 };
 
 namespace fgw_api {

@@ -32,6 +32,10 @@ struct StepOut {
   double next_dt, volume;
   double dqmax, dtco;
   CgState cg;
+  // coupled top: exchanged, bounce, vent, vent_thin, evap, the mode-3 clamp
+  double cpl[6];
+  // coupler window: applied, discarded, surface gain, held seepage (per area)
+  double win[4];
 };
 
 // Slots of the per-block partial-reduction buffer.
@@ -45,7 +49,13 @@ enum PartialSlot {
   kPDqmax = 6,   // max dq (adaptive controller)
   kPDtco = 7,    // min Courant dt
   kPVol = 8,     // owned volume after the step
-  kPSlots = 9
+  kPExch = 9,    // coupled top: exchanged volume (bookkeeping)
+  kPBounce = 10, // coupled top: bounce-back volume (bookkeeping)
+  kPEvap = 11,   // coupled top: evaporation correction (bookkeeping)
+  kPClamp = 12,  // coupled top: the mode-3 upward-only clamp volume (bookkeeping)
+  kPVent = 13,   // coupled top: vented volume (send walk)
+  kPThin = 14,   // coupled top: vents the legacy rule would have dropped (send walk)
+  kPSlots = 15
 };
 
 // Launch geometry of the reducing cell kernels (fixed per domain so every
@@ -74,7 +84,14 @@ struct Device {
   double *qx = nullptr, *qy = nullptr, *qzf = nullptr;    // fluxes
   double *vloss = nullptr, *room = nullptr, *sup = nullptr, *sdn = nullptr;
   int* colflag = nullptr;
-  uint8_t* satf = nullptr;  // per-cell saturation flag of the post-allocation snapshot
+  uint8_t* satf = nullptr;
+  // coupled top: surface fields (FREHG_GW_SURF_* order, (ny+2)(nx+2) each;
+  // surf_own marks the ones allocated here) and the exchange mode
+  double* surf[8] = {};
+  bool surf_own[8] = {};
+  int8_t* cmode = nullptr;
+  CplDev* cpl_dev = nullptr;  // the kernels' copy of cpl_host (f.cpl when attached)
+  CplDev cpl_host{};  // per-cell saturation flag of the post-allocation snapshot
   // linear system: coefficients and vectors carry a zero margin of sy cells
   // on both ends; the pointers below point at cell 0.
   double *diag = nullptr, *gxp = nullptr, *gyp = nullptr, *gzp = nullptr, *rhs = nullptr;
@@ -116,6 +133,12 @@ void launch_finalize(const Device& D, double* wc_out, double co_max);
 void launch_step_info(const Device& D, double dq_grow, double dq_shrink, double dt_min,
                       double dt_max);
 void launch_volume(const Device& D, const double* wc);
+// Coupled top: exchange modes (before the predictor), bookkeeping (after the
+// corrector's fluxes), and the coupler window's opening and seepage.
+void launch_cpl_mode(const Device& D, const double* hn);
+void launch_cpl_book(const Device& D, const double* wcn);
+void launch_cpl_begin_window(const Device& D);
+void launch_cpl_seepage(const Device& D, double dt);
 void launch_init_state(const Device& D, int form, double constant, const double* field,
                        const double* bath, double offset);
 // FP64 Jacobi-PCG (PETSc KSPCG semantics); returns a CUDA error code.

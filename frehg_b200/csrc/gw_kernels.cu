@@ -32,6 +32,21 @@ __device__ inline double ghost_head(int code, double value, double interior, dou
   return interior;
 }
 
+// ghostHead with the coupled rule (Predictor.cpp:80-83, density ratio 1): a
+// hydrostatic stage above the edge column's bed follows the live surface
+// there, (bed - zc) + depth.  cc = the edge column.
+__device__ inline double ghost_head_at(const Dims& d, const Fields& f, int code, double value,
+                                       double interior, double zc, long long cc) {
+  if (code == kHydro && (f.cpl != nullptr)) {
+    const double bed = f.cpl->bath[cc];
+    if (value > bed) {
+      const double hydro = bed - zc;
+      return hydro + f.cpl->dept[cc];
+    }
+  }
+  return ghost_head(code, value, interior, zc);
+}
+
 struct SumOp {
   __device__ double operator()(double a, double b) const { return a + b; }
 };
@@ -70,7 +85,7 @@ __device__ __forceinline__ void ghosts_body(Dims d, Fields f, double* h, double*
   const long long nxg = 2LL * d.ny * d.nz, nyg = 2LL * d.nx * d.nz;
   for (long long t = bid * static_cast<long long>(blockDim.x) + threadIdx.x; t < nxg + nyg;
        t += static_cast<long long>(G) * blockDim.x) {
-    long long g, c;
+    long long g, c, cc;
     int code;
     double val;
     if (t < nxg) {
@@ -80,7 +95,7 @@ __device__ __forceinline__ void ghosts_body(Dims d, Fields f, double* h, double*
       const int ii = side == 0 ? 1 : d.nx;
       c = cidx(d, j, ii, k);
       g = side == 0 ? c - d.sx : c + d.sx;
-      const long long cc = col2(d, j, ii);
+      cc = col2(d, j, ii);
       code = side == 0 ? f.xmc[cc] : f.xpc[cc];
       val = side == 0 ? f.xmv[cc] : f.xpv[cc];
     } else {
@@ -91,11 +106,11 @@ __device__ __forceinline__ void ghosts_body(Dims d, Fields f, double* h, double*
       const int jj = side == 0 ? 1 : d.ny;
       c = cidx(d, jj, i, k);
       g = side == 0 ? c - d.sy : c + d.sy;
-      const long long cc = col2(d, jj, i);
+      cc = col2(d, jj, i);
       code = side == 0 ? f.ymc[cc] : f.ypc[cc];
       val = side == 0 ? f.ymv[cc] : f.ypv[cc];
     }
-    if (h) h[g] = ghost_head(code, val, h[c], f.bot[c] + 0.5 * f.dz[c]);
+    if (h) h[g] = ghost_head_at(d, f, code, val, h[c], f.bot[c] + 0.5 * f.dz[c], cc);
     if (wc) wc[g] = is_head(code) ? f.wcs[c] : wc[c];
   }
 }
@@ -169,7 +184,7 @@ __device__ __forceinline__ void closure_corr_body(Dims d, Fields f,
       const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
       const int code = i == 0 ? f.xmc[cc] : f.xpc[cc];
       const double val = i == 0 ? f.xmv[cc] : f.xpv[cc];
-      hv = ghost_head(code, val, ai ? xi : hi0, zc);
+      hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc);
     } else if (iin && (j == 0 || j == d.ny + 1)) {
       const long long ci = (j == 0) ? c + d.sy : c - d.sy;
       const long long cc = col2(d, j == 0 ? 1 : d.ny, i);
@@ -177,7 +192,7 @@ __device__ __forceinline__ void closure_corr_body(Dims d, Fields f,
       const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
       const int code = j == 0 ? f.ymc[cc] : f.ypc[cc];
       const double val = j == 0 ? f.ymv[cc] : f.ypv[cc];
-      hv = ghost_head(code, val, ai ? xi : hi0, zc);
+      hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc);
     }
     const KrParts p = vg_kr_parts(so, hv);
     hp[c] = hv;
@@ -207,6 +222,7 @@ __global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
 // (the same expression on the same data, so the stored matrix is the
 // reference's up to the rounding of its z legs).  Legs toward an inactive
 // cell or out of the domain are stored as 0 (PETSc ignores column -1).
+template <bool CPL>
 __device__ __forceinline__ void assemble_body(
     Dims d, Fields f, const double* __restrict__ kxf, const double* __restrict__ kyf,
     const double* __restrict__ kzff, const double* __restrict__ hn,
@@ -284,7 +300,18 @@ __device__ __forceinline__ void assemble_body(
     if (north && cyp == kFlux) gct += gyp;
     if (south && cym == kFlux) gct += gym;
     if (!(k == d.nz - 1 && botc != kHead)) gct -= gzp;
-    if (!top || topc == kHead) gct -= gzm;
+    // Coupled top (Predictor.cpp:527-547): the exchange mode decides the
+    // Dirichlet leg, the surface depth and window budget feed the RHS.
+    int cm = 0;
+    double dep = 0.0, avl = 0.0, wcrc = 0.0;
+    if (CPL && top) {
+      cm = f.cpl->cmode[col];
+      dep = f.cpl->dept[col];
+      avl = f.cpl->avail[col];
+      wcrc = f.wcr[c];
+    }
+    const bool dirichlet_top = CPL ? (cm == 1 || (d.pc && cm == 3)) : (topc == kHead);
+    if (!top || dirichlet_top) gct -= gzm;
 
     double b = storage * hnc * volume;
     b -= dtg * volume * kzp / dzc;
@@ -319,7 +346,24 @@ __device__ __forceinline__ void assemble_body(
       if (botc == kFlux) b += dtg * volume * (vbot + kzp) / dzc;
       else if (botc == kHead) b -= gzp * vbot;
     }
-    if (top) {
+    if (top && CPL) {  // Predictor.cpp:627-674
+      if (cm == 1) {
+        b -= gzm * dep;
+      } else if (d.pc && cm == 3) {
+        // the ghost head is 0: the leg sits in the diagonal only
+      } else if (cm == 2) {
+        const double roomTop = fmax(0.0, (0.9999 * wcsc - wcnc) * dzc);
+        const double take = fmin(avl, roomTop);
+        const double qsup = -take / dtg;
+        b += -dtg * volume * (qsup + kzm) / dzc;
+      } else {
+        double qtop = 0.0;
+        if (topc == kFlux &&
+            ((vtop > 0.0 && wcnc < wcsc) || (vtop < 0.0 && wcnc > wcrc)))
+          qtop = vtop;
+        b += -dtg * volume * (qtop + kzm) / dzc;
+      }
+    } else if (top) {
       if (topc == kHead) b -= gzm * vtop;
       else if (topc == kFlux) b += -dtg * volume * (vtop + kzm) / dzc;
     }
@@ -331,13 +375,14 @@ __device__ __forceinline__ void assemble_body(
   }
 }
 
+template <bool CPL>
 __global__ void __launch_bounds__(kBlock, 2) k_assemble(
     Dims d, Fields f, const double* __restrict__ kxf, const double* __restrict__ kyf,
     const double* __restrict__ kzff, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ ch, const double* __restrict__ dtgp,
     double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
     double* __restrict__ gzps, double* __restrict__ rhs) {
-  assemble_body(d, f, kxf, kyf, kzff, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs, blockIdx.x,
+  assemble_body<CPL>(d, f, kxf, kyf, kzff, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs, blockIdx.x,
                 gridDim.x);
 }
 
@@ -348,6 +393,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_assemble(
 // j = 0) and the z face above it (plus the bottom face for k = nz-1), into
 // the face arrays the corrector's k_flux overwrites later in the step.  A
 // separate pass keeps the assembly's loads to six face values.
+template <bool CPL>
 __device__ __forceinline__ void faces_body(Dims d, Fields f, PassK pk, double* __restrict__ kx,
                                            double* __restrict__ ky, double* __restrict__ kzf,
                                            const int bid, const int G) {
@@ -376,18 +422,20 @@ __device__ __forceinline__ void faces_body(Dims d, Fields f, PassK pk, double* _
       const ZFlank zu{pk.kcz[cu], f.ksz[cu], f.dz[cu], (k >= 1) ? f.act[cu] : int8_t(0)};
       const ZFlank zc{pk.kcz[c], f.ksz[c], f.dz[c], f.act[c]};
       const int topc = f.topc[col], botc = f.botc[col];
-      kzf[fz] = face_z(d, zu, zc, k, topc, botc);
+      const double dep = (CPL && k == 0) ? f.cpl->dept[col] : 0.0;
+      kzf[fz] = face_z<CPL>(d, zu, zc, k, topc, botc, dep);
       if (k == d.nz - 1) {
         const ZFlank none{0.0, 0.0, 0.0, 0};
-        kzf[fz + 1] = face_z(d, zc, none, d.nz, topc, botc);
+        kzf[fz + 1] = face_z<CPL>(d, zc, none, d.nz, topc, botc, 0.0);
       }
     }
   }
 }
 
+template <bool CPL>
 __global__ void __launch_bounds__(kBlock, 4) k_faces(Dims d, Fields f, PassK pk, double* kx,
                                                      double* ky, double* kzf) {
-  faces_body(d, f, pk, kx, ky, kzf, blockIdx.x, gridDim.x);
+  faces_body<CPL>(d, f, pk, kx, ky, kzf, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- fluxes
@@ -474,10 +522,57 @@ __device__ inline double flux_zv(const Dims& d, const Fields& f, const ZFlank& u
   return 0.0;
 }
 
+// The coupled exchange face above top cell c of column col
+// (Corrector.cpp:388-465, density ratios 1): by exchange mode, the supply-
+// limited take of the remaining surface water, the saturated Darcy flux
+// capped by the window's budget, the pressurized seepage face (upward only;
+// the clamped volume is booked by k_cpl_book), or the dry seepage face with
+// the guarded top flux.  Debits the column's budget; hc = predicted head,
+// wcc = theta of the cell.
+__device__ inline double flux_top_coupled(const Dims& d, const Fields& f, long long col,
+                                          long long c, double hc, double wcc, double dtg) {
+  const double ks = f.ksz[c], dzc = f.dz[c], dep = f.cpl->dept[col];
+  const int m = f.cpl->cmode[col];
+  const double delta = 0.5 * dzc;
+  double q;
+  if (m == 2) {
+    const double roomTop = fmax(0.0, (0.9999 * f.wcs[c] - wcc) * dzc);
+    const double take = fmin(f.cpl->avail[col], roomTop);
+    q = -take * d.az / dtg;
+    f.cpl->avail[col] -= take;
+  } else if (m == 1) {
+    q = d.az * ks * ((hc - dep) / delta - 1.0);
+    if (q < 0.0) {
+      const double need = -q * dtg / d.az;
+      const double av = f.cpl->avail[col];
+      if (need > av) {
+        q = -av * d.az / dtg;
+        f.cpl->avail[col] = 0.0;
+      } else {
+        f.cpl->avail[col] = av - need;
+      }
+    }
+  } else if (d.pc && m == 3) {
+    q = d.az * ks * ((hc - dep) / delta - 1.0);
+    if (q <= 0.0) q = 0.0;
+  } else {
+    const Soil so = soil_at(f, c);
+    const double kface = 0.5 * (vg_k(so, dep, ks) + vg_k(so, hc, ks));
+    q = d.az * kface * ((hc - dep) / delta - 1.0);
+    if (q <= 0.0) q = 0.0;
+    if (f.topc[col] == kFlux) {
+      const double v = f.topv[col];
+      if ((v > 0.0 && wcc > f.wcr[c]) || v < 0.0) q += v * d.az;
+    }
+  }
+  return q;
+}
+
 // Thread c owns the x+ and y+ faces of its cell (the domain's west and south
 // boundary faces through the ghost cells i = 0, j = 0) and the z face above
 // it (plus the bottom face for k = nz-1).  Each face's loads are issued
 // before its rules run.
+template <bool CPL>
 __device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
                                                     const double* __restrict__ hp,
                                                     const double* __restrict__ wcn,
@@ -486,7 +581,10 @@ __device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
                                                     double* __restrict__ kzf,
                                                     double* __restrict__ qx,
                                                     double* __restrict__ qy,
-                                                    double* __restrict__ qzf, const int bid, const int G) {
+                                                    double* __restrict__ qzf,
+                                                    const double* __restrict__ dtgp,
+                                                    const int bid, const int G) {
+  const double dtg = CPL ? *dtgp : 0.0;
   for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
@@ -541,18 +639,23 @@ __device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
       qy[c] = flux_lat(d, f, vy, d.dy, j == 0, j == d.ny, codey, valy, n, hp);
     }
     if (doZ) {
-      const long long fz = fidx(d, j, i, k);
-      kzf[fz] = face_z(d, zu, zc, k, topc, botc);
-      qzf[fz] = flux_zv(d, f, zu, zc, hpu, hpc, k, topc, topv, botc, botv, cu, hp);
+      const long long fz = fidx(d, j, i, k), col = col2(d, j, i);
+      const double dep = (CPL && k == 0) ? f.cpl->dept[col] : 0.0;
+      kzf[fz] = face_z<CPL>(d, zu, zc, k, topc, botc, dep);
+      if (CPL && zc.act && !(k >= 1 && zu.act))
+        qzf[fz] = flux_top_coupled(d, f, col, c, hpc, wcn[c], dtg);
+      else
+        qzf[fz] = flux_zv(d, f, zu, zc, hpu, hpc, k, topc, topv, botc, botv, cu, hp);
       if (k == d.nz - 1) {
         const ZFlank none{0.0, 0.0, 0.0, 0};
-        kzf[fz + 1] = face_z(d, zc, none, d.nz, topc, botc);
+        kzf[fz + 1] = face_z<CPL>(d, zc, none, d.nz, topc, botc, 0.0);
         qzf[fz + 1] = flux_zv(d, f, zc, none, hpc, 0.0, d.nz, topc, topv, botc, botv, c, hp);
       }
     }
   }
 }
 
+template <bool CPL>
 __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
                                                     const double* __restrict__ hp,
                                                     const double* __restrict__ wcn,
@@ -561,8 +664,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
                                                     double* __restrict__ kzf,
                                                     double* __restrict__ qx,
                                                     double* __restrict__ qy,
-                                                    double* __restrict__ qzf) {
-  flux_body(d, f, pk, hp, wcn, kx, ky, kzf, qx, qy, qzf, blockIdx.x, gridDim.x);
+                                                    double* __restrict__ qzf,
+                                                    const double* __restrict__ dtgp) {
+  flux_body<CPL>(d, f, pk, hp, wcn, kx, ky, kzf, qx, qy, qzf, dtgp, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- theta update
@@ -752,7 +856,9 @@ __device__ __forceinline__ CellPost classify_cell(
       const bool adjsat = (n.azp && szp) || (n.kxp != 0.0 && sxp) ||
                           (n.kxm != 0.0 && sxm) || (n.kyp != 0.0 && syp) ||
                           (n.kym != 0.0 && sym) ||
-                          (top ? (topc == kHead && topv >= 0.0) : (szm != 0));
+                          (top ? (f.cpl ? f.cpl->dept[col] > 0.0  // coupled: a wet surface
+                                        : (topc == kHead && topv >= 0.0))
+                               : (szm != 0));
       if (!adjsat) {
         if (before < 0.9999 * so.ts) hout = vg_head(so, before);
       } else if (!d.off) {
@@ -814,13 +920,76 @@ __global__ void __launch_bounds__(kBlock, 3) k_classify(
   classify_body(d, f, kx, ky, kzf, wcR, hR, satf, wc_out, h_out, room, sup, sdn, colflag, part_adj, part_drop, blockIdx.x, gridDim.x);
 }
 
+// A coupled column's surface during its send walks: the vent deposits
+// (Reallocate.cpp:463-490) land in these copies, written back after the
+// column, and in the vent books.
+struct VentState {
+  double eta, dept, avail, gain;
+  double vent, thin;
+  double min_depth;
+  int vent_all;
+};
+
+// What the upward walk could not place, dv > 0, leaves through the top of
+// column face `ll` of a coupled column: onto the surface when it is wet, the
+// amount exceeds min_depth or every vent deposits; else it is lost.
+__device__ inline void vent_top(const Dims& d, double dv, double dtg, double& qface,
+                                VentState& v, double& lost) {
+  const double dd = dv / d.az;
+  if (v.vent_all || v.dept > 0.0 || dd > v.min_depth) {
+    if (!(v.dept > 0.0 || dd > v.min_depth)) v.thin += dv;
+    v.eta += dd;
+    v.dept += dd;
+    v.avail += dd;
+    v.gain += dd;
+    qface += dv / dtg;
+    v.vent += dv;
+  } else {
+    lost -= dv;
+  }
+}
+
+__device__ inline void vent_load(const Fields& f, long long col, VentState& v) {
+  v.eta = f.cpl->eta[col];
+  v.dept = f.cpl->dept[col];
+  v.avail = f.cpl->avail[col];
+  v.gain = f.cpl->gain[col];
+  v.min_depth = f.cpl->min_depth;
+  v.vent_all = f.cpl->vent_all;
+}
+
+__device__ inline void vent_store(const Fields& f, long long col, const VentState& v) {
+  f.cpl->eta[col] = v.eta;
+  f.cpl->dept[col] = v.dept;
+  f.cpl->avail[col] = v.avail;
+  f.cpl->gain[col] = v.gain;
+}
+
+// Block sums of the walk's books: the overflow into slot kPLost and, in
+// coupled runs, the vents into kPVent / kPThin.
+template <bool CPL>
+__device__ inline void walk_books(const Dims& d, double lost, const VentState& v, double* partial,
+                                  int nblk, int bid) {
+  const double s = block_reduce(lost, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[kPLost * nblk + bid] = s;
+  if (CPL) {
+    const double sv = block_reduce(v.vent, SumOp(), 0.0);
+    if (threadIdx.x == 0) partial[kPVent * nblk + bid] = sv;
+    const double st = block_reduce(v.thin, SumOp(), 0.0);
+    if (threadIdx.x == 0) partial[kPThin * nblk + bid] = st;
+  }
+}
+
 // Phase 2: the vertical send walks, one thread per flagged column, k
-// ascending (Reallocate.cpp:410-540, uncoupled, no transport window).
+// ascending (Reallocate.cpp:410-540, no transport window).
+template <bool CPL>
 __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
                        const double* __restrict__ sdn, double* qzf, const int* __restrict__ colflag,
-                       const double* __restrict__ dtgp, double* partial, const int bid, const int G) {
+                       const double* __restrict__ dtgp, double* partial, int nblk, const int bid,
+                       const int G) {
   const double dtg = *dtgp;
   double lost = 0.0;
+  VentState v{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0};
   const long long ncolint = static_cast<long long>(d.nx) * d.ny;
   for (long long t = bid * static_cast<long long>(blockDim.x) + threadIdx.x; t < ncolint;
        t += static_cast<long long>(G) * blockDim.x) {
@@ -829,6 +998,7 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
     if (!colflag[col]) continue;
     const long long base = cidx(d, j, i, 0), fb = fidx(d, j, i, 0);
     const bool topHead = f.topc[col] == kHead;
+    if (CPL) vent_load(f, col, v);
     for (int k = 0; k < d.nz; ++k) {
       if (!f.act[base + k]) continue;
       double dv = sup[base + k];
@@ -846,7 +1016,9 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
           }
         }
         if (dv > 0.0) {
-          if (topHead) {
+          if (CPL) {
+            vent_top(d, dv, dtg, qzf[fb + ll], v, lost);
+          } else if (topHead) {
             qzf[fb + ll] += dv / dtg;
           } else {
             while (ll + 1 < d.nz && dv > 0.0) {
@@ -881,15 +1053,17 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
         lost -= dv;
       }
     }
+    if (CPL) vent_store(f, col, v);
   }
-  const double s = block_reduce(lost, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[bid] = s;
+  walk_books<CPL>(d, lost, v, partial, nblk, bid);
 }
 
+template <bool CPL>
 __global__ void k_walk_thread(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
                        const double* __restrict__ sdn, double* qzf, const int* __restrict__ colflag,
-                       const double* __restrict__ dtgp, double* partial) {
-  walk_thread_body(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, blockIdx.x, gridDim.x);
+                       const double* __restrict__ dtgp, double* partial, int nblk) {
+  walk_thread_body<CPL>(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, nblk, blockIdx.x,
+                   gridDim.x);
 }
 
 // The same walk with one warp per flagged column.  The column's room, theta,
@@ -960,9 +1134,11 @@ __device__ inline void walk_take(double& dv, int m, double* rs, double* ws, cons
 // staged column (Reallocate.cpp:410-540): upward through the cells with room
 // up to the first inactive cell above or the surface, then out through a
 // head top or back down; downward to the bottom; what finds no room is lost.
-__device__ inline void walk_cell(int kk, double upv, double dnv, int nz, bool topHead, double* rs,
-                                 double* ws, const double* vs, double* qs, unsigned* rbits,
-                                 const unsigned* ibits, double dtg, double& lost) {
+template <bool CPL>
+__device__ inline void walk_cell(const Dims& d, int kk, double upv, double dnv, int nz, bool topHead,
+                                 double* rs, double* ws, const double* vs, double* qs,
+                                 unsigned* rbits, const unsigned* ibits, double dtg, double& lost,
+                                 VentState& v) {
   double dv = upv;
   if (dv > 0.0) {
     // Upward: cells kk-1, kk-2, ... up to the first inactive cell above
@@ -979,7 +1155,9 @@ __device__ inline void walk_cell(int kk, double upv, double dnv, int nz, bool to
       ll = m;
     }
     if (dv > 0.0) {
-      if (topHead) {
+      if (CPL) {
+        vent_top(d, dv, dtg, qs[ll], v, lost);
+      } else if (topHead) {
         qs[ll] += dv / dtg;
       } else {
         while (dv > 0.0) {
@@ -1005,13 +1183,15 @@ __device__ inline void walk_cell(int kk, double upv, double dnv, int nz, bool to
   }
 }
 
+template <bool CPL>
 __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ room,
                                                  const double* __restrict__ sup,
                                                  const double* __restrict__ sdn, double* qzf,
                                                  const int* __restrict__ colflag,
                                                  const double* __restrict__ dtgp,
-                                                 double* partial, const int bid, const int G) {
+                                                 double* partial, int nblk, const int bid,
+                                                 const int G) {
   extern __shared__ __align__(16) unsigned char walk_smem[];
   const double dtg = *dtgp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1023,6 +1203,7 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
   unsigned* rbits = reinterpret_cast<unsigned*>(qs + nz + 1);
   unsigned* ibits = rbits + nw;  // inactive cells
   double lost = 0.0;
+  VentState v{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0};
   const long long ncolint = static_cast<long long>(d.nx) * d.ny;
   const long long nwarps = static_cast<long long>(G) * kWalkWarps;
   for (long long t = bid * static_cast<long long>(kWalkWarps) + warp; t < ncolint;
@@ -1032,6 +1213,7 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
     if (!colflag[col]) continue;
     const long long base = cidx(d, j, i, 0), fb = fidx(d, j, i, 0);
     const bool topHead = f.topc[col] == kHead;
+    if (CPL && lane == 0) vent_load(f, col, v);
     for (int k0 = 0; k0 < nz; k0 += 32) {
       const int k = k0 + lane;
       double r = 0.0;
@@ -1067,27 +1249,187 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
         mask &= mask - 1;
         const double upv = __shfl_sync(0xffffffffu, su, b);
         const double dnv = __shfl_sync(0xffffffffu, sd, b);
-        if (lane == 0) walk_cell(k0 + b, upv, dnv, nz, topHead, rs, ws, vs, qs, rbits, ibits, dtg,
-                                 lost);
+        if (lane == 0)
+          walk_cell<CPL>(d, k0 + b, upv, dnv, nz, topHead, rs, ws, vs, qs, rbits, ibits, dtg, lost, v);
         __syncwarp();
       }
     }
     for (int k = lane; k < nz; k += 32) wc[base + k] = ws[k];
     for (int k = lane; k <= nz; k += 32) qzf[fb + k] = qs[k];
+    if (CPL && lane == 0) vent_store(f, col, v);
     __syncwarp();
   }
-  const double s = block_reduce(lost, SumOp(), 0.0);
-  if (threadIdx.x == 0) partial[bid] = s;
+  walk_books<CPL>(d, lost, v, partial, nblk, bid);
 }
 
+template <bool CPL>
 __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ room,
                                                  const double* __restrict__ sup,
                                                  const double* __restrict__ sdn, double* qzf,
                                                  const int* __restrict__ colflag,
                                                  const double* __restrict__ dtgp,
-                                                 double* partial) {
-  walk_body(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, blockIdx.x, gridDim.x);
+                                                 double* partial, int nblk) {
+  walk_body<CPL>(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, nblk, blockIdx.x, gridDim.x);
+}
+
+// ---------------------------------------------------------------- coupled top
+// First active cell of column (j, i), or -1.
+__device__ inline int first_active(const Dims& d, const Fields& f, int j, int i) {
+  const long long base = cidx(d, j, i, 0);
+  for (int k = 0; k < d.nz; ++k)
+    if (f.act[base + k]) return k;
+  return -1;
+}
+
+// classifyCoupledTopImpl<PC> (Corrector.cpp:55-115), one thread per column:
+// 1 = a wet surface whose saturated demand the window's water funds, 2 = a
+// wet surface it cannot fund, 3 = (consistent form) a dry surface over a
+// top cell pressurized past dz/2, 0 = dry.
+__global__ void k_cpl_mode(Dims d, Fields f, const double* __restrict__ h,
+                           const double* __restrict__ dtgp) {
+  const double dtg = *dtgp;
+  const long long ncol = static_cast<long long>(d.nx) * d.ny;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < ncol;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(t / d.nx) + 1, i = static_cast<int>(t % d.nx) + 1;
+    const long long col = col2(d, j, i);
+    const int kt = first_active(d, f, j, i);
+    const double dep = f.cpl->dept[col];
+    int8_t m = 0;
+    if (kt < 0 || dep <= 0.0) {
+      if (d.pc && kt >= 0) {
+        const long long c = cidx(d, j, i, kt);
+        if (h[c] > 0.5 * f.dz[c]) m = 3;
+      }
+    } else {
+      const long long c = cidx(d, j, i, kt);
+      const double ks = f.ksz[c];
+      const double qest = 2.0 * ks * (h[c] - dep) / f.dz[c] - ks;
+      m = (qest < 0.0 && -qest * dtg > f.cpl->avail[col]) ? 2 : 1;
+    }
+    f.cpl->cmode[col] = m;
+  }
+}
+
+// applyCoupledTopBookkeeping (Corrector.cpp:539-627, no ET), one thread per
+// column after the corrector's fluxes: the exchanged volume, the bounce-back
+// of infiltration a full top cell cannot take under a dry surface, the
+// seepage accumulator and the evaporation correction; also books the
+// consistent form's mode-3 upward-only clamp from the flux pass's inputs
+// (Corrector.cpp:431-445).  wcn = theta of the step start (the corrector's
+// theta until the update), hp = predicted head.  nblk blocks, one partial
+// per block in each book.
+__global__ void k_cpl_book(Dims d, Fields f, const double* __restrict__ hp,
+                           const double* __restrict__ wcn, const double* __restrict__ qzf,
+                           const double* __restrict__ dtgp, double* partial, int nblk) {
+  const double dtg = *dtgp;
+  double se = 0.0, sb = 0.0, sv = 0.0, sc = 0.0;
+  const long long ncol = static_cast<long long>(d.nx) * d.ny;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < ncol;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(t / d.nx) + 1, i = static_cast<int>(t % d.nx) + 1;
+    const long long col = col2(d, j, i);
+    const int kt = first_active(d, f, j, i);
+    if (kt < 0) continue;
+    const long long c = cidx(d, j, i, kt);
+    const double q = qzf[fidx(d, j, i, kt)];
+    double dep = f.cpl->dept[col];
+    se += q * dtg;
+    if (d.pc && f.cpl->cmode[col] == 3) {
+      const double qr = d.az * f.ksz[c] * ((hp[c] - dep) / (0.5 * f.dz[c]) - 1.0);
+      if (qr <= 0.0) sc += -qr * dtg;
+    }
+    if (q < 0.0 && dep <= f.cpl->min_depth) {
+      const double volume = d.az * f.dz[c];
+      if ((f.wcs[c] - wcn[c]) < -q * dtg / volume) {
+        const double dd = -q * dtg / d.az;
+        f.cpl->eta[col] += dd;
+        dep += dd;
+        f.cpl->dept[col] = dep;
+        f.cpl->avail[col] += dd;
+        f.cpl->gain[col] += dd;
+        if (f.cpl->book_bounce) f.cpl->bounce[col] += dd;
+        sb += dd * d.az;
+      }
+    }
+    double acc = f.cpl->seep[col] + q * dtg / d.az;
+    const double tv = f.topv[col];
+    if (f.topc[col] == kFlux && tv > 0.0 && wcn[c] > f.wcr[c] && dep <= f.cpl->min_depth) {
+      acc -= tv * dtg;
+      sv += tv * dtg * d.az;
+    }
+    f.cpl->seep[col] = acc;
+  }
+  const double r0 = block_reduce(se, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[kPExch * nblk + blockIdx.x] = r0;
+  const double r1 = block_reduce(sb, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[kPBounce * nblk + blockIdx.x] = r1;
+  const double r2 = block_reduce(sv, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[kPEvap * nblk + blockIdx.x] = r2;
+  const double r3 = block_reduce(sc, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[kPClamp * nblk + blockIdx.x] = r3;
+}
+
+// Coupler::beginWindow (Exchange.cpp:21-52): the window's infiltration
+// budget from the refreshed depth, the deposit tally cleared.
+__global__ void k_cpl_begin_window(Dims d, Fields f) {
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < d.ncol;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(t / d.nx2), i = static_cast<int>(t % d.nx2);
+    if (j >= 1 && j <= d.ny && i >= 1 && i <= d.nx) {
+      f.cpl->avail[t] = f.cpl->dept[t];
+      f.cpl->gain[t] = 0.0;
+    }
+    if (f.cpl->book_bounce) f.cpl->bounce[t] = 0.0;
+  }
+}
+
+// Coupler::applySeepage (Exchange.cpp:54-107) and reduceAudit (:109-127):
+// infiltration applied in full down to the bed, seepage applied onto a wet
+// surface or once it exceeds min_depth, else held; qss = the window's rate.
+// Books per block: applied, clamp remainder, gain and held seepage.
+__global__ void k_cpl_seepage(Dims d, Fields f, double* __restrict__ qss,
+                              const double* __restrict__ bottom, double dt, double* partial,
+                              int nblk) {
+  double sa = 0.0, sd = 0.0, sg = 0.0, sh = 0.0;
+  const long long ncol = static_cast<long long>(d.nx) * d.ny;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < ncol;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(t / d.nx) + 1, i = static_cast<int>(t % d.nx) + 1;
+    const long long col = col2(d, j, i);
+    const double a = f.cpl->seep[col];
+    double gain = f.cpl->gain[col], held = a;
+    qss[col] = a / dt;
+    if (a < 0.0) {
+      const double before = f.cpl->eta[col];
+      double e = before + a;
+      if (e < bottom[col]) e = bottom[col];
+      f.cpl->eta[col] = e;
+      const double change = e - before;
+      gain += change;
+      sa += change;
+      sd += change - a;
+      held = 0.0;
+    } else if (f.cpl->dept[col] > f.cpl->min_depth || a > f.cpl->min_depth) {
+      f.cpl->eta[col] += a;
+      gain += a;
+      sa += a;
+      held = 0.0;
+    }
+    f.cpl->gain[col] = gain;
+    f.cpl->seep[col] = held;
+    sg += gain;
+    sh += held;
+  }
+  const double r0 = block_reduce(sa, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[0 * nblk + blockIdx.x] = r0;
+  const double r1 = block_reduce(sd, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[1 * nblk + blockIdx.x] = r1;
+  const double r2 = block_reduce(sg, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[2 * nblk + blockIdx.x] = r2;
+  const double r3 = block_reduce(sh, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[3 * nblk + blockIdx.x] = r3;
 }
 
 // ---------------------------------------------------------------- clamp, audit, controller
@@ -1278,7 +1620,7 @@ __device__ double reduce_slot(const double* p, int n, Op op, double identity) {
 // 0.75, Courant cap, [dt_min, dt_max] clamp).
 // The step's dtg is read from out->next_dt, where the step found it, and the
 // controller's next dt replaces it there.
-__device__ __forceinline__ void step_info_body(const double* partial, int nblk, int off,
+__device__ __forceinline__ void step_info_body(const double* partial, int nblk, int off, int cpl,
                                                double dq_grow, double dq_shrink, double dt_min,
                                                double dt_max, double dtg, StepOut* out) {
   const double ss = reduce_slot(partial + kPSs * nblk, nblk, SumOp(), 0.0);
@@ -1307,17 +1649,35 @@ __device__ __forceinline__ void step_info_body(const double* partial, int nblk, 
     if (next < dt_min) next = dt_min;
     out->next_dt = next;
   }
+  if (cpl) {
+    // exchanged, bounce, vent, vent_thin, evap, mode-3 clamp (frehg_gw_coupled_audit order);
+    // the reallocation's vent books are zero when it is disabled
+    const int slot[6] = {kPExch, kPBounce, kPVent, kPThin, kPEvap, kPClamp};
+    for (int s = 0; s < 6; ++s) {
+      double v = reduce_slot(partial + slot[s] * nblk, nblk, SumOp(), 0.0);
+      if (off && (slot[s] == kPVent || slot[s] == kPThin)) v = 0.0;
+      if (threadIdx.x == 0) out->cpl[s] = v;
+    }
+  }
 }
 
-__global__ void k_step_info(const double* partial, int nblk, int off, double dq_grow,
+__global__ void k_step_info(const double* partial, int nblk, int off, int cpl, double dq_grow,
                             double dq_shrink, double dt_min, double dt_max, StepOut* out) {
   const double dtg = out->next_dt;  // read by every thread before thread 0 replaces it
-  step_info_body(partial, nblk, off, dq_grow, dq_shrink, dt_min, dt_max, dtg, out);
+  step_info_body(partial, nblk, off, cpl, dq_grow, dq_shrink, dt_min, dt_max, dtg, out);
 }
 
 __global__ void k_volume_final(const double* partial, int nblk, StepOut* out) {
   const double vol = reduce_slot(partial, nblk, SumOp(), 0.0);
   if (threadIdx.x == 0) out->volume = vol;
+}
+
+// The coupler window's four books (k_cpl_seepage) in a fixed order.
+__global__ void k_cpl_window_final(const double* partial, int nblk, StepOut* out) {
+  for (int s = 0; s < 4; ++s) {
+    const double v = reduce_slot(partial + s * nblk, nblk, SumOp(), 0.0);
+    if (threadIdx.x == 0) out->win[s] = v;
+  }
 }
 
 // ---------------------------------------------------------------- batched phases
@@ -1362,7 +1722,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_assemble_batch(const StepArgs* ta
   __shared__ StepArgs sa;
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
-  assemble_body(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp,
+  assemble_body<false>(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp,
                 sa.gyp, sa.gzp, sa.rhs, bid, G);
 }
 
@@ -1372,7 +1732,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_faces_batch(const StepArgs* tab, 
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
   const PassK pk{sa.kcx, sa.kcy, sa.kcz, sa.wcn};
-  faces_body(sa.d, sa.f, pk, sa.kx, sa.ky, sa.kzf, bid, G);
+  faces_body<false>(sa.d, sa.f, pk, sa.kx, sa.ky, sa.kzf, bid, G);
 }
 
 __global__ void __launch_bounds__(kBlock) k_closure_corr_batch(const StepArgs* tab,
@@ -1389,7 +1749,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux_batch(const StepArgs* tab, c
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
   const PassK pk{sa.kcx, sa.kcy, sa.kcz, sa.wcn};
-  flux_body(sa.d, sa.f, pk, sa.hp, sa.wcn, sa.kx, sa.ky, sa.kzf, sa.qx, sa.qy, sa.qzf, bid, G);
+  flux_body<false>(sa.d, sa.f, pk, sa.hp, sa.wcn, sa.kx, sa.ky, sa.kzf, sa.qx, sa.qy, sa.qzf, &sa.dtg, bid,
+            G);
 }
 
 __global__ void __launch_bounds__(kBlock, 4) k_update_wc_batch(const StepArgs* tab,
@@ -1417,11 +1778,11 @@ __global__ void __launch_bounds__(kBlock) k_walk_batch(const StepArgs* tab, cons
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
   if (sa.warp_walk) {
-    walk_body(sa.d, sa.f, sa.wc_out, sa.room, sa.sup, sa.sdn, sa.qzf, sa.colflag, &sa.dtg,
-              sa.partial + kPLost * sa.nblk, bid, G);
+    walk_body<false>(sa.d, sa.f, sa.wc_out, sa.room, sa.sup, sa.sdn, sa.qzf, sa.colflag, &sa.dtg,
+              sa.partial, sa.nblk, bid, G);
   } else {
-    walk_thread_body(sa.d, sa.f, sa.wc_out, sa.room, sa.sup, sa.sdn, sa.qzf, sa.colflag, &sa.dtg,
-                     sa.partial + kPLost * sa.nblk, bid, G);
+    walk_thread_body<false>(sa.d, sa.f, sa.wc_out, sa.room, sa.sup, sa.sdn, sa.qzf, sa.colflag, &sa.dtg,
+                     sa.partial, sa.nblk, bid, G);
   }
 }
 
@@ -1442,8 +1803,8 @@ __global__ void k_step_info_batch(const StepArgs* tab) {
   for (int w = threadIdx.x; w < static_cast<int>(sizeof(StepArgs) / 8); w += blockDim.x)
     dst[w] = src[w];
   __syncthreads();
-  step_info_body(sa.partial, sa.nblk, sa.d.off, sa.dq_grow, sa.dq_shrink, sa.dt_min, sa.dt_max,
-                 sa.dtg, sa.out);
+  step_info_body(sa.partial, sa.nblk, sa.d.off, (sa.f.cpl != nullptr), sa.dq_grow, sa.dq_shrink, sa.dt_min,
+                 sa.dt_max, sa.dtg, sa.out);
 }
 
 // The members' step records into one array, for a single read-back.
@@ -1495,8 +1856,10 @@ void launch_closure_pred(const Device& D, const double* h) {
 // The predictor's faces go through D.kx, D.ky, D.kzf (free until k_flux).
 void launch_assemble(const Device& D, const double* hn, const double* wcn) {
   const PassK pk{D.kcx, D.kcy, D.kcz, wcn};
-  k_faces<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.kx, D.ky, D.kzf);
-  k_assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.kx, D.ky, D.kzf, hn, wcn, D.ch,
+  const auto faces = (D.f.cpl != nullptr) ? k_faces<true> : k_faces<false>;
+  const auto assemble = (D.f.cpl != nullptr) ? k_assemble<true> : k_assemble<false>;
+  faces<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.kx, D.ky, D.kzf);
+  assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.kx, D.ky, D.kzf, hn, wcn, D.ch,
                                                      dtg_slot(D), D.diag, D.gxp, D.gyp, D.gzp,
                                                      D.rhs);
   D.launches += 2;
@@ -1510,8 +1873,9 @@ void launch_closure_corr(const Device& D, const double* hn) {
 
 void launch_flux(const Device& D, const double* wcn) {
   PassK pk{D.kcx, D.kcy, D.kcz, wcn};
-  k_flux<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.hp, wcn, D.kx, D.ky, D.kzf, D.qx,
-                                                 D.qy, D.qzf);
+  const auto flux = (D.f.cpl != nullptr) ? k_flux<true> : k_flux<false>;
+  flux<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.hp, wcn, D.kx, D.ky, D.kzf, D.qx,
+                                                 D.qy, D.qzf, dtg_slot(D));
   ++D.launches;
 }
 
@@ -1538,14 +1902,17 @@ constexpr size_t kWalkSmemMax = 96 * 1024;
 void launch_walk(const Device& D, double* wc_out) {
   const size_t smem = kWalkWarps * walk_warp_bytes(D.d.nz);
   if (D.d.nz <= kWalkMaxNz && smem <= kWalkSmemMax &&
-      raise_smem_limit(reinterpret_cast<const void*>(k_walk), smem) == cudaSuccess) {
-    k_walk<<<cells_grid(D), kBlock, smem, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
-                                                      D.qzf, D.colflag, dtg_slot(D),
-                                                      D.partial + kPLost * D.nblk);
+      raise_smem_limit(reinterpret_cast<const void*>((D.f.cpl != nullptr) ? k_walk<true> : k_walk<false>),
+                       smem) == cudaSuccess) {
+    const auto walk = (D.f.cpl != nullptr) ? k_walk<true> : k_walk<false>;
+    walk<<<cells_grid(D), kBlock, smem, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
+                                                      D.qzf, D.colflag, dtg_slot(D), D.partial,
+                                                      D.nblk);
   } else {
-    k_walk_thread<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
+    const auto walk = (D.f.cpl != nullptr) ? k_walk_thread<true> : k_walk_thread<false>;
+    walk<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
                                                           D.qzf, D.colflag, dtg_slot(D),
-                                                          D.partial + kPLost * D.nblk);
+                                                          D.partial, D.nblk);
   }
   ++D.launches;
 }
@@ -1558,9 +1925,40 @@ void launch_finalize(const Device& D, double* wc_out, double co_max) {
 
 void launch_step_info(const Device& D, double dq_grow, double dq_shrink,
                       double dt_min, double dt_max) {
-  k_step_info<<<1, kBlock, 0, D.stream>>>(D.partial, D.nblk, D.d.off, dq_grow, dq_shrink, dt_min,
-                                          dt_max, D.out);
+  k_step_info<<<1, kBlock, 0, D.stream>>>(D.partial, D.nblk, D.d.off, (D.f.cpl != nullptr), dq_grow,
+                                          dq_shrink, dt_min, dt_max, D.out);
   ++D.launches;
+}
+
+int column_blocks(const Device& D) {
+  const long long n = static_cast<long long>(D.d.nx) * D.d.ny;
+  return static_cast<int>(std::min<long long>((n + kBlock - 1) / kBlock, 4096));
+}
+
+void launch_cpl_mode(const Device& D, const double* hn) {
+  k_cpl_mode<<<column_blocks(D), kBlock, 0, D.stream>>>(D.d, D.f, hn, dtg_slot(D));
+  ++D.launches;
+}
+
+void launch_cpl_book(const Device& D, const double* wcn) {
+  k_cpl_book<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.hp, wcn, D.qzf, dtg_slot(D),
+                                                     D.partial, D.nblk);
+  ++D.launches;
+}
+
+void launch_cpl_begin_window(const Device& D) {
+  const int nb = static_cast<int>(std::min<long long>((D.d.ncol + kBlock - 1) / kBlock, 4096));
+  k_cpl_begin_window<<<nb, kBlock, 0, D.stream>>>(D.d, D.f);
+  ++D.launches;
+}
+
+// The window's books use the first four partial slots (free once the step
+// record is out).
+void launch_cpl_seepage(const Device& D, double dt) {
+  k_cpl_seepage<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.surf[6], D.surf[7], dt,
+                                                        D.partial, D.nblk);
+  k_cpl_window_final<<<1, kBlock, 0, D.stream>>>(D.partial, D.nblk, D.out);
+  D.launches += 2;
 }
 
 void launch_init_state(const Device& D, int form, double constant, const double* field,

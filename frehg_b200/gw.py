@@ -17,7 +17,8 @@ from typing import Optional
 
 import numpy as np
 
-from .abi import FIELD, STATUS_NAMES, GwDesc, StepInfo, field_shape, make_desc
+from .abi import (FIELD, STATUS_NAMES, SURF, CoupledAudit, Coupling, GwDesc, StepInfo,
+                  field_shape, make_desc)
 from .config import IC_FORMS, GwConfig, rasterize
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -66,10 +67,18 @@ def load_library(path: str = LIB_PATH):
     lib.frehg_gw_phase_times.restype = C.c_int
     lib.frehg_gw_kernel_launches.argtypes = [H]
     lib.frehg_gw_kernel_launches.restype = C.c_longlong
+    lib.frehg_gw_attach_coupling.argtypes = [H, C.POINTER(Coupling)]
+    lib.frehg_gw_get_surface.argtypes = [H, C.c_int, _dp]
+    lib.frehg_gw_set_surface.argtypes = [H, C.c_int, _dp]
+    lib.frehg_gw_surface_ptr.argtypes = [H, C.c_int, C.POINTER(C.c_void_p)]
+    lib.frehg_gw_coupled_audit_get.argtypes = [H, C.POINTER(CoupledAudit)]
+    lib.frehg_gw_elevation_offset.argtypes = [H]
+    lib.frehg_gw_elevation_offset.restype = C.c_double
     for name in ("frehg_gw_create", "frehg_gw_destroy", "frehg_gw_set_stream",
                  "frehg_gw_set_bc_values", "frehg_gw_init_state", "frehg_gw_set_state",
                  "frehg_gw_step", "frehg_gw_next_dt", "frehg_gw_get_field", "frehg_gw_restore",
-                 "frehg_gw_owned_volume"):
+                 "frehg_gw_owned_volume", "frehg_gw_attach_coupling", "frehg_gw_get_surface",
+                 "frehg_gw_set_surface", "frehg_gw_surface_ptr", "frehg_gw_coupled_audit_get"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -258,3 +267,38 @@ class RichardsSolver:
 
     def kernelLaunches(self) -> int:
         return int(self.lib.frehg_gw_kernel_launches(self.h))
+
+    # -- coupled top (RichardsSolver::attachCoupling, RichardsSolver.hpp:132-186) --
+    def attachCoupling(self, min_depth: float, vent_all: bool = False, book_bounce: bool = False,
+                       device_fields: Optional[dict] = None) -> None:
+        """Switches the coupled top on.  The surface fields live on the
+        device, (ny+2, nx+2) each, elevations in the mesh's offset frame;
+        ``device_fields`` maps names of :data:`frehg_b200.abi.SURF` to device
+        addresses the caller owns, the others are allocated (zeroed)."""
+        c = Coupling(float(min_depth), int(bool(vent_all)), int(bool(book_bounce)))
+        for name, ptr in (device_fields or {}).items():
+            c.field[SURF[name]] = int(ptr)
+        _check(self.lib, self.lib.frehg_gw_attach_coupling(self.h, C.byref(c)))
+
+    def surface(self, name: str) -> np.ndarray:
+        out = np.empty((self.ny + 2, self.nx + 2))
+        _check(self.lib, self.lib.frehg_gw_get_surface(self.h, SURF[name], out.ctypes.data_as(_dp)))
+        return out
+
+    def setSurface(self, name: str, value) -> None:
+        v = np.ascontiguousarray(np.broadcast_to(value, (self.ny + 2, self.nx + 2)), np.float64)
+        _check(self.lib, self.lib.frehg_gw_set_surface(self.h, SURF[name], v.ctypes.data_as(_dp)))
+
+    def surfacePointer(self, name: str) -> int:
+        p = C.c_void_p()
+        _check(self.lib, self.lib.frehg_gw_surface_ptr(self.h, SURF[name], C.byref(p)))
+        return p.value
+
+    def couplingAudit(self) -> dict:
+        """The GwStepAudit cpl* terms of the last step and pcClampVolume."""
+        a = CoupledAudit()
+        _check(self.lib, self.lib.frehg_gw_coupled_audit_get(self.h, C.byref(a)))
+        return a.as_dict()
+
+    def elevationOffset(self) -> float:
+        return float(self.lib.frehg_gw_elevation_offset(self.h))

@@ -72,6 +72,8 @@ def load():
     lib.oracle_gw_coupler_step.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp,
                                            C.POINTER(WindowAudit)]
     lib.oracle_gw_coupler_state.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp]
+    lib.oracle_gw_bath.argtypes = [C.c_void_p, _dp]
+    lib.oracle_gw_coupler_restore.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
     _lib = lib
     return lib
 
@@ -200,6 +202,15 @@ class OracleSolver:
         v = [C.c_double(), C.c_double(), C.c_double()]
         self.lib.oracle_gw_coupler_state(self.h, t, *[C.byref(x) for x in v])
         return tuple(x.value for x in v)
+
+    def coupler_restore(self, t: float, dtg: float, lag: float) -> None:
+        self.lib.oracle_gw_coupler_restore(self.h, t, dtg, lag)
+
+    def bath_halo(self) -> np.ndarray:
+        """The mesh bed, offset frame, (ny+2, nx+2) with the mirrored halo."""
+        out = np.empty((self.ny + 2, self.nx + 2))
+        self.lib.oracle_gw_bath(self.h, out.ctypes.data_as(_dp))
+        return out
 
     def _check(self, rc: int) -> None:
         if rc != 0:

@@ -1872,3 +1872,14 @@ void oracle_gw_coupler_state(const oracle_gw* s, double t, double* next_dt, doub
   if (dtg) *dtg = s->cdtg;
   if (lag) *lag = s->csync ? 0.0 : (t - s->ctsub);
 }
+
+/* The mesh bed (TerrainMetric bath), offset frame, (ny+2)(nx+2) with the
+ * mirrored halo. */
+void oracle_gw_bath(const oracle_gw* s, double* out) { memcpy(out, s->bath, s->n2 * sizeof(double)); }
+
+/* Coupler::restore (Coupler.hpp:98-100): the adaptive subsurface dt and the
+ * subsurface clock t - lag. */
+void oracle_gw_coupler_restore(oracle_gw* s, double t, double dtg, double lag) {
+  s->cdtg = dtg;
+  s->ctsub = t - lag;
+}

@@ -52,6 +52,9 @@ int oracle_gw_coupler_step(oracle_gw* s, double t, double dt, const double* bott
                            frehg_gw_window_audit* out);
 void oracle_gw_coupler_state(const oracle_gw* s, double t, double* next_dt, double* dtg,
                              double* lag);
+void oracle_gw_coupler_restore(oracle_gw* s, double t, double dtg, double lag);
+/* The mesh bed, offset frame, (ny+2)*(nx+2) with the mirrored halo. */
+void oracle_gw_bath(const oracle_gw* s, double* out);
 
 /* Pointwise closures (src/gw/VanGenuchten.hpp:45-128), exported for the
  * golden-value tests. */
