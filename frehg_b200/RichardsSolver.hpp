@@ -12,6 +12,7 @@
 // copies them in (INTEGRATION.md shows the wiring).
 #pragma once
 
+#include <array>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -126,6 +127,24 @@ class RichardsSolver {
   long long activeCells() const { return frehg_gw_active_cells(h_); }
   frehg_gw_handle* handle() const { return h_; }
 
+  /// RichardsSolver::attachCoupling (RichardsSolver.hpp:180-186): the
+  /// GwCoupling views as device arrays ((ny+2)*(nx+2) each; null entries are
+  /// allocated by the library).
+  void attachCoupling(const frehg_gw_coupling& c) { check(frehg_gw_attach_coupling(h_, &c)); }
+  /// Host copy of a coupled surface field (FREHG_GW_SURF_*).
+  std::vector<double> surface(int which) const {
+    std::vector<double> out(static_cast<size_t>(ny_ + 2) * static_cast<size_t>(nx_ + 2));
+    check(frehg_gw_get_surface(h_, which, out.data()));
+    return out;
+  }
+  void setSurface(int which, const double* host) { check(frehg_gw_set_surface(h_, which, host)); }
+  /// The GwStepAudit cpl* terms of the last step and pcClampVolume.
+  frehg_gw_coupled_audit couplingAudit() const {
+    frehg_gw_coupled_audit a{};
+    check(frehg_gw_coupled_audit_get(h_, &a));
+    return a;
+  }
+
  private:
   static void check(int rc) {
     if (rc != FREHG_GW_OK) throw FatalError(rc, frehg_gw_last_error());
@@ -140,6 +159,44 @@ class RichardsSolver {
   int nx_, ny_, nz_;
   GwStepAudit audit_;
   SolveStats last_;
+};
+
+/// coupling::Coupler (src/coupling/Coupler.hpp) for one coupled solver: the
+/// subsurface side of the coupled step.  The caller's surface solve (its
+/// free-surface phase and depth refresh) runs before step(t, dt), on the
+/// solver's surface fields; its velocity phase after.
+class Coupler {
+ public:
+  Coupler(RichardsSolver& gw, bool sync, double dt, double dtInit, double tStart = 0.0)
+      : gw_(gw) {
+    const frehg_gw_coupler_opts o{sync ? 1 : 0, dt, dtInit, tStart};
+    check(frehg_gw_coupler_init(gw_.handle(), &o));
+  }
+  /// Coupler::step(t, dt): open the window, take the sync step or the
+  /// subcycled steps that fit, apply the seepage, reduce the audit.
+  void step(double t, double dt) { check(frehg_gw_coupler_step(gw_.handle(), t, dt, &audit_)); }
+  double nextDt() const { return state(0.0)[0]; }
+  double currentDtg() const { return state(0.0)[1]; }
+  double gwLag(double t) const { return state(t)[2]; }
+  void restore(double t, double dtg, double lag) {
+    check(frehg_gw_coupler_restore(gw_.handle(), t, dtg, lag));
+  }
+  const frehg_gw_window_audit& audit() const { return audit_; }
+  std::vector<double> seepageRate() const { return gw_.surface(FREHG_GW_SURF_QSS); }
+  std::vector<double> gain() const { return gw_.surface(FREHG_GW_SURF_GAIN); }
+  std::vector<double> seepAccum() const { return gw_.surface(FREHG_GW_SURF_SEEP_ACCUM); }
+
+ private:
+  static void check(int rc) {
+    if (rc != FREHG_GW_OK) throw FatalError(rc, frehg_gw_last_error());
+  }
+  std::array<double, 3> state(double t) const {
+    std::array<double, 3> v{};
+    check(frehg_gw_coupler_state(gw_.handle(), t, &v[0], &v[1], &v[2]));
+    return v;
+  }
+  RichardsSolver& gw_;
+  frehg_gw_window_audit audit_{};
 };
 
 }  // namespace frehg_b200

@@ -66,6 +66,58 @@ int main() {
       if (!(std::fabs(resid) <= 1e-12 * std::fmax(v, 1.0))) return 2;
       prev = v;
     }
+    // The coupled top under the Coupler mirror: a 2 cm pond over the box,
+    // sync windows of 5 s, the surface a stand-in without lateral flow (its
+    // depth refreshed from eta before each window).  The coupled budget
+    // closes: d(V_gw + V_surface + held seepage) = the external boundary
+    // inflow + bounce - evaporation - Ss storage + reallocation - clamp loss
+    // + the infiltration the bed clamp could not take from the surface.
+    std::vector<int> flux_top(ncol, FREHG_GW_BC_FLUX);
+    d.top_code = flux_top.data();
+    frehg_b200::RichardsSolver cg(d, FREHG_GW_IC_HEAD, -1.0);
+    frehg_gw_coupling c{};
+    c.min_depth = 1e-3;
+    cg.attachCoupling(c);
+    const size_t n2 = static_cast<size_t>(nx + 2) * (ny + 2);
+    const double off = frehg_gw_elevation_offset(cg.handle());
+    std::vector<double> bottom(n2, off), eta(n2, off + 0.02), dep(n2, 0.02);
+    cg.setSurface(FREHG_GW_SURF_BOTTOM, bottom.data());
+    cg.setSurface(FREHG_GW_SURF_ETA, eta.data());
+    frehg_b200::Coupler cp(cg, true, 5.0, 5.0);
+    auto surface_volume = [&](const std::vector<double>& e, const std::vector<double>& acc) {
+      double v = 0.0;
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+          const size_t k = static_cast<size_t>(j) * (nx + 2) + i;
+          v += (e[k] - bottom[k]) + acc[k];
+        }
+      return v * d.dx * d.dy;
+    };
+    double total = cg.ownedVolume() + surface_volume(eta, cg.surface(FREHG_GW_SURF_SEEP_ACCUM));
+    double tc = 0.0;
+    for (int w = 0; w < 6; ++w) {
+      const double dt = cp.nextDt();
+      tc += dt;
+      eta = cg.surface(FREHG_GW_SURF_ETA);
+      for (size_t k = 0; k < n2; ++k) {
+        const double dd = eta[k] - bottom[k];
+        dep[k] = dd <= c.min_depth ? 0.0 : dd;
+      }
+      cg.setSurface(FREHG_GW_SURF_DEPTH, dep.data());
+      cp.step(tc, dt);
+      const auto& a = cp.audit();
+      const double now = cg.ownedVolume() + surface_volume(cg.surface(FREHG_GW_SURF_ETA),
+                                                           cg.surface(FREHG_GW_SURF_SEEP_ACCUM));
+      const double src = (a.gw.boundary_in + a.cpl.exchanged + a.cpl.vent) + a.cpl.bounce -
+                         a.cpl.evap - a.gw.ss_storage + a.gw.realloc_adjust - a.gw.vloss +
+                         a.discarded;
+      const double resid = (now - total) - src;
+      std::printf("window %d dt %.4g substeps %ld exchanged %.4e applied %.4e residual %.3e\n", w,
+                  dt, a.substeps, a.cpl.exchanged, a.applied, resid);
+      if (!(std::fabs(resid) <= 1e-12 * std::fmax(now, 1.0))) return 3;
+      if (!(a.cpl.exchanged < 0.0)) return 4;  // the pond infiltrates
+      total = now;
+    }
   } catch (const frehg_b200::FatalError& e) {
     std::fprintf(stderr, "FatalError(%d): %s\n", e.status(), e.what());
     return 1;

@@ -188,3 +188,46 @@ def test_batch_refuses_coupled_members():
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("sync", [True, False])
+def test_coupled_budget_closes(sync):
+    # The coupled closure (Coupler.hpp:51-57) with the stand-in surface's
+    # rain as the surface source: d(V_gw + V_surface + held seepage) = rain +
+    # the external boundary inflow (boundary_in + exchanged + vent) + bounce
+    # - evaporation - Ss storage + reallocation - clamp loss + the
+    # infiltration remainder the bed clamp kept from the surface.
+    cfg = cases.coupled_box("consistent")
+    g = RichardsSolver(copy.deepcopy(cfg))
+    o = OracleSolver(copy.deepcopy(cfg))
+    try:
+        g.attachCoupling(MIN_DEPTH)
+        cp = Coupler(g, sync, 5.0, 2.0)
+        bath = o.bath_halo()
+        eta, rain = cases.coupled_surface(bath)
+        g.setSurface("eta", eta)
+        g.setSurface("bottom", bath)
+
+        def surface_volume():
+            e, a = g.surface("eta"), g.surface("seep_accum")
+            return float(np.sum((e - bath)[1:-1, 1:-1]) + np.sum(a[1:-1, 1:-1]))
+
+        total = g.ownedVolume() + surface_volume()
+        t = 0.0
+        for n in range(10):
+            dt = cp.nextDt()
+            t += dt
+            e = g.surface("eta") + rain * dt
+            g.setSurface("eta", e)
+            g.setSurface("dept", refresh_depth(e, bath))
+            total += float(np.sum((rain * dt)[1:-1, 1:-1]))
+            a = cp.step(t, dt)
+            now = g.ownedVolume() + surface_volume()
+            src = ((a["gw"]["boundary_in"] + a["cpl"]["exchanged"] + a["cpl"]["vent"]) +
+                   a["cpl"]["bounce"] - a["cpl"]["evap"] - a["gw"]["ss_storage"] +
+                   a["gw"]["realloc_adjust"] - a["gw"]["vloss"] + a["discarded"])
+            assert abs((now - total) - src) <= 1e-12 * max(now, 1.0), (n, now - total, src)
+            total = now
+    finally:
+        g.close()
+        o.close()
