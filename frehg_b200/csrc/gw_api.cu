@@ -269,7 +269,7 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     hnd->atol = desc->atol;
     hnd->maxit = desc->max_iterations;
     hnd->precision = desc->precision;
-    hnd->outer_rtol = desc->outer_rtol > 0 ? desc->outer_rtol : 1e-10;
+    hnd->outer_rtol = desc->outer_rtol > 0 ? desc->outer_rtol : 1e-11;
     hnd->max_outer = desc->max_outer > 0 ? desc->max_outer : 30;
     hnd->dt_min = desc->dt_min;
     hnd->dt_max = desc->dt_max;
@@ -434,7 +434,7 @@ cudaError_t enqueue_predictor(frehg_gw_handle* h) {
   fgw::launch_ghosts(D, hn, wcn);
   if (D.f.cpl) fgw::launch_cpl_mode(D, hn);
   fgw::launch_closure_pred(D, hn);
-  fgw::launch_assemble(D, hn, wcn);
+  fgw::launch_assemble(D, hn, wcn, h->precision == FREHG_GW_PRECISION_MIXED);
   if (h->precision == FREHG_GW_PRECISION_MIXED) return fgw::launch_line_factor(D);
   return cudaGetLastError();
 }

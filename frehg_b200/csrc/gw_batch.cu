@@ -89,10 +89,9 @@ int solve_blocks_per_sm(const SolveClass& c, size_t smem) {
 }
 
 int solve_max_blocks(const Device& D, const SolveClass& c) {
-  (void)c;
   // The member's reduction buffer holds 4 max(cg_grid, cg_grid32) doubles;
-  // a solve on G blocks uses 3 G of them.
-  const int cap = (4 * std::max(D.cg_grid, D.cg_grid32)) / 3;
+  // a solve on G blocks uses 3 G of them (FP64) or 4 G (mixed).
+  const int cap = (4 * std::max(D.cg_grid, D.cg_grid32)) / (c.kind == 1 ? 4 : 3);
   return std::max(1, cap);
 }
 

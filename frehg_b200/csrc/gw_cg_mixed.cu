@@ -1,10 +1,13 @@
 // Mixed-precision predictor solve: FP32 inner preconditioned CG inside FP64
 // defect correction on the true residual.
 //
-//   x = 0
+//   x = h^n (the step-start head, written by the assembly; PETSc's x = 0
+//            stays with the FP64 form, whose iteration counts are the
+//            reference's)
 //   repeat (outer sweep o = 0, 1, ...):
 //     x <- x + d;  r = b - A x  in FP64 with the FP64 coefficients
-//     stop when ||r||_2 <= outer_rtol ||b||_2
+//     stop when ||r||_2 <= outer_rtol ||b||_2 (after at least one
+//     correction: h^n passing the test is not accurate enough)
 //     solve A d = r approximately in FP32: CG preconditioned by the exact
 //     solve of each column's vertical tridiagonal block (line Jacobi along
 //     k), stopped at inner_rtol of the initial preconditioned norm
@@ -116,11 +119,12 @@ struct MixedArgs {
   double *x0, *x1;
   const float *diag32, *gxp32, *gyp32, *gzp32, *dinv32, *l32;
   float *r32, *z32, *p0, *p1, *w32, *d32;
-  double* part;  // 3 x G
+  double* part;  // 4 x G
   CgState* st;
   double outer_rtol, inner_rtol, atol;
   int max_inner, max_outer, max_total;
   int tc;
+  int warm;  // x0 holds the starting iterate (h^n, written by the assembly)
 };
 
 // Forward/backward LDL^T sweeps of one column: z = T^-1 r.  r and z live in
@@ -388,10 +392,23 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
   double* const q0 = a.part;
   double* const q1 = a.part + G;
   double* const q2 = a.part + 2 * G;
+  double* const q3 = a.part + 3 * G;
 
+  // A warm start begins from the assembly's x0 = h^n; the outer test is
+  // relative to ||b||, reduced here since the first residual is no longer b.
+  double bb = 0.0;
   for (long long c = t0; c < N; c += stride) {
-    a.x0[c] = 0.0;
+    if (a.warm) {
+      const double bv = a.b[c];
+      bb += bv * bv;
+    } else {
+      a.x0[c] = 0.0;
+    }
     a.d32[c] = 0.0f;
+  }
+  if (a.warm) {
+    const double s0 = block_sum_all(bb);
+    if (threadIdx.x == 0) q3[bid] = s0;
   }
   if (!grid_sync(a.st, G)) return;
 
@@ -489,12 +506,14 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
     const double zn0 = sqrt(reduce_partials(q1, G));
     double beta = reduce_partials(q2, G);
     final_buf = (o & 1) ? 0 : 1;
-    if (o == 0) bnorm = rnorm;
+    if (o == 0) bnorm = a.warm ? sqrt(reduce_partials(q3, G)) : rnorm;
     if (!isfinite(rnorm)) {
       reason = -9;
       break;
     }
-    if (rnorm <= fmax(a.outer_rtol * bnorm, a.atol)) {
+    // A warm start always takes one correction, so that h^n itself, which
+    // can meet the residual test, is never returned unrefined.
+    if ((o > 0 || !a.warm) && rnorm <= fmax(a.outer_rtol * bnorm, a.atol)) {
       reason = (rnorm < a.atol) ? 3 : 2;
       break;
     }
@@ -505,7 +524,10 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
     ++outer;
     for (long long c = t0; c < N; c += stride) a.d32[c] = 0.0f;
     // Inner FP32 PCG on A d = r32.
-    const double itol = a.inner_rtol * zn0;
+    // Each inner solve reduces its start by inner_rtol, the last one only as
+    // far as the outer target needs (with a factor 2 of margin).
+    const double need = (rnorm > 0.0) ? 0.5 * a.outer_rtol * bnorm / rnorm : a.inner_rtol;
+    const double itol = fmax(a.inner_rtol, need) * zn0;
     double betaold = 1.0;
     for (int i = 0; i < a.max_inner && total < a.max_total; ++i) {
       if (beta == 0.0 || (i > 0 && beta * betaold <= 0.0)) break;
@@ -709,6 +731,7 @@ MixedArgs make_mixed_args(const Device& D, double atol, int maxit, double outer_
   a.max_outer = max_outer;
   a.max_total = maxit;
   a.tc = tc;
+  a.warm = 1;
   return a;
 }
 

@@ -18,7 +18,7 @@ struct frehg_gw_handle {
   std::vector<int> codes;      // host copy, 6 x ncol
   std::vector<double> values;  // host staging, 6 x ncol
   bool values_pinned = false;  // staging page-locked with cudaHostRegister
-  double rtol = 1e-8, atol = 1e-14, outer_rtol = 1e-10;
+  double rtol = 1e-8, atol = 1e-14, outer_rtol = 1e-11;
   int maxit = 1000, max_outer = 30, precision = 0;
   double dt_min = 0, dt_max = 0, dq_grow = 0.01, dq_shrink = 0.02, co_max = 2.0;
   double next_dt = 0.0;

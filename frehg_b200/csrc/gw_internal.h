@@ -104,7 +104,7 @@ struct Device {
   double* xalt = nullptr;  // FP64 ping-pong partner of x (mixed outer sweeps)
   // reductions
   double* partial = nullptr;   // kPSlots x nblk
-  double* cgpart = nullptr;    // 3 x cg grid
+  double* cgpart = nullptr;    // 4 x cg grid
   int nblk = 0;                // grid of the reducing cell kernels
   int cg_grid = 0;             // co-resident grid of the CG kernel
   int cg_grid32 = 0;
@@ -123,7 +123,8 @@ struct Device {
 // ---------------------------------------------------------------- launchers
 void launch_ghosts(const Device& D, double* h, double* wc);
 void launch_closure_pred(const Device& D, const double* h);
-void launch_assemble(const Device& D, const double* hn, const double* wcn);
+// warm: also write the mixed solve's starting iterate x = h^n (active cells).
+void launch_assemble(const Device& D, const double* hn, const double* wcn, bool warm);
 void launch_closure_corr(const Device& D, const double* hn);
 void launch_flux(const Device& D, const double* wcn);
 void launch_update_wc(const Device& D, const double* hn, const double* wcn);

@@ -228,14 +228,18 @@ __device__ __forceinline__ void assemble_body(
     const double* __restrict__ kzff, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ ch, const double* __restrict__ dtgp,
     double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
-    double* __restrict__ gzps, double* __restrict__ rhs, const int bid, const int G) {
+    double* __restrict__ gzps, double* __restrict__ rhs, double* __restrict__ xw, const int bid,
+    const int G) {
   const double dx = d.dx, dy = d.dy;
   const double dtg = *dtgp;
   for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
-    if (j < 1 || j > d.ny || i < 1 || i > d.nx) continue;
+    if (j < 1 || j > d.ny || i < 1 || i > d.nx) {
+      if (xw) xw[c] = 0.0;
+      continue;
+    }
     const long long cw = c - d.sx, ce = c + d.sx, cs = c - d.sy, cn = c + d.sy;
     const long long cu = (k >= 1) ? c - 1 : c, cl = (k + 1 < d.nz) ? c + 1 : c;
     const long long col = col2(d, j, i);
@@ -269,6 +273,7 @@ __device__ __forceinline__ void assemble_body(
       sinyc = f.siny[c];
       sinys = f.siny[cs];
     }
+    if (xw) xw[c] = ac ? hnc : 0.0;  // the mixed solve's starting iterate
     if (!ac) {
       diag[c] = 1.0;
       gxps[c] = 0.0;
@@ -381,9 +386,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_assemble(
     const double* __restrict__ kzff, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ ch, const double* __restrict__ dtgp,
     double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
-    double* __restrict__ gzps, double* __restrict__ rhs) {
-  assemble_body<CPL>(d, f, kxf, kyf, kzff, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs, blockIdx.x,
-                gridDim.x);
+    double* __restrict__ gzps, double* __restrict__ rhs, double* __restrict__ xw) {
+  assemble_body<CPL>(d, f, kxf, kyf, kzff, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs, xw,
+                     blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- predictor faces
@@ -1723,7 +1728,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_assemble_batch(const StepArgs* ta
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
   assemble_body<false>(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp,
-                sa.gyp, sa.gzp, sa.rhs, bid, G);
+                sa.gyp, sa.gzp, sa.rhs, sa.mixed ? sa.x : nullptr, bid, G);
 }
 
 __global__ void __launch_bounds__(kBlock, 4) k_faces_batch(const StepArgs* tab, const int* first,
@@ -1854,14 +1859,14 @@ void launch_closure_pred(const Device& D, const double* h) {
 }
 
 // The predictor's faces go through D.kx, D.ky, D.kzf (free until k_flux).
-void launch_assemble(const Device& D, const double* hn, const double* wcn) {
+void launch_assemble(const Device& D, const double* hn, const double* wcn, bool warm) {
   const PassK pk{D.kcx, D.kcy, D.kcz, wcn};
   const auto faces = (D.f.cpl != nullptr) ? k_faces<true> : k_faces<false>;
   const auto assemble = (D.f.cpl != nullptr) ? k_assemble<true> : k_assemble<false>;
   faces<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.kx, D.ky, D.kzf);
   assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.kx, D.ky, D.kzf, hn, wcn, D.ch,
                                                      dtg_slot(D), D.diag, D.gxp, D.gyp, D.gzp,
-                                                     D.rhs);
+                                                     D.rhs, warm ? D.x : nullptr);
   D.launches += 2;
 }
 

@@ -260,7 +260,7 @@ size_t frehg_gw_device_bytes(const frehg_gw_desc* d) {
   if (d->precision == FREHG_GW_PRECISION_MIXED) b += 12 * r(4 * ns) + r(8 * ns);
   const size_t nblk = std::min<size_t>((n3 + 255) / 256, 512 * 8);
   const size_t cg = std::max<size_t>((n3 + 255) / 256, 512 * 4);
-  b += r(8 * 9 * nblk) + r(8 * 4 * cg) + r(112);
+  b += r(8 * fgw::kPSlots * nblk) + r(8 * 4 * cg) + r(sizeof(fgw::StepOut));
   const size_t page = 2u << 20;
   return (b + page - 1) / page * page;
 }

@@ -138,7 +138,8 @@ typedef struct frehg_gw_desc {
   double rtol, atol;
   int max_iterations;
   int precision;      /* FREHG_GW_PRECISION_* */
-  double outer_rtol;  /* mixed: ||b - A x|| / ||b|| target of the FP64 outer loop */
+  double outer_rtol;  /* mixed: ||b - A x|| / ||b|| target of the FP64 outer loop
+                         (0 = 1e-11) */
   int max_outer;      /* mixed: outer-iteration cap */
 } frehg_gw_desc;
 

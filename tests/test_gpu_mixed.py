@@ -1,5 +1,5 @@
 """The mixed-precision form: FP32 inner line-preconditioned CG inside FP64
-defect correction (true residual <= 1e-10 ||b||).
+defect correction (true residual <= 1e-11 ||b||), started from h^n.
 
 Its reference is the FP64 oracle solved tightly (Jacobi CG, rtol 1e-13) from
 the same state each step: the default oracle stops its CG at a
@@ -49,7 +49,8 @@ def run(cfg, steps):
             t += dtg
             info = gpu.step(t, dtg)
             cpu.step(t, dtg)
-            assert info["outer_iterations"] >= 1
+            # Started from h^n, the solve still takes at least one correction.
+            assert info["outer_iterations"] >= 1 and info["status"] == 0
             err = rel_linf(gpu.field("h"), cpu.field("h"))
             worst = max(worst, err)
             assert err <= H_TOL, f"step {n}: head error {err:.3e} vs the tight FP64 solve"
