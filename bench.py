@@ -39,16 +39,17 @@ ALG_BYTES_MIXED_INNER = 68    # FP32 inner iteration: stencil pass 8 words, upda
 ALG_BYTES_MIXED_SWEEP = 80    # FP64 outer residual sweep: x, b, 4 coefficients, d, l,
                               # dinv in; x, r, z, p out
 ALG_BYTES_MIXED_OUTER = 4     # d reset after each outer sweep that continues
-ALG_BYTES_MIXED_INIT = 12     # x = 0, d = 0 at entry
+ALG_BYTES_MIXED_INIT = 12     # b read for ||b||, d = 0 at entry (the assembly writes
+                              # the starting iterate x = h^n)
 ALG_BYTES_FIXED = 536         # FP64 step outside the solve
 METRIC = "cell-steps/s at 512x512x128"
 # DRAM bytes (read + write) per algorithmic byte of k_cg_mixed, from the ncu
 # capture summarised in profiles/ (256x256x128 slab, one steady-state launch);
 # scaled to the timed launches by their algorithmic bytes.
-MIXED_TRAFFIC_PER_ALG_BYTE = 1.029
+MIXED_TRAFFIC_PER_ALG_BYTE = 1.032
 # Bytes frehg_gw_step reads back per step: the device step record (nine FP64
-# audit and controller terms and the solver's exit state).
-STEP_RECORD_BYTES = 112
+# audit and controller terms, the solver's exit state, the coupled-top books).
+STEP_RECORD_BYTES = 192
 
 
 def mixed_alg_bytes(cells, inner, outer, launches):
