@@ -47,7 +47,8 @@ namespace {
 constexpr int kFactorBlock = 256;
 constexpr int kTileCells = 4096;  // tc * nz <= kTileCells (2 x 16 KB of FP32 staging)
 
-// Cast the FP64 coefficients to FP32 and factor every column's tridiagonal
+// Deep columns (nz > 256; shallower ones take line_factor_warp_body below):
+// cast the FP64 coefficients to FP32 and factor every column's tridiagonal
 // block T = LDL^T (pivots in FP64, stored as FP32 1/d_k and l_k).
 __device__ __forceinline__ void line_factor_body(Dims d, const double* __restrict__ diag,
                                                               const double* __restrict__ gxp,
@@ -111,6 +112,122 @@ __global__ void __launch_bounds__(kFactorBlock) k_line_factor(Dims d, const doub
                                                               float* gyp32, float* gzp32,
                                                               float* dinv32, float* l32, int tc) {
   line_factor_body(d, diag, gxp, gyp, gzp, diag32, gxp32, gyp32, gzp32, dinv32, l32, tc, blockIdx.x, gridDim.x);
+}
+
+// The same factorization with one warp per column (nz <= 256): lane `lane`
+// holds the E consecutive cells k = lane * E + e.  The pivot recurrence
+// d_k = a_k - e_{k-1}^2 / d_{k-1} (a = diag, e = gzp) is the Moebius map of the
+// matrix M_k = [[a_k, -e_{k-1}^2], [1, 0]] acting on (numerator, denominator),
+// d_k = n_k / m_k with (n_k, m_k) the first column of M_k ... M_0.  A lane
+// composes its E matrices, a Hillis-Steele warp scan composes the lanes', and
+// each lane replays its cells from its exclusive prefix.  Products are
+// rescaled by their largest entry at every step (the map is projective), so
+// nothing overflows; the arithmetic is FP64 throughout.  l_k = e_k / d_k as in
+// the serial sweep; the FP32 casts of the four coefficients ride along.
+struct M2 {
+  double a, b, c, d;  // [[a, b], [c, d]]
+};
+
+__device__ inline M2 m2_mul(const M2& x, const M2& y) {  // x * y, rescaled
+  M2 r{x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c,
+       x.c * y.b + x.d * y.d};
+  const double s = fmax(fmax(fabs(r.a), fabs(r.b)), fmax(fabs(r.c), fabs(r.d)));
+  if (s > 0.0 && isfinite(s)) {
+    const double is = 1.0 / s;
+    r.a *= is;
+    r.b *= is;
+    r.c *= is;
+    r.d *= is;
+  }
+  return r;
+}
+
+__device__ inline M2 m2_shfl_up(const M2& x, int off) {
+  return M2{__shfl_up_sync(0xffffffffu, x.a, off), __shfl_up_sync(0xffffffffu, x.b, off),
+            __shfl_up_sync(0xffffffffu, x.c, off), __shfl_up_sync(0xffffffffu, x.d, off)};
+}
+
+template <int E>
+__device__ __forceinline__ void line_factor_warp_body(
+    Dims d, const double* __restrict__ diag, const double* __restrict__ gxp,
+    const double* __restrict__ gyp, const double* __restrict__ gzp, float* __restrict__ diag32,
+    float* __restrict__ gxp32, float* __restrict__ gyp32, float* __restrict__ gzp32,
+    float* __restrict__ dinv32, float* __restrict__ l32, const int bid, const int G) {
+  const int lane = threadIdx.x & 31, nz = d.nz, k0 = lane * E;
+  const long long nw = static_cast<long long>(G) * (blockDim.x >> 5);
+  for (long long col = static_cast<long long>(bid) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       col < d.ncol; col += nw) {
+    const long long cb = col * nz;
+    double av[E], ev[E], xv[E], yv[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int k = k0 + e;
+      av[e] = 1.0;
+      ev[e] = xv[e] = yv[e] = 0.0;
+      if (k < nz) {
+        av[e] = diag[cb + k];
+        ev[e] = gzp[cb + k];
+        xv[e] = gxp[cb + k];
+        yv[e] = gyp[cb + k];
+      }
+    }
+    const double eprev_lane = __shfl_up_sync(0xffffffffu, ev[E - 1], 1);  // e_{k0-1}
+    // This lane's maps, composed (later cells on the left).
+    M2 L{1.0, 0.0, 0.0, 1.0};
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int k = k0 + e;
+      if (k < nz) {
+        const double ep = (k == 0) ? 0.0 : (e == 0 ? eprev_lane : ev[e - 1]);
+        L = m2_mul(M2{av[e], -ep * ep, 1.0, 0.0}, L);
+      }
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const M2 q = m2_shfl_up(L, off);
+      if (lane >= off) L = m2_mul(L, q);
+    }
+    M2 X = m2_shfl_up(L, 1);
+    if (lane == 0) X = M2{1.0, 0.0, 0.0, 1.0};
+    double n = X.a, m = X.c;  // (numerator, denominator) of d_{k0-1}
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int k = k0 + e;
+      if (k >= nz) break;
+      const long long c = cb + k;
+      const double ep = (k == 0) ? 0.0 : (e == 0 ? eprev_lane : ev[e - 1]);
+      const double n2 = av[e] * n - ep * ep * m;
+      m = n;
+      n = n2;
+      const double s = fmax(fabs(n), fabs(m));
+      if (s > 0.0 && isfinite(s)) {
+        n /= s;
+        m /= s;
+      }
+      const double dk = n / m;
+      diag32[c] = static_cast<float>(av[e]);
+      gxp32[c] = static_cast<float>(xv[e]);
+      gyp32[c] = static_cast<float>(yv[e]);
+      gzp32[c] = static_cast<float>(ev[e]);
+      dinv32[c] = (dk > 0.0 && isfinite(dk)) ? static_cast<float>(1.0 / dk)
+                                             : static_cast<float>(1.0 / av[e]);
+      l32[c] = (k + 1 < nz) ? static_cast<float>(ev[e] / dk) : 0.0f;
+    }
+  }
+}
+
+template <int E>
+__global__ void __launch_bounds__(kFactorBlock) k_line_factor_warp(
+    Dims d, const double* __restrict__ diag, const double* __restrict__ gxp,
+    const double* __restrict__ gyp, const double* __restrict__ gzp, float* diag32, float* gxp32,
+    float* gyp32, float* gzp32, float* dinv32, float* l32) {
+  line_factor_warp_body<E>(d, diag, gxp, gyp, gzp, diag32, gxp32, gyp32, gzp32, dinv32, l32,
+                           blockIdx.x, gridDim.x);
+}
+
+// Cells per lane of the warp factorization (0: the tiled path, nz > 256).
+__host__ __device__ inline int factor_lane_cells(int nz) {
+  return nz <= 32 ? 1 : nz <= 64 ? 2 : nz <= 128 ? 4 : nz <= 256 ? 8 : 0;
 }
 
 struct MixedArgs {
@@ -696,7 +813,9 @@ int host_tile_cols(int nz) {
 }
 
 size_t mixed_smem(int nz) { return 2 * sizeof(float) * host_tile_cols(nz) * (nz + 1); }
-size_t factor_smem(int nz) { return 2 * sizeof(double) * host_tile_cols(nz) * (nz + 1); }
+size_t factor_smem(int nz) {
+  return factor_lane_cells(nz) ? 0 : 2 * sizeof(double) * host_tile_cols(nz) * (nz + 1);
+}
 
 MixedArgs make_mixed_args(const Device& D, double atol, int maxit, double outer_rtol,
                           int max_outer) {
@@ -744,6 +863,16 @@ int cg32_grid(int sm_count, long long ncell) {
 
 cudaError_t launch_line_factor(Device& D) {
   const int nz = D.d.nz;
+  const int fe = factor_lane_cells(nz);
+  if (fe) {
+    const int fgrid = line_factor_blocks(D);
+    auto k = fe == 1 ? k_line_factor_warp<1> : fe == 2 ? k_line_factor_warp<2>
+           : fe == 4 ? k_line_factor_warp<4> : k_line_factor_warp<8>;
+    k<<<fgrid, kFactorBlock, 0, D.stream>>>(D.d, D.diag, D.gxp, D.gyp, D.gzp, D.diag32, D.gxp32,
+                                            D.gyp32, D.gzp32, D.dinv32, D.l32);
+    ++D.launches;
+    return cudaGetLastError();
+  }
   const size_t fsm = factor_smem(nz);
   const cudaError_t ea = raise_smem_limit(reinterpret_cast<const void*>(k_line_factor), fsm);
   if (ea != cudaSuccess) return ea;
@@ -848,8 +977,27 @@ __global__ void __launch_bounds__(kFactorBlock) k_line_factor_batch(const StepAr
     dst[w] = src[w];
   const int bid = blockIdx.x - first[si], G = first[si + 1] - first[si];
   __syncthreads();
-  line_factor_body(sa.d, sa.diag, sa.gxp, sa.gyp, sa.gzp, sa.diag32, sa.gxp32, sa.gyp32,
-                   sa.gzp32, sa.dinv32, sa.l32, sa.tc, bid, G);
+  switch (factor_lane_cells(sa.d.nz)) {
+    case 1:
+      line_factor_warp_body<1>(sa.d, sa.diag, sa.gxp, sa.gyp, sa.gzp, sa.diag32, sa.gxp32,
+                               sa.gyp32, sa.gzp32, sa.dinv32, sa.l32, bid, G);
+      break;
+    case 2:
+      line_factor_warp_body<2>(sa.d, sa.diag, sa.gxp, sa.gyp, sa.gzp, sa.diag32, sa.gxp32,
+                               sa.gyp32, sa.gzp32, sa.dinv32, sa.l32, bid, G);
+      break;
+    case 4:
+      line_factor_warp_body<4>(sa.d, sa.diag, sa.gxp, sa.gyp, sa.gzp, sa.diag32, sa.gxp32,
+                               sa.gyp32, sa.gzp32, sa.dinv32, sa.l32, bid, G);
+      break;
+    case 8:
+      line_factor_warp_body<8>(sa.d, sa.diag, sa.gxp, sa.gyp, sa.gzp, sa.diag32, sa.gxp32,
+                               sa.gyp32, sa.gzp32, sa.dinv32, sa.l32, bid, G);
+      break;
+    default:
+      line_factor_body(sa.d, sa.diag, sa.gxp, sa.gyp, sa.gzp, sa.diag32, sa.gxp32, sa.gyp32,
+                       sa.gzp32, sa.dinv32, sa.l32, sa.tc, bid, G);
+  }
 }
 
 }  // namespace
@@ -857,6 +1005,10 @@ __global__ void __launch_bounds__(kFactorBlock) k_line_factor_batch(const StepAr
 int line_tile_cols(int nz) { return host_tile_cols(nz); }
 
 int line_factor_blocks(const Device& D) {
+  if (factor_lane_cells(D.d.nz)) {  // one warp per column, kFactorBlock / 32 per block
+    const long long per = kFactorBlock / 32;
+    return static_cast<int>(std::min<long long>((D.d.ncol + per - 1) / per, 16LL * D.sm_count));
+  }
   const int tc = host_tile_cols(D.d.nz);
   const long long ntiles = (D.d.ncol + tc - 1) / tc;
   return static_cast<int>(std::min<long long>(ntiles, 4LL * D.sm_count));

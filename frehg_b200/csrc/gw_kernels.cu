@@ -938,7 +938,7 @@ struct VentState {
 // What the upward walk could not place, dv > 0, leaves through the top of
 // column face `ll` of a coupled column: onto the surface when it is wet, the
 // amount exceeds min_depth or every vent deposits; else it is lost.
-__device__ inline void vent_top(const Dims& d, double dv, double dtg, double& qface,
+__device__ inline void vent_top(const Dims& d, double dv, double idtg, double& qface,
                                 VentState& v, double& lost) {
   const double dd = dv / d.az;
   if (v.vent_all || v.dept > 0.0 || dd > v.min_depth) {
@@ -947,7 +947,7 @@ __device__ inline void vent_top(const Dims& d, double dv, double dtg, double& qf
     v.dept += dd;
     v.avail += dd;
     v.gain += dd;
-    qface += dv / dtg;
+    qface += dv * idtg;
     v.vent += dv;
   } else {
     lost -= dv;
@@ -1022,7 +1022,7 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
         }
         if (dv > 0.0) {
           if (CPL) {
-            vent_top(d, dv, dtg, qzf[fb + ll], v, lost);
+            vent_top(d, dv, 1.0 / dtg, qzf[fb + ll], v, lost);
           } else if (topHead) {
             qzf[fb + ll] += dv / dtg;
           } else {
@@ -1121,15 +1121,18 @@ __device__ inline int bits_lowest(const unsigned* w, int lo, int hi) {
 
 // Deposit at cell m: take min(room, dv), add take / dtg to face `face` with
 // `plus` (true: +=, false: -=), and clear m's room bit once its room is used up.
-__device__ inline void walk_take(double& dv, int m, double* rs, double* ws, const double* vs,
-                                 double* qs, unsigned* rbits, int face, bool plus, double dtg) {
+// The divisions by the cell volume and by dtg are multiplications by their
+// reciprocals (ivs staged per column, idtg once per kernel): a walk runs on
+// one lane, and FP64 divisions were most of its issue slots.
+__device__ inline void walk_take(double& dv, int m, double* rs, double* ws, const double* ivs,
+                                 double* qs, unsigned* rbits, int face, bool plus, double idtg) {
   const double take = (rs[m] > dv) ? dv : rs[m];
-  ws[m] += take / vs[m];
+  ws[m] += take * ivs[m];
   rs[m] -= take;
   if (plus) {
-    qs[face] += take / dtg;
+    qs[face] += take * idtg;
   } else {
-    qs[face] -= take / dtg;
+    qs[face] -= take * idtg;
   }
   dv -= take;
   if (!(rs[m] > 0.0)) rbits[m >> 5] &= ~(1u << (m & 31));
@@ -1141,8 +1144,8 @@ __device__ inline void walk_take(double& dv, int m, double* rs, double* ws, cons
 // head top or back down; downward to the bottom; what finds no room is lost.
 template <bool CPL>
 __device__ inline void walk_cell(const Dims& d, int kk, double upv, double dnv, int nz, bool topHead,
-                                 double* rs, double* ws, const double* vs, double* qs,
-                                 unsigned* rbits, const unsigned* ibits, double dtg, double& lost,
+                                 double* rs, double* ws, const double* ivs, double* qs,
+                                 unsigned* rbits, const unsigned* ibits, double idtg, double& lost,
                                  VentState& v) {
   double dv = upv;
   if (dv > 0.0) {
@@ -1156,19 +1159,19 @@ __device__ inline void walk_cell(const Dims& d, int kk, double upv, double dnv, 
         ll = lim;
         break;
       }
-      walk_take(dv, m, rs, ws, vs, qs, rbits, m + 1, true, dtg);
+      walk_take(dv, m, rs, ws, ivs, qs, rbits, m + 1, true, idtg);
       ll = m;
     }
     if (dv > 0.0) {
       if (CPL) {
-        vent_top(d, dv, dtg, qs[ll], v, lost);
+        vent_top(d, dv, idtg, qs[ll], v, lost);
       } else if (topHead) {
-        qs[ll] += dv / dtg;
+        qs[ll] += dv * idtg;
       } else {
         while (dv > 0.0) {
           const int m = bits_lowest(rbits, ll + 1, nz - 1);
           if (m < 0) break;
-          walk_take(dv, m, rs, ws, vs, qs, rbits, m, false, dtg);
+          walk_take(dv, m, rs, ws, ivs, qs, rbits, m, false, idtg);
           ll = m;
         }
         lost -= dv;
@@ -1181,7 +1184,7 @@ __device__ inline void walk_cell(const Dims& d, int kk, double upv, double dnv, 
     while (dv > 0.0) {
       const int m = bits_lowest(rbits, ll + 1, nz - 1);
       if (m < 0) break;
-      walk_take(dv, m, rs, ws, vs, qs, rbits, m, false, dtg);
+      walk_take(dv, m, rs, ws, ivs, qs, rbits, m, false, idtg);
       ll = m;
     }
     lost -= dv;
@@ -1198,13 +1201,13 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
                                                  double* partial, int nblk, const int bid,
                                                  const int G) {
   extern __shared__ __align__(16) unsigned char walk_smem[];
-  const double dtg = *dtgp;
+  const double idtg = 1.0 / *dtgp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nz = d.nz, nw = walk_words(nz);
   double* rs = reinterpret_cast<double*>(walk_smem + warp * walk_warp_bytes(nz));
   double* ws = rs + nz;
-  double* vs = ws + nz;
-  double* qs = vs + nz;  // nz + 1 faces
+  double* ivs = ws + nz;  // 1 / cell volume
+  double* qs = ivs + nz;  // nz + 1 faces
   unsigned* rbits = reinterpret_cast<unsigned*>(qs + nz + 1);
   unsigned* ibits = rbits + nw;  // inactive cells
   double lost = 0.0;
@@ -1227,7 +1230,7 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
         r = room[base + k];
         rs[k] = r;
         ws[k] = wc[base + k];
-        vs[k] = d.az * f.dz[base + k];
+        ivs[k] = 1.0 / (d.az * f.dz[base + k]);
         inact = !f.act[base + k];
       }
       const unsigned rb = __ballot_sync(0xffffffffu, r > 0.0);
@@ -1255,7 +1258,8 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
         const double upv = __shfl_sync(0xffffffffu, su, b);
         const double dnv = __shfl_sync(0xffffffffu, sd, b);
         if (lane == 0)
-          walk_cell<CPL>(d, k0 + b, upv, dnv, nz, topHead, rs, ws, vs, qs, rbits, ibits, dtg, lost, v);
+          walk_cell<CPL>(d, k0 + b, upv, dnv, nz, topHead, rs, ws, ivs, qs, rbits, ibits, idtg, lost,
+                         v);
         __syncwarp();
       }
     }
