@@ -508,7 +508,9 @@ int frehg_gw_server_stats(const frehg_gw_server* s, frehg_gw_server_stats_t* st)
   auto* m = const_cast<frehg_gw_server*>(s);
   std::lock_guard<std::mutex> lk(m->mu);
   st->active = static_cast<int>(s->active.size() + s->ready.size());
-  st->queued = static_cast<int>(s->queue.size());
+  // As frehg_gw_server_tick counts them: waiting, being admitted or retired by
+  // the worker (a request in the worker's hands is in no container).
+  st->queued = static_cast<int>(s->queue.size() + s->retiring.size()) + s->busy;
   st->completed = s->completed;
   st->ticks = s->ticks;
   st->cell_steps = s->cell_steps;

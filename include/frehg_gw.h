@@ -355,7 +355,8 @@ typedef struct {
 } frehg_gw_request_status;
 
 typedef struct {
-  int active, queued;
+  int active;  /* requests in the running batch */
+  int queued;  /* waiting, or in the worker's hands being admitted or retired */
   long long completed, ticks, cell_steps;
   size_t device_bytes_used, device_bytes_budget;
   double busy_s;           /* time spent inside frehg_gw_server_tick */
