@@ -113,6 +113,37 @@ __device__ inline double vg_head(const Soil& s, double wc) {
   return 0.0;
 }
 
+// theta(h) and h(theta) of the classification, through logarithms: 2 log + 2
+// exp in place of 2 pow each (the initial state keeps the pow forms above).
+__device__ inline double vg_theta_fast(const Soil& s, double h) {
+  const double m = 1.0 - 1.0 / s.vgn;
+  double wc;
+  if (h > s.aev) {
+    wc = s.ts;
+  } else {
+    const double ah = fabs(s.vga * h);
+    const double se = (ah > 0.0) ? exp(-m * log1p(exp(s.vgn * log(ah)))) : 1.0;
+    wc = s.tr + (s.ts - s.tr) * se;
+  }
+  if (wc > s.ts) {
+    wc = s.ts;
+  } else if (wc < s.tr) {
+    wc = s.tr;
+  }
+  return wc;
+}
+
+__device__ inline double vg_head_fast(const Soil& s, double wc) {
+  const double m = 1.0 - 1.0 / s.vgn;
+  if (wc - s.tr < 1.0e-7) wc = s.tr + 1.0e-7;
+  if (wc < s.ts) {
+    const double ratio = (s.ts - s.tr) / (wc - s.tr);
+    const double x = expm1(log(ratio) / m);  // ratio^(1/m) - 1
+    return -(1.0 / s.vga) * exp(log(x) / s.vgn);
+  }
+  return 0.0;
+}
+
 // The closures below share t = |alpha h|^n, u = 1 + t and Se = u^-m between
 // K(h) and C(h), and rewrite the reference's nested powers by exact identities
 // (Se^(1/m) = 1/u, so 1 - Se^(1/m) = t/u; Se^(1/2) = sqrt(Se);

@@ -865,9 +865,9 @@ __device__ __forceinline__ CellPost classify_cell(
                                         : (topc == kHead && topv >= 0.0))
                                : (szm != 0));
       if (!adjsat) {
-        if (before < 0.9999 * so.ts) hout = vg_head(so, before);
+        if (before < 0.9999 * so.ts) hout = vg_head_fast(so, before);
       } else if (!d.off) {
-        const double after = vg_theta(so, hout);
+        const double after = vg_theta_fast(so, hout);
         wout = after;
         rm = (so.ts - after) * volume;
         if (d.redistribute && after < before) {
