@@ -73,6 +73,9 @@ def load():
                                            C.POINTER(WindowAudit)]
     lib.oracle_gw_coupler_state.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp]
     lib.oracle_gw_bath.argtypes = [C.c_void_p, _dp]
+    lib.oracle_gw_enable_transport_window.argtypes = [C.c_void_p]
+    lib.oracle_gw_reset_transport_window.argtypes = [C.c_void_p]
+    lib.oracle_gw_window.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.oracle_gw_coupler_restore.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
     _lib = lib
     return lib
@@ -205,6 +208,24 @@ class OracleSolver:
 
     def coupler_restore(self, t: float, dtg: float, lag: float) -> None:
         self.lib.oracle_gw_coupler_restore(self.h, t, dtg, lag)
+
+    # ------------------------------------------------------------ transport window
+    WINDOWS = {"x": 0, "y": 1, "z": 2, "vent": 3}
+
+    def enable_transport_window(self) -> None:
+        self._check(self.lib.oracle_gw_enable_transport_window(self.h))
+
+    def reset_transport_window(self) -> None:
+        self.lib.oracle_gw_reset_transport_window(self.h)
+
+    def window(self, name: str) -> np.ndarray:
+        """Window volumes in the halo layouts ((ny+2, nx+2, nz[+1]) or
+        (ny+2, nx+2) for the vent)."""
+        nzf = self.nz + 1 if name == "z" else self.nz
+        shape = (self.ny + 2, self.nx + 2) if name == "vent" else (self.ny + 2, self.nx + 2, nzf)
+        out = np.empty(shape)
+        self._check(self.lib.oracle_gw_window(self.h, self.WINDOWS[name], out.ctypes.data_as(_dp)))
+        return out
 
     def bath_halo(self) -> np.ndarray:
         """The mesh bed, offset frame, (ny+2, nx+2) with the mirrored halo."""

@@ -66,6 +66,10 @@ struct oracle_gw {
    * subsurface dt and clock */
   int csync;
   double cdt, cdtg, ctsub, clast_dt;
+  /* transport window (RichardsSolver.hpp:229-248): face volumes of the window
+   * in the qx / qy / qzF layouts, the walks' path records, vented volume */
+  int win;
+  double *wx, *wy, *wz, *pcorr, *wvent;
 };
 
 #define I2(s, j, i) ((size_t)(j) * (size_t)((s)->nx + 2) + (size_t)(i))
@@ -185,7 +189,8 @@ void oracle_gw_destroy(oracle_gw* s) {
                     &s->qx, &s->qy, &s->qz, &s->vloss, &s->room, &s->sup, &s->sdown,
                     &s->wcsnap, &s->hsnap, &s->topv, &s->botv, &s->xmv, &s->xpv, &s->ymv,
                     &s->ypv, &s->vals7, &s->rhs, &s->sol, &s->eta, &s->dept, &s->seep,
-                    &s->avail, &s->gain, &s->bounce, &s->qss};
+                    &s->avail, &s->gain, &s->bounce, &s->qss, &s->wx, &s->wy, &s->wz,
+                    &s->pcorr, &s->wvent};
   for (size_t n = 0; n < sizeof dbl / sizeof dbl[0]; ++n) free(*dbl[n]);
   free(s->ktop);
   free(s->gid);
@@ -1341,6 +1346,22 @@ static split_t gradient_split(const oracle_gw* s, int j, int i, int k) { /* :205
   return r;
 }
 
+/* The transport window's record of one transfer (Reallocate.cpp:418-446):
+ * from cell `from` to cell `to` (or through the column top when to < 0),
+ * mirrored by the legacy rule on face `face` with `sign`; the correction
+ * moves the rate onto every face the water crossed. */
+static void path_record(oracle_gw* s, int j, int i, int from, int to, double vol, int face,
+                        double sign, double dtg) {
+  if (!s->win) return;
+  const double rate = vol / dtg;
+  s->pcorr[IF(s, j, i, face)] -= sign * rate;
+  if (to < from) {
+    for (int f = to + 1; f <= from; ++f) s->pcorr[IF(s, j, i, f)] += rate;
+  } else {
+    for (int f = from + 1; f <= to; ++f) s->pcorr[IF(s, j, i, f)] -= rate;
+  }
+}
+
 static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped_out) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   const double az = s->az;
@@ -1444,6 +1465,7 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
               s->wc[c] += take / (az * s->dz[c]);
               s->room[c] -= take;
               s->qz[IF(s, j, i, ll + 1)] += take / dtg;
+              path_record(s, j, i, k, ll, take, ll + 1, 1.0, dtg);
               dV -= take;
             }
           }
@@ -1458,6 +1480,8 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
                 s->avail[col] += d;
                 s->gain[col] += d;
                 s->qz[IF(s, j, i, ll)] += dV / dtg;
+                path_record(s, j, i, k, ll - 1, dV, ll, 1.0, dtg);
+                if (s->win) s->wvent[col] += dV;
                 vent += dV;
               } else {
                 lost -= dV;
@@ -1465,6 +1489,7 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
               dV = 0.0;
             } else if (top_head) {
               s->qz[IF(s, j, i, ll)] += dV / dtg;
+              path_record(s, j, i, k, ll - 1, dV, ll, 1.0, dtg);
               dV = 0.0;
             } else {
               while (ll + 1 < nz && dV > 0.0) {
@@ -1475,6 +1500,7 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
                   s->wc[c] += take / (az * s->dz[c]);
                   s->room[c] -= take;
                   s->qz[IF(s, j, i, ll)] -= take / dtg;
+                  path_record(s, j, i, k, ll, take, ll, -1.0, dtg);
                   dV -= take;
                 }
               }
@@ -1494,6 +1520,7 @@ static void reallocate(oracle_gw* s, double dtg, double* adjust, double* dropped
               s->wc[c] += take / (az * s->dz[c]);
               s->room[c] -= take;
               s->qz[IF(s, j, i, ll)] -= take / dtg;
+              path_record(s, j, i, k, ll, take, ll, -1.0, dtg);
               dV -= take;
             }
           }
@@ -1614,12 +1641,20 @@ int oracle_gw_step(oracle_gw* s, double t, double dtg, frehg_gw_step_info* info)
   out.ss_storage = update_wc(s, dtg);
   /* post-allocation and the clamp (:784-787) */
   double adjust = 0.0, dropped = 0.0;
+  if (s->win) memset(s->pcorr, 0, s->n3f * sizeof(double));
   reallocate(s, dtg, &adjust, &dropped);
   out.realloc_adjust = adjust;
   out.realloc_dropped = dropped;
   out.vloss = finalize_wc(s);
   enforce_moisture_bc(s);
   out.boundary_in = boundary_inflow(s, dtg);
+  if (s->win) { /* accumulateTransportWindow (RichardsSolver.cpp:826-847), every slot */
+    for (size_t c = 0; c < s->n3; ++c) {
+      s->wx[c] += s->qx[c] * dtg;
+      s->wy[c] += s->qy[c] * dtg;
+    }
+    for (size_t f = 0; f < s->n3f; ++f) s->wz[f] += (s->qz[f] + s->pcorr[f]) * dtg;
+  }
   s->dtg_next = adapt(s, dtg);
   out.cg_iterations = its;
   out.outer_iterations = 1;
@@ -1882,4 +1917,42 @@ void oracle_gw_bath(const oracle_gw* s, double* out) { memcpy(out, s->bath, s->n
 void oracle_gw_coupler_restore(oracle_gw* s, double t, double dtg, double lag) {
   s->cdtg = dtg;
   s->ctsub = t - lag;
+}
+
+/* RichardsSolver::enableTransportWindow / resetTransportWindow
+ * (RichardsSolver.cpp:796-824). */
+int oracle_gw_enable_transport_window(oracle_gw* s) {
+  if (s->win) return FREHG_GW_OK;
+  s->wx = xcalloc(s->n3, sizeof(double));
+  s->wy = xcalloc(s->n3, sizeof(double));
+  s->wz = xcalloc(s->n3f, sizeof(double));
+  s->pcorr = xcalloc(s->n3f, sizeof(double));
+  s->wvent = xcalloc(s->n2, sizeof(double));
+  if (!s->wx || !s->wy || !s->wz || !s->pcorr || !s->wvent) {
+    set_err("oracle_gw_enable_transport_window: out of memory");
+    return FREHG_GW_ENOMEM;
+  }
+  s->win = 1;
+  return FREHG_GW_OK;
+}
+
+void oracle_gw_reset_transport_window(oracle_gw* s) {
+  if (!s->win) return;
+  memset(s->wx, 0, s->n3 * sizeof(double));
+  memset(s->wy, 0, s->n3 * sizeof(double));
+  memset(s->wz, 0, s->n3f * sizeof(double));
+  memset(s->wvent, 0, s->n2 * sizeof(double));
+}
+
+/* Window volumes in the halo layouts: 0 x faces (qx layout), 1 y faces, 2 z
+ * faces (qzF layout, path records included), 3 the vented volume per column. */
+int oracle_gw_window(const oracle_gw* s, int which, double* out) {
+  if (!s->win) {
+    set_err("oracle_gw_window: transport window not enabled");
+    return FREHG_GW_ESTATE;
+  }
+  const double* src = which == 0 ? s->wx : which == 1 ? s->wy : which == 2 ? s->wz : s->wvent;
+  const size_t n = which == 2 ? s->n3f : which == 3 ? s->n2 : s->n3;
+  memcpy(out, src, n * sizeof(double));
+  return FREHG_GW_OK;
 }

@@ -56,6 +56,12 @@ void oracle_gw_coupler_restore(oracle_gw* s, double t, double dtg, double lag);
 /* The mesh bed, offset frame, (ny+2)*(nx+2) with the mirrored halo. */
 void oracle_gw_bath(const oracle_gw* s, double* out);
 
+/* Transport window (RichardsSolver::enableTransportWindow / reset /
+ * windowVolumeX/Y/Z / windowVentVolume, RichardsSolver.hpp:229-248). */
+int oracle_gw_enable_transport_window(oracle_gw* s);
+void oracle_gw_reset_transport_window(oracle_gw* s);
+int oracle_gw_window(const oracle_gw* s, int which, double* out);
+
 /* Pointwise closures (src/gw/VanGenuchten.hpp:45-128), exported for the
  * golden-value tests. */
 double oracle_vg_theta(double vga, double vgn, double ts, double tr, double aev, double h);

@@ -86,6 +86,9 @@ def load(omp: bool = False):
                                        C.c_double, C.c_int]
     lib.ref_coupler_step.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp]
     lib.ref_coupler_state.argtypes = [C.c_void_p, C.c_double, _dp]
+    lib.ref_enable_transport_window.argtypes = [C.c_void_p]
+    lib.ref_reset_transport_window.argtypes = [C.c_void_p]
+    lib.ref_window.argtypes = [C.c_void_p, C.c_int, _dp]
     _libs[path] = lib
     return lib
 
@@ -301,3 +304,22 @@ class RefSolver:
         out = np.zeros(3)
         self.lib.ref_coupler_state(self.h, t, out.ctypes.data_as(_dp))
         return tuple(out.tolist())
+
+    # -- transport window --------------------------------------------------------
+    WINDOWS = {"x": 0, "y": 1, "z": 2, "vent": 3}
+
+    def enable_transport_window(self) -> None:
+        self.lib.ref_enable_transport_window(self.h)
+
+    def reset_transport_window(self) -> None:
+        self.lib.ref_reset_transport_window(self.h)
+
+    def window(self, name: str) -> np.ndarray:
+        """Window volumes in the halo layouts ((ny+2, nx+2, nz[+1]) or
+        (ny+2, nx+2) for the vent)."""
+        shape = {"x": self._halo_shape("qx"), "y": self._halo_shape("qy"),
+                 "z": self._halo_shape("qz"), "vent": (self.ny + 2, self.nx + 2)}[name]
+        out = np.empty(shape)
+        if self.lib.ref_window(self.h, self.WINDOWS[name], out.ctypes.data_as(_dp)) != 0:
+            raise KeyError(name)
+        return out

@@ -485,6 +485,23 @@ int ref_coupler_step(void* h, double t, double dt, double* out) {
   }
 }
 
+/// RichardsSolver::enableTransportWindow / resetTransportWindow.
+void ref_enable_transport_window(void* h) { static_cast<RefSim*>(h)->gw->enableTransportWindow(); }
+void ref_reset_transport_window(void* h) { static_cast<RefSim*>(h)->gw->resetTransportWindow(); }
+
+/// Window volumes: 0 windowVolumeX (qx layout), 1 windowVolumeY, 2
+/// windowVolumeZ (qzF layout), 3 windowVentVolume ((ny+2)*(nx+2)).
+int ref_window(void* h, int which, double* out) {
+  const auto& gw = *static_cast<RefSim*>(h)->gw;
+  if (which == 0) copyOut(gw.windowVolumeX(), out);
+  else if (which == 1) copyOut(gw.windowVolumeY(), out);
+  else if (which == 2) copyOut(gw.windowVolumeZ(), out);
+  else if (which == 3)
+    std::memcpy(out, gw.windowVentVolume().data(), gw.windowVentVolume().span() * sizeof(double));
+  else return 1;
+  return 0;
+}
+
 /// Coupler::nextDt, currentDtg, gwLag(t).
 void ref_coupler_state(void* h, double t, double* out) {
   const auto& c = *static_cast<RefSim*>(h)->coupler;
