@@ -19,6 +19,7 @@ FIELD = {
     "h": 0, "wc": 1, "qx": 2, "qy": 3, "qz": 4, "kx": 5, "ky": 6, "kz": 7,
     "wcn": 8, "dz3d": 9, "bot3d": 10, "ax": 11, "ay": 12, "sinx": 13, "cosx": 14,
     "siny": 15, "cosy": 16, "vloss": 17,
+    "win_x": 18, "win_y": 19, "win_z": 20, "win_vent": 21,
 }
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -159,23 +160,27 @@ def make_desc(cfg: GwConfig, ras: Rasterized = None) -> Tuple[GwDesc, list]:
     return desc, keep
 
 
-def field_shape(field: str, nx: int, ny: int, nz: int) -> Tuple[int, int, int]:
-    if field in ("qx", "kx", "ax", "sinx", "cosx"):
+def field_shape(field: str, nx: int, ny: int, nz: int) -> Tuple[int, ...]:
+    if field in ("qx", "kx", "ax", "sinx", "cosx", "win_x"):
         return (ny, nx + 1, nz)
-    if field in ("qy", "ky", "ay", "siny", "cosy"):
+    if field in ("qy", "ky", "ay", "siny", "cosy", "win_y"):
         return (ny + 1, nx, nz)
-    if field in ("qz", "kz"):
+    if field in ("qz", "kz", "win_z"):
         return (ny, nx, nz + 1)
+    if field == "win_vent":
+        return (ny, nx)
     return (ny, nx, nz)
 
 
 def interior_from_halo(field: str, full: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
     """Slice a reference halo-layout field ((ny+2, nx+2, nz[+1])) to the ABI
     shape of :func:`field_shape`."""
-    if field in ("qx", "kx", "ax", "sinx", "cosx"):
+    if field in ("qx", "kx", "ax", "sinx", "cosx", "win_x"):
         return full[1:ny + 1, 0:nx + 1, :nz]
-    if field in ("qy", "ky", "ay", "siny", "cosy"):
+    if field in ("qy", "ky", "ay", "siny", "cosy", "win_y"):
         return full[0:ny + 1, 1:nx + 1, :nz]
-    if field in ("qz", "kz"):
+    if field in ("qz", "kz", "win_z"):
         return full[1:ny + 1, 1:nx + 1, :nz + 1]
+    if field == "win_vent":
+        return full[1:ny + 1, 1:nx + 1]
     return full[1:ny + 1, 1:nx + 1, :nz]

@@ -451,6 +451,7 @@ void enqueue_corrector(frehg_gw_handle* h) {
   if (h->profiling) cudaEventRecord(h->ev[3], D.stream);
   fgw::launch_classify(D, D.wc[nxt], D.h[nxt]);
   fgw::launch_walk(D, D.wc[nxt]);
+  if (D.win_x) fgw::launch_window_accum(D);
   if (h->profiling) cudaEventRecord(h->ev[4], D.stream);
   fgw::launch_finalize(D, D.wc[nxt], h->co_max);
   fgw::launch_step_info(D, h->dq_grow, h->dq_shrink, h->dt_min, h->dt_max);
@@ -562,8 +563,14 @@ size_t frehg_gw_field_size(const frehg_gw_handle* h, int field) {
     case FREHG_GW_FIELD_QY: case FREHG_GW_FIELD_KY: case FREHG_GW_FIELD_AY:
     case FREHG_GW_FIELD_SINY: case FREHG_GW_FIELD_COSY:
       return (ny + 1) * nx * nz;
-    case FREHG_GW_FIELD_QZ: case FREHG_GW_FIELD_KZ:
+    case FREHG_GW_FIELD_QZ: case FREHG_GW_FIELD_KZ: case FREHG_GW_FIELD_WINDOW_Z:
       return ny * nx * (nz + 1);
+    case FREHG_GW_FIELD_WINDOW_X:
+      return ny * (nx + 1) * nz;
+    case FREHG_GW_FIELD_WINDOW_Y:
+      return (ny + 1) * nx * nz;
+    case FREHG_GW_FIELD_WINDOW_VENT:
+      return ny * nx;
     default:
       return (field >= 0 && field < FREHG_GW_FIELD_COUNT) ? ny * nx * nz : 0;
   }
@@ -594,7 +601,22 @@ int frehg_gw_get_field(frehg_gw_handle* h, int field, double* out) {
     case FREHG_GW_FIELD_COSY: src = D.cosy; kind = 2; break;
     case FREHG_GW_FIELD_QZ: src = D.qzf; kind = 3; break;
     case FREHG_GW_FIELD_KZ: src = D.kzf; kind = 3; break;
+    case FREHG_GW_FIELD_WINDOW_X: src = D.win_x; kind = 1; break;
+    case FREHG_GW_FIELD_WINDOW_Y: src = D.win_y; kind = 2; break;
+    case FREHG_GW_FIELD_WINDOW_Z: src = D.win_z; kind = 3; break;
+    case FREHG_GW_FIELD_WINDOW_VENT: src = D.win_vent; kind = 4; break;
     default: return fail(FREHG_GW_EINVAL, "unknown field");
+  }
+  if (!src) return fail(FREHG_GW_ESTATE, "get_field: transport window not enabled");
+  if (kind == 4) {  // a column field, (ny+2)(nx+2) on the device
+    std::vector<double> full(static_cast<size_t>(d.ncol));
+    CUDA_TRY(cudaStreamSynchronize(D.stream), "get_field");
+    CUDA_TRY(cudaMemcpy(full.data(), src, full.size() * sizeof(double), cudaMemcpyDeviceToHost),
+             "get_field");
+    size_t q = 0;
+    for (int j = 1; j <= d.ny; ++j)
+      for (int i = 1; i <= d.nx; ++i) out[q++] = full[fgw::col2(d, j, i)];
+    return FREHG_GW_OK;
   }
   const size_t n = static_cast<size_t>(kind == 3 ? d.ncol * (d.nz + 1) : d.ncell);
   std::vector<double> full(n);
@@ -611,6 +633,43 @@ int frehg_gw_get_field(frehg_gw_handle* h, int field, double* out) {
   for (int j = j0; j <= d.ny; ++j)
     for (int i = i0; i <= d.nx; ++i)
       for (int k = 0; k < d.nz; ++k) out[q++] = full[fgw::cidx(d, j, i, k)];
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_enable_transport_window(frehg_gw_handle* h) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  fgw::Device& D = h->D;
+  if (D.win_x) return FREHG_GW_OK;
+  const size_t n3 = static_cast<size_t>(D.d.ncell), nf = static_cast<size_t>(D.d.ncol) * (D.d.nz + 1);
+  double** f[5] = {&D.win_x, &D.win_y, &D.win_z, &D.pcorr, &D.win_vent};
+  const size_t n[5] = {n3, n3, nf, nf, static_cast<size_t>(D.d.ncol)};
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "enable_transport_window");
+  for (int w = 0; w < 5; ++w) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, n[w] * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      for (int u = 0; u < w; ++u) *f[u] = nullptr;  // freed with the handle
+      return fail(FREHG_GW_ENOMEM, "enable_transport_window: allocation failed");
+    }
+    D.allocs.push_back(p);
+    CUDA_TRY(cudaMemsetAsync(p, 0, n[w] * sizeof(double), D.stream), "enable_transport_window");
+    *f[w] = static_cast<double*>(p);
+  }
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "enable_transport_window");
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_reset_transport_window(frehg_gw_handle* h) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  fgw::Device& D = h->D;
+  if (!D.win_x) return FREHG_GW_OK;  // as the reference: a no-op until enabled
+  const size_t n3 = static_cast<size_t>(D.d.ncell), nf = static_cast<size_t>(D.d.ncol) * (D.d.nz + 1);
+  CUDA_TRY(cudaMemsetAsync(D.win_x, 0, n3 * sizeof(double), D.stream), "reset_transport_window");
+  CUDA_TRY(cudaMemsetAsync(D.win_y, 0, n3 * sizeof(double), D.stream), "reset_transport_window");
+  CUDA_TRY(cudaMemsetAsync(D.win_z, 0, nf * sizeof(double), D.stream), "reset_transport_window");
+  CUDA_TRY(cudaMemsetAsync(D.win_vent, 0, static_cast<size_t>(D.d.ncol) * sizeof(double),
+                           D.stream), "reset_transport_window");
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "reset_transport_window");
   return FREHG_GW_OK;
 }
 

@@ -91,7 +91,11 @@ struct Device {
   bool surf_own[8] = {};
   int8_t* cmode = nullptr;
   CplDev* cpl_dev = nullptr;  // the kernels' copy of cpl_host (f.cpl when attached)
-  CplDev cpl_host{};  // per-cell saturation flag of the post-allocation snapshot
+  CplDev cpl_host{};
+  // transport window (null until enabled): face volumes in the qx / qy / qzF
+  // layouts, the walks' path records (qzF layout), vented volume per column
+  double *win_x = nullptr, *win_y = nullptr, *win_z = nullptr, *pcorr = nullptr,
+         *win_vent = nullptr;  // per-cell saturation flag of the post-allocation snapshot
   // linear system: coefficients and vectors carry a zero margin of sy cells
   // on both ends; the pointers below point at cell 0.
   double *diag = nullptr, *gxp = nullptr, *gyp = nullptr, *gzp = nullptr, *rhs = nullptr;
@@ -140,6 +144,8 @@ void launch_cpl_mode(const Device& D, const double* hn);
 void launch_cpl_book(const Device& D, const double* wcn);
 void launch_cpl_begin_window(const Device& D);
 void launch_cpl_seepage(const Device& D, double dt);
+// Transport window: the step's q dtg (and path records) into the window.
+void launch_window_accum(const Device& D);
 void launch_init_state(const Device& D, int form, double constant, const double* field,
                        const double* bath, double offset);
 // FP64 Jacobi-PCG (PETSc KSPCG semantics); returns a CUDA error code.

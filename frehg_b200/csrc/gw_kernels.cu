@@ -933,12 +933,13 @@ struct VentState {
   double vent, thin;
   double min_depth;
   int vent_all;
+  double wv;  // this column's vented volume (transport window)
 };
 
 // What the upward walk could not place, dv > 0, leaves through the top of
 // column face `ll` of a coupled column: onto the surface when it is wet, the
 // amount exceeds min_depth or every vent deposits; else it is lost.
-__device__ inline void vent_top(const Dims& d, double dv, double idtg, double& qface,
+__device__ inline bool vent_top(const Dims& d, double dv, double idtg, double& qface,
                                 VentState& v, double& lost) {
   const double dd = dv / d.az;
   if (v.vent_all || v.dept > 0.0 || dd > v.min_depth) {
@@ -947,10 +948,27 @@ __device__ inline void vent_top(const Dims& d, double dv, double idtg, double& q
     v.dept += dd;
     v.avail += dd;
     v.gain += dd;
-    qface += dv * idtg;
+    qface += __dmul_rn(dv, idtg);
     v.vent += dv;
+    v.wv += dv;
+    return true;
+  }
+  lost -= dv;
+  return false;
+}
+
+// The transport window's record of one transfer of `rate` from cell `from`
+// to cell `to` of a column (to = the cell above the column's top for a
+// release through it), mirrored by the legacy rule on face `face` with
+// `sign` (Reallocate.cpp:418-446): the column's path corrections pc (faces
+// 0..nz) move the rate from the mirrored face onto every face crossed.
+__device__ inline void path_record(double* pc, int from, int to, double rate, int face,
+                                   double sign) {
+  pc[face] -= sign * rate;
+  if (to < from) {
+    for (int f = to + 1; f <= from; ++f) pc[f] += rate;
   } else {
-    lost -= dv;
+    for (int f = from + 1; f <= to; ++f) pc[f] -= rate;
   }
 }
 
@@ -961,6 +979,7 @@ __device__ inline void vent_load(const Fields& f, long long col, VentState& v) {
   v.gain = f.cpl->gain[col];
   v.min_depth = f.cpl->min_depth;
   v.vent_all = f.cpl->vent_all;
+  v.wv = 0.0;
 }
 
 __device__ inline void vent_store(const Fields& f, long long col, const VentState& v) {
@@ -990,11 +1009,11 @@ __device__ inline void walk_books(const Dims& d, double lost, const VentState& v
 template <bool CPL>
 __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
                        const double* __restrict__ sdn, double* qzf, const int* __restrict__ colflag,
-                       const double* __restrict__ dtgp, double* partial, int nblk, const int bid,
-                       const int G) {
+                       const double* __restrict__ dtgp, double* partial, int nblk,
+                       double* pcorr, double* wvent, const int bid, const int G) {
   const double dtg = *dtgp;
   double lost = 0.0;
-  VentState v{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0};
+  VentState v{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0.0};
   const long long ncolint = static_cast<long long>(d.nx) * d.ny;
   for (long long t = bid * static_cast<long long>(blockDim.x) + threadIdx.x; t < ncolint;
        t += static_cast<long long>(G) * blockDim.x) {
@@ -1004,6 +1023,9 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
     const long long base = cidx(d, j, i, 0), fb = fidx(d, j, i, 0);
     const bool topHead = f.topc[col] == kHead;
     if (CPL) vent_load(f, col, v);
+    double* pc = pcorr ? pcorr + fb : nullptr;  // transport window: this column's path records
+    if (pc)
+      for (int q = 0; q <= d.nz; ++q) pc[q] = 0.0;
     for (int k = 0; k < d.nz; ++k) {
       if (!f.act[base + k]) continue;
       double dv = sup[base + k];
@@ -1017,14 +1039,17 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
             wc[c] += take / (d.az * f.dz[c]);
             room[c] -= take;
             qzf[fb + ll + 1] += take / dtg;
+            if (pc) path_record(pc, k, ll, take / dtg, ll + 1, 1.0);
             dv -= take;
           }
         }
         if (dv > 0.0) {
           if (CPL) {
-            vent_top(d, dv, 1.0 / dtg, qzf[fb + ll], v, lost);
+            if (vent_top(d, dv, 1.0 / dtg, qzf[fb + ll], v, lost) && pc)
+              path_record(pc, k, ll - 1, dv / dtg, ll, 1.0);
           } else if (topHead) {
             qzf[fb + ll] += dv / dtg;
+            if (pc) path_record(pc, k, ll - 1, dv / dtg, ll, 1.0);
           } else {
             while (ll + 1 < d.nz && dv > 0.0) {
               ++ll;
@@ -1034,6 +1059,7 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
                 wc[c] += take / (d.az * f.dz[c]);
                 room[c] -= take;
                 qzf[fb + ll] -= take / dtg;
+                if (pc) path_record(pc, k, ll, take / dtg, ll, -1.0);
                 dv -= take;
               }
             }
@@ -1052,13 +1078,17 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
             wc[c] += take / (d.az * f.dz[c]);
             room[c] -= take;
             qzf[fb + ll] -= take / dtg;
+            if (pc) path_record(pc, k, ll, take / dtg, ll, -1.0);
             dv -= take;
           }
         }
         lost -= dv;
       }
     }
-    if (CPL) vent_store(f, col, v);
+    if (CPL) {
+      vent_store(f, col, v);
+      if (wvent) wvent[col] += v.wv;
+    }
   }
   walk_books<CPL>(d, lost, v, partial, nblk, bid);
 }
@@ -1066,9 +1096,10 @@ __device__ __forceinline__ void walk_thread_body(Dims d, Fields f, double* wc, d
 template <bool CPL>
 __global__ void k_walk_thread(Dims d, Fields f, double* wc, double* room, const double* __restrict__ sup,
                        const double* __restrict__ sdn, double* qzf, const int* __restrict__ colflag,
-                       const double* __restrict__ dtgp, double* partial, int nblk) {
-  walk_thread_body<CPL>(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, nblk, blockIdx.x,
-                   gridDim.x);
+                       const double* __restrict__ dtgp, double* partial, int nblk,
+                       double* pcorr, double* wvent) {
+  walk_thread_body<CPL>(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, nblk, pcorr, wvent,
+                        blockIdx.x, gridDim.x);
 }
 
 // The same walk with one warp per flagged column.  The column's room, theta,
@@ -1125,15 +1156,21 @@ __device__ inline int bits_lowest(const unsigned* w, int lo, int hi) {
 // reciprocals (ivs staged per column, idtg once per kernel): a walk runs on
 // one lane, and FP64 divisions were most of its issue slots.
 __device__ inline void walk_take(double& dv, int m, double* rs, double* ws, const double* ivs,
-                                 double* qs, unsigned* rbits, int face, bool plus, double idtg) {
+                                 double* qs, unsigned* rbits, int face, bool plus, double idtg,
+                                 double* pc, int from) {
   const double take = (rs[m] > dv) ? dv : rs[m];
   ws[m] += take * ivs[m];
   rs[m] -= take;
+  // The rate is rounded on its own (no fused multiply-add), so every kernel
+  // that inlines this walk -- with or without the path record that reuses
+  // the rate -- adds the same value.
+  const double rate = __dmul_rn(take, idtg);
   if (plus) {
-    qs[face] += take * idtg;
+    qs[face] += rate;
   } else {
-    qs[face] -= take * idtg;
+    qs[face] -= rate;
   }
+  if (pc) path_record(pc, from, m, rate, face, plus ? 1.0 : -1.0);
   dv -= take;
   if (!(rs[m] > 0.0)) rbits[m >> 5] &= ~(1u << (m & 31));
 }
@@ -1146,7 +1183,7 @@ template <bool CPL>
 __device__ inline void walk_cell(const Dims& d, int kk, double upv, double dnv, int nz, bool topHead,
                                  double* rs, double* ws, const double* ivs, double* qs,
                                  unsigned* rbits, const unsigned* ibits, double idtg, double& lost,
-                                 VentState& v) {
+                                 VentState& v, double* pc) {
   double dv = upv;
   if (dv > 0.0) {
     // Upward: cells kk-1, kk-2, ... up to the first inactive cell above
@@ -1159,19 +1196,22 @@ __device__ inline void walk_cell(const Dims& d, int kk, double upv, double dnv, 
         ll = lim;
         break;
       }
-      walk_take(dv, m, rs, ws, ivs, qs, rbits, m + 1, true, idtg);
+      walk_take(dv, m, rs, ws, ivs, qs, rbits, m + 1, true, idtg, pc, kk);
       ll = m;
     }
     if (dv > 0.0) {
       if (CPL) {
-        vent_top(d, dv, idtg, qs[ll], v, lost);
+        if (vent_top(d, dv, idtg, qs[ll], v, lost) && pc)
+          path_record(pc, kk, ll - 1, __dmul_rn(dv, idtg), ll, 1.0);
       } else if (topHead) {
-        qs[ll] += dv * idtg;
+        const double rate = __dmul_rn(dv, idtg);
+        qs[ll] += rate;
+        if (pc) path_record(pc, kk, ll - 1, rate, ll, 1.0);
       } else {
         while (dv > 0.0) {
           const int m = bits_lowest(rbits, ll + 1, nz - 1);
           if (m < 0) break;
-          walk_take(dv, m, rs, ws, ivs, qs, rbits, m, false, idtg);
+          walk_take(dv, m, rs, ws, ivs, qs, rbits, m, false, idtg, pc, kk);
           ll = m;
         }
         lost -= dv;
@@ -1184,7 +1224,7 @@ __device__ inline void walk_cell(const Dims& d, int kk, double upv, double dnv, 
     while (dv > 0.0) {
       const int m = bits_lowest(rbits, ll + 1, nz - 1);
       if (m < 0) break;
-      walk_take(dv, m, rs, ws, ivs, qs, rbits, m, false, idtg);
+      walk_take(dv, m, rs, ws, ivs, qs, rbits, m, false, idtg, pc, kk);
       ll = m;
     }
     lost -= dv;
@@ -1198,8 +1238,8 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ sdn, double* qzf,
                                                  const int* __restrict__ colflag,
                                                  const double* __restrict__ dtgp,
-                                                 double* partial, int nblk, const int bid,
-                                                 const int G) {
+                                                 double* partial, int nblk, double* pcorr,
+                                                 double* wvent, const int bid, const int G) {
   extern __shared__ __align__(16) unsigned char walk_smem[];
   const double idtg = 1.0 / *dtgp;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1211,7 +1251,7 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
   unsigned* rbits = reinterpret_cast<unsigned*>(qs + nz + 1);
   unsigned* ibits = rbits + nw;  // inactive cells
   double lost = 0.0;
-  VentState v{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0};
+  VentState v{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0.0};
   const long long ncolint = static_cast<long long>(d.nx) * d.ny;
   const long long nwarps = static_cast<long long>(G) * kWalkWarps;
   for (long long t = bid * static_cast<long long>(kWalkWarps) + warp; t < ncolint;
@@ -1222,6 +1262,9 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
     const long long base = cidx(d, j, i, 0), fb = fidx(d, j, i, 0);
     const bool topHead = f.topc[col] == kHead;
     if (CPL && lane == 0) vent_load(f, col, v);
+    double* pc = pcorr ? pcorr + fb : nullptr;  // transport window: this column's path records
+    if (pc)
+      for (int q = lane; q <= nz; q += 32) pc[q] = 0.0;
     for (int k0 = 0; k0 < nz; k0 += 32) {
       const int k = k0 + lane;
       double r = 0.0;
@@ -1259,13 +1302,16 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
         const double dnv = __shfl_sync(0xffffffffu, sd, b);
         if (lane == 0)
           walk_cell<CPL>(d, k0 + b, upv, dnv, nz, topHead, rs, ws, ivs, qs, rbits, ibits, idtg, lost,
-                         v);
+                         v, pc);
         __syncwarp();
       }
     }
     for (int k = lane; k < nz; k += 32) wc[base + k] = ws[k];
     for (int k = lane; k <= nz; k += 32) qzf[fb + k] = qs[k];
-    if (CPL && lane == 0) vent_store(f, col, v);
+    if (CPL && lane == 0) {
+      vent_store(f, col, v);
+      if (wvent) wvent[col] += v.wv;
+    }
     __syncwarp();
   }
   walk_books<CPL>(d, lost, v, partial, nblk, bid);
@@ -1278,8 +1324,10 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ sdn, double* qzf,
                                                  const int* __restrict__ colflag,
                                                  const double* __restrict__ dtgp,
-                                                 double* partial, int nblk) {
-  walk_body<CPL>(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, nblk, blockIdx.x, gridDim.x);
+                                                 double* partial, int nblk, double* pcorr,
+                                                 double* wvent) {
+  walk_body<CPL>(d, f, wc, room, sup, sdn, qzf, colflag, dtgp, partial, nblk, pcorr, wvent,
+                 blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- coupled top
@@ -1790,10 +1838,10 @@ __global__ void __launch_bounds__(kBlock) k_walk_batch(const StepArgs* tab, cons
   load_member(tab, first, n, sa, bid, G);
   if (sa.warp_walk) {
     walk_body<false>(sa.d, sa.f, sa.wc_out, sa.room, sa.sup, sa.sdn, sa.qzf, sa.colflag, &sa.dtg,
-              sa.partial, sa.nblk, bid, G);
+              sa.partial, sa.nblk, nullptr, nullptr, bid, G);
   } else {
     walk_thread_body<false>(sa.d, sa.f, sa.wc_out, sa.room, sa.sup, sa.sdn, sa.qzf, sa.colflag, &sa.dtg,
-                     sa.partial, sa.nblk, bid, G);
+                     sa.partial, sa.nblk, nullptr, nullptr, bid, G);
   }
 }
 
@@ -1918,13 +1966,43 @@ void launch_walk(const Device& D, double* wc_out) {
     const auto walk = (D.f.cpl != nullptr) ? k_walk<true> : k_walk<false>;
     walk<<<cells_grid(D), kBlock, smem, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
                                                       D.qzf, D.colflag, dtg_slot(D), D.partial,
-                                                      D.nblk);
+                                                      D.nblk, D.pcorr, D.win_vent);
   } else {
     const auto walk = (D.f.cpl != nullptr) ? k_walk_thread<true> : k_walk_thread<false>;
     walk<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, wc_out, D.room, D.sup, D.sdn,
                                                           D.qzf, D.colflag, dtg_slot(D),
-                                                          D.partial, D.nblk);
+                                                          D.partial, D.nblk, D.pcorr, D.win_vent);
   }
+  ++D.launches;
+}
+
+// accumulateTransportWindow (RichardsSolver.cpp:826-847): q dtg of every x, y
+// and z face slot into the window, the z faces with the walks' path records
+// (written this step in the flagged columns only; the others have none).
+__global__ void k_window_accum(Dims d, const double* __restrict__ qx,
+                               const double* __restrict__ qy, const double* __restrict__ qzf,
+                               const double* __restrict__ pcorr, const int* __restrict__ colflag,
+                               const double* __restrict__ dtgp, double* __restrict__ wx,
+                               double* __restrict__ wy, double* __restrict__ wz) {
+  const double dtg = *dtgp;
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long t0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  for (long long c = t0; c < d.ncell; c += stride) {
+    wx[c] += qx[c] * dtg;
+    wy[c] += qy[c] * dtg;
+  }
+  const long long nf = d.ncol * (d.nz + 1);
+  for (long long q = t0; q < nf; q += stride) {
+    const long long col = q / (d.nz + 1);
+    const double corr = colflag[col] ? pcorr[q] : 0.0;
+    wz[q] += (qzf[q] + corr) * dtg;
+  }
+}
+
+void launch_window_accum(const Device& D) {
+  k_window_accum<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.qx, D.qy, D.qzf, D.pcorr,
+                                                         D.colflag, dtg_slot(D), D.win_x,
+                                                         D.win_y, D.win_z);
   ++D.launches;
 }
 

@@ -74,11 +74,14 @@ def load_library(path: str = LIB_PATH):
     lib.frehg_gw_coupled_audit_get.argtypes = [H, C.POINTER(CoupledAudit)]
     lib.frehg_gw_elevation_offset.argtypes = [H]
     lib.frehg_gw_elevation_offset.restype = C.c_double
+    lib.frehg_gw_enable_transport_window.argtypes = [H]
+    lib.frehg_gw_reset_transport_window.argtypes = [H]
     for name in ("frehg_gw_create", "frehg_gw_destroy", "frehg_gw_set_stream",
                  "frehg_gw_set_bc_values", "frehg_gw_init_state", "frehg_gw_set_state",
                  "frehg_gw_step", "frehg_gw_next_dt", "frehg_gw_get_field", "frehg_gw_restore",
                  "frehg_gw_owned_volume", "frehg_gw_attach_coupling", "frehg_gw_get_surface",
-                 "frehg_gw_set_surface", "frehg_gw_surface_ptr", "frehg_gw_coupled_audit_get"):
+                 "frehg_gw_set_surface", "frehg_gw_surface_ptr", "frehg_gw_coupled_audit_get",
+                 "frehg_gw_enable_transport_window", "frehg_gw_reset_transport_window"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -302,3 +305,22 @@ class RichardsSolver:
 
     def elevationOffset(self) -> float:
         return float(self.lib.frehg_gw_elevation_offset(self.h))
+
+    # -- transport window (RichardsSolver.hpp:229-248) ----------------------------
+    def enableTransportWindow(self) -> None:
+        _check(self.lib, self.lib.frehg_gw_enable_transport_window(self.h))
+
+    def resetTransportWindow(self) -> None:
+        _check(self.lib, self.lib.frehg_gw_reset_transport_window(self.h))
+
+    def windowVolumeX(self) -> np.ndarray:
+        return self.field("win_x")
+
+    def windowVolumeY(self) -> np.ndarray:
+        return self.field("win_y")
+
+    def windowVolumeZ(self) -> np.ndarray:
+        return self.field("win_z")
+
+    def windowVentVolume(self) -> np.ndarray:
+        return self.field("win_vent")

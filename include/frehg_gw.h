@@ -102,7 +102,13 @@ enum {
   FREHG_GW_FIELD_SINY = 15,     /* like QY */
   FREHG_GW_FIELD_COSY = 16,
   FREHG_GW_FIELD_VLOSS = 17,    /* cumulative clamp volume per cell */
-  FREHG_GW_FIELD_COUNT = 18
+  /* Transport window (frehg_gw_enable_transport_window), volumes [m^3] since
+   * the last reset: */
+  FREHG_GW_FIELD_WINDOW_X = 18,    /* like QX */
+  FREHG_GW_FIELD_WINDOW_Y = 19,    /* like QY */
+  FREHG_GW_FIELD_WINDOW_Z = 20,    /* like QZ, the walks' transfers on every face they cross */
+  FREHG_GW_FIELD_WINDOW_VENT = 21, /* (ny, nx): vented onto a coupled surface */
+  FREHG_GW_FIELD_COUNT = 22
 };
 
 /* Static description of one domain.  Host pointers; the library copies what
@@ -230,6 +236,18 @@ long long frehg_gw_active_cells(const frehg_gw_handle* h);
  * [2] corrector, [3] post-allocation, [4] clamp, audit and controller. */
 int frehg_gw_set_profiling(frehg_gw_handle* h, int on);
 int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5);
+
+/* The transport window (RichardsSolver::enableTransportWindow,
+ * resetTransportWindow, windowVolumeX/Y/Z, windowVentVolume,
+ * src/gw/RichardsSolver.hpp:229-248; accumulateTransportWindow,
+ * RichardsSolver.cpp:826-847): once enabled, every step adds the face volumes
+ * q dtg of all faces into the window fields (FREHG_GW_FIELD_WINDOW_*), and the
+ * post-allocation walks record each transfer on every face it crosses in the z
+ * window (the step's QZ keeps the reference's receiver-face mirror).  The
+ * window stays on the device for a transport consumer; reset zeroes it.  The
+ * ET vapour and root-sink windows are outside this drop-in. */
+int frehg_gw_enable_transport_window(frehg_gw_handle* h);
+int frehg_gw_reset_transport_window(frehg_gw_handle* h);
 
 /* Kernels this handle has launched since creation. */
 long long frehg_gw_kernel_launches(const frehg_gw_handle* h);
