@@ -754,10 +754,11 @@ struct SplitIn {
 __device__ inline Split gradient_split(const Dims& d, const SplitIn& n, int k) {
   double dh0 = 0.0, dh1 = 0.0, dh2 = 0.0, dh3 = 0.0, dh4 = 0.0, dh5 = 0.0;
   if (d.full3d) {
-    if (n.axp && n.kxp > 0.0) dh0 = (n.hxp - n.hc) / d.dx;
-    if (n.axm && n.kxm > 0.0) dh1 = (n.hc - n.hxm) / d.dx;
-    if (n.ayp && n.kyp > 0.0) dh2 = (n.hyp - n.hc) / d.dy;
-    if (n.aym && n.kym > 0.0) dh3 = (n.hc - n.hym) / d.dy;
+    const double idx = 1.0 / d.dx, idy = 1.0 / d.dy;
+    if (n.axp && n.kxp > 0.0) dh0 = (n.hxp - n.hc) * idx;
+    if (n.axm && n.kxm > 0.0) dh1 = (n.hc - n.hxm) * idx;
+    if (n.ayp && n.kyp > 0.0) dh2 = (n.hyp - n.hc) * idy;
+    if (n.aym && n.kym > 0.0) dh3 = (n.hc - n.hym) * idy;
   }
   if (k + 1 < d.nz && n.azp && n.kzb > 0.0) {
     const double dzp = 0.5 * (n.dzc + n.dzp);
