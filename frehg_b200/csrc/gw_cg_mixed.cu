@@ -783,15 +783,24 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
   }
 }
 
+// Blocks per SM of the mixed solves: as many as fit without register spills
+// (three; two for 8 cells per lane and for the batched forms, whose member
+// records add registers).  At four the 64-register cap spilled 126 bytes a
+// thread and the 512x512x128 solve ran 5 % slower (12.5 against 11.8 ms).
 template <int V, int E>
-__global__ void __launch_bounds__(kCgBlock, 4) k_cg_mixed(MixedArgs a) {
+constexpr int mixed_min_blocks(bool batch) {
+  return (E == 8 || (batch && (V == 4 || E == 8))) ? 2 : 3;
+}
+
+template <int V, int E>
+__global__ void __launch_bounds__(kCgBlock, mixed_min_blocks<V, E>(false)) k_cg_mixed(MixedArgs a) {
   cg_mixed_body<V, E>(a, blockIdx.x, gridDim.x);
 }
 
 // One cooperative launch over several domains of the same (V, E) class:
 // instance i owns blocks [first[i], first[i+1]) and runs its own solve.
 template <int V, int E>
-__global__ void __launch_bounds__(kCgBlock, 4)
+__global__ void __launch_bounds__(kCgBlock, mixed_min_blocks<V, E>(true))
     k_cg_mixed_batch(const MixedArgs* __restrict__ tab, const int* __restrict__ first, int n) {
   __shared__ MixedArgs sa;
   __shared__ int sb, sg;
