@@ -46,7 +46,7 @@ METRIC = "cell-steps/s at 512x512x128"
 # DRAM bytes (read + write) per algorithmic byte of k_cg_mixed, from the ncu
 # capture summarised in profiles/ (256x256x128 slab, one steady-state launch);
 # scaled to the timed launches by their algorithmic bytes.
-MIXED_TRAFFIC_PER_ALG_BYTE = 1.032
+MIXED_TRAFFIC_PER_ALG_BYTE = 1.022
 # Bytes frehg_gw_step reads back per step: the device step record (nine FP64
 # audit and controller terms, the solver's exit state, the coupled-top books).
 STEP_RECORD_BYTES = 192
