@@ -170,7 +170,7 @@ __device__ __forceinline__ void cg64_body(const Cg64Args& a, const int bid, cons
   }
 }
 
-__global__ void __launch_bounds__(kCgBlock, 3) k_cg64(Cg64Args a) {
+__global__ void __launch_bounds__(kCgBlock, 2) k_cg64(Cg64Args a) {
   cg64_body(a, blockIdx.x, gridDim.x);
 }
 
@@ -346,7 +346,9 @@ __device__ __forceinline__ void cg64v_body(const Cg64Args& a, const int bid, con
   }
 }
 
-__global__ void __launch_bounds__(kCgBlock, 3) k_cg64v(Cg64Args a) {
+// Two blocks per SM: at three the 80-register cap spilled (24 bytes a thread
+// here, 52 in k_cg64) and the 512x512x128 FP64 solve took 251 ms against 236.
+__global__ void __launch_bounds__(kCgBlock, 2) k_cg64v(Cg64Args a) {
   cg64v_body(a, blockIdx.x, gridDim.x);
 }
 
