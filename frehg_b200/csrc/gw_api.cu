@@ -125,9 +125,13 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     d.sy = static_cast<long long>(H.nx + 2) * H.nz;
     d.ncell = H.ncell;
     d.ncol = H.ncol;
+    d.mz = fgw::div_magic(static_cast<unsigned>(H.nz));
+    d.mx2 = fgw::div_magic(static_cast<unsigned>(H.nx + 2));
     d.dx = desc->dx;
     d.dy = desc->dy;
     d.az = desc->dx * desc->dy;
+    d.idx = 1.0 / desc->dx;
+    d.idy = 1.0 / desc->dy;
     d.ss = desc->specific_storage;
     d.full3d = desc->use_full3d ? 1 : 0;
     d.pc = desc->pc_consistent ? 1 : 0;

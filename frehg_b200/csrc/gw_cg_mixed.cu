@@ -853,7 +853,10 @@ MixedArgs make_mixed_args(const Device& D, double atol, int maxit, double outer_
   a.part = D.cgpart;
   a.st = &D.out->cg;
   a.outer_rtol = outer_rtol;
-  a.inner_rtol = 1.0e-5;
+  // Reduction asked of every inner solve but the last: 1e-4 minimised the
+  // total inner iterations of the two corrections on slab crops (96^2 and
+  // 128^2 x 128 systems: 22, 24, 18 against 24, 26, 20 at 1e-5).
+  a.inner_rtol = 1.0e-4;
   a.atol = atol;
   a.max_inner = maxit;
   a.max_outer = max_outer;

@@ -28,8 +28,12 @@ struct Dims {
   long long ncell;       // (ny+2)(nx+2)nz
   long long ncol;        // (ny+2)(nx+2)
   double dx, dy, az;
+  double idx, idy;       // 1 / dx, 1 / dy
   double ss;             // specific storage
   int full3d, pc, harm, off, redistribute, terrain;
+  // Multipliers of the divisions by nz and by nx + 2 (div_magic); the
+  // domain's cell count is below 2^32.
+  unsigned long long mz, mx2;
 };
 
 // The coupled top's device state (GwCoupling), one per coupled domain: the
@@ -67,11 +71,23 @@ __host__ __device__ inline long long fidx(const Dims& d, int j, int i, int k) {
 __host__ __device__ inline long long col2(const Dims& d, int j, int i) {
   return static_cast<long long>(j) * d.nx2 + i;
 }
+// Division of n < 2^32 by an invariant divisor q >= 2 as the high word of
+// n * M with M = floor((2^64 - 1) / q) + 1 (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994):
+// n M / 2^64 = n / q + n e / 2^64 with 0 <= e < 1, and n q < 2^64 keeps the
+// second term below the distance from n / q up to the next integer.  M = 0
+// stands for q = 1.
+__host__ __device__ inline unsigned long long div_magic(unsigned q) {
+  return q < 2 ? 0ULL : ~0ULL / q + 1ULL;
+}
+__device__ inline unsigned div_by(unsigned long long n, unsigned long long m) {
+  return m == 0ULL ? static_cast<unsigned>(n) : static_cast<unsigned>(__umul64hi(n, m));
+}
 __device__ inline void unflatten(const Dims& d, long long c, int& j, int& i, int& k) {
-  const long long col = c / d.nz;
-  k = static_cast<int>(c - col * d.nz);
-  j = static_cast<int>(col / d.nx2);
-  i = static_cast<int>(col - static_cast<long long>(j) * d.nx2);
+  const unsigned col = div_by(static_cast<unsigned long long>(c), d.mz);
+  k = static_cast<int>(static_cast<unsigned>(c) - col * static_cast<unsigned>(d.nz));
+  j = static_cast<int>(div_by(col, d.mx2));
+  i = static_cast<int>(col - static_cast<unsigned>(j) * static_cast<unsigned>(d.nx2));
 }
 __device__ inline bool is_head(int code) { return code == kHead || code == kHydro; }
 

@@ -230,7 +230,6 @@ __device__ __forceinline__ void assemble_body(
     double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
     double* __restrict__ gzps, double* __restrict__ rhs, double* __restrict__ xw, const int bid,
     const int G) {
-  const double dx = d.dx, dy = d.dy;
   const double dtg = *dtgp;
   for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(G) * blockDim.x) {
@@ -285,18 +284,23 @@ __device__ __forceinline__ void assemble_body(
     const bool east = i == d.nx, west = i == 1, north = j == d.ny, south = j == 1;
     const bool top = (k == 0) || !au;
     const double volume = d.az * dzc;
-    double gxp = -kxp * dtg * cosxc / (dx * dx) * (axc * dx);
-    double gxm = -kxm * dtg * cosxw / (dx * dx) * (axw * dx);
-    double gyp = -kyp * dtg * cosyc / (dy * dy) * (ayc * dy);
-    double gym = -kym * dtg * cosys / (dy * dy) * (ays * dy);
+    // The reference's legs K dt cos / dx^2 * (A dx) and K dt / (dz dzf) *
+    // volume, and its RHS terms dt volume (...) / dz, with the lengths
+    // cancelled: K dt cos A (1/dx), K dt az / dzf and dt az (...) (equal up
+    // to rounding; three divisions per cell instead of nine).
+    double gxp = -kxp * dtg * cosxc * (axc * d.idx);
+    double gxm = -kxm * dtg * cosxw * (axw * d.idx);
+    double gyp = -kyp * dtg * cosyc * (ayc * d.idy);
+    double gym = -kym * dtg * cosys * (ays * d.idy);
     if (east && is_head(cxp)) gxp *= 2.0;
     if (west && is_head(cxm)) gxm *= 2.0;
     if (north && is_head(cyp)) gyp *= 2.0;
     if (south && is_head(cym)) gym *= 2.0;
+    const double kdt = dtg * d.az;  // dt * volume / dz
     double dzf = (k == d.nz - 1) ? 0.5 * dzc : 0.5 * (dzc + dzl);
-    const double gzp = -kzp * dtg / (dzc * dzf) * volume;
+    const double gzp = -kzp * kdt / dzf;
     dzf = top ? 0.5 * dzc : 0.5 * (dzc + dzu);
-    const double gzm = -kzm * dtg / (dzc * dzf) * volume;
+    const double gzm = -kzm * kdt / dzf;
 
     const double storage = chc + d.ss * wcnc / wcsc;
     double gct = storage * volume - (gxp + gxm + gyp + gym);
@@ -319,8 +323,8 @@ __device__ __forceinline__ void assemble_body(
     if (!top || dirichlet_top) gct -= gzm;
 
     double b = storage * hnc * volume;
-    b -= dtg * volume * kzp / dzc;
-    b += dtg * volume * kzm / dzc;
+    b -= kdt * kzp;
+    b += kdt * kzm;
     if (d.terrain) {
       double sg = (bote > botc_) ? 1.0 : -1.0;
       b += sg * dtg * axc * kxp * sinxc;
@@ -348,7 +352,7 @@ __device__ __forceinline__ void assemble_body(
       else b -= gym * hns;
     }
     if (k == d.nz - 1) {
-      if (botc == kFlux) b += dtg * volume * (vbot + kzp) / dzc;
+      if (botc == kFlux) b += kdt * (vbot + kzp);
       else if (botc == kHead) b -= gzp * vbot;
     }
     if (top && CPL) {  // Predictor.cpp:627-674
@@ -360,17 +364,17 @@ __device__ __forceinline__ void assemble_body(
         const double roomTop = fmax(0.0, (0.9999 * wcsc - wcnc) * dzc);
         const double take = fmin(avl, roomTop);
         const double qsup = -take / dtg;
-        b += -dtg * volume * (qsup + kzm) / dzc;
+        b += -kdt * (qsup + kzm);
       } else {
         double qtop = 0.0;
         if (topc == kFlux &&
             ((vtop > 0.0 && wcnc < wcsc) || (vtop < 0.0 && wcnc > wcrc)))
           qtop = vtop;
-        b += -dtg * volume * (qtop + kzm) / dzc;
+        b += -kdt * (qtop + kzm);
       }
     } else if (top) {
       if (topc == kHead) b -= gzm * vtop;
-      else if (topc == kFlux) b += -dtg * volume * (vtop + kzm) / dzc;
+      else if (topc == kFlux) b += -kdt * (vtop + kzm);
     }
     diag[c] = gct;
     gxps[c] = (!east && ae) ? gxp : 0.0;
@@ -451,27 +455,29 @@ __global__ void __launch_bounds__(kBlock, 4) k_faces(Dims d, Fields f, PassK pk,
 // Darcy flux of a lateral face from loaded values (computeFluxesImpl's x / y
 // branches): a = the face's lower-index flank, b = its upper one; lo_edge /
 // hi_edge mark the domain's boundary faces, whose BC code and value apply.
+// ih = 1 / dx (1 / dy): the head difference over the spacing (half of it at
+// the domain's edges) is a product with the reciprocal, equal up to rounding.
 struct LatFlux {
   double kca, kcb, ksa, ksb, hpa, hpb, wa, wb, wsa, wsb, bota, botb;
   double area, cosv, sinv;
   int8_t acta, actb;
 };
 
-__device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux& v, double h,
+__device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux& v, double ih,
                                   bool lo_edge, bool hi_edge, int code, double value, long long b,
                                   const double* __restrict__ hp) {
   double q;
   if (lo_edge) {
-    q = v.area * v.kcb * v.cosv * (v.hpb - v.hpa) / (0.5 * h);
+    q = v.area * v.kcb * v.cosv * (v.hpb - v.hpa) * (2.0 * ih);
     if (code == kNoFlux) q = 0.0;
     else if (code == kFlux) q = -value * v.area;
     return q;
   }
-  double kf, delta = h;
+  double kf, idelta = ih;
   const double sg = (v.botb > v.bota) ? 1.0 : -1.0;
   if (hi_edge) {
     kf = v.kca;
-    delta = 0.5 * h;
+    idelta = 2.0 * ih;
   } else {
     if (d.pc) {
       kf = d.harm ? face_harm(v.kca, v.ksa, 1.0, v.kcb, v.ksb, 1.0) : 0.5 * (v.kca + v.kcb);
@@ -480,7 +486,7 @@ __device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux&
     }
     if (!v.acta || !v.actb) kf = 0.0;
   }
-  q = v.area * (kf * v.cosv * (v.hpb - v.hpa) / delta + sg * kf * v.sinv);
+  q = v.area * (kf * v.cosv * (v.hpb - v.hpa) * idelta + sg * kf * v.sinv);
   if (!d.full3d && ((v.acta && v.wa < v.wsa) || (v.actb && v.wb < v.wsb))) q = 0.0;
   if (hi_edge) {
     if (code == kNoFlux) q = 0.0;
@@ -635,13 +641,13 @@ __device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
       const Flank a{vx.kca, vx.ksa, vx.wa, vx.wsa, vx.acta};
       const Flank b{vx.kcb, vx.ksb, vx.wb, vx.wsb, vx.actb};
       kx[c] = face_lat(d, a, b, i == 0, i == d.nx, codex);
-      qx[c] = flux_lat(d, f, vx, d.dx, i == 0, i == d.nx, codex, valx, e, hp);
+      qx[c] = flux_lat(d, f, vx, d.idx, i == 0, i == d.nx, codex, valx, e, hp);
     }
     if (doY) {
       const Flank a{vy.kca, vy.ksa, vy.wa, vy.wsa, vy.acta};
       const Flank b{vy.kcb, vy.ksb, vy.wb, vy.wsb, vy.actb};
       ky[c] = face_lat(d, a, b, j == 0, j == d.ny, codey);
-      qy[c] = flux_lat(d, f, vy, d.dy, j == 0, j == d.ny, codey, valy, n, hp);
+      qy[c] = flux_lat(d, f, vy, d.idy, j == 0, j == d.ny, codey, valy, n, hp);
     }
     if (doZ) {
       const long long fz = fidx(d, j, i, k), col = col2(d, j, i);
@@ -754,7 +760,7 @@ struct SplitIn {
 __device__ inline Split gradient_split(const Dims& d, const SplitIn& n, int k) {
   double dh0 = 0.0, dh1 = 0.0, dh2 = 0.0, dh3 = 0.0, dh4 = 0.0, dh5 = 0.0;
   if (d.full3d) {
-    const double idx = 1.0 / d.dx, idy = 1.0 / d.dy;
+    const double idx = d.idx, idy = d.idy;
     if (n.axp && n.kxp > 0.0) dh0 = (n.hxp - n.hc) * idx;
     if (n.axm && n.kxm > 0.0) dh1 = (n.hc - n.hxm) * idx;
     if (n.ayp && n.kyp > 0.0) dh2 = (n.hyp - n.hc) * idy;
@@ -848,12 +854,16 @@ __device__ __forceinline__ CellPost classify_cell(
     const double volume = d.az * n.dzc;
     if (before >= so.ts) {
       if (!d.off) {
+        // A cell exactly at theta_s (the whole saturated zone) has no excess:
+        // its split would send 0 each way, so it is not computed.
         const double excess = (before - so.ts) * volume;
-        const Split sp = gradient_split(d, n, k);
-        up = excess * sp.up;
-        dn = excess * sp.down;
-        adj -= excess - up - dn;
-        drop += excess - up - dn;
+        if (excess > 0.0) {
+          const Split sp = gradient_split(d, n, k);
+          up = excess * sp.up;
+          dn = excess * sp.down;
+          adj -= excess - up - dn;
+          drop += excess - up - dn;
+        }
         wout = so.ts;
       }
     } else {
@@ -1318,8 +1328,10 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
   walk_books<CPL>(d, lost, v, partial, nblk, bid);
 }
 
+// Four blocks per SM (three for the coupled form's vent state): without a
+// minimum ptxas settled on 64 / 80 registers with spills.
 template <bool CPL>
-__global__ void __launch_bounds__(kBlock) k_walk(Dims d, Fields f, double* wc,
+__global__ void __launch_bounds__(kBlock, CPL ? 3 : 4) k_walk(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ room,
                                                  const double* __restrict__ sup,
                                                  const double* __restrict__ sdn, double* qzf,

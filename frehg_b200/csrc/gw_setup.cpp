@@ -70,6 +70,10 @@ int build_host_domain(const frehg_gw_desc& d, HostDomain& o, std::string& err) {
       return FREHG_GW_EINVAL;
     }
   }
+  if (static_cast<long long>(d.nx + 2) * (d.ny + 2) * d.nz >= (1LL << 32)) {
+    err = "(nx+2)(ny+2)nz must stay below 2^32 cells";
+    return FREHG_GW_EINVAL;
+  }
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   o.nx = nx;
   o.ny = ny;

@@ -118,7 +118,7 @@ enum {
  * codes arrive per cell / per column rather than as type maps and polygons. */
 typedef struct frehg_gw_desc {
   int abi_version; /* FREHG_GW_ABI_VERSION */
-  int nx, ny, nz;
+  int nx, ny, nz;          /* (nx+2)(ny+2)nz below 2^32 */
   double dx, dy;
   const double* dz_layers; /* nz nominal layer thicknesses (Grid::dzK) */
   double dz_stretch;       /* domain.dz_stretch (scaled terrain layer weights) */
