@@ -34,11 +34,16 @@ sys.path.insert(0, ROOT)
 # Algorithmic bytes per active cell (interior cells, each array read or
 # written once per pass).
 ALG_BYTES_PER_CG_ITER = 128   # FP64 Jacobi-PCG iteration: 16 words
-ALG_BYTES_MIXED_INNER = 68    # FP32 inner iteration: stencil pass 8 words, update +
-                              # line solve 9 words (d, p, r, w, dinv, l in; d, r, z out)
-ALG_BYTES_MIXED_SWEEP = 80    # FP64 outer residual sweep: x, b, 4 coefficients, d, l,
-                              # dinv in; x, r, z, p out
-ALG_BYTES_MIXED_OUTER = 4     # d reset after each outer sweep that continues
+ALG_BYTES_MIXED_INNER = 64    # FP32 inner iteration: stencil pass 10 words (z, p_old,
+                              # d, diag, gxp, gyp, gzp in; p, w, d out; d += alpha p of
+                              # the previous iteration), update + line solve 6 words
+                              # (r, w, dinv, l in; r, z out)
+ALG_BYTES_MIXED_FIRST = 12    # less in each inner solve's first iteration (p = z:
+                              # neither p_old nor d)
+ALG_BYTES_MIXED_SWEEP = 76    # FP64 outer residual sweep: x, b, 4 coefficients, d, l,
+                              # dinv in; x, r, z out
+ALG_BYTES_MIXED_OUTER = 8     # per correction: its last update's p, read by the next
+                              # sweep, and the d reset
 ALG_BYTES_MIXED_INIT = 12     # b read for ||b||, d = 0 at entry (the assembly writes
                               # the starting iterate x = h^n)
 ALG_BYTES_FIXED = 536         # FP64 step outside the solve
@@ -46,7 +51,7 @@ METRIC = "cell-steps/s at 512x512x128"
 # DRAM bytes (read + write) per algorithmic byte of k_cg_mixed, from the ncu
 # capture summarised in profiles/ (256x256x128 slab, one steady-state launch);
 # scaled to the timed launches by their algorithmic bytes.
-MIXED_TRAFFIC_PER_ALG_BYTE = 1.022
+MIXED_TRAFFIC_PER_ALG_BYTE = 1.023
 # Bytes frehg_gw_step reads back per step: the device step record (nine FP64
 # audit and controller terms, the solver's exit state, the coupled-top books).
 STEP_RECORD_BYTES = 192
@@ -56,8 +61,9 @@ def mixed_alg_bytes(cells, inner, outer, launches):
     """Algorithmic bytes of `launches` k_cg_mixed launches that ran `inner`
     inner iterations and `outer` outer corrections in total."""
     sweeps = outer + launches
-    return cells * (ALG_BYTES_MIXED_INNER * inner + ALG_BYTES_MIXED_SWEEP * sweeps +
-                    ALG_BYTES_MIXED_OUTER * outer + ALG_BYTES_MIXED_INIT * launches)
+    return cells * (ALG_BYTES_MIXED_INNER * inner - ALG_BYTES_MIXED_FIRST * outer +
+                    ALG_BYTES_MIXED_SWEEP * sweeps + ALG_BYTES_MIXED_OUTER * outer +
+                    ALG_BYTES_MIXED_INIT * launches)
 
 
 def parse():

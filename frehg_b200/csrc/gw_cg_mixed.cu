@@ -29,9 +29,11 @@
 // so the per-column sweeps are bank-conflict free), let one thread per column
 // run the LDL^T sweeps, and write back coalesced.
 // Phase A (direction update + stencil product) is cell-parallel as in the
-// FP64 kernel.  FP32 inner traffic per cell and iteration: phase A 8 words
-// (z, p_old, diag, gxp, gyp, gzp in; p_new, w out), phase B 9 words (d, p, r,
-// w, dinv, l in; d, r, z out) -> 68 B.
+// FP64 kernel.  The correction update d += alpha p of an iteration is applied
+// by the next iteration's phase A, which reads that p as p_old anyway (the
+// last one of an inner solve by the outer pass).  FP32 inner traffic per cell
+// and iteration: phase A 10 words (z, p_old, d, diag, gxp, gyp, gzp in;
+// p_new, w, d out), phase B 6 words (r, w, dinv, l in; r, z out) -> 64 B.
 #include <cfloat>
 #include <cstring>
 
@@ -418,34 +420,53 @@ __device__ inline void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) =
 // lower/upper z legs of the group come from gzp[c-1] and the group's own).
 // (A (x + d))_c in FP64 with the FP64 coefficients, in the SpMV's fixed
 // summation order (ym, xm, zm, diag, zp, xp, yp).
-__device__ inline double outer_ax(const MixedArgs& a, const double* __restrict__ xo, long long c,
+// The correction of cell c with the inner solve's last update pal * pend
+// still pending (pal = 0: none, pend not read).
+__device__ inline float corr_at(const MixedArgs& a, const float* __restrict__ pend, float pal,
+                                long long c) {
+  float v = a.d32[c];
+  if (pal != 0.0f) v += pal * pend[c];
+  return v;
+}
+__device__ inline double x_at(const MixedArgs& a, const double* __restrict__ xo,
+                              const float* __restrict__ pend, float pal, long long c) {
+  return xo[c] + static_cast<double>(corr_at(a, pend, pal, c));
+}
+__device__ inline double outer_ax(const MixedArgs& a, const double* __restrict__ xo,
+                                  const float* __restrict__ pend, float pal, long long c,
                                   long long sx, long long sy) {
-  const double xc = xo[c] + static_cast<double>(a.d32[c]);
-  double ax = a.gyp[c - sy] * (xo[c - sy] + static_cast<double>(a.d32[c - sy]));
-  ax += a.gxp[c - sx] * (xo[c - sx] + static_cast<double>(a.d32[c - sx]));
-  ax += a.gzp[c - 1] * (xo[c - 1] + static_cast<double>(a.d32[c - 1]));
+  const double xc = x_at(a, xo, pend, pal, c);
+  double ax = a.gyp[c - sy] * x_at(a, xo, pend, pal, c - sy);
+  ax += a.gxp[c - sx] * x_at(a, xo, pend, pal, c - sx);
+  ax += a.gzp[c - 1] * x_at(a, xo, pend, pal, c - 1);
   ax += a.diag[c] * xc;
-  ax += a.gzp[c] * (xo[c + 1] + static_cast<double>(a.d32[c + 1]));
-  ax += a.gxp[c] * (xo[c + sx] + static_cast<double>(a.d32[c + sx]));
-  ax += a.gyp[c] * (xo[c + sy] + static_cast<double>(a.d32[c + sy]));
+  ax += a.gzp[c] * x_at(a, xo, pend, pal, c + 1);
+  ax += a.gxp[c] * x_at(a, xo, pend, pal, c + sx);
+  ax += a.gyp[c] * x_at(a, xo, pend, pal, c + sy);
   return ax;
 }
 
-template <int V>
+// FIRST (the first iteration of an inner solve): p = z, and p_old is not
+// read.  Otherwise p = z + bc p_old and d += pal p_old (the previous
+// iteration's update).
+template <int V, bool FIRST>
 __device__ inline double phase_a(const MixedArgs& a, float bc, const float* __restrict__ pold,
-                                 float* __restrict__ pnew, long long t0, long long stride) {
+                                 float* __restrict__ pnew, float pal, long long t0,
+                                 long long stride) {
   const long long N = a.d.ncell, sx = a.d.sx, sy = a.d.sy;
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   double pw = 0.0;
   if constexpr (V == 4) {
     for (long long q = t0; q < N / 4; q += stride) {
       const long long c = 4 * q;
-      const float4 z = ld4(a.z32 + c), p = ld4(pold + c);
-      const float4 zxm = ld4(a.z32 + c - sx), pxm = ld4(pold + c - sx);
-      const float4 zxp = ld4(a.z32 + c + sx), pxp = ld4(pold + c + sx);
-      const float4 zym = ld4(a.z32 + c - sy), pym = ld4(pold + c - sy);
-      const float4 zyp = ld4(a.z32 + c + sy), pyp = ld4(pold + c + sy);
-      const float pkm = a.z32[c - 1] + bc * pold[c - 1];
-      const float pkp = a.z32[c + 4] + bc * pold[c + 4];
+      const float4 z = ld4(a.z32 + c), p = FIRST ? zero4 : ld4(pold + c);
+      const float4 zxm = ld4(a.z32 + c - sx), pxm = FIRST ? zero4 : ld4(pold + c - sx);
+      const float4 zxp = ld4(a.z32 + c + sx), pxp = FIRST ? zero4 : ld4(pold + c + sx);
+      const float4 zym = ld4(a.z32 + c - sy), pym = FIRST ? zero4 : ld4(pold + c - sy);
+      const float4 zyp = ld4(a.z32 + c + sy), pyp = FIRST ? zero4 : ld4(pold + c + sy);
+      const float pkm = FIRST ? a.z32[c - 1] : a.z32[c - 1] + bc * pold[c - 1];
+      const float pkp = FIRST ? a.z32[c + 4] : a.z32[c + 4] + bc * pold[c + 4];
+      float4 dd = FIRST ? zero4 : ld4(a.d32 + c);
       const float4 dg = ld4(a.diag32 + c);
       const float4 gx = ld4(a.gxp32 + c), gxm = ld4(a.gxp32 + c - sx);
       const float4 gy = ld4(a.gyp32 + c), gym = ld4(a.gyp32 + c - sy);
@@ -466,23 +487,34 @@ __device__ inline double phase_a(const MixedArgs& a, float bc, const float* __re
             dg.w * P.w + gz.w * pkp + gx.w * (zxp.w + bc * pxp.w) + gy.w * (zyp.w + bc * pyp.w);
       st4(pnew + c, P);
       st4(a.w32 + c, W);
+      if (!FIRST) {
+        dd.x += pal * p.x;
+        dd.y += pal * p.y;
+        dd.z += pal * p.z;
+        dd.w += pal * p.w;
+        st4(a.d32 + c, dd);
+      }
       pw += static_cast<double>(P.x) * W.x;
       pw += static_cast<double>(P.y) * W.y;
       pw += static_cast<double>(P.z) * W.z;
       pw += static_cast<double>(P.w) * W.w;
     }
   } else {
+    auto pv = [&](long long m) { return FIRST ? a.z32[m] : a.z32[m] + bc * pold[m]; };
     for (long long c = t0; c < N; c += stride) {
-      const float pc = a.z32[c] + bc * pold[c];
-      float wv = a.gyp32[c - sy] * (a.z32[c - sy] + bc * pold[c - sy]);
-      wv += a.gxp32[c - sx] * (a.z32[c - sx] + bc * pold[c - sx]);
-      wv += a.gzp32[c - 1] * (a.z32[c - 1] + bc * pold[c - 1]);
+      const float po = FIRST ? 0.0f : pold[c];
+      const float dv = FIRST ? 0.0f : a.d32[c];
+      const float pc = pv(c);
+      float wv = a.gyp32[c - sy] * pv(c - sy);
+      wv += a.gxp32[c - sx] * pv(c - sx);
+      wv += a.gzp32[c - 1] * pv(c - 1);
       wv += a.diag32[c] * pc;
-      wv += a.gzp32[c] * (a.z32[c + 1] + bc * pold[c + 1]);
-      wv += a.gxp32[c] * (a.z32[c + sx] + bc * pold[c + sx]);
-      wv += a.gyp32[c] * (a.z32[c + sy] + bc * pold[c + sy]);
+      wv += a.gzp32[c] * pv(c + 1);
+      wv += a.gxp32[c] * pv(c + sx);
+      wv += a.gyp32[c] * pv(c + sy);
       pnew[c] = pc;
       a.w32[c] = wv;
+      if (!FIRST) a.d32[c] = dv + pal * po;
       pw += static_cast<double>(pc) * wv;
     }
   }
@@ -531,10 +563,25 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
 
   double bnorm = 0.0, rnorm = 0.0;
   int total = 0, outer = 0, reason = 0, final_buf = 0;
+  // The last inner iteration's update d += s_pal * p_(s_pbuf), applied by
+  // the next phase A or outer pass (s_pal = 0: none).  Shared rather than
+  // loop-carried registers: those spilled the 80-register budget of three
+  // blocks per SM.  Thread 0 writes them only after a grid sync that follows
+  // every read of the old values; the next reads follow another grid sync.
+  __shared__ float s_pal;
+  __shared__ int s_pbuf;
+  if (threadIdx.x == 0) {
+    s_pal = 0.0f;
+    s_pbuf = 0;
+  }
+  __syncthreads();
   for (int o = 0;; ++o) {
+    const float pal = s_pal;
+    const float* __restrict__ pend = s_pbuf ? a.p1 : a.p0;
     const double* __restrict__ xo = (o & 1) ? a.x1 : a.x0;
     double* __restrict__ xn = (o & 1) ? a.x0 : a.x1;
-    // Outer pass: x_new = x + d, r = b - A x_new (FP64), r32, z = T^-1 r32.
+    // Outer pass: x_new = x + d (with the pending update), r = b - A x_new
+    // (FP64), r32, z = T^-1 r32.
     double rn2 = 0.0, zz = 0.0, zr = 0.0;
     if constexpr (E > 0) {
       for (long long col = gwarp; col < d.ncol; col += nwarp) {
@@ -548,8 +595,8 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
           xv[e] = 0.0;
           if (k0 + e < nz) {
             const long long c = cb + k0 + e;
-            const double rr = a.b[c] - outer_ax(a, xo, c, sx, sy);
-            xv[e] = xo[c] + static_cast<double>(a.d32[c]);
+            const double rr = a.b[c] - outer_ax(a, xo, pend, pal, c, sx, sy);
+            xv[e] = x_at(a, xo, pend, pal, c);
             rn2 += rr * rr;
             rv[e] = static_cast<float>(rr);
           }
@@ -564,11 +611,9 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
             zz += static_cast<double>(zv[e]) * zv[e];
             zr += static_cast<double>(zv[e]) * rv[e];
           }
-          lk[e] = 0.0f;
         }
         st_col<E>(a.r32, cb, lane, nz, vec, rv);
         st_col<E>(a.z32, cb, lane, nz, vec, zv);
-        st_col<E>(a.p0, cb, lane, nz, vec, lk);
       }
     } else {
     for (long long t = bid; t < ntiles; t += G) {
@@ -578,16 +623,8 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
       for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
         const long long c = base + f;
         const int col = f / nz, k = f - col * nz;
-        const double xc = xo[c] + static_cast<double>(a.d32[c]);
-        double ax = a.gyp[c - sy] * (xo[c - sy] + static_cast<double>(a.d32[c - sy]));
-        ax += a.gxp[c - sx] * (xo[c - sx] + static_cast<double>(a.d32[c - sx]));
-        ax += a.gzp[c - 1] * (xo[c - 1] + static_cast<double>(a.d32[c - 1]));
-        ax += a.diag[c] * xc;
-        ax += a.gzp[c] * (xo[c + 1] + static_cast<double>(a.d32[c + 1]));
-        ax += a.gxp[c] * (xo[c + sx] + static_cast<double>(a.d32[c + sx]));
-        ax += a.gyp[c] * (xo[c + sy] + static_cast<double>(a.d32[c + sy]));
-        const double rr = a.b[c] - ax;
-        xn[c] = xc;
+        const double rr = a.b[c] - outer_ax(a, xo, pend, pal, c, sx, sy);
+        xn[c] = x_at(a, xo, pend, pal, c);
         rn2 += rr * rr;
         const float r32 = static_cast<float>(rr);
         a.r32[c] = r32;
@@ -605,7 +642,6 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
         const int col = f / nz, k = f - col * nz;
         const float z = s_z[col * nzp + k];
         a.z32[c] = z;
-        a.p0[c] = 0.0f;
         zz += static_cast<double>(z) * z;
         zr += static_cast<double>(z) * s_r[col * nzp + k];
       }
@@ -639,6 +675,7 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
       break;
     }
     ++outer;
+    if (threadIdx.x == 0) s_pal = 0.0f;  // the outer pass applied it
     for (long long c = t0; c < N; c += stride) a.d32[c] = 0.0f;
     // Inner FP32 PCG on A d = r32.
     // Each inner solve reduces its start by inner_rtol, the last one only as
@@ -651,7 +688,8 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
       const float bc = (i == 0) ? 0.0f : static_cast<float>(beta / betaold);
       const float* __restrict__ pold = (i & 1) ? a.p1 : a.p0;
       float* __restrict__ pnew = (i & 1) ? a.p0 : a.p1;
-      const double pw = phase_a<V>(a, bc, pold, pnew, t0, stride);
+      const double pw = (i == 0) ? phase_a<V, true>(a, bc, pold, pnew, 0.0f, t0, stride)
+                                 : phase_a<V, false>(a, bc, pold, pnew, s_pal, t0, stride);
       s = block_sum_all(pw);
       if (threadIdx.x == 0) q0[bid] = s;
       if (!grid_sync(a.st, G)) return;
@@ -660,26 +698,24 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
       const float al = static_cast<float>(beta / dpi);
       betaold = beta;
       ++total;
+      if (threadIdx.x == 0) {  // d += al p_new, applied by the next phase A or outer pass
+        s_pal = al;
+        s_pbuf = (i & 1) ? 0 : 1;
+      }
       zz = 0.0;
       zr = 0.0;
       if constexpr (E > 0) {
         for (long long col = gwarp; col < d.ncol; col += nwarp) {
           const long long cb = col * nz;
           const int k0 = lane * E;
-          float pn[E], wv[E], rv[E], dv[E], lk[E], di[E], zv[E];
-          ld_col<E>(pnew, cb, lane, nz, vec, pn);
+          float wv[E], rv[E], lk[E], di[E], zv[E];
           ld_col<E>(a.w32, cb, lane, nz, vec, wv);
           ld_col<E>(a.r32, cb, lane, nz, vec, rv);
-          ld_col<E>(a.d32, cb, lane, nz, vec, dv);
           ld_col<E>(a.l32, cb, lane, nz, vec, lk);
           ld_col<E>(a.dinv32, cb, lane, nz, vec, di);
 #pragma unroll
-          for (int e = 0; e < E; ++e) {
-            dv[e] += al * pn[e];
-            rv[e] -= al * wv[e];
-          }
+          for (int e = 0; e < E; ++e) rv[e] -= al * wv[e];
           warp_column_solve<E>(lk, di, lane, nz, rv, zv);
-          st_col<E>(a.d32, cb, lane, nz, vec, dv);
           st_col<E>(a.r32, cb, lane, nz, vec, rv);
           st_col<E>(a.z32, cb, lane, nz, vec, zv);
 #pragma unroll
@@ -699,17 +735,12 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
           for (int f = 4 * threadIdx.x; f < ncells; f += 4 * blockDim.x) {
             const long long c = base + f;
             const int col = f / nz, k = f - col * nz;
-            const float4 pn = ld4(pnew + c), w = ld4(a.w32 + c);
-            float4 dd = ld4(a.d32 + c), r = ld4(a.r32 + c);
-            dd.x += al * pn.x;
-            dd.y += al * pn.y;
-            dd.z += al * pn.z;
-            dd.w += al * pn.w;
+            const float4 w = ld4(a.w32 + c);
+            float4 r = ld4(a.r32 + c);
             r.x -= al * w.x;
             r.y -= al * w.y;
             r.z -= al * w.z;
             r.w -= al * w.w;
-            st4(a.d32 + c, dd);
             st4(a.r32 + c, r);
             float* sr = s_r + col * nzp + k;
             sr[0] = r.x;
@@ -721,7 +752,6 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
           for (int f = threadIdx.x; f < ncells; f += blockDim.x) {
             const long long c = base + f;
             const int col = f / nz, k = f - col * nz;
-            a.d32[c] += al * pnew[c];
             const float r = a.r32[c] - al * a.w32[c];
             a.r32[c] = r;
             s_r[col * nzp + k] = r;
