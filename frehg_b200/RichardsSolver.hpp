@@ -145,6 +145,22 @@ class RichardsSolver {
     return a;
   }
 
+  /// RichardsSolver::attachScalar (baroclinic on) / attachTemperature /
+  /// setDensityCoefficients (RichardsSolver.hpp:191-225): the scalars'
+  /// device fields are allocated here; hand them over before each step with
+  /// setScalar (host) or write scalarPointer (device).
+  void attachDensity(bool saline, bool thermal, const frehg_gw_density& c) {
+    check(frehg_gw_attach_density(h_, saline ? 1 : 0, thermal ? 1 : 0, &c));
+  }
+  void setScalar(int which, const double* host) { check(frehg_gw_set_scalar(h_, which, host)); }
+  double* scalarPointer(int which) { return frehg_gw_scalar_ptr(h_, which); }
+  /// densityRatio / viscosityRatio / densityRatioFaceY / densityRatioFaceZ
+  /// (RichardsSolver.hpp:392-400), in the ABI shapes.
+  std::vector<double> densityRatio() const { return field(FREHG_GW_FIELD_RHO); }
+  std::vector<double> viscosityRatio() const { return field(FREHG_GW_FIELD_VISC); }
+  std::vector<double> densityRatioFaceY() const { return field(FREHG_GW_FIELD_RHO_Y); }
+  std::vector<double> densityRatioFaceZ() const { return field(FREHG_GW_FIELD_RHO_Z); }
+
  private:
   static void check(int rc) {
     if (rc != FREHG_GW_OK) throw FatalError(rc, frehg_gw_last_error());

@@ -20,6 +20,8 @@ FIELD = {
     "wcn": 8, "dz3d": 9, "bot3d": 10, "ax": 11, "ay": 12, "sinx": 13, "cosx": 14,
     "siny": 15, "cosy": 16, "vloss": 17,
     "win_x": 18, "win_y": 19, "win_z": 20, "win_vent": 21,
+    "rho": 22, "visc": 23, "rho_x": 24, "rho_y": 25, "rho_z": 26, "visc_x": 27, "visc_y": 28,
+    "visc_z": 29,
 }
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -79,6 +81,17 @@ class CoupledAudit(C.Structure):
 class Coupling(C.Structure):
     _fields_ = [("min_depth", C.c_double), ("vent_all", C.c_int), ("book_bounce", C.c_int),
                 ("field", C.c_void_p * 8)]
+
+
+class Density(C.Structure):
+    """frehg_gw_density: the density-coupling coefficients."""
+    _fields_ = [("beta_saline", C.c_double), ("beta_saline_visc", C.c_double),
+                ("thermal_expansion", C.c_double), ("reference_temperature", C.c_double),
+                ("reallocation_gradient", C.c_int)]
+
+
+# FREHG_GW_SCALAR_*: the density coupling's scalars.
+SCALARS = {"salt": 0, "salt_surf": 1, "temp": 2, "temp_surf": 3}
 
 
 class CouplerOpts(C.Structure):
@@ -160,12 +173,17 @@ def make_desc(cfg: GwConfig, ras: Rasterized = None) -> Tuple[GwDesc, list]:
     return desc, keep
 
 
+X_FACES = ("qx", "kx", "ax", "sinx", "cosx", "win_x", "rho_x", "visc_x")
+Y_FACES = ("qy", "ky", "ay", "siny", "cosy", "win_y", "rho_y", "visc_y")
+Z_FACES = ("qz", "kz", "win_z", "rho_z", "visc_z")
+
+
 def field_shape(field: str, nx: int, ny: int, nz: int) -> Tuple[int, ...]:
-    if field in ("qx", "kx", "ax", "sinx", "cosx", "win_x"):
+    if field in X_FACES:
         return (ny, nx + 1, nz)
-    if field in ("qy", "ky", "ay", "siny", "cosy", "win_y"):
+    if field in Y_FACES:
         return (ny + 1, nx, nz)
-    if field in ("qz", "kz", "win_z"):
+    if field in Z_FACES:
         return (ny, nx, nz + 1)
     if field == "win_vent":
         return (ny, nx)
@@ -175,11 +193,11 @@ def field_shape(field: str, nx: int, ny: int, nz: int) -> Tuple[int, ...]:
 def interior_from_halo(field: str, full: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
     """Slice a reference halo-layout field ((ny+2, nx+2, nz[+1])) to the ABI
     shape of :func:`field_shape`."""
-    if field in ("qx", "kx", "ax", "sinx", "cosx", "win_x"):
+    if field in X_FACES:
         return full[1:ny + 1, 0:nx + 1, :nz]
-    if field in ("qy", "ky", "ay", "siny", "cosy", "win_y"):
+    if field in Y_FACES:
         return full[0:ny + 1, 1:nx + 1, :nz]
-    if field in ("qz", "kz", "win_z"):
+    if field in Z_FACES:
         return full[1:ny + 1, 1:nx + 1, :nz + 1]
     if field == "win_vent":
         return full[1:ny + 1, 1:nx + 1]

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libfrehg_gw.so")
 SOURCES = ["gw_api.cu", "gw_kernels.cu", "gw_cg.cu", "gw_cg_mixed.cu", "gw_batch.cu", "gw_serve.cu",
-           "gw_couple.cu",
+           "gw_couple.cu", "gw_density.cu",
            "gw_setup.cpp"]
 HEADERS = ["gw_device.cuh", "gw_internal.h", "gw_setup.h", "gw_coop.cuh", "gw_handle.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

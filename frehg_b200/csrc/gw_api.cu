@@ -5,6 +5,7 @@
 // frehg_gw_last_error().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -392,6 +393,7 @@ int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc)
         hh[fgw::cidx(d, j, i, k)] = head[q];
         ww[fgw::cidx(d, j, i, k)] = wc[q];
       }
+  if (D.f.baro) fgw::launch_baro(D);  // refreshDerivedState (RichardsSolver.cpp:880-890)
   for (int b = 0; b < 2; ++b) {
     CUDA_TRY(cudaMemcpy(D.h[b], hh.data(), d.ncell * sizeof(double), cudaMemcpyHostToDevice),
              "set_state");
@@ -435,6 +437,9 @@ cudaError_t enqueue_predictor(frehg_gw_handle* h) {
   fgw::Device& D = h->D;
   double* hn = D.h[D.cur];
   double* wcn = D.wc[D.cur];
+  // the density ratios first, so the hydrostatic edge ghosts see this step's
+  // (RichardsSolver.cpp:739-746)
+  if (D.f.baro) fgw::launch_baro(D);
   fgw::launch_ghosts(D, hn, wcn);
   if (D.f.cpl) fgw::launch_cpl_mode(D, hn);
   fgw::launch_closure_pred(D, hn);
@@ -569,10 +574,12 @@ size_t frehg_gw_field_size(const frehg_gw_handle* h, int field) {
       return (ny + 1) * nx * nz;
     case FREHG_GW_FIELD_QZ: case FREHG_GW_FIELD_KZ: case FREHG_GW_FIELD_WINDOW_Z:
       return ny * nx * (nz + 1);
-    case FREHG_GW_FIELD_WINDOW_X:
+    case FREHG_GW_FIELD_WINDOW_X: case FREHG_GW_FIELD_RHO_X: case FREHG_GW_FIELD_VISC_X:
       return ny * (nx + 1) * nz;
-    case FREHG_GW_FIELD_WINDOW_Y:
+    case FREHG_GW_FIELD_WINDOW_Y: case FREHG_GW_FIELD_RHO_Y: case FREHG_GW_FIELD_VISC_Y:
       return (ny + 1) * nx * nz;
+    case FREHG_GW_FIELD_RHO_Z: case FREHG_GW_FIELD_VISC_Z:
+      return ny * nx * (nz + 1);
     case FREHG_GW_FIELD_WINDOW_VENT:
       return ny * nx;
     default:
@@ -609,7 +616,21 @@ int frehg_gw_get_field(frehg_gw_handle* h, int field, double* out) {
     case FREHG_GW_FIELD_WINDOW_Y: src = D.win_y; kind = 2; break;
     case FREHG_GW_FIELD_WINDOW_Z: src = D.win_z; kind = 3; break;
     case FREHG_GW_FIELD_WINDOW_VENT: src = D.win_vent; kind = 4; break;
+    case FREHG_GW_FIELD_RHO: src = D.rrho; break;
+    case FREHG_GW_FIELD_VISC: src = D.rvisc; break;
+    case FREHG_GW_FIELD_RHO_X: src = D.rxp; kind = 1; break;
+    case FREHG_GW_FIELD_VISC_X: src = D.vxp; kind = 1; break;
+    case FREHG_GW_FIELD_RHO_Y: src = D.ryp; kind = 2; break;
+    case FREHG_GW_FIELD_VISC_Y: src = D.vyp; kind = 2; break;
+    case FREHG_GW_FIELD_RHO_Z: src = D.rzp; kind = 3; break;
+    case FREHG_GW_FIELD_VISC_Z: src = D.vzp; kind = 3; break;
     default: return fail(FREHG_GW_EINVAL, "unknown field");
+  }
+  if (!src && field >= FREHG_GW_FIELD_RHO) {  // no density coupling: every ratio is 1
+    const size_t cnt = static_cast<size_t>(kind == 1 ? d.nx + 1 : d.nx) *
+                       (kind == 2 ? d.ny + 1 : d.ny) * (kind == 3 ? d.nz + 1 : d.nz);
+    std::fill(out, out + cnt, 1.0);
+    return FREHG_GW_OK;
   }
   if (!src) return fail(FREHG_GW_ESTATE, "get_field: transport window not enabled");
   if (kind == 4) {  // a column field, (ny+2)(nx+2) on the device

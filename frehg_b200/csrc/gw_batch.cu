@@ -505,6 +505,8 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
       return fail(FREHG_GW_EUNSUPPORTED, "batch: a coupled-top member steps on its own");
     if (members[i]->D.win_x)
       return fail(FREHG_GW_EUNSUPPORTED, "batch: a member with a transport window steps on its own");
+    if (members[i]->D.f.baro)
+      return fail(FREHG_GW_EUNSUPPORTED, "batch: a member with density coupling steps on its own");
     for (int j = 0; j < i; ++j)
       if (members[j] == members[i]) return fail(FREHG_GW_EINVAL, "batch: member given twice");
   }
@@ -548,6 +550,8 @@ int frehg_gw_batch_set_members(frehg_gw_batch* b, frehg_gw_handle* const* member
       return fail(FREHG_GW_EUNSUPPORTED, "batch: a coupled-top member steps on its own");
     if (members[i]->D.win_x)
       return fail(FREHG_GW_EUNSUPPORTED, "batch: a member with a transport window steps on its own");
+    if (members[i]->D.f.baro)
+      return fail(FREHG_GW_EUNSUPPORTED, "batch: a member with density coupling steps on its own");
   }
   const cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return cuda_fail(e, "batch: set members");

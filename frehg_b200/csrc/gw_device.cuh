@@ -49,6 +49,16 @@ struct CplDev {
   int8_t* cmode;
 };
 
+// Density coupling (Baroclinic.cpp): the cell density ratio and the face
+// means of the density and viscosity ratios, written at the start of every
+// step from the attached scalars (halo layouts: x / y faces like qx / qy,
+// z faces like qzF).  Kernels reach them through Fields::baro, null without
+// an attached scalar (every ratio is then exactly 1).
+struct BaroDev {
+  const double *rrho, *rxp, *ryp, *rzp, *vxp, *vyp, *vzp;
+  int dgrad;  // the post-allocation split against the face r (not 1)
+};
+
 // Device pointers of one domain (see gw_internal.h for ownership).
 struct Fields {
   // soil (halo layout, mirrored ghosts)
@@ -60,6 +70,7 @@ struct Fields {
   const int *topc, *botc, *xmc, *xpc, *ymc, *ypc;
   const double *topv, *botv, *xmv, *xpv, *ymv, *ypv;
   const CplDev* cpl;  // coupled top, null when off
+  const BaroDev* baro;  // density coupling, null when off
 };
 
 __host__ __device__ inline long long cidx(const Dims& d, int j, int i, int k) {

@@ -96,6 +96,17 @@ struct Device {
   // layouts, the walks' path records (qzF layout), vented volume per column
   double *win_x = nullptr, *win_y = nullptr, *win_z = nullptr, *pcorr = nullptr,
          *win_vent = nullptr;  // per-cell saturation flag of the post-allocation snapshot
+  // density coupling (null until attached): the scalars (FREHG_GW_SCALAR_*
+  // order, halo layouts; null when that scalar is not attached), the ratio
+  // fields (cells, x / y faces like qx / qy, z faces like qzF) and their
+  // coefficients
+  double* scal[4] = {};
+  double *rrho = nullptr, *rvisc = nullptr, *rxp = nullptr, *ryp = nullptr, *rzp = nullptr,
+         *vxp = nullptr, *vyp = nullptr, *vzp = nullptr;
+  BaroDev* baro_dev = nullptr;  // the kernels' copy of baro_host (f.baro when attached)
+  BaroDev baro_host{};
+  int saline = 0, thermal = 0;
+  double beta_s = 0.0, beta_sv = 0.0, beta_t = 0.0, t_ref = 0.0;
   // linear system: coefficients and vectors carry a zero margin of sy cells
   // on both ends; the pointers below point at cell 0.
   double *diag = nullptr, *gxp = nullptr, *gyp = nullptr, *gzp = nullptr, *rhs = nullptr;
@@ -138,6 +149,8 @@ void launch_finalize(const Device& D, double* wc_out, double co_max);
 void launch_step_info(const Device& D, double dq_grow, double dq_shrink, double dt_min,
                       double dt_max);
 void launch_volume(const Device& D, const double* wc);
+// Density coupling: the cell and face ratios from the attached scalars.
+void launch_baro(const Device& D);
 // Coupled top: exchange modes (before the predictor), bookkeeping (after the
 // corrector's fluxes), and the coupler window's opening and seepage.
 void launch_cpl_mode(const Device& D, const double* hn);

@@ -25,26 +25,29 @@ namespace fgw {
 
 namespace {
 
-__device__ inline double ghost_head(int code, double value, double interior, double zc) {
-  // enforceHeadBc / ghostHead, uncoupled (src/gw/Predictor.cpp:66-87).
+__device__ inline double ghost_head(int code, double value, double interior, double zc,
+                                    double r) {
+  // enforceHeadBc / ghostHead, uncoupled (src/gw/Predictor.cpp:66-87); r =
+  // the edge face's density ratio.
   if (code == kHead) return value;
-  if (code == kHydro) return value - zc;
+  if (code == kHydro) return (value - zc) * r;
   return interior;
 }
 
-// ghostHead with the coupled rule (Predictor.cpp:80-83, density ratio 1): a
-// hydrostatic stage above the edge column's bed follows the live surface
-// there, (bed - zc) + depth.  cc = the edge column.
+// ghostHead with the coupled rule (Predictor.cpp:80-83): a hydrostatic stage
+// above the edge column's bed follows the live surface there, (bed - zc) r +
+// depth (depth r on the plus sides).  cc = the edge column.
 __device__ inline double ghost_head_at(const Dims& d, const Fields& f, int code, double value,
-                                       double interior, double zc, long long cc) {
+                                       double interior, double zc, long long cc, double r,
+                                       bool plus) {
   if (code == kHydro && (f.cpl != nullptr)) {
     const double bed = f.cpl->bath[cc];
     if (value > bed) {
-      const double hydro = bed - zc;
-      return hydro + f.cpl->dept[cc];
+      const double hydro = (bed - zc) * r;
+      return plus ? hydro + f.cpl->dept[cc] * r : hydro + f.cpl->dept[cc];
     }
   }
-  return ghost_head(code, value, interior, zc);
+  return ghost_head(code, value, interior, zc, r);
 }
 
 struct SumOp {
@@ -88,6 +91,7 @@ __device__ __forceinline__ void ghosts_body(Dims d, Fields f, double* h, double*
     long long g, c, cc;
     int code;
     double val;
+    bool plus, xs;
     if (t < nxg) {
       const int side = static_cast<int>(t / (static_cast<long long>(d.ny) * d.nz));
       const long long rem = t - static_cast<long long>(side) * d.ny * d.nz;
@@ -98,6 +102,8 @@ __device__ __forceinline__ void ghosts_body(Dims d, Fields f, double* h, double*
       cc = col2(d, j, ii);
       code = side == 0 ? f.xmc[cc] : f.xpc[cc];
       val = side == 0 ? f.xmv[cc] : f.xpv[cc];
+      plus = side != 0;
+      xs = true;
     } else {
       const long long u = t - nxg;
       const int side = static_cast<int>(u / (static_cast<long long>(d.nx) * d.nz));
@@ -109,8 +115,13 @@ __device__ __forceinline__ void ghosts_body(Dims d, Fields f, double* h, double*
       cc = col2(d, jj, i);
       code = side == 0 ? f.ymc[cc] : f.ypc[cc];
       val = side == 0 ? f.ymv[cc] : f.ypv[cc];
+      plus = side != 0;
+      xs = false;
     }
-    if (h) h[g] = ghost_head_at(d, f, code, val, h[c], f.bot[c] + 0.5 * f.dz[c], cc);
+    // the edge face's density ratio: slot g on the minus sides, c on the plus
+    const long long fs = plus ? c : g;
+    const double r = (f.baro == nullptr) ? 1.0 : xs ? f.baro->rxp[fs] : f.baro->ryp[fs];
+    if (h) h[g] = ghost_head_at(d, f, code, val, h[c], f.bot[c] + 0.5 * f.dz[c], cc, r, plus);
     if (wc) wc[g] = is_head(code) ? f.wcs[c] : wc[c];
   }
 }
@@ -184,7 +195,9 @@ __device__ __forceinline__ void closure_corr_body(Dims d, Fields f,
       const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
       const int code = i == 0 ? f.xmc[cc] : f.xpc[cc];
       const double val = i == 0 ? f.xmv[cc] : f.xpv[cc];
-      hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc);
+      // the edge face's density ratio: the ghost's slot west, the edge cell's east
+      const double r = (f.baro == nullptr) ? 1.0 : f.baro->rxp[i == 0 ? c : ci];
+      hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc, r, i != 0);
     } else if (iin && (j == 0 || j == d.ny + 1)) {
       const long long ci = (j == 0) ? c + d.sy : c - d.sy;
       const long long cc = col2(d, j == 0 ? 1 : d.ny, i);
@@ -192,7 +205,8 @@ __device__ __forceinline__ void closure_corr_body(Dims d, Fields f,
       const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
       const int code = j == 0 ? f.ymc[cc] : f.ypc[cc];
       const double val = j == 0 ? f.ymv[cc] : f.ypv[cc];
-      hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc);
+      const double r = (f.baro == nullptr) ? 1.0 : f.baro->ryp[j == 0 ? c : ci];
+      hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc, r, j != 0);
     }
     const KrParts p = vg_kr_parts(so, hv);
     hp[c] = hv;
@@ -222,7 +236,7 @@ __global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
 // (the same expression on the same data, so the stored matrix is the
 // reference's up to the rounding of its z legs).  Legs toward an inactive
 // cell or out of the domain are stored as 0 (PETSc ignores column -1).
-template <bool CPL>
+template <bool CPL, bool BARO>
 __device__ __forceinline__ void assemble_body(
     Dims d, Fields f, const double* __restrict__ kxf, const double* __restrict__ kyf,
     const double* __restrict__ kzff, const double* __restrict__ hn,
@@ -272,6 +286,26 @@ __device__ __forceinline__ void assemble_body(
       sinyc = f.siny[c];
       sinys = f.siny[cs];
     }
+    // Density coupling (the reference's assembly with its ratios): r v of each
+    // face for the legs, the cell's r_rho for the storage; 1 without.
+    double bxc = 1.0, bxw = 1.0, byc = 1.0, bys = 1.0, rzpf = 1.0, rzmf = 1.0;
+    double vzpf = 1.0, vzmf = 1.0, rxc = 1.0, rxw = 1.0, ryc = 1.0, rys = 1.0, rrc = 1.0;
+    if (BARO) {
+      const BaroDev& B = *f.baro;
+      rxc = B.rxp[c];
+      rxw = B.rxp[cw];
+      ryc = B.ryp[c];
+      rys = B.ryp[cs];
+      bxc = rxc * B.vxp[c];
+      bxw = rxw * B.vxp[cw];
+      byc = ryc * B.vyp[c];
+      bys = rys * B.vyp[cs];
+      rzmf = B.rzp[fz];
+      rzpf = B.rzp[fz + 1];
+      vzmf = B.vzp[fz];
+      vzpf = B.vzp[fz + 1];
+      rrc = B.rrho[c];
+    }
     if (xw) xw[c] = ac ? hnc : 0.0;  // the mixed solve's starting iterate
     if (!ac) {
       diag[c] = 1.0;
@@ -292,17 +326,25 @@ __device__ __forceinline__ void assemble_body(
     double gxm = -kxm * dtg * cosxw * (axw * d.idx);
     double gyp = -kyp * dtg * cosyc * (ayc * d.idy);
     double gym = -kym * dtg * cosys * (ays * d.idy);
+    if (BARO) {
+      gxp *= bxc;
+      gxm *= bxw;
+      gyp *= byc;
+      gym *= bys;
+    }
     if (east && is_head(cxp)) gxp *= 2.0;
     if (west && is_head(cxm)) gxm *= 2.0;
     if (north && is_head(cyp)) gyp *= 2.0;
     if (south && is_head(cym)) gym *= 2.0;
     const double kdt = dtg * d.az;  // dt * volume / dz
+    // the z faces' K with their r v (and the gravity terms' r^2 v)
+    const double kzpb = BARO ? kzp * rzpf * vzpf : kzp, kzmb = BARO ? kzm * rzmf * vzmf : kzm;
     double dzf = (k == d.nz - 1) ? 0.5 * dzc : 0.5 * (dzc + dzl);
-    const double gzp = -kzp * kdt / dzf;
+    const double gzp = -kzpb * kdt / dzf;
     dzf = top ? 0.5 * dzc : 0.5 * (dzc + dzu);
-    const double gzm = -kzm * kdt / dzf;
+    const double gzm = -kzmb * kdt / dzf;
 
-    const double storage = chc + d.ss * wcnc / wcsc;
+    const double storage = BARO ? (chc + d.ss * wcnc / wcsc) * rrc : chc + d.ss * wcnc / wcsc;
     double gct = storage * volume - (gxp + gxm + gyp + gym);
     if (east && cxp == kFlux) gct += gxp;
     if (west && cxm == kFlux) gct += gxm;
@@ -323,36 +365,38 @@ __device__ __forceinline__ void assemble_body(
     if (!top || dirichlet_top) gct -= gzm;
 
     double b = storage * hnc * volume;
-    b -= kdt * kzp;
-    b += kdt * kzm;
+    b -= kdt * (BARO ? kzpb * rzpf : kzp);
+    b += kdt * (BARO ? kzmb * rzmf : kzm);
     if (d.terrain) {
+      // along-layer gravity; the consistent form carries r^2 v of the face
+      const bool rb = BARO && d.pc;
       double sg = (bote > botc_) ? 1.0 : -1.0;
-      b += sg * dtg * axc * kxp * sinxc;
+      b += sg * dtg * axc * kxp * sinxc * (rb ? bxc * rxc : 1.0);
       sg = (botc_ > botw) ? -1.0 : 1.0;
-      b += sg * dtg * axw * kxm * sinxw;
+      b += sg * dtg * axw * kxm * sinxw * (rb ? bxw * rxw : 1.0);
       sg = (botn > botc_) ? 1.0 : -1.0;
-      b += sg * dtg * ayc * kyp * sinyc;
+      b += sg * dtg * ayc * kyp * sinyc * (rb ? byc * ryc : 1.0);
       sg = (botc_ > bots) ? -1.0 : 1.0;
-      b += sg * dtg * ays * kym * sinys;
+      b += sg * dtg * ays * kym * sinys * (rb ? bys * rys : 1.0);
     }
     if (east) {
-      if (cxp == kFlux) b += axc * vxp * dtg;
+      if (cxp == kFlux) b += axc * vxp * dtg * rxc;
       else b -= gxp * hne;
     }
     if (west) {
-      if (cxm == kFlux) b += axw * vxm * dtg;
+      if (cxm == kFlux) b += axw * vxm * dtg * rxw;
       else b -= gxm * hnw;
     }
     if (north) {
-      if (cyp == kFlux) b += ayc * vyp * dtg;
+      if (cyp == kFlux) b += ayc * vyp * dtg * ryc;
       else b -= gyp * hnn;
     }
     if (south) {
-      if (cym == kFlux) b += ays * vym * dtg;
+      if (cym == kFlux) b += ays * vym * dtg * rys;
       else b -= gym * hns;
     }
     if (k == d.nz - 1) {
-      if (botc == kFlux) b += kdt * (vbot + kzp);
+      if (botc == kFlux) b += kdt * rzpf * (vbot + kzpb);
       else if (botc == kHead) b -= gzp * vbot;
     }
     if (top && CPL) {  // Predictor.cpp:627-674
@@ -364,17 +408,17 @@ __device__ __forceinline__ void assemble_body(
         const double roomTop = fmax(0.0, (0.9999 * wcsc - wcnc) * dzc);
         const double take = fmin(avl, roomTop);
         const double qsup = -take / dtg;
-        b += -kdt * (qsup + kzm);
+        b += -kdt * rzmf * (qsup + kzmb);
       } else {
         double qtop = 0.0;
         if (topc == kFlux &&
             ((vtop > 0.0 && wcnc < wcsc) || (vtop < 0.0 && wcnc > wcrc)))
           qtop = vtop;
-        b += -kdt * (qtop + kzm);
+        b += -kdt * rzmf * (qtop + kzmb);
       }
     } else if (top) {
       if (topc == kHead) b -= gzm * vtop;
-      else if (topc == kFlux) b += -kdt * (vtop + kzm);
+      else if (topc == kFlux) b += -kdt * rzmf * (vtop + kzmb);
     }
     diag[c] = gct;
     gxps[c] = (!east && ae) ? gxp : 0.0;
@@ -384,15 +428,15 @@ __device__ __forceinline__ void assemble_body(
   }
 }
 
-template <bool CPL>
+template <bool CPL, bool BARO>
 __global__ void __launch_bounds__(kBlock, 2) k_assemble(
     Dims d, Fields f, const double* __restrict__ kxf, const double* __restrict__ kyf,
     const double* __restrict__ kzff, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ ch, const double* __restrict__ dtgp,
     double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
     double* __restrict__ gzps, double* __restrict__ rhs, double* __restrict__ xw) {
-  assemble_body<CPL>(d, f, kxf, kyf, kzff, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs, xw,
-                     blockIdx.x, gridDim.x);
+  assemble_body<CPL, BARO>(d, f, kxf, kyf, kzff, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs,
+                           xw, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- predictor faces
@@ -457,6 +501,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_faces(Dims d, Fields f, PassK pk,
 // hi_edge mark the domain's boundary faces, whose BC code and value apply.
 // ih = 1 / dx (1 / dy): the head difference over the spacing (half of it at
 // the domain's edges) is a product with the reciprocal, equal up to rounding.
+// rf, vf: the face's density and viscosity ratios (1 without density
+// coupling): v on the pressure term, r v on the consistent form's gravity.
 struct LatFlux {
   double kca, kcb, ksa, ksb, hpa, hpb, wa, wb, wsa, wsb, bota, botb;
   double area, cosv, sinv;
@@ -465,10 +511,10 @@ struct LatFlux {
 
 __device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux& v, double ih,
                                   bool lo_edge, bool hi_edge, int code, double value, long long b,
-                                  const double* __restrict__ hp) {
+                                  const double* __restrict__ hp, double rf, double vf) {
   double q;
   if (lo_edge) {
-    q = v.area * v.kcb * v.cosv * (v.hpb - v.hpa) * (2.0 * ih);
+    q = v.area * v.kcb * vf * v.cosv * (v.hpb - v.hpa) * (2.0 * ih);
     if (code == kNoFlux) q = 0.0;
     else if (code == kFlux) q = -value * v.area;
     return q;
@@ -486,7 +532,8 @@ __device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux&
     }
     if (!v.acta || !v.actb) kf = 0.0;
   }
-  q = v.area * (kf * v.cosv * (v.hpb - v.hpa) * idelta + sg * kf * v.sinv);
+  q = v.area * (kf * vf * v.cosv * (v.hpb - v.hpa) * idelta +
+                sg * kf * (d.pc ? rf * vf : 1.0) * v.sinv);
   if (!d.full3d && ((v.acta && v.wa < v.wsa) || (v.actb && v.wb < v.wsb))) q = 0.0;
   if (hi_edge) {
     if (code == kNoFlux) q = 0.0;
@@ -496,27 +543,30 @@ __device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux&
 }
 
 // Darcy flux of z-face plane k from loaded values (computeFluxesImpl's z
-// branch): u = cell k-1, l = cell k.
+// branch): u = cell k-1, l = cell k; rz, vz = the face's density and
+// viscosity ratios (1 without density coupling), gravity r and the
+// conductance's v.
 __device__ inline double flux_zv(const Dims& d, const Fields& f, const ZFlank& u, const ZFlank& l,
                                  double hpu, double hpl, int k, int topc, double topv, int botc,
-                                 double botv, long long cu, const double* __restrict__ hp) {
+                                 double botv, long long cu, const double* __restrict__ hp,
+                                 double rz, double vz) {
   const bool below = (k < d.nz) && l.act;
   const bool above = (k >= 1) && u.act;
   if (below && !above) {  // face above a column's top cell
     if (topc == kFlux) return topv * d.az;
     if (topc == kHead) {
       const double delta = 0.5 * l.dz;
-      return d.az * l.ks * ((hpl - topv) / delta - 1.0);
+      return d.az * l.ks * vz * ((hpl - topv) / delta - rz);
     }
     return 0.0;
   }
   if (k == d.nz && above) {  // bottom boundary face
     const double kf = u.kc;
     if (botc == kFlux) return botv * d.az;
-    if (botc == kGravity) return -kf * d.az;
+    if (botc == kGravity) return -kf * vz * rz * d.az;
     if (botc == kHead) {
       const double delta = 0.5 * u.dz;
-      return d.az * kf * ((botv - hpu) / delta - 1.0);
+      return d.az * kf * vz * ((botv - hpu) / delta - rz);
     }
     return 0.0;
   }
@@ -528,7 +578,7 @@ __device__ inline double flux_zv(const Dims& d, const Fields& f, const ZFlank& u
       kf = 0.5 * (vg_k(soil_at(f, cu), hp[cu], l.ks) + l.kc);
     }
     const double delta = 0.5 * (u.dz + l.dz);
-    return d.az * kf * ((hpl - hpu) / delta - 1.0);
+    return d.az * kf * vz * ((hpl - hpu) / delta - rz);
   }
   return 0.0;
 }
@@ -541,7 +591,8 @@ __device__ inline double flux_zv(const Dims& d, const Fields& f, const ZFlank& u
 // the guarded top flux.  Debits the column's budget; hc = predicted head,
 // wcc = theta of the cell.
 __device__ inline double flux_top_coupled(const Dims& d, const Fields& f, long long col,
-                                          long long c, double hc, double wcc, double dtg) {
+                                          long long c, double hc, double wcc, double dtg,
+                                          double rz, double vz) {
   const double ks = f.ksz[c], dzc = f.dz[c], dep = f.cpl->dept[col];
   const int m = f.cpl->cmode[col];
   const double delta = 0.5 * dzc;
@@ -552,7 +603,7 @@ __device__ inline double flux_top_coupled(const Dims& d, const Fields& f, long l
     q = -take * d.az / dtg;
     f.cpl->avail[col] -= take;
   } else if (m == 1) {
-    q = d.az * ks * ((hc - dep) / delta - 1.0);
+    q = d.az * ks * vz * ((hc - dep) / delta - rz);
     if (q < 0.0) {
       const double need = -q * dtg / d.az;
       const double av = f.cpl->avail[col];
@@ -564,12 +615,12 @@ __device__ inline double flux_top_coupled(const Dims& d, const Fields& f, long l
       }
     }
   } else if (d.pc && m == 3) {
-    q = d.az * ks * ((hc - dep) / delta - 1.0);
+    q = d.az * ks * vz * ((hc - dep) / delta - rz);
     if (q <= 0.0) q = 0.0;
   } else {
     const Soil so = soil_at(f, c);
     const double kface = 0.5 * (vg_k(so, dep, ks) + vg_k(so, hc, ks));
-    q = d.az * kface * ((hc - dep) / delta - 1.0);
+    q = d.az * kface * vz * ((hc - dep) / delta - rz);
     if (q <= 0.0) q = 0.0;
     if (f.topc[col] == kFlux) {
       const double v = f.topv[col];
@@ -583,7 +634,7 @@ __device__ inline double flux_top_coupled(const Dims& d, const Fields& f, long l
 // boundary faces through the ghost cells i = 0, j = 0) and the z face above
 // it (plus the bottom face for k = nz-1).  Each face's loads are issued
 // before its rules run.
-template <bool CPL>
+template <bool CPL, bool BARO>
 __device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
                                                     const double* __restrict__ hp,
                                                     const double* __restrict__ wcn,
@@ -641,32 +692,37 @@ __device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
       const Flank a{vx.kca, vx.ksa, vx.wa, vx.wsa, vx.acta};
       const Flank b{vx.kcb, vx.ksb, vx.wb, vx.wsb, vx.actb};
       kx[c] = face_lat(d, a, b, i == 0, i == d.nx, codex);
-      qx[c] = flux_lat(d, f, vx, d.idx, i == 0, i == d.nx, codex, valx, e, hp);
+      qx[c] = flux_lat(d, f, vx, d.idx, i == 0, i == d.nx, codex, valx, e, hp,
+                       BARO ? f.baro->rxp[c] : 1.0, BARO ? f.baro->vxp[c] : 1.0);
     }
     if (doY) {
       const Flank a{vy.kca, vy.ksa, vy.wa, vy.wsa, vy.acta};
       const Flank b{vy.kcb, vy.ksb, vy.wb, vy.wsb, vy.actb};
       ky[c] = face_lat(d, a, b, j == 0, j == d.ny, codey);
-      qy[c] = flux_lat(d, f, vy, d.idy, j == 0, j == d.ny, codey, valy, n, hp);
+      qy[c] = flux_lat(d, f, vy, d.idy, j == 0, j == d.ny, codey, valy, n, hp,
+                       BARO ? f.baro->ryp[c] : 1.0, BARO ? f.baro->vyp[c] : 1.0);
     }
     if (doZ) {
       const long long fz = fidx(d, j, i, k), col = col2(d, j, i);
       const double dep = (CPL && k == 0) ? f.cpl->dept[col] : 0.0;
+      const double rz = BARO ? f.baro->rzp[fz] : 1.0, vz = BARO ? f.baro->vzp[fz] : 1.0;
       kzf[fz] = face_z<CPL>(d, zu, zc, k, topc, botc, dep);
       if (CPL && zc.act && !(k >= 1 && zu.act))
-        qzf[fz] = flux_top_coupled(d, f, col, c, hpc, wcn[c], dtg);
+        qzf[fz] = flux_top_coupled(d, f, col, c, hpc, wcn[c], dtg, rz, vz);
       else
-        qzf[fz] = flux_zv(d, f, zu, zc, hpu, hpc, k, topc, topv, botc, botv, cu, hp);
+        qzf[fz] = flux_zv(d, f, zu, zc, hpu, hpc, k, topc, topv, botc, botv, cu, hp, rz, vz);
       if (k == d.nz - 1) {
         const ZFlank none{0.0, 0.0, 0.0, 0};
         kzf[fz + 1] = face_z<CPL>(d, zc, none, d.nz, topc, botc, 0.0);
-        qzf[fz + 1] = flux_zv(d, f, zc, none, hpc, 0.0, d.nz, topc, topv, botc, botv, c, hp);
+        qzf[fz + 1] = flux_zv(d, f, zc, none, hpc, 0.0, d.nz, topc, topv, botc, botv, c, hp,
+                              BARO ? f.baro->rzp[fz + 1] : 1.0,
+                              BARO ? f.baro->vzp[fz + 1] : 1.0);
       }
     }
   }
 }
 
-template <bool CPL>
+template <bool CPL, bool BARO>
 __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
                                                     const double* __restrict__ hp,
                                                     const double* __restrict__ wcn,
@@ -677,7 +733,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
                                                     double* __restrict__ qy,
                                                     double* __restrict__ qzf,
                                                     const double* __restrict__ dtgp) {
-  flux_body<CPL>(d, f, pk, hp, wcn, kx, ky, kzf, qx, qy, qzf, dtgp, blockIdx.x, gridDim.x);
+  flux_body<CPL, BARO>(d, f, pk, hp, wcn, kx, ky, kzf, qx, qy, qzf, dtgp, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- theta update
@@ -691,6 +747,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
 // and clears the column flags the classification then sets.
 // All loads of a cell are issued before its first store and before any
 // branch on loaded data, so one memory round trip serves the cell.
+// BARO: density coupling (updateWaterContent with its ratios): the storage
+// weighs by the cell's r_rho, each face flux by its face's r.
+template <bool BARO>
 __device__ __forceinline__ void update_wc_body(
     Dims d, Fields f, const double* __restrict__ hp, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ qx, const double* __restrict__ qy,
@@ -712,7 +771,18 @@ __device__ __forceinline__ void update_wc_body(
       const double hnc = hn[c], dzc = f.dz[c];
       const double qxp = qx[c], qxm = qx[c - d.sx], qyp = qy[c], qym = qy[c - d.sy];
       const double qzt = qzf[fz], qzb = qzf[fz + 1];
-      if (ac) {
+      if (ac && BARO) {
+        const BaroDev& B = *f.baro;
+        const double r = B.rrho[c];
+        const double volume = d.az * dzc;
+        const double dh = hpc - hnc;
+        const double coeff = volume * (r + r * d.ss * dh / ts);
+        const double dqx = dtg * (qxp * B.rxp[c] - qxm * B.rxp[c - d.sx]);
+        const double dqy = dtg * (qyp * B.ryp[c] - qym * B.ryp[c - d.sy]);
+        const double dqz = dtg * (qzb * B.rzp[fz + 1] - qzt * B.rzp[fz]);
+        upd = (w0 * r * volume + dqx + dqy + dqz) / coeff;
+        acc += upd * volume * r * d.ss * dh / ts;
+      } else if (ac) {
         const double volume = d.az * dzc;
         const double dh = hpc - hnc;
         const double coeff = volume * (1.0 + d.ss * dh / ts);
@@ -731,13 +801,14 @@ __device__ __forceinline__ void update_wc_body(
   if (threadIdx.x == 0) partial[bid] = s;
 }
 
+template <bool BARO>
 __global__ void __launch_bounds__(kBlock, 4) k_update_wc(
     Dims d, Fields f, const double* __restrict__ hp, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ qx, const double* __restrict__ qy,
     const double* __restrict__ qzf, const double* __restrict__ dtgp, double* __restrict__ wcu,
     uint8_t* __restrict__ satf, int* __restrict__ colflag, double* partial) {
-  update_wc_body(d, f, hp, hn, wcn, qx, qy, qzf, dtgp, wcu, satf, colflag, partial, blockIdx.x,
-                 gridDim.x);
+  update_wc_body<BARO>(d, f, hp, hn, wcn, qx, qy, qzf, dtgp, wcu, satf, colflag, partial,
+                       blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- post-allocation
@@ -754,6 +825,7 @@ struct SplitIn {
   double hc, hxp, hxm, hyp, hym, hzp, hzm;
   double kxp, kxm, kyp, kym, kzb, kzt;
   double dzc, dzp, dzm;
+  double gzb, gzt;  // gravity of the lower / upper z face: 1, or its r_rho (density gradient)
   int8_t axp, axm, ayp, aym, azp, azm;
 };
 
@@ -768,11 +840,11 @@ __device__ inline Split gradient_split(const Dims& d, const SplitIn& n, int k) {
   }
   if (k + 1 < d.nz && n.azp && n.kzb > 0.0) {
     const double dzp = 0.5 * (n.dzc + n.dzp);
-    dh4 = (n.hzp - n.hc) / dzp - 1.0;
+    dh4 = (n.hzp - n.hc) / dzp - n.gzb;
   }
   if (k >= 1 && n.azm && n.kzt > 0.0) {
     const double dzm = 0.5 * (n.dzc + n.dzm);
-    dh5 = (n.hc - n.hzm) / dzm - 1.0;
+    dh5 = (n.hc - n.hzm) / dzm - n.gzt;
   }
   double tot = 0.0, gz;
   if (dh0 * dh1 >= 0.0) tot += fabs(0.5 * (dh0 + dh1));
@@ -812,6 +884,7 @@ struct CellPost {
   double wout, hout, rm, up, dn;
 };
 
+template <bool BARO>
 __device__ __forceinline__ CellPost classify_cell(
     const Dims& d, const Fields& f, const double* __restrict__ kx, const double* __restrict__ ky,
     const double* __restrict__ kzf, const double* __restrict__ wcR,
@@ -838,6 +911,12 @@ __device__ __forceinline__ CellPost classify_cell(
   n.dzc = f.dz[c];
   n.dzp = f.dz[cp];
   n.dzm = f.dz[cm];
+  n.gzb = 1.0;
+  n.gzt = 1.0;
+  if (BARO && f.baro->dgrad) {  // densityReallocationGradient (Reallocate.cpp:223-233)
+    n.gzb = f.baro->rzp[fz + 1];
+    n.gzt = f.baro->rzp[fz];
+  }
   n.axp = f.act[c + d.sx];
   n.axm = f.act[c - d.sx];
   n.ayp = f.act[c + d.sy];
@@ -898,6 +977,7 @@ __device__ __forceinline__ CellPost classify_cell(
   return CellPost{wout, hout, rm, up, dn};
 }
 
+template <bool BARO>
 __device__ __forceinline__ void classify_body(
     Dims d, Fields f, const double* __restrict__ kx, const double* __restrict__ ky,
     const double* __restrict__ kzf, const double* __restrict__ wcR,
@@ -912,7 +992,7 @@ __device__ __forceinline__ void classify_body(
     unflatten(d, c, j, i, k);
     CellPost r{wcR[c], hR[c], 0.0, 0.0, 0.0};
     if (j >= 1 && j <= d.ny && i >= 1 && i <= d.nx) {
-      r = classify_cell(d, f, kx, ky, kzf, wcR, hR, satf, c, j, i, k, adj, drop);
+      r = classify_cell<BARO>(d, f, kx, ky, kzf, wcR, hR, satf, c, j, i, k, adj, drop);
       if (r.up > 0.0 || r.dn > 0.0) colflag[col2(d, j, i)] = 1;
     }
     wc_out[c] = r.wout;
@@ -927,13 +1007,15 @@ __device__ __forceinline__ void classify_body(
   if (threadIdx.x == 0) part_drop[bid] = s2;
 }
 
+template <bool BARO>
 __global__ void __launch_bounds__(kBlock, 3) k_classify(
     Dims d, Fields f, const double* __restrict__ kx, const double* __restrict__ ky,
     const double* __restrict__ kzf, const double* __restrict__ wcR,
     const double* __restrict__ hR, const uint8_t* __restrict__ satf, double* __restrict__ wc_out,
     double* __restrict__ h_out, double* __restrict__ room, double* __restrict__ sup,
     double* __restrict__ sdn, int* colflag, double* part_adj, double* part_drop) {
-  classify_body(d, f, kx, ky, kzf, wcR, hR, satf, wc_out, h_out, room, sup, sdn, colflag, part_adj, part_drop, blockIdx.x, gridDim.x);
+  classify_body<BARO>(d, f, kx, ky, kzf, wcR, hR, satf, wc_out, h_out, room, sup, sdn, colflag,
+                      part_adj, part_drop, blockIdx.x, gridDim.x);
 }
 
 // A coupled column's surface during its send walks: the vent deposits
@@ -1369,8 +1451,10 @@ __global__ void k_cpl_mode(Dims d, Fields f, const double* __restrict__ h,
     int8_t m = 0;
     if (kt < 0 || dep <= 0.0) {
       if (d.pc && kt >= 0) {
+        // pressurized past r dz / 2 (r = the top face's density ratio)
         const long long c = cidx(d, j, i, kt);
-        if (h[c] > 0.5 * f.dz[c]) m = 3;
+        const double r = (f.baro == nullptr) ? 1.0 : f.baro->rzp[fidx(d, j, i, kt)];
+        if (h[c] > r * 0.5 * f.dz[c]) m = 3;
       }
     } else {
       const long long c = cidx(d, j, i, kt);
@@ -1407,7 +1491,10 @@ __global__ void k_cpl_book(Dims d, Fields f, const double* __restrict__ hp,
     double dep = f.cpl->dept[col];
     se += q * dtg;
     if (d.pc && f.cpl->cmode[col] == 3) {
-      const double qr = d.az * f.ksz[c] * ((hp[c] - dep) / (0.5 * f.dz[c]) - 1.0);
+      const long long fz = fidx(d, j, i, kt);
+      const double rz = (f.baro == nullptr) ? 1.0 : f.baro->rzp[fz];
+      const double vz = (f.baro == nullptr) ? 1.0 : f.baro->vzp[fz];
+      const double qr = d.az * f.ksz[c] * vz * ((hp[c] - dep) / (0.5 * f.dz[c]) - rz);
       if (qr <= 0.0) sc += -qr * dtg;
     }
     if (q < 0.0 && dep <= f.cpl->min_depth) {
@@ -1794,7 +1881,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_assemble_batch(const StepArgs* ta
   __shared__ StepArgs sa;
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
-  assemble_body<false>(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp,
+  assemble_body<false, false>(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp,
                 sa.gyp, sa.gzp, sa.rhs, sa.mixed ? sa.x : nullptr, bid, G);
 }
 
@@ -1821,7 +1908,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux_batch(const StepArgs* tab, c
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
   const PassK pk{sa.kcx, sa.kcy, sa.kcz, sa.wcn};
-  flux_body<false>(sa.d, sa.f, pk, sa.hp, sa.wcn, sa.kx, sa.ky, sa.kzf, sa.qx, sa.qy, sa.qzf, &sa.dtg, bid,
+  flux_body<false, false>(sa.d, sa.f, pk, sa.hp, sa.wcn, sa.kx, sa.ky, sa.kzf, sa.qx, sa.qy, sa.qzf, &sa.dtg, bid,
             G);
 }
 
@@ -1830,7 +1917,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_update_wc_batch(const StepArgs* t
   __shared__ StepArgs sa;
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
-  update_wc_body(sa.d, sa.f, sa.hp, sa.hn, sa.wcn, sa.qx, sa.qy, sa.qzf, &sa.dtg, sa.wcu, sa.satf,
+  update_wc_body<false>(sa.d, sa.f, sa.hp, sa.hn, sa.wcn, sa.qx, sa.qy, sa.qzf, &sa.dtg, sa.wcu, sa.satf,
                  sa.colflag, sa.partial + kPSs * sa.nblk, bid, G);
 }
 
@@ -1839,7 +1926,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_classify_batch(const StepArgs* ta
   __shared__ StepArgs sa;
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
-  classify_body(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.wcu, sa.hp, sa.satf, sa.wc_out, sa.h_out,
+  classify_body<false>(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.wcu, sa.hp, sa.satf, sa.wc_out, sa.h_out,
                 sa.room, sa.sup, sa.sdn, sa.colflag, sa.partial + kPAdj * sa.nblk,
                 sa.partial + kPDrop * sa.nblk, bid, G);
 }
@@ -1929,7 +2016,9 @@ void launch_closure_pred(const Device& D, const double* h) {
 void launch_assemble(const Device& D, const double* hn, const double* wcn, bool warm) {
   const PassK pk{D.kcx, D.kcy, D.kcz, wcn};
   const auto faces = (D.f.cpl != nullptr) ? k_faces<true> : k_faces<false>;
-  const auto assemble = (D.f.cpl != nullptr) ? k_assemble<true> : k_assemble<false>;
+  const bool cpl = D.f.cpl != nullptr, baro = D.f.baro != nullptr;
+  const auto assemble = cpl ? (baro ? k_assemble<true, true> : k_assemble<true, false>)
+                            : (baro ? k_assemble<false, true> : k_assemble<false, false>);
   faces<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.kx, D.ky, D.kzf);
   assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.kx, D.ky, D.kzf, hn, wcn, D.ch,
                                                      dtg_slot(D), D.diag, D.gxp, D.gyp, D.gzp,
@@ -1945,21 +2034,25 @@ void launch_closure_corr(const Device& D, const double* hn) {
 
 void launch_flux(const Device& D, const double* wcn) {
   PassK pk{D.kcx, D.kcy, D.kcz, wcn};
-  const auto flux = (D.f.cpl != nullptr) ? k_flux<true> : k_flux<false>;
+  const bool cpl = D.f.cpl != nullptr, baro = D.f.baro != nullptr;
+  const auto flux = cpl ? (baro ? k_flux<true, true> : k_flux<true, false>)
+                        : (baro ? k_flux<false, true> : k_flux<false, false>);
   flux<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.hp, wcn, D.kx, D.ky, D.kzf, D.qx,
                                                  D.qy, D.qzf, dtg_slot(D));
   ++D.launches;
 }
 
 void launch_update_wc(const Device& D, const double* hn, const double* wcn) {
-  k_update_wc<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.hp, hn, wcn, D.qx, D.qy, D.qzf,
+  const auto update = (D.f.baro != nullptr) ? k_update_wc<true> : k_update_wc<false>;
+  update<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.hp, hn, wcn, D.qx, D.qy, D.qzf,
                                                       dtg_slot(D), D.wcu, D.satf, D.colflag,
                                                       D.partial + kPSs * D.nblk);
   ++D.launches;
 }
 
 void launch_classify(const Device& D, double* wc_out, double* h_out) {
-  k_classify<<<cells_grid(D), kBlock, 0, D.stream>>>(
+  const auto classify = (D.f.baro != nullptr) ? k_classify<true> : k_classify<false>;
+  classify<<<cells_grid(D), kBlock, 0, D.stream>>>(
       D.d, D.f, D.kx, D.ky, D.kzf, D.wcu, D.hp, D.satf, wc_out, h_out, D.room, D.sup, D.sdn,
       D.colflag,
       D.partial + kPAdj * D.nblk, D.partial + kPDrop * D.nblk);

@@ -17,8 +17,8 @@ from typing import Optional
 
 import numpy as np
 
-from .abi import (FIELD, STATUS_NAMES, SURF, CoupledAudit, Coupling, GwDesc, StepInfo,
-                  field_shape, make_desc)
+from .abi import (FIELD, SCALARS, STATUS_NAMES, SURF, CoupledAudit, Coupling, Density, GwDesc,
+                  StepInfo, field_shape, make_desc)
 from .config import IC_FORMS, GwConfig, rasterize
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -76,12 +76,18 @@ def load_library(path: str = LIB_PATH):
     lib.frehg_gw_elevation_offset.restype = C.c_double
     lib.frehg_gw_enable_transport_window.argtypes = [H]
     lib.frehg_gw_reset_transport_window.argtypes = [H]
+    lib.frehg_gw_attach_density.argtypes = [H, C.c_int, C.c_int, C.POINTER(Density)]
+    lib.frehg_gw_set_scalar.argtypes = [H, C.c_int, _dp]
+    lib.frehg_gw_get_scalar.argtypes = [H, C.c_int, _dp]
+    lib.frehg_gw_scalar_ptr.argtypes = [H, C.c_int]
+    lib.frehg_gw_scalar_ptr.restype = C.c_void_p
     for name in ("frehg_gw_create", "frehg_gw_destroy", "frehg_gw_set_stream",
                  "frehg_gw_set_bc_values", "frehg_gw_init_state", "frehg_gw_set_state",
                  "frehg_gw_step", "frehg_gw_next_dt", "frehg_gw_get_field", "frehg_gw_restore",
                  "frehg_gw_owned_volume", "frehg_gw_attach_coupling", "frehg_gw_get_surface",
                  "frehg_gw_set_surface", "frehg_gw_surface_ptr", "frehg_gw_coupled_audit_get",
-                 "frehg_gw_enable_transport_window", "frehg_gw_reset_transport_window"):
+                 "frehg_gw_enable_transport_window", "frehg_gw_reset_transport_window",
+                 "frehg_gw_attach_density", "frehg_gw_set_scalar", "frehg_gw_get_scalar"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -305,6 +311,54 @@ class RichardsSolver:
 
     def elevationOffset(self) -> float:
         return float(self.lib.frehg_gw_elevation_offset(self.h))
+
+    # -- density coupling (RichardsSolver.hpp:191-225, Baroclinic.cpp) -----------
+    def attachDensity(self, saline: bool = True, thermal: bool = False,
+                      beta_saline: float = 0.000744, beta_saline_visc: float = 0.0022,
+                      thermal_expansion: float = 0.0, reference_temperature: float = 20.0,
+                      reallocation_gradient: bool = False) -> None:
+        """attachScalar (baroclinic on) / attachTemperature /
+        setDensityCoefficients: the scalars' device fields are allocated
+        (zeroed); every step computes the ratios from their current values.
+        Defaults are DensityCouplingConfig's."""
+        d = Density(float(beta_saline), float(beta_saline_visc), float(thermal_expansion),
+                    float(reference_temperature), int(bool(reallocation_gradient)))
+        _check(self.lib, self.lib.frehg_gw_attach_density(self.h, int(bool(saline)),
+                                                          int(bool(thermal)), C.byref(d)))
+
+    def _scalar_shape(self, name: str):
+        return ((self.ny + 2, self.nx + 2, self.nz) if SCALARS[name] in (0, 2)
+                else (self.ny + 2, self.nx + 2))
+
+    def setScalar(self, name: str, value) -> None:
+        """Hand a scalar over in the halo layout (names of
+        :data:`frehg_b200.abi.SCALARS`)."""
+        v = np.ascontiguousarray(np.broadcast_to(value, self._scalar_shape(name)), np.float64)
+        _check(self.lib, self.lib.frehg_gw_set_scalar(self.h, SCALARS[name], v.ctypes.data_as(_dp)))
+
+    def scalar(self, name: str) -> np.ndarray:
+        out = np.empty(self._scalar_shape(name))
+        _check(self.lib, self.lib.frehg_gw_get_scalar(self.h, SCALARS[name], out.ctypes.data_as(_dp)))
+        return out
+
+    def scalarPointer(self, name: str) -> int:
+        """Device address of a scalar field, for a producer on the device."""
+        p = self.lib.frehg_gw_scalar_ptr(self.h, SCALARS[name])
+        if not p:
+            raise FatalError(1, f"scalar {name} not attached")
+        return p
+
+    def densityRatio(self) -> np.ndarray:
+        return self.field("rho")
+
+    def viscosityRatio(self) -> np.ndarray:
+        return self.field("visc")
+
+    def densityRatioFaceY(self) -> np.ndarray:
+        return self.field("rho_y")
+
+    def densityRatioFaceZ(self) -> np.ndarray:
+        return self.field("rho_z")
 
     # -- transport window (RichardsSolver.hpp:229-248) ----------------------------
     def enableTransportWindow(self) -> None:

@@ -108,7 +108,16 @@ enum {
   FREHG_GW_FIELD_WINDOW_Y = 19,    /* like QY */
   FREHG_GW_FIELD_WINDOW_Z = 20,    /* like QZ, the walks' transfers on every face they cross */
   FREHG_GW_FIELD_WINDOW_VENT = 21, /* (ny, nx): vented onto a coupled surface */
-  FREHG_GW_FIELD_COUNT = 22
+  /* density coupling (frehg_gw_attach_density): the ratios of the last step */
+  FREHG_GW_FIELD_RHO = 22,      /* r_rho per cell, like HEAD */
+  FREHG_GW_FIELD_VISC = 23,     /* r_visc per cell, like HEAD */
+  FREHG_GW_FIELD_RHO_X = 24,    /* r_rho face means, like QX */
+  FREHG_GW_FIELD_RHO_Y = 25,    /* like QY */
+  FREHG_GW_FIELD_RHO_Z = 26,    /* like QZ */
+  FREHG_GW_FIELD_VISC_X = 27,   /* r_visc face means, like QX */
+  FREHG_GW_FIELD_VISC_Y = 28,   /* like QY */
+  FREHG_GW_FIELD_VISC_Z = 29,   /* like QZ */
+  FREHG_GW_FIELD_COUNT = 30
 };
 
 /* Static description of one domain.  Host pointers; the library copies what
@@ -248,6 +257,51 @@ int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5);
  * ET vapour and root-sink windows are outside this drop-in. */
 int frehg_gw_enable_transport_window(frehg_gw_handle* h);
 int frehg_gw_reset_transport_window(frehg_gw_handle* h);
+
+/* Density coupling: the baroclinic ratios of a transported salinity and/or
+ * temperature (RichardsSolver::attachScalar with baroclinic on,
+ * attachTemperature and setDensityCoefficients, src/gw/RichardsSolver.hpp:
+ * 191-225; updateBaroclinicFaces, src/gw/Baroclinic.cpp:46-186).  At the start
+ * of every step, from the scalars' current values,
+ *   r_rho  = 1 + beta_saline s - thermal_expansion (T - T0)
+ *   r_visc = 1 / (1 + beta_saline_visc s)
+ * per cell (ghosts included), and their face means between active flanks with
+ * the reference's edge rules; the legs carry r v, the z gravity terms r^2 v
+ * (the consistent form's along-layer terms too), prescribed boundary fluxes r,
+ * the theta update weighs each face flux by its r and the storage by the
+ * cell's, and hydrostatic edge ghosts scale by the face r.  Without an
+ * attached scalar every ratio is exactly 1. */
+typedef struct frehg_gw_density {
+  double beta_saline;           /* r_rho slope per unit s (DensityCouplingConfig: 0.000744) */
+  double beta_saline_visc;      /* r_visc slope (0.0022) */
+  double thermal_expansion;     /* beta_T per unit T (0 = no thermal term) */
+  double reference_temperature; /* T0 (20) */
+  int reallocation_gradient;    /* 1: the post-allocation split measures the vertical
+                                   gradient against the face r_rho instead of 1
+                                   (densityReallocationGradient) */
+} frehg_gw_density;
+
+enum {
+  FREHG_GW_SCALAR_SALINE = 0,      /* s per cell, (ny+2)*(nx+2)*nz halo layout: the
+                                      ghosts carry the side values the transport
+                                      module enforces */
+  FREHG_GW_SCALAR_SALINE_SURF = 1, /* surface s above the top faces of coupled
+                                      columns, (ny+2)*(nx+2) */
+  FREHG_GW_SCALAR_TEMP = 2,        /* T per cell, like SALINE */
+  FREHG_GW_SCALAR_TEMP_SURF = 3    /* like SALINE_SURF */
+};
+
+/* Attach the scalars (saline and/or thermal, at least one) with the density
+ * coefficients; allocates their device fields, zeroed, and the ratio fields.
+ * Once only; a handle in a batch refuses it (FREHG_GW_EUNSUPPORTED). */
+int frehg_gw_attach_density(frehg_gw_handle* h, int saline, int thermal,
+                            const frehg_gw_density* coeffs);
+/* Copy a scalar from host memory (layout per FREHG_GW_SCALAR_*), or read it
+ * back (out); either pointer may be NULL.  A device-resident producer writes
+ * frehg_gw_scalar_ptr's field on the handle's stream instead. */
+int frehg_gw_set_scalar(frehg_gw_handle* h, int which, const double* values);
+int frehg_gw_get_scalar(frehg_gw_handle* h, int which, double* out);
+double* frehg_gw_scalar_ptr(frehg_gw_handle* h, int which);
 
 /* Kernels this handle has launched since creation. */
 long long frehg_gw_kernel_launches(const frehg_gw_handle* h);

@@ -13,8 +13,8 @@ import os
 
 import numpy as np
 
-from frehg_b200.abi import (FIELD, SURF, CoupledAudit, CouplerOpts, GwDesc, StepInfo,
-                            WindowAudit, field_shape, make_desc)
+from frehg_b200.abi import (FIELD, SCALARS, SURF, CoupledAudit, CouplerOpts, Density, GwDesc,
+                            StepInfo, WindowAudit, field_shape, make_desc)
 from frehg_b200.config import IC_FORMS, GwConfig, rasterize
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -77,6 +77,8 @@ def load():
     lib.oracle_gw_reset_transport_window.argtypes = [C.c_void_p]
     lib.oracle_gw_window.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.oracle_gw_coupler_restore.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+    lib.oracle_gw_attach_density.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(Density)]
+    lib.oracle_gw_scalar.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
     _lib = lib
     return lib
 
@@ -168,6 +170,31 @@ class OracleSolver:
 
     def elevation_offset(self) -> float:
         return self.lib.oracle_gw_elevation_offset(self.h)
+
+    # ------------------------------------------------------------ density coupling
+    def attach_density(self, saline: bool = True, thermal: bool = False,
+                       beta_saline: float = 0.000744, beta_saline_visc: float = 0.0022,
+                       thermal_expansion: float = 0.0, reference_temperature: float = 20.0,
+                       reallocation_gradient: bool = False) -> None:
+        d = Density(beta_saline, beta_saline_visc, thermal_expansion, reference_temperature,
+                    int(reallocation_gradient))
+        self._check(self.lib.oracle_gw_attach_density(self.h, int(saline), int(thermal),
+                                                      C.byref(d)))
+
+    def _scalar_shape(self, which):
+        return ((self.ny + 2, self.nx + 2, self.nz) if SCALARS[which] in (0, 2)
+                else (self.ny + 2, self.nx + 2))
+
+    def scalar(self, which: str) -> np.ndarray:
+        out = np.empty(self._scalar_shape(which))
+        self._check(self.lib.oracle_gw_scalar(self.h, SCALARS[which], out.ctypes.data_as(_dp),
+                                              None))
+        return out
+
+    def set_scalar(self, which: str, value) -> None:
+        v = np.ascontiguousarray(np.broadcast_to(value, self._scalar_shape(which)), np.float64)
+        self._check(self.lib.oracle_gw_scalar(self.h, SCALARS[which], None,
+                                              v.ctypes.data_as(_dp)))
 
     # ------------------------------------------------------------ coupled top
     def attach_coupling(self, min_depth: float, vent_all: bool = False,

@@ -4,11 +4,11 @@
  * halo layout: 3D fields are (ny+2, nx+2, nz) with k fastest and a one-cell
  * halo in j and i (src/core/Types.hpp:35-43); z-face fields carry nz+1
  * planes, plane k being the face above cell k (RichardsSolver.hpp:584-591).
- * Single rank: every domain edge is a physical boundary, halo exchanges are
- * no-ops, and the density / viscosity ratios of the reference formulas are
- * exactly 1 (RichardsSolver.cpp:141-150), so they are omitted — multiplying
- * by 1.0 is exact, which keeps every expression's rounding the reference's.
- * Expressions keep the reference's evaluation order.
+ * Single rank: every domain edge is a physical boundary and halo exchanges
+ * are no-ops.  The density / viscosity ratios of the reference formulas sit
+ * at the reference's places in every expression; without an attached scalar
+ * they stay exactly 1 (RichardsSolver.cpp:141-150), and multiplying by 1.0 is
+ * exact.  Expressions keep the reference's evaluation order.
  */
 #include "gw_oracle.h"
 
@@ -70,6 +70,14 @@ struct oracle_gw {
    * in the qx / qy / qzF layouts, the walks' path records, vented volume */
   int win;
   double *wx, *wy, *wz, *pcorr, *wvent;
+  /* density coupling (RichardsSolver.hpp:191-225, Baroclinic.cpp): the
+   * attached scalars (cells n3, surfaces n2), the coefficients, and the cell
+   * and face ratios (x / y faces n3, z faces n3f), 1 until a step computes
+   * them from an attached scalar */
+  int baro, saline, thermal, dgrad;
+  double beta_s, beta_sv, beta_t, t_ref;
+  double *s3, *s2, *t3, *t2;
+  double *rrho, *rvisc, *rxp, *ryp, *rzp, *vxp, *vyp, *vzp;
 };
 
 #define I2(s, j, i) ((size_t)(j) * (size_t)((s)->nx + 2) + (size_t)(i))
@@ -190,7 +198,8 @@ void oracle_gw_destroy(oracle_gw* s) {
                     &s->wcsnap, &s->hsnap, &s->topv, &s->botv, &s->xmv, &s->xpv, &s->ymv,
                     &s->ypv, &s->vals7, &s->rhs, &s->sol, &s->eta, &s->dept, &s->seep,
                     &s->avail, &s->gain, &s->bounce, &s->qss, &s->wx, &s->wy, &s->wz,
-                    &s->pcorr, &s->wvent};
+                    &s->pcorr, &s->wvent, &s->s3, &s->s2, &s->t3, &s->t2, &s->rrho,
+                    &s->rvisc, &s->rxp, &s->ryp, &s->rzp, &s->vxp, &s->vyp, &s->vzp};
   for (size_t n = 0; n < sizeof dbl / sizeof dbl[0]; ++n) free(*dbl[n]);
   free(s->ktop);
   free(s->gid);
@@ -432,6 +441,15 @@ oracle_gw* oracle_gw_create(const frehg_gw_desc* d) {
   for (size_t n = 0; n < sizeof f3 / sizeof f3[0]; ++n) *f3[n] = xcalloc(n3, sizeof(double));
   s->kz = xcalloc(n3f, sizeof(double));
   s->qz = xcalloc(n3f, sizeof(double));
+  /* the ratio fields start at 1 (RichardsSolver.cpp:141-150) */
+  double** r3[] = {&s->rrho, &s->rvisc, &s->rxp, &s->ryp, &s->vxp, &s->vyp};
+  for (size_t n = 0; n < 6; ++n) {
+    *r3[n] = xcalloc(n3, sizeof(double));
+    for (size_t c = 0; c < n3; ++c) (*r3[n])[c] = 1.0;
+  }
+  s->rzp = xcalloc(n3f, sizeof(double));
+  s->vzp = xcalloc(n3f, sizeof(double));
+  for (size_t f = 0; f < n3f; ++f) s->rzp[f] = s->vzp[f] = 1.0;
   s->ktop = xcalloc((size_t)d->nx * d->ny, sizeof(int));
   s->gid = xcalloc(n3, sizeof(int));
   int** c2[] = {&s->topc, &s->botc, &s->xmc, &s->xpc, &s->ymc, &s->ypc};
@@ -520,18 +538,19 @@ int oracle_gw_set_bc_values(oracle_gw* s, const double* top, const double* bot,
 }
 
 /* ------------------------------------------------------------------ ghosts */
-/* enforceHeadBc + ghostHead (Predictor.cpp:66-87, 757-817), density ratio 1.
- * In a coupled run a hydrostatic stage above the edge column's bed follows
- * the live surface there: (bed - zc) + depth. */
+/* enforceHeadBc + ghostHead (Predictor.cpp:66-87, 757-817): hydrostatic edges
+ * scale by the edge face's density ratio r.  In a coupled run a hydrostatic
+ * stage above the edge column's bed follows the live surface there:
+ * (bed - zc) r + depth (depth r on the plus sides). */
 static double ghost_head(const oracle_gw* s, int code, double value, double interior, double zc,
-                         size_t col) {
+                         size_t col, double r, int plus) {
   if (code == HEAD) return value;
   if (code == HYDRO) {
     if (s->cpl && value > s->bath[col]) {
-      const double hydro = (s->bath[col] - zc);
-      return hydro + s->dept[col];
+      const double hydro = (s->bath[col] - zc) * r;
+      return plus ? hydro + s->dept[col] * r : hydro + s->dept[col];
     }
-    return (value - zc);
+    return (value - zc) * r;
   }
   return interior;
 }
@@ -542,24 +561,119 @@ static void enforce_head_bc(oracle_gw* s) {
     for (int k = 0; k < nz; ++k) {
       size_t c = I3(s, j, 1, k);
       double zc = s->bot[c] + 0.5 * s->dz[c];
-      s->h[I3(s, j, 0, k)] =
-          ghost_head(s, s->xmc[I2(s, j, 1)], s->xmv[I2(s, j, 1)], s->h[c], zc, I2(s, j, 1));
+      s->h[I3(s, j, 0, k)] = ghost_head(s, s->xmc[I2(s, j, 1)], s->xmv[I2(s, j, 1)], s->h[c], zc,
+                                        I2(s, j, 1), s->rxp[I3(s, j, 0, k)], 0);
       c = I3(s, j, nx, k);
       zc = s->bot[c] + 0.5 * s->dz[c];
-      s->h[I3(s, j, nx + 1, k)] =
-          ghost_head(s, s->xpc[I2(s, j, nx)], s->xpv[I2(s, j, nx)], s->h[c], zc, I2(s, j, nx));
+      s->h[I3(s, j, nx + 1, k)] = ghost_head(s, s->xpc[I2(s, j, nx)], s->xpv[I2(s, j, nx)],
+                                             s->h[c], zc, I2(s, j, nx), s->rxp[c], 1);
     }
   for (int i = 1; i <= nx; ++i)
     for (int k = 0; k < nz; ++k) {
       size_t c = I3(s, 1, i, k);
       double zc = s->bot[c] + 0.5 * s->dz[c];
-      s->h[I3(s, 0, i, k)] =
-          ghost_head(s, s->ymc[I2(s, 1, i)], s->ymv[I2(s, 1, i)], s->h[c], zc, I2(s, 1, i));
+      s->h[I3(s, 0, i, k)] = ghost_head(s, s->ymc[I2(s, 1, i)], s->ymv[I2(s, 1, i)], s->h[c], zc,
+                                        I2(s, 1, i), s->ryp[I3(s, 0, i, k)], 0);
       c = I3(s, ny, i, k);
       zc = s->bot[c] + 0.5 * s->dz[c];
-      s->h[I3(s, ny + 1, i, k)] =
-          ghost_head(s, s->ypc[I2(s, ny, i)], s->ypv[I2(s, ny, i)], s->h[c], zc, I2(s, ny, i));
+      s->h[I3(s, ny + 1, i, k)] = ghost_head(s, s->ypc[I2(s, ny, i)], s->ypv[I2(s, ny, i)],
+                                             s->h[c], zc, I2(s, ny, i), s->ryp[c], 1);
     }
+}
+
+/* updateBaroclinicFaces (Baroclinic.cpp:46-186): with an attached scalar, the
+ * cell ratios over the whole halo box, then their face means between active
+ * flanks.  Minus-side edge faces average the interior cell with its ghost (a
+ * head edge takes the ghost's ratio one-sided), plus-side edge faces take the
+ * ghost's ratio under a head edge and stay 1 otherwise, the face above a
+ * column's top cell averages it with the surface scalar's ratio (coupled) or
+ * its own (uncoupled), the bottom boundary face stays 1. */
+static void update_baroclinic(oracle_gw* s) {
+  if (!s->baro || (!s->saline && !s->thermal)) return;
+  const int nx = s->nx, ny = s->ny, nz = s->nz;
+  const double bs = s->beta_s, bsv = s->beta_sv, bt = s->beta_t, t0 = s->t_ref;
+  for (size_t c = 0; c < s->n3; ++c) {
+    const double sv = s->saline ? s->s3[c] : 0.0;
+    const double dtv = s->thermal ? s->t3[c] - t0 : 0.0;
+    s->rrho[c] = 1.0 + bs * sv - bt * dtv;
+    s->rvisc[c] = 1.0 / (1.0 + bsv * sv);
+  }
+  for (int j = 1; j <= ny; ++j) /* x faces, slot i = face i+1/2 */
+    for (int i = 0; i <= nx; ++i)
+      for (int k = 0; k < nz; ++k) {
+        double rr = 1.0, rv = 1.0;
+        if (i == 0) {
+          if (s->gid[I3(s, j, 1, k)] >= 0) {
+            const size_t a = I3(s, j, 1, k), g = I3(s, j, 0, k);
+            if (is_head(s->xmc[I2(s, j, 1)])) {
+              rr = s->rrho[g];
+              rv = s->rvisc[g];
+            } else {
+              rr = 0.5 * (s->rrho[a] + s->rrho[g]);
+              rv = 0.5 * (s->rvisc[a] + s->rvisc[g]);
+            }
+          }
+        } else if (i == nx) {
+          if (s->gid[I3(s, j, i, k)] >= 0 && is_head(s->xpc[I2(s, j, i)])) {
+            rr = s->rrho[I3(s, j, i + 1, k)];
+            rv = s->rvisc[I3(s, j, i + 1, k)];
+          }
+        } else if (s->gid[I3(s, j, i, k)] >= 0 && s->gid[I3(s, j, i + 1, k)] >= 0) {
+          const size_t a = I3(s, j, i, k), b = I3(s, j, i + 1, k);
+          rr = 0.5 * (s->rrho[a] + s->rrho[b]);
+          rv = 0.5 * (s->rvisc[a] + s->rvisc[b]);
+        }
+        s->rxp[I3(s, j, i, k)] = rr;
+        s->vxp[I3(s, j, i, k)] = rv;
+      }
+  for (int j = 0; j <= ny; ++j) /* y faces */
+    for (int i = 1; i <= nx; ++i)
+      for (int k = 0; k < nz; ++k) {
+        double rr = 1.0, rv = 1.0;
+        if (j == 0) {
+          if (s->gid[I3(s, 1, i, k)] >= 0) {
+            const size_t a = I3(s, 1, i, k), g = I3(s, 0, i, k);
+            if (is_head(s->ymc[I2(s, 1, i)])) {
+              rr = s->rrho[g];
+              rv = s->rvisc[g];
+            } else {
+              rr = 0.5 * (s->rrho[a] + s->rrho[g]);
+              rv = 0.5 * (s->rvisc[a] + s->rvisc[g]);
+            }
+          }
+        } else if (j == ny) {
+          if (s->gid[I3(s, j, i, k)] >= 0 && is_head(s->ypc[I2(s, j, i)])) {
+            rr = s->rrho[I3(s, j + 1, i, k)];
+            rv = s->rvisc[I3(s, j + 1, i, k)];
+          }
+        } else if (s->gid[I3(s, j, i, k)] >= 0 && s->gid[I3(s, j + 1, i, k)] >= 0) {
+          const size_t a = I3(s, j, i, k), b = I3(s, j + 1, i, k);
+          rr = 0.5 * (s->rrho[a] + s->rrho[b]);
+          rv = 0.5 * (s->rvisc[a] + s->rvisc[b]);
+        }
+        s->ryp[I3(s, j, i, k)] = rr;
+        s->vyp[I3(s, j, i, k)] = rv;
+      }
+  for (int j = 1; j <= ny; ++j) /* z faces, plane k above cell k */
+    for (int i = 1; i <= nx; ++i)
+      for (int k = 0; k <= nz; ++k) {
+        const int below = (k < nz) && s->gid[I3(s, j, i, k)] >= 0;
+        const int above = (k >= 1) && s->gid[I3(s, j, i, k - 1)] >= 0;
+        double rr = 1.0, rv = 1.0;
+        if (below && above) {
+          const size_t a = I3(s, j, i, k - 1), b = I3(s, j, i, k);
+          rr = 0.5 * (s->rrho[a] + s->rrho[b]);
+          rv = 0.5 * (s->rvisc[a] + s->rvisc[b]);
+        } else if (below) {
+          const size_t b = I3(s, j, i, k), col = I2(s, j, i);
+          const double sg = s->saline ? (s->cpl ? s->s2[col] : s->s3[b]) : 0.0;
+          const double tg = s->thermal ? (s->cpl ? s->t2[col] : s->t3[b]) - t0 : 0.0;
+          rr = 0.5 * (s->rrho[b] + 1.0 + bs * sg - bt * tg);
+          rv = 0.5 * (s->rvisc[b] + 1.0 / (1.0 + bsv * sg));
+        }
+        s->rzp[IF(s, j, i, k)] = rr;
+        s->vzp[IF(s, j, i, k)] = rv;
+      }
 }
 
 /* enforceMoistureBc (Corrector.cpp:709-756). */
@@ -630,6 +744,7 @@ int oracle_gw_set_state(oracle_gw* s, const double* head, const double* wc) {
         s->h[I3(s, j, i, k)] = head[q];
         s->wc[I3(s, j, i, k)] = wc[q];
       }
+  update_baroclinic(s);
   enforce_head_bc(s);
   enforce_moisture_bc(s);
   memcpy(s->hn, s->h, s->n3 * sizeof(double));
@@ -653,7 +768,7 @@ static void classify_coupled_top(oracle_gw* s, double dtg) {
       if (kt < 0 || s->dept[col] <= 0.0) {
         if (s->pc && kt >= 0) {
           const size_t c = I3(s, j, i, kt);
-          if (s->h[c] > 0.5 * s->dz[c]) {
+          if (s->h[c] > s->rzp[IF(s, j, i, kt)] * 0.5 * s->dz[c]) {
             s->cmode[col] = 3;
             continue;
           }
@@ -835,20 +950,25 @@ static void assemble(oracle_gw* s, double dtg) {
         const int east = (i == nx), west = (i == 1), north = (j == ny), south = (j == 1);
         const int top = (k == 0) || (s->gid[c - 1] < 0);
         const double volume = az * s->dz[c];
-        double gxp = -s->kx[c] * dtg * s->cosx[c] / (dx * dx) * (s->ax[c] * dx);
-        double gxm = -s->kx[cw] * dtg * s->cosx[cw] / (dx * dx) * (s->ax[cw] * dx);
-        double gyp = -s->ky[c] * dtg * s->cosy[c] / (dy * dy) * (s->ay[c] * dy);
-        double gym = -s->ky[cs] * dtg * s->cosy[cs] / (dy * dy) * (s->ay[cs] * dy);
+        double gxp = -s->kx[c] * dtg * s->rxp[c] * s->vxp[c] * s->cosx[c] / (dx * dx) *
+                     (s->ax[c] * dx);
+        double gxm = -s->kx[cw] * dtg * s->rxp[cw] * s->vxp[cw] * s->cosx[cw] / (dx * dx) *
+                     (s->ax[cw] * dx);
+        double gyp = -s->ky[c] * dtg * s->ryp[c] * s->vyp[c] * s->cosy[c] / (dy * dy) *
+                     (s->ay[c] * dy);
+        double gym = -s->ky[cs] * dtg * s->ryp[cs] * s->vyp[cs] * s->cosy[cs] / (dy * dy) *
+                     (s->ay[cs] * dy);
         if (east && is_head(s->xpc[col])) gxp *= 2.0;
         if (west && is_head(s->xmc[col])) gxm *= 2.0;
         if (north && is_head(s->ypc[col])) gyp *= 2.0;
         if (south && is_head(s->ymc[col])) gym *= 2.0;
         double dzf = (k == nz - 1) ? 0.5 * s->dz[c] : 0.5 * (s->dz[c] + s->dz[c + 1]);
-        const double gzp = -s->kz[IF(s, j, i, k + 1)] * dtg / (s->dz[c] * dzf) * volume;
+        const size_t fp = IF(s, j, i, k + 1), fm = IF(s, j, i, k);
+        const double gzp = -s->kz[fp] * dtg * s->rzp[fp] * s->vzp[fp] / (s->dz[c] * dzf) * volume;
         dzf = top ? 0.5 * s->dz[c] : 0.5 * (s->dz[c] + s->dz[c - 1]);
-        const double gzm = -s->kz[IF(s, j, i, k)] * dtg / (s->dz[c] * dzf) * volume;
+        const double gzm = -s->kz[fm] * dtg * s->rzp[fm] * s->vzp[fm] / (s->dz[c] * dzf) * volume;
 
-        const double storage = (s->ch[c] + ss * s->wcn[c] / s->wcs[c]);
+        const double storage = (s->ch[c] + ss * s->wcn[c] / s->wcs[c]) * s->rrho[c];
         double gct = storage * volume - (gxp + gxm + gyp + gym);
         if (east && s->xpc[col] == FLUX) gct += gxp;
         if (west && s->xmc[col] == FLUX) gct += gxm;
@@ -864,9 +984,21 @@ static void assemble(oracle_gw* s, double dtg) {
         }
 
         double b = storage * s->hn[c] * volume;
-        b -= dtg * volume * s->kz[IF(s, j, i, k + 1)] / s->dz[c];
-        b += dtg * volume * s->kz[IF(s, j, i, k)] / s->dz[c];
-        if (s->follow_terrain) {
+        b -= dtg * volume * s->kz[fp] * s->rzp[fp] * s->rzp[fp] * s->vzp[fp] / s->dz[c];
+        b += dtg * volume * s->kz[fm] * s->rzp[fm] * s->rzp[fm] * s->vzp[fm] / s->dz[c];
+        if (s->follow_terrain && s->pc) {
+          /* the along-layer terms in the z-gravity form r^2 v (consistent) */
+          double sg = (s->bot[ce] > s->bot[c]) ? 1.0 : -1.0;
+          b += sg * dtg * s->ax[c] * s->kx[c] * s->rxp[c] * s->rxp[c] * s->vxp[c] * s->sinx[c];
+          sg = (s->bot[c] > s->bot[cw]) ? -1.0 : 1.0;
+          b += sg * dtg * s->ax[cw] * s->kx[cw] * s->rxp[cw] * s->rxp[cw] * s->vxp[cw] *
+               s->sinx[cw];
+          sg = (s->bot[cn] > s->bot[c]) ? 1.0 : -1.0;
+          b += sg * dtg * s->ay[c] * s->ky[c] * s->ryp[c] * s->ryp[c] * s->vyp[c] * s->siny[c];
+          sg = (s->bot[c] > s->bot[cs]) ? -1.0 : 1.0;
+          b += sg * dtg * s->ay[cs] * s->ky[cs] * s->ryp[cs] * s->ryp[cs] * s->vyp[cs] *
+               s->siny[cs];
+        } else if (s->follow_terrain) {
           double sg = (s->bot[ce] > s->bot[c]) ? 1.0 : -1.0;
           b += sg * dtg * s->ax[c] * s->kx[c] * s->sinx[c];
           sg = (s->bot[c] > s->bot[cw]) ? -1.0 : 1.0;
@@ -877,24 +1009,26 @@ static void assemble(oracle_gw* s, double dtg) {
           b += sg * dtg * s->ay[cs] * s->ky[cs] * s->siny[cs];
         }
         if (east) {
-          if (s->xpc[col] == FLUX) b += s->ax[c] * s->xpv[col] * dtg;
+          if (s->xpc[col] == FLUX) b += s->rxp[c] * s->ax[c] * s->xpv[col] * dtg;
           else b -= gxp * s->hn[ce];
         }
         if (west) {
-          if (s->xmc[col] == FLUX) b += s->ax[cw] * s->xmv[col] * dtg;
+          if (s->xmc[col] == FLUX) b += s->rxp[cw] * s->ax[cw] * s->xmv[col] * dtg;
           else b -= gxm * s->hn[cw];
         }
         if (north) {
-          if (s->ypc[col] == FLUX) b += s->ay[c] * s->ypv[col] * dtg;
+          if (s->ypc[col] == FLUX) b += s->ryp[c] * s->ay[c] * s->ypv[col] * dtg;
           else b -= gyp * s->hn[cn];
         }
         if (south) {
-          if (s->ymc[col] == FLUX) b += s->ay[cs] * s->ymv[col] * dtg;
+          if (s->ymc[col] == FLUX) b += s->ryp[cs] * s->ay[cs] * s->ymv[col] * dtg;
           else b -= gym * s->hn[cs];
         }
         if (k == nz - 1) {
           if (s->botc[col] == FLUX) {
-            b += dtg * volume * (s->botv[col] + s->kz[IF(s, j, i, nz)]) / s->dz[c];
+            const size_t fb = IF(s, j, i, nz);
+            b += dtg * s->rzp[fb] * volume *
+                 (s->botv[col] + s->kz[fb] * s->rzp[fb] * s->vzp[fb]) / s->dz[c];
           } else if (s->botc[col] == HEAD) {
             b -= gzp * s->botv[col];
           }
@@ -909,20 +1043,23 @@ static void assemble(oracle_gw* s, double dtg) {
             const double roomTop = fmax(0.0, (0.9999 * s->wcs[c] - s->wcn[c]) * s->dz[c]);
             const double take = fmin(s->avail[col], roomTop);
             const double qSupply = -take / dtg;
-            b += -dtg * volume * (qSupply + s->kz[IF(s, j, i, k)]) / s->dz[c];
+            b += -dtg * s->rzp[fm] * volume * (qSupply + s->kz[fm] * s->rzp[fm] * s->vzp[fm]) /
+                 s->dz[c];
           } else {
             double qtop = 0.0;
             if (s->topc[col] == FLUX) {
               const double v = s->topv[col];
               if ((v > 0.0 && s->wcn[c] < s->wcs[c]) || (v < 0.0 && s->wcn[c] > s->wcr[c])) qtop = v;
             }
-            b += -dtg * volume * (qtop + s->kz[IF(s, j, i, k)]) / s->dz[c];
+            b += -dtg * s->rzp[fm] * volume * (qtop + s->kz[fm] * s->rzp[fm] * s->vzp[fm]) /
+                 s->dz[c];
           }
         } else if (top) {
           if (s->topc[col] == HEAD) {
             b -= gzm * s->topv[col];
           } else if (s->topc[col] == FLUX) {
-            b += -dtg * volume * (s->topv[col] + s->kz[IF(s, j, i, k)]) / s->dz[c];
+            b += -dtg * s->rzp[fm] * volume *
+                 (s->topv[col] + s->kz[fm] * s->rzp[fm] * s->vzp[fm]) / s->dz[c];
           }
         }
         double* v = s->vals7 + 7 * (size_t)row;
@@ -1050,7 +1187,7 @@ static void fluxes(oracle_gw* s, double dtg) {
         if (i == 0) {
           const size_t c = I3(s, j, 1, k);
           const double kf = vg_k(soil_at(s, c), s->h[c], s->ksx[c]);
-          q = faceA * kf * s->cosx[f] * (s->h[c] - s->h[f]) / (0.5 * dx);
+          q = faceA * kf * s->vxp[f] * s->cosx[f] * (s->h[c] - s->h[f]) / (0.5 * dx);
         } else {
           const size_t c = f, e = I3(s, j, i + 1, k);
           const double kc = vg_k(soil_at(s, c), s->h[c], s->ksx[c]);
@@ -1071,7 +1208,12 @@ static void fluxes(oracle_gw* s, double dtg) {
             }
             if (s->gid[c] < 0 || s->gid[e] < 0) kf = 0.0;
           }
-          q = faceA * (kf * s->cosx[f] * (s->h[e] - s->h[c]) / delta + sg * kf * s->sinx[f]);
+          if (s->pc) /* along-layer gravity with r v (the theta update adds the second r) */
+            q = faceA * (kf * s->vxp[f] * s->cosx[f] * (s->h[e] - s->h[c]) / delta +
+                         sg * kf * s->rxp[f] * s->vxp[f] * s->sinx[f]);
+          else
+            q = faceA * (kf * s->vxp[f] * s->cosx[f] * (s->h[e] - s->h[c]) / delta +
+                         sg * kf * s->sinx[f]);
           if (!s->full3d && ((s->gid[c] >= 0 && s->wc[c] < s->wcs[c]) ||
                              (s->gid[e] >= 0 && s->wc[e] < s->wcs[e])))
             q = 0.0;
@@ -1096,7 +1238,7 @@ static void fluxes(oracle_gw* s, double dtg) {
         if (j == 0) {
           const size_t c = I3(s, 1, i, k);
           const double kf = vg_k(soil_at(s, c), s->h[c], s->ksy[c]);
-          q = faceA * kf * s->cosy[f] * (s->h[c] - s->h[f]) / (0.5 * dy);
+          q = faceA * kf * s->vyp[f] * s->cosy[f] * (s->h[c] - s->h[f]) / (0.5 * dy);
         } else {
           const size_t c = f, n = I3(s, j + 1, i, k);
           const double kc = vg_k(soil_at(s, c), s->h[c], s->ksy[c]);
@@ -1117,7 +1259,12 @@ static void fluxes(oracle_gw* s, double dtg) {
             }
             if (s->gid[c] < 0 || s->gid[n] < 0) kf = 0.0;
           }
-          q = faceA * (kf * s->cosy[f] * (s->h[n] - s->h[c]) / delta + sg * kf * s->siny[f]);
+          if (s->pc)
+            q = faceA * (kf * s->vyp[f] * s->cosy[f] * (s->h[n] - s->h[c]) / delta +
+                         sg * kf * s->ryp[f] * s->vyp[f] * s->siny[f]);
+          else
+            q = faceA * (kf * s->vyp[f] * s->cosy[f] * (s->h[n] - s->h[c]) / delta +
+                         sg * kf * s->siny[f]);
           if (!s->full3d && ((s->gid[c] >= 0 && s->wc[c] < s->wcs[c]) ||
                              (s->gid[n] >= 0 && s->wc[n] < s->wcs[n])))
             q = 0.0;
@@ -1137,6 +1284,7 @@ static void fluxes(oracle_gw* s, double dtg) {
     for (int i = 1; i <= nx; ++i)
       for (int k = 0; k <= nz; ++k) {
         const size_t col = I2(s, j, i);
+        const double rz = s->rzp[IF(s, j, i, k)], vz = s->vzp[IF(s, j, i, k)];
         const int below = (k < nz) && s->gid[I3(s, j, i, k)] >= 0;
         const int above = (k >= 1) && s->gid[I3(s, j, i, k - 1)] >= 0;
         double q = 0.0;
@@ -1153,7 +1301,7 @@ static void fluxes(oracle_gw* s, double dtg) {
             q = -take * az / dtg;
             s->avail[col] -= take;
           } else if (m == 1) {
-            q = az * ks * ((s->h[c] - depth) / delta - 1.0);
+            q = az * ks * vz * ((s->h[c] - depth) / delta - rz);
             if (q < 0.0) {
               const double need = -q * dtg / az;
               if (need > s->avail[col]) {
@@ -1164,7 +1312,7 @@ static void fluxes(oracle_gw* s, double dtg) {
               }
             }
           } else if (s->pc && m == 3) {
-            q = az * ks * ((s->h[c] - depth) / delta - 1.0);
+            q = az * ks * vz * ((s->h[c] - depth) / delta - rz);
             if (q <= 0.0) {
               s->pc_clamp += -q * dtg;
               q = 0.0;
@@ -1173,7 +1321,7 @@ static void fluxes(oracle_gw* s, double dtg) {
             const double kGhost = vg_k(soil_at(s, c), depth, ks);
             const double kCell = vg_k(soil_at(s, c), s->h[c], ks);
             const double kface = 0.5 * (kGhost + kCell);
-            q = az * kface * ((s->h[c] - depth) / delta - 1.0);
+            q = az * kface * vz * ((s->h[c] - depth) / delta - rz);
             if (q <= 0.0) q = 0.0;
             if (s->topc[col] == FLUX) {
               const double v = s->topv[col];
@@ -1187,7 +1335,7 @@ static void fluxes(oracle_gw* s, double dtg) {
             q = s->topv[col] * az;
           } else if (code == HEAD) {
             const double delta = 0.5 * s->dz[c];
-            q = az * s->ksz[c] * ((s->h[c] - s->topv[col]) / delta - 1.0);
+            q = az * s->ksz[c] * vz * ((s->h[c] - s->topv[col]) / delta - rz);
           }
         } else if (k == nz && above) {
           const size_t c = I3(s, j, i, k - 1);
@@ -1196,10 +1344,10 @@ static void fluxes(oracle_gw* s, double dtg) {
           if (code == FLUX) {
             q = s->botv[col] * az;
           } else if (code == GRAVITY) {
-            q = -kf * az;
+            q = -kf * vz * rz * az;
           } else if (code == HEAD) {
             const double delta = 0.5 * s->dz[c];
-            q = az * kf * ((s->botv[col] - s->h[c]) / delta - 1.0);
+            q = az * kf * vz * ((s->botv[col] - s->h[c]) / delta - rz);
           }
         } else if (above && below) {
           const size_t up = I3(s, j, i, k - 1), lo = I3(s, j, i, k);
@@ -1215,7 +1363,7 @@ static void fluxes(oracle_gw* s, double dtg) {
             kf = 0.5 * (ka + kb);
           }
           const double delta = 0.5 * (s->dz[up] + s->dz[lo]);
-          q = az * kf * ((s->h[lo] - s->h[up]) / delta - 1.0);
+          q = az * kf * vz * ((s->h[lo] - s->h[up]) / delta - rz);
         }
         s->qz[IF(s, j, i, k)] = q;
       }
@@ -1269,13 +1417,16 @@ static double update_wc(oracle_gw* s, double dtg) {
         const size_t c = I3(s, j, i, k);
         if (s->gid[c] < 0) continue;
         const double volume = az * s->dz[c];
-        const double coeff = volume * (1.0 + ss * (s->h[c] - s->hn[c]) / s->wcs[c]);
-        const double dqx = dtg * (s->qx[c] - s->qx[I3(s, j, i - 1, k)]);
-        const double dqy = dtg * (s->qy[c] - s->qy[I3(s, j - 1, i, k)]);
-        const double dqz = dtg * (s->qz[IF(s, j, i, k + 1)] - s->qz[IF(s, j, i, k)]);
-        const double upd = (s->wcn[c] * volume + dqx + dqy + dqz) / coeff;
+        const double r = s->rrho[c];
+        const double coeff = volume * (r + r * ss * (s->h[c] - s->hn[c]) / s->wcs[c]);
+        const size_t cw = I3(s, j, i - 1, k), cs = I3(s, j - 1, i, k);
+        const size_t fp = IF(s, j, i, k + 1), fm = IF(s, j, i, k);
+        const double dqx = dtg * (s->qx[c] * s->rxp[c] - s->qx[cw] * s->rxp[cw]);
+        const double dqy = dtg * (s->qy[c] * s->ryp[c] - s->qy[cs] * s->ryp[cs]);
+        const double dqz = dtg * (s->qz[fp] * s->rzp[fp] - s->qz[fm] * s->rzp[fm]);
+        const double upd = (s->wcn[c] * r * volume + dqx + dqy + dqz) / coeff;
         s->wc[c] = upd;
-        sum += upd * volume * ss * (s->h[c] - s->hn[c]) / s->wcs[c];
+        sum += upd * volume * r * ss * (s->h[c] - s->hn[c]) / s->wcs[c];
       }
   return sum;
 }
@@ -1298,13 +1449,13 @@ static split_t gradient_split(const oracle_gw* s, int j, int i, int k) { /* :205
               ? (hR[c] - hR[I3(s, j - 1, i, k)]) / s->dy : 0.0;
   if (ACT(j, i, k + 1) && s->kz[IF(s, j, i, k + 1)] > 0.0) {
     const double dzp = 0.5 * (s->dz[c] + s->dz[c + 1]);
-    dh[4] = (hR[c + 1] - hR[c]) / dzp - 1.0;
+    dh[4] = (hR[c + 1] - hR[c]) / dzp - (s->dgrad ? s->rzp[IF(s, j, i, k + 1)] : 1.0);
   } else {
     dh[4] = 0.0;
   }
   if (ACT(j, i, k - 1) && s->kz[IF(s, j, i, k)] > 0.0) {
     const double dzm = 0.5 * (s->dz[c] + s->dz[c - 1]);
-    dh[5] = (hR[c] - hR[c - 1]) / dzm - 1.0;
+    dh[5] = (hR[c] - hR[c - 1]) / dzm - (s->dgrad ? s->rzp[IF(s, j, i, k)] : 1.0);
   } else {
     dh[5] = 0.0;
   }
@@ -1615,7 +1766,9 @@ int oracle_gw_step(oracle_gw* s, double t, double dtg, frehg_gw_step_info* info)
     set_err("oracle_gw_step: no state");
     return FREHG_GW_ESTATE;
   }
-  /* step-start refresh (RichardsSolver.cpp:743-748) */
+  /* step-start refresh (RichardsSolver.cpp:743-748): the ratios first, so
+   * the hydrostatic edge ghosts see this step's */
+  update_baroclinic(s);
   enforce_head_bc(s);
   enforce_moisture_bc(s);
   memcpy(s->hn, s->h, s->n3 * sizeof(double));
@@ -1719,6 +1872,14 @@ int oracle_gw_get_field(const oracle_gw* s, int field, double* out) {
     case FREHG_GW_FIELD_COSY: src = s->cosy; kind = 2; break;
     case FREHG_GW_FIELD_QZ: src = s->qz; kind = 3; break;
     case FREHG_GW_FIELD_KZ: src = s->kz; kind = 3; break;
+    case FREHG_GW_FIELD_RHO: src = s->rrho; break;
+    case FREHG_GW_FIELD_VISC: src = s->rvisc; break;
+    case FREHG_GW_FIELD_RHO_X: src = s->rxp; kind = 1; break;
+    case FREHG_GW_FIELD_VISC_X: src = s->vxp; kind = 1; break;
+    case FREHG_GW_FIELD_RHO_Y: src = s->ryp; kind = 2; break;
+    case FREHG_GW_FIELD_VISC_Y: src = s->vyp; kind = 2; break;
+    case FREHG_GW_FIELD_RHO_Z: src = s->rzp; kind = 3; break;
+    case FREHG_GW_FIELD_VISC_Z: src = s->vzp; kind = 3; break;
     default: set_err("oracle_gw_get_field: unknown field"); return FREHG_GW_EINVAL;
   }
   size_t q = 0;
@@ -1954,5 +2115,48 @@ int oracle_gw_window(const oracle_gw* s, int which, double* out) {
   const double* src = which == 0 ? s->wx : which == 1 ? s->wy : which == 2 ? s->wz : s->wvent;
   const size_t n = which == 2 ? s->n3f : which == 3 ? s->n2 : s->n3;
   memcpy(out, src, n * sizeof(double));
+  return FREHG_GW_OK;
+}
+
+/* ------------------------------------------------------------------ density coupling
+ * attachScalar (baroclinic on) + attachTemperature + setDensityCoefficients
+ * (RichardsSolver.hpp:191-225) with the scalar fields owned here, zeroed. */
+int oracle_gw_attach_density(oracle_gw* s, int saline, int thermal, const frehg_gw_density* dc) {
+  if (!dc || (!saline && !thermal)) {
+    set_err("oracle_gw_attach_density: no scalar or no coefficients");
+    return FREHG_GW_EINVAL;
+  }
+  s->baro = 1;
+  s->saline = saline != 0;
+  s->thermal = thermal != 0;
+  s->beta_s = dc->beta_saline;
+  s->beta_sv = dc->beta_saline_visc;
+  s->beta_t = dc->thermal_expansion;
+  s->t_ref = dc->reference_temperature;
+  s->dgrad = dc->reallocation_gradient != 0;
+  if (s->saline && !s->s3) {
+    s->s3 = xcalloc(s->n3, sizeof(double));
+    s->s2 = xcalloc(s->n2, sizeof(double));
+  }
+  if (s->thermal && !s->t3) {
+    s->t3 = xcalloc(s->n3, sizeof(double));
+    s->t2 = xcalloc(s->n2, sizeof(double));
+  }
+  return FREHG_GW_OK;
+}
+
+/* Scalar `which` (FREHG_GW_SCALAR_*): copied out when out is given, then
+ * overwritten from in when in is given. */
+int oracle_gw_scalar(oracle_gw* s, int which, double* out, const double* in) {
+  double* f = which == FREHG_GW_SCALAR_SALINE ? s->s3 : which == FREHG_GW_SCALAR_SALINE_SURF ? s->s2
+            : which == FREHG_GW_SCALAR_TEMP ? s->t3 : which == FREHG_GW_SCALAR_TEMP_SURF ? s->t2
+                                                                                : NULL;
+  if (!f) {
+    set_err("oracle_gw_scalar: scalar not attached");
+    return FREHG_GW_EINVAL;
+  }
+  const size_t n = (which == FREHG_GW_SCALAR_SALINE || which == FREHG_GW_SCALAR_TEMP) ? s->n3 : s->n2;
+  if (out) memcpy(out, f, n * sizeof(double));
+  if (in) memcpy(f, in, n * sizeof(double));
   return FREHG_GW_OK;
 }

@@ -62,6 +62,13 @@ int oracle_gw_enable_transport_window(oracle_gw* s);
 void oracle_gw_reset_transport_window(oracle_gw* s);
 int oracle_gw_window(const oracle_gw* s, int which, double* out);
 
+/* Density coupling (RichardsSolver::attachScalar / attachTemperature /
+ * setDensityCoefficients, RichardsSolver.hpp:191-225; Baroclinic.cpp) with the
+ * scalars owned by the oracle (halo layouts, FREHG_GW_SCALAR_*); the ratios
+ * come back through oracle_gw_get_field (FREHG_GW_FIELD_RHO .. VISC_Z). */
+int oracle_gw_attach_density(oracle_gw* s, int saline, int thermal, const frehg_gw_density* dc);
+int oracle_gw_scalar(oracle_gw* s, int which, double* out, const double* in);
+
 /* Pointwise closures (src/gw/VanGenuchten.hpp:45-128), exported for the
  * golden-value tests. */
 double oracle_vg_theta(double vga, double vgn, double ts, double tr, double aev, double h);

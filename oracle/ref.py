@@ -17,7 +17,7 @@ from typing import Optional
 
 import numpy as np
 
-from frehg_b200.abi import interior_from_halo
+from frehg_b200.abi import SCALARS, interior_from_halo
 from frehg_b200.config import GwConfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -89,6 +89,9 @@ def load(omp: bool = False):
     lib.ref_enable_transport_window.argtypes = [C.c_void_p]
     lib.ref_reset_transport_window.argtypes = [C.c_void_p]
     lib.ref_window.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.ref_attach_density.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_int]
+    lib.ref_scalar.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
     _libs[path] = lib
     return lib
 
@@ -208,7 +211,7 @@ class RefSolver:
 
     # -- observation -----------------------------------------------------------
     def _halo_shape(self, name):
-        nz = self.nz + 1 if name in ("qz", "kz") else self.nz
+        nz = self.nz + 1 if name in ("qz", "kz", "rho_z") else self.nz
         return (self.ny + 2, self.nx + 2, nz)
 
     def halo_field(self, name: str) -> np.ndarray:
@@ -323,3 +326,29 @@ class RefSolver:
         if self.lib.ref_window(self.h, self.WINDOWS[name], out.ctypes.data_as(_dp)) != 0:
             raise KeyError(name)
         return out
+
+    # -- density coupling ---------------------------------------------------------
+    def attach_density(self, saline: bool = True, thermal: bool = False,
+                       beta_saline: float = 0.000744, beta_saline_visc: float = 0.0022,
+                       thermal_expansion: float = 0.0, reference_temperature: float = 20.0,
+                       reallocation_gradient: bool = False) -> None:
+        """attachScalar (baroclinic on) / attachTemperature /
+        setDensityCoefficients with harness-owned scalar views, zeroed."""
+        self.lib.ref_attach_density(self.h, int(saline), int(thermal), beta_saline,
+                                    beta_saline_visc, thermal_expansion, reference_temperature,
+                                    int(reallocation_gradient))
+
+    def _scalar_shape(self, which):
+        return ((self.ny + 2, self.nx + 2, self.nz) if SCALARS[which] in (0, 2)
+                else (self.ny + 2, self.nx + 2))
+
+    def scalar(self, which: str) -> np.ndarray:
+        out = np.empty(self._scalar_shape(which))
+        if self.lib.ref_scalar(self.h, SCALARS[which], out.ctypes.data_as(_dp), None) != 0:
+            raise KeyError(which)
+        return out
+
+    def set_scalar(self, which: str, value) -> None:
+        v = np.ascontiguousarray(np.broadcast_to(value, self._scalar_shape(which)), np.float64)
+        if self.lib.ref_scalar(self.h, SCALARS[which], None, v.ctypes.data_as(_dp)) != 0:
+            raise KeyError(which)

@@ -78,6 +78,9 @@ struct RefSim {
   frehg::gw::GwCoupling coupling;
   std::unique_ptr<frehg::swe::SurfaceSolver> surface;
   std::unique_ptr<frehg::coupling::Coupler> coupler;
+  // density coupling: harness-owned scalar views (ref_attach_density)
+  frehg::Field3<double> salt, temp;
+  frehg::Field2<double> saltSurf, tempSurf;
 };
 
 std::string g_error;
@@ -279,6 +282,10 @@ int ref_get(void* h, const char* name, double* out) {
   else if (n == "ky") copyOut(gw.faceConductivityY(), out);
   else if (n == "kz") copyOut(gw.faceConductivityZFace(), out);
   else if (n == "vloss") copyOut(gw.vlossField(), out);
+  else if (n == "rho") copyOut(gw.densityRatio(), out);
+  else if (n == "visc") copyOut(gw.viscosityRatio(), out);
+  else if (n == "rho_y") copyOut(gw.densityRatioFaceY(), out);
+  else if (n == "rho_z") copyOut(gw.densityRatioFaceZ(), out);
   else if (n == "dz3d") copyOut(mesh.dz3d(), out);
   else if (n == "bot3d") copyOut(mesh.bot3d(), out);
   else if (n == "ax") copyOut(mesh.areaX(), out);
@@ -499,6 +506,54 @@ int ref_window(void* h, int which, double* out) {
   else if (which == 3)
     std::memcpy(out, gw.windowVentVolume().data(), gw.windowVentVolume().span() * sizeof(double));
   else return 1;
+  return 0;
+}
+
+/// RichardsSolver::attachScalar (baroclinic on) / attachTemperature /
+/// setDensityCoefficients with harness-owned scalar views, zeroed.
+int ref_attach_density(void* h, int saline, int thermal, double beta_s, double beta_sv,
+                       double beta_t, double t_ref, int dgrad) {
+  RefSim& s = *static_cast<RefSim*>(h);
+  const std::size_t ny2 = static_cast<std::size_t>(s.grid->nyLocal()) + 2;
+  const std::size_t nx2 = static_cast<std::size_t>(s.grid->nxLocal()) + 2;
+  const std::size_t nz = static_cast<std::size_t>(s.grid->nz());
+  frehg::DensityCouplingConfig dc;
+  dc.enabled = true;
+  dc.betaSaline = beta_s;
+  dc.betaSalineViscosity = beta_sv;
+  dc.thermalExpansion = beta_t;
+  dc.referenceTemperature = t_ref;
+  dc.densityReallocationGradient = dgrad != 0;
+  s.gw->setDensityCoefficients(dc);
+  if (saline) {
+    s.salt = frehg::Field3<double>("salt", ny2, nx2, nz);
+    s.saltSurf = frehg::Field2<double>("salt_surf", ny2, nx2);
+  }
+  s.gw->attachScalar(s.salt, s.saltSurf, true);
+  if (thermal) {
+    s.temp = frehg::Field3<double>("temp", ny2, nx2, nz);
+    s.tempSurf = frehg::Field2<double>("temp_surf", ny2, nx2);
+    s.gw->attachTemperature(s.temp, s.tempSurf);
+  }
+  return 0;
+}
+
+/// Scalar `which` (0 salinity, 1 surface salinity, 2 temperature, 3 surface
+/// temperature): copied out when out is given, then overwritten from in.
+int ref_scalar(void* h, int which, double* out, const double* in) {
+  RefSim& s = *static_cast<RefSim*>(h);
+  double* f = nullptr;
+  std::size_t n = 0;
+  if (which == 0 && s.salt.size()) { f = s.salt.data(); n = s.salt.span(); }
+  else if (which == 1 && s.saltSurf.size()) { f = s.saltSurf.data(); n = s.saltSurf.span(); }
+  else if (which == 2 && s.temp.size()) { f = s.temp.data(); n = s.temp.span(); }
+  else if (which == 3 && s.tempSurf.size()) { f = s.tempSurf.data(); n = s.tempSurf.span(); }
+  if (!f) {
+    g_error = "scalar not attached";
+    return 1;
+  }
+  if (out) std::memcpy(out, f, n * sizeof(double));
+  if (in) std::memcpy(f, in, n * sizeof(double));
   return 0;
 }
 

@@ -266,6 +266,22 @@ def coupled_surface(bath_halo: np.ndarray, seed: int = 5):
     return bath_halo + pond, rain
 
 
+def density_scalars(nx: int, ny: int, nz: int, step: int = 0, seed: int = 3):
+    """Seeded salinity [g/L] and temperature [C] in the halo layouts
+    ((ny+2, nx+2, nz) cells, ghosts included, and (ny+2, nx+2) surfaces), as
+    a transport module would hand them over after its step `step`: a saline
+    wedge rising toward +x with noise, a warm top layer, both drifting with
+    the step so that each step's ratios differ."""
+    rng = np.random.default_rng(seed)
+    j, i, k = np.meshgrid(np.arange(ny + 2), np.arange(nx + 2), np.arange(nz), indexing="ij")
+    wedge = 35.0 * np.clip((i / (nx + 1)) + (k / max(nz - 1, 1)) - 0.6 + 0.05 * step, 0.0, 1.0)
+    salt = wedge + 2.0 * rng.random((ny + 2, nx + 2, nz))
+    temp = 12.0 + 10.0 * np.exp(-k / max(nz / 4.0, 1.0)) + 0.3 * step + rng.random((ny + 2, nx + 2, nz))
+    salt_surf = 5.0 + 30.0 * rng.random((ny + 2, nx + 2))
+    temp_surf = 25.0 + 3.0 * rng.random((ny + 2, nx + 2))
+    return salt, salt_surf, temp, temp_surf
+
+
 SCENARIOS = {
     "closed_column": lambda: closed_column(),
     "closed_column_ss": lambda: closed_column(1.0e-4),
