@@ -265,7 +265,9 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
         ras = rasterize(cfg)
         vals = (ras.top_value, ras.bot_value, ras.xm_value, ras.xp_value, ras.ym_value,
                 ras.yp_value)
-        h2d = 6 * (nx + 2) * (ny + 2) * 8
+        # what the library uploads: the top and bottom slots ((nx+2)(ny+2)
+        # each) and the four sides' edge entries
+        h2d = (2 * (nx + 2) * (ny + 2) + 2 * ny + 2 * nx) * 8
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):

@@ -318,20 +318,37 @@ int frehg_gw_set_stream(frehg_gw_handle* h, void* stream) {
 int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* bot,
                            const double* xm, const double* xp, const double* ym, const double* yp) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
-  const fgw::Dims& d = h->D.d;
+  fgw::Device& D = h->D;
+  const fgw::Dims& d = D.d;
   const long long nc = d.ncol;
+  // The staging is rewritten below: the previous upload must have landed
+  // (a no-op after a step, which synchronizes at its end).
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "set_bc_values");
+  const double off = h->offset;
+  bool bad = false;
+  // Interior row j of a per-column slot from the caller's (ny, nx) array.
+  auto row = [&](int slot, const double* src, int j) {
+    const long long base = slot * nc + fgw::col2(d, j, 1);
+    const int* cd = h->codes.data() + base;
+    double* dst = h->values.data() + base;
+    const double* sr = src + static_cast<long long>(j - 1) * d.nx;
+    bool b = false;
+    for (int i = 0; i < d.nx; ++i) {
+      const double v = sr[i] + (cd[i] == FREHG_GW_BC_HEAD_HYDROSTATIC ? off : 0.0);
+      dst[i] = v;
+      b |= !std::isfinite(v);
+    }
+    bad |= b;
+  };
   auto put = [&](int slot, long long col, double v) {
     const int code = h->codes[slot * nc + col];
-    h->values[slot * nc + col] = v + (code == FREHG_GW_BC_HEAD_HYDROSTATIC ? h->offset : 0.0);
+    v += (code == FREHG_GW_BC_HEAD_HYDROSTATIC ? off : 0.0);
+    h->values[slot * nc + col] = v;
+    bad |= !std::isfinite(v);
   };
   for (int j = 1; j <= d.ny; ++j) {
-    for (int i = 1; i <= d.nx; ++i) {
-      const long long q = static_cast<long long>(j - 1) * d.nx + (i - 1);
-      if (top) put(0, fgw::col2(d, j, i), top[q]);
-      if (bot) put(1, fgw::col2(d, j, i), bot[q]);
-    }
-  }
-  for (int j = 1; j <= d.ny; ++j) {
+    if (top) row(0, top, j);
+    if (bot) row(1, bot, j);
     if (xm) put(2, fgw::col2(d, j, 1), xm[j - 1]);
     if (xp) put(3, fgw::col2(d, j, d.nx), xp[j - 1]);
   }
@@ -339,12 +356,25 @@ int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* 
     if (ym) put(4, fgw::col2(d, 1, i), ym[i - 1]);
     if (yp) put(5, fgw::col2(d, d.ny, i), yp[i - 1]);
   }
-  for (double v : h->values)
-    if (!std::isfinite(v)) return fail(FREHG_GW_EINVAL, "non-finite boundary value");
-  CUDA_TRY(cudaMemcpyAsync(h->D.values, h->values.data(), h->values.size() * sizeof(double),
-                           cudaMemcpyHostToDevice, h->D.stream),
-           "set_bc_values");
-  CUDA_TRY(cudaStreamSynchronize(h->D.stream), "set_bc_values");
+  if (bad) return fail(FREHG_GW_EINVAL, "non-finite boundary value");
+  // Upload what the kernels read: the top and bottom slots whole, the side
+  // slots' edge entries (a column of the x edges, a row of the y edges).
+  const size_t w = sizeof(double), pitch = static_cast<size_t>(d.nx2) * w;
+  auto slot1d = [&](int slot, long long col, size_t n) {
+    return cudaMemcpyAsync(D.values + slot * nc + col, h->values.data() + slot * nc + col, n * w,
+                           cudaMemcpyHostToDevice, D.stream);
+  };
+  auto xedge = [&](int slot, int i) {
+    const long long col = fgw::col2(d, 1, i);
+    return cudaMemcpy2DAsync(D.values + slot * nc + col, pitch, h->values.data() + slot * nc + col,
+                             pitch, w, static_cast<size_t>(d.ny), cudaMemcpyHostToDevice, D.stream);
+  };
+  if (top) CUDA_TRY(slot1d(0, 0, static_cast<size_t>(nc)), "set_bc_values");
+  if (bot) CUDA_TRY(slot1d(1, 0, static_cast<size_t>(nc)), "set_bc_values");
+  if (xm) CUDA_TRY(xedge(2, 1), "set_bc_values");
+  if (xp) CUDA_TRY(xedge(3, d.nx), "set_bc_values");
+  if (ym) CUDA_TRY(slot1d(4, fgw::col2(d, 1, 1), static_cast<size_t>(d.nx)), "set_bc_values");
+  if (yp) CUDA_TRY(slot1d(5, fgw::col2(d, d.ny, 1), static_cast<size_t>(d.nx)), "set_bc_values");
   return FREHG_GW_OK;
 }
 
