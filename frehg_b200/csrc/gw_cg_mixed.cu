@@ -694,7 +694,7 @@ __device__ __forceinline__ void cg_mixed_body(const MixedArgs& a, const int bid,
       if (threadIdx.x == 0) q0[bid] = s;
       if (!grid_sync(a.st, G)) return;
       const double dpi = reduce_partials(q0, G);
-      if (!(dpi > 0.0)) break;  // inner breakdown: keep d, let the FP64 sweep judge
+      if (!(dpi > 0.0)) break;  // inner breakdown: keep d, the FP64 sweep decides
       const float al = static_cast<float>(beta / dpi);
       betaold = beta;
       ++total;
