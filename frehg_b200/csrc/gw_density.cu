@@ -66,7 +66,8 @@ __global__ void k_baro_faces(Dims d, Fields f, BaroCoef k, const double* __restr
        u += static_cast<long long>(gridDim.x) * blockDim.x) {
     const long long col = u / nzp;
     const int kk = static_cast<int>(u - col * nzp);
-    const int j = static_cast<int>(col / d.nx2), i = static_cast<int>(col - j * d.nx2);
+    const int j = static_cast<int>(col / d.nx2);
+    const int i = static_cast<int>(col - static_cast<long long>(j) * d.nx2);
     if (kk < d.nz) {
       const long long c = cidx(d, j, i, kk);
       if (j >= 1 && j <= d.ny && i <= d.nx) {  // x face slot (j, i): face i + 1/2
