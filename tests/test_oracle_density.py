@@ -114,3 +114,30 @@ def test_unattached_ratios_are_one():
     o.advance()
     for name in ("rho", "visc", "rho_x", "rho_y", "rho_z", "visc_x", "visc_y", "visc_z"):
         assert np.all(o.field(name) == 1.0), name
+
+
+def test_density_restart_bitwise():
+    # refreshDerivedState (RichardsSolver.cpp:880-890) recomputes the ratios
+    # before the ghosts: a state overwritten mid-run then stepped matches.
+    cfg = cases.SCENARIOS["hydrostatic_side"]()
+    r = refmod.RefSolver(cfg, pc="jacobi")
+    o = OracleSolver(cfg)
+    kw = DENSITY["both_gradient"]
+    for x in (r, o):
+        x.attach_density(**kw)
+    for n in range(3):
+        hand_over(r, o, cfg, n, True, True)
+        r.advance()
+        o.advance()
+    h, wc = o.field("h"), o.field("wc")
+    h = h + 0.01 * np.sin(np.arange(h.size)).reshape(h.shape)
+    hand_over(r, o, cfg, 7, True, True)
+    r.set_state_interior(h, wc)
+    o.set_state(h, wc)
+    for name in ("h", "rho", "rho_y", "rho_z"):
+        np.testing.assert_array_equal(o.field(name), r.field(name), err_msg=name)
+    for n in range(3):
+        hand_over(r, o, cfg, 8 + n, True, True)
+        r.advance()
+        o.advance()
+        compare(r, o, f"after restart {n}")
