@@ -75,7 +75,8 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
                    help="form of the headline value; the other form is timed too")
     p.add_argument("--size", default="512,512,128")
-    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--e2e-steps", type=int, default=-1,
+                   help="steps of the e2e leg (-1: the timed steps themselves, replayed)")
     p.add_argument("--cpu-sample", default="64,64,128")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="slab", choices=["slab", "ensemble", "serve"],
@@ -227,6 +228,9 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
     active = gw.activeCells()
     for _ in range(args.warmup):
         gw.advance()
+    # The e2e leg replays the timed steps from this state (the step gets
+    # cheaper as the run proceeds, so both legs must time the same steps).
+    ck = gw.checkpoint() if e2e_steps else None
     gw.setProfiling(True)
     launches0 = gw.kernelLaunches()
     iters, outer, solve_ms = 0, 0, 0.0
@@ -258,6 +262,8 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
                solve_ms=solve_ms, launches=launches, clocks=clocks.summary(), active=active,
                e2e=None)
     if e2e_steps:
+        e2e_steps = args.steps if e2e_steps < 0 else e2e_steps
+        gw.restore(ck)
         # End to end through the public API, as a driver calls it each step:
         # that step's boundary values uploaded from host memory (the handle's
         # page-locked staging), the step, and its audit record read back.  The
