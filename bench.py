@@ -112,8 +112,14 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.first = threading.Event()
+        self.start_n = 0
 
     def __enter__(self):
+        # nvidia-smi's start-up (its NVML initialisation) runs before the
+        # region: the region starts once the first sample has arrived, and the
+        # summary keeps the samples taken inside it (the pre-region one only
+        # when the region was shorter than the sampling period).
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
@@ -121,6 +127,8 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.first.wait(timeout=5.0)
+            self.start_n = len(self.lines)
         except Exception:
             self.proc = None
         return self
@@ -128,6 +136,7 @@ class ClockSampler:
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
+            self.first.set()
 
     def __exit__(self, *exc):
         if self.proc:
@@ -140,7 +149,8 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        inside = self.lines[self.start_n:]
+        for ln in (inside if inside else self.lines):
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
