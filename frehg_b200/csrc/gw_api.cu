@@ -321,9 +321,6 @@ int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* 
   fgw::Device& D = h->D;
   const fgw::Dims& d = D.d;
   const long long nc = d.ncol;
-  // The staging is rewritten below: the previous upload must have landed
-  // (a no-op after a step, which synchronizes at its end).
-  CUDA_TRY(cudaStreamSynchronize(D.stream), "set_bc_values");
   const double off = h->offset;
   bool bad = false;
   // Interior row j of a per-column slot from the caller's (ny, nx) array.
@@ -375,6 +372,9 @@ int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* 
   if (xp) CUDA_TRY(xedge(3, d.nx), "set_bc_values");
   if (ym) CUDA_TRY(slot1d(4, fgw::col2(d, 1, 1), static_cast<size_t>(d.nx)), "set_bc_values");
   if (yp) CUDA_TRY(slot1d(5, fgw::col2(d, d.ny, 1), static_cast<size_t>(d.nx)), "set_bc_values");
+  // Landed before returning: a batch or a server steps the member on a
+  // stream of its own, and the staging is free for the next call.
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "set_bc_values");
   return FREHG_GW_OK;
 }
 

@@ -186,10 +186,9 @@ int frehg_gw_destroy(frehg_gw_handle* h);
 int frehg_gw_set_stream(frehg_gw_handle* h, void* cuda_stream);
 
 /* Boundary values (host arrays shaped like the codes; NULL keeps the current
- * values).  Hydrostatic stages are given in the unshifted datum.  The arrays
- * are read before the call returns; the upload to the device (the top and
- * bottom values, the sides' edge entries) is queued on the handle's stream
- * ahead of the next step. */
+ * values).  Hydrostatic stages are given in the unshifted datum.  The upload
+ * (the top and bottom values, the sides' edge entries: all the step reads)
+ * has landed when the call returns. */
 int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top_value,
                            const double* bot_value, const double* xm_value,
                            const double* xp_value, const double* ym_value,
