@@ -141,3 +141,23 @@ def test_density_restart_bitwise():
         r.advance()
         o.advance()
         compare(r, o, f"after restart {n}")
+
+
+def test_density_with_transport_window_bitwise():
+    # The window accumulates the step's volumetric face fluxes q dtg and the
+    # walks' path records; with the density ratios in the fluxes it must
+    # still follow the reference's bit for bit.
+    cfg = cases.SCENARIOS["hydrostatic_side"]()
+    r = refmod.RefSolver(cfg, pc="jacobi")
+    o = OracleSolver(cfg)
+    kw = DENSITY["both_gradient"]
+    for x in (r, o):
+        x.attach_density(**kw)
+        x.enable_transport_window()
+    for n in range(6):
+        hand_over(r, o, cfg, n, True, True)
+        r.advance()
+        o.advance()
+        compare(r, o, f"window step {n}")
+        for name in ("x", "y", "z"):
+            np.testing.assert_array_equal(o.window(name), r.window(name), err_msg=f"{name} {n}")
