@@ -175,3 +175,42 @@ def test_unattached_ratios_are_one_and_batch_refuses_density():
     finally:
         a.close()
         b.close()
+
+
+def test_density_with_transport_window_matches_oracle():
+    # FP64 form in lockstep with the oracle, density coupling and the window
+    # both on: the windows within 1e-8 of their scale (floor: the faces'
+    # gravity term K A times the elapsed time, as in the window test).
+    from frehg_b200.abi import interior_from_halo
+
+    cfg = copy.deepcopy(cases.SCENARIOS["hydrostatic_side"]())
+    cfg.solver.precision = "fp64"
+    kw = DENSITY["both_gradient"]
+    g = RichardsSolver(copy.deepcopy(cfg))
+    o = OracleSolver(cfg)
+    try:
+        g.attachDensity(**kw)
+        o.attach_density(**kw)
+        g.enableTransportWindow()
+        o.enable_transport_window()
+        d = cfg.domain
+        t = elapsed = 0.0
+        names = {"x": "win_x", "y": "win_y", "z": "win_z"}
+        for n in range(6):
+            hand_over(g, o, cfg, n, kw)
+            dtg = o.next_dt()
+            t += dtg
+            elapsed += dtg
+            o.step(t, dtg)
+            info = g.step(t, dtg)
+            check(g, o, cfg, info, False, f"step {n}")
+            floor = {"x": float(np.max(np.abs(g.field("kx") * g.field("ax")))),
+                     "y": float(np.max(np.abs(g.field("ky") * g.field("ay")))),
+                     "z": float(np.max(np.abs(g.field("kz")))) * d.dx * d.dy}
+            for w, name in names.items():
+                ref = interior_from_halo(name, o.window(w), d.nx, d.ny, d.nz)
+                fl = max(floor[w] * elapsed, 1e-15)
+                assert rel(g.field(name), ref, fl) <= 1e-8, f"window {w} step {n}"
+    finally:
+        g.close()
+        o.close()
