@@ -171,6 +171,13 @@ class OracleSolver:
     def elevation_offset(self) -> float:
         return self.lib.oracle_gw_elevation_offset(self.h)
 
+    def set_boundary_values(self, top=None, bottom=None, xm=None, xp=None, ym=None, yp=None):
+        """updateBoundaryValues: per-column / per-edge values (None keeps)."""
+        arrs = [None if v is None else np.ascontiguousarray(v, np.float64)
+                for v in (top, bottom, xm, xp, ym, yp)]
+        self._check(self.lib.oracle_gw_set_bc_values(
+            self.h, *[None if a is None else a.ctypes.data_as(_dp) for a in arrs]))
+
     # ------------------------------------------------------------ density coupling
     def attach_density(self, saline: bool = True, thermal: bool = False,
                        beta_saline: float = 0.000744, beta_saline_visc: float = 0.0022,

@@ -131,3 +131,35 @@ def test_cg_iteration_cap_reports_divergence():
         with pytest.raises(FatalError) as e:
             g.advance()
         assert e.value.status == 5
+
+
+def test_partial_boundary_updates_match_oracle():
+    # updateBoundaryValues with some slots only (None keeps the others): the
+    # upload sends the top and bottom slots and the sides' edge entries, and
+    # the step must follow the oracle given the same updates.
+    cfg = cases.SCENARIOS["side_flux"]()
+    d = cfg.domain
+    gpu = RichardsSolver(cfg)
+    cpu = OracleSolver(cfg)
+    rng = np.random.default_rng(9)
+    try:
+        updates = [dict(top=-1e-6 * (1.0 + rng.random((d.ny, d.nx)))),
+                   dict(xm=2e-6 * rng.random(d.ny), xp=-1e-6 * rng.random(d.ny)),
+                   dict(ym=1e-6 * rng.random(d.nx)),
+                   dict(yp=-2e-6 * rng.random(d.nx), bottom=np.zeros((d.ny, d.nx))),
+                   dict()]
+        for n, u in enumerate(updates):
+            gpu.setBoundaryValues(**u)
+            cpu.set_boundary_values(**u)
+            dtg = cpu.next_dt()
+            cpu.t += dtg
+            cpu.step(cpu.t, dtg)
+            gpu.step(cpu.t, dtg)
+            assert rel_linf(gpu.field("h"), cpu.field("h"), 1.0) <= H_TOL, f"h step {n}"
+            for name in ("qx", "qy", "qz"):
+                kname, area = FLUX_SCALE[name]
+                a = d.dx * d.dy if area is None else cpu.field(area)
+                floor = max(1e-12, float(np.max(np.abs(cpu.field(kname)) * a)))
+                assert rel_linf(gpu.field(name), cpu.field(name), floor) <= F_TOL, f"{name} {n}"
+    finally:
+        gpu.close()
