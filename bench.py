@@ -8,7 +8,16 @@ clamp, audit, adaptive controller) per timed step, dt driven by the
 step's own controller from dt0 = 60 s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-    python bench.py --impl reference ...   # the reference's CPU step
+    python bench.py --impl reference ...   # the reference's CPU step, full slab
+
+At N = 1 the line also carries, each measured outside the timed region:
+``latency`` (p50 / p99 of the per-step solve and step device times),
+``mixed_error`` (the mixed form against the tight FP64 form over a 10-step
+trajectory: head, flux, storage, audit, iteration counts), ``serve`` (a
+short Poisson stream through the serving loop: p50 / p99 request latency,
+cell-steps/s), ``ensemble`` (a 64-member batch, both forms, against stepping
+the members one by one) and ``cpu_baseline`` (the reference's step on
+crops, both preconditioner lanes, with CG iteration counts).
 
 With N > 1 the script runs under torchrun, one rank per GPU; every rank
 steps its own independent domain (an ensemble member with its own seed), so
@@ -77,7 +86,6 @@ def parse():
     p.add_argument("--size", default="512,512,128")
     p.add_argument("--e2e-steps", type=int, default=-1,
                    help="steps of the e2e leg (-1: the timed steps themselves, replayed)")
-    p.add_argument("--cpu-sample", default="64,64,128")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="slab", choices=["slab", "ensemble", "serve"],
                    help="slab: the 512x512x128 headline; ensemble: many uneven domains "
@@ -88,6 +96,18 @@ def parse():
     p.add_argument("--members", type=int, default=256)
     p.add_argument("--seq-steps", type=int, default=3,
                    help="ensemble: steps of the member-by-member comparison loop")
+    p.add_argument("--ref-steps", type=int, default=2,
+                   help="reference arm: at most this many timed full-size steps (each takes "
+                        "tens of seconds on the host), after one warm-up step")
+    p.add_argument("--error-steps", type=int, default=10,
+                   help="slab: steps of the mixed-vs-FP64 trajectory behind mixed_error "
+                        "(0: skip)")
+    p.add_argument("--summary-members", type=int, default=64,
+                   help="slab: members of the ensemble summary (0: skip)")
+    p.add_argument("--summary-requests", type=int, default=16,
+                   help="slab: requests of the served-stream summary (0: skip)")
+    p.add_argument("--summary-rate", type=float, default=100.0,
+                   help="slab: arrival rate of the served-stream summary, req/s")
     return p.parse_args()
 
 
@@ -166,62 +186,139 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(sample: str, threads: int, warmup: int = 1, steps=None, budget_s: float = 10.0):
-    """The reference's own CPU step (its src/gw compiled on host shims, OpenMP
-    shim backend, the reference's default bjacobi-ICC(0) CG) on a bounded crop
-    of the same workload.  Without `steps`, steps until `budget_s` elapses."""
+def slab_config(size: str) -> dict:
+    """The workload both arms name in their line's ``config``."""
+    nx, ny, nz = (int(v) for v in size.split(","))
+    return {"workload": f"terrain-following heterogeneous slab {nx}x{ny}x{nz} "
+                        "(hillslope, seeded), dt0 60 s adaptive",
+            "active_cells_per_gpu": nx * ny * nz,
+            "l2": "inputs larger than L2 (13 GB working set)"}
+
+
+def ref_lane(size: str, pc: str, threads: int, warmup: int, steps: int):
+    """The reference's own CPU step (its src/gw compiled on host shims,
+    OpenMP shim backend) on the slab of ``size``: ``warmup`` untimed steps
+    (the first, dt0 = 60 s, is the costly one), then ``steps`` timed.  CG
+    iterations are reported for the timed steps and for all of them."""
     from frehg_b200 import workloads
     from oracle import ref as refmod
-    if not refmod.available(omp=True):
-        return None
-    nx, ny, nz = (int(v) for v in sample.split(","))
-    cfg = workloads.hillslope(nx, ny, nz, per_cell_soil=False)
+    nx, ny, nz = (int(v) for v in size.split(","))
+    cfg = workloads.hillslope(nx, ny, nz)
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    r = refmod.RefSolver(cfg, pc="icc", omp=True)
-    for _ in range(max(warmup, 1)):
+    t_setup = time.perf_counter()
+    r = refmod.RefSolver(cfg, pc=pc, omp=True)
+    setup_s = time.perf_counter() - t_setup
+    its_all = []
+    for _ in range(warmup):
         r.advance()
+        its_all.append(r.last_solve()[0])
+    its = []
     t0 = time.perf_counter()
-    n = 0
-    while True:
+    for _ in range(steps):
         r.advance()
-        n += 1
-        if steps is not None and n >= steps:
-            break
-        if steps is None and (time.perf_counter() - t0 > budget_s or n >= 20):
-            break
+        its.append(r.last_solve()[0])
     dt = time.perf_counter() - t0
     _, ktop = r.gid()
     active = int(sum(nz - k for k in ktop.ravel()))
     r.close()
-    return {"value": active * n / dt, "unit": "cell-steps/s", "cores": threads,
+    its_all += its
+    return {"value": active * steps / dt, "unit": "cell-steps/s", "size": size, "pc": pc,
+            "steps": steps, "warmup": warmup, "s_per_step": dt / steps, "setup_s": setup_s,
+            "cg_iterations_mean": sum(its) / len(its), "cg_iterations_max": max(its),
+            "cg_iterations_all_steps": its_all}
+
+
+PC_NAMES = {"icc": "bjacobi-ICC(0) (the reference's default)",
+            "jacobi": "Jacobi (-gw_pc_type jacobi, the GPU FP64 form's preconditioner)"}
+
+
+def cpu_baseline(threads: int):
+    """The reference's CPU step on bounded crops of the slab (about 30 s of
+    host work): both preconditioner lanes on a 64x64x128 crop and the default
+    lane on a 128x128x128 crop, one warm-up and three timed steps each.
+    ``value`` is the default lane on the larger crop; the sweep shows how the
+    per-cell throughput and the CG counts move with the lateral size (the
+    reference arm, ``--impl reference``, times the full slab)."""
+    from oracle import ref as refmod
+    if not refmod.available(omp=True):
+        return None
+    lanes = {}
+    for size, pc in (("64,64,128", "icc"), ("64,64,128", "jacobi"), ("128,128,128", "icc")):
+        lanes[f"{pc}_{size.replace(',', 'x')}"] = ref_lane(size, pc, threads, 1, 3)
+    best = lanes["icc_128x128x128"]
+    return {"value": best["value"], "unit": "cell-steps/s", "cores": threads,
             "kind": "reference",
-            "sample": f"{nx}x{ny}x{nz} crop of the slab, {n} steps after {max(warmup, 1)} "
-                      "warm-up, reference src/gw on host shims (OpenMP), bjacobi-ICC(0) CG"}
+            "sample": "128x128x128 crop of the slab, 3 steps after the dt0 = 60 s step, "
+                      "reference src/gw on host shims (OpenMP), bjacobi-ICC(0) CG; "
+                      "lanes: both preconditioners on a 64x64x128 crop too",
+            "lanes": lanes}
 
 
 def run_reference(args, rank):
+    """``--impl reference``: the reference's own step on the host cores, on
+    the full slab this arm's line names (setup untimed; one warm-up step, the
+    dt0 = 60 s one; then at most ``--ref-steps`` timed steps, since one
+    full-size step takes tens of seconds), bjacobi-ICC(0), all host threads."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    res = cpu_baseline(args.cpu_sample, threads, warmup=args.warmup, steps=args.steps)
-    if res is None:
+    from oracle import ref as refmod
+    if not refmod.available(omp=True):
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref (reference sources on host shims) not built"}))
         return
+    steps = max(1, min(args.steps, args.ref_steps))
+    res = ref_lane(args.size, "icc", threads, 1, steps)
+    sample = (f"the full {args.size.replace(',', 'x')} slab: {steps} timed steps after 1 "
+              "warm-up (the dt0 = 60 s step), reference src/gw on host shims (OpenMP), "
+              f"{PC_NAMES['icc']} CG")
     line = {
         "metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "steps": steps, "warmup": 1, "steps_requested": args.steps,
+        "warmup_requested": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": f"terrain-following heterogeneous slab, {args.cpu_sample} crop "
-                               f"(CPU-sized sample of {args.size}), dt0 60 s adaptive",
-                   "parallelism": f"{threads} host threads"},
-        "cpu_baseline": {k: res[k] for k in ("kind", "cores", "sample")} | {"value": res["value"],
-                                                                           "unit": "cell-steps/s"},
+        "config": slab_config(args.size),
+        "cpu_baseline": {"kind": "reference", "cores": threads, "sample": sample,
+                         "value": res["value"], "unit": "cell-steps/s"},
         "e2e": {"value": res["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "lane": res,
     }
     print(json.dumps(line))
+
+
+def latency_summary(solve_ms, step_ms) -> dict:
+    """p50 / p99 of the per-step device times (CUDA events around each phase
+    of every timed step): the predictor solve alone and the whole step."""
+    a, b = np.asarray(solve_ms), np.asarray(step_ms)
+    return {"solve_p50_ms": float(np.percentile(a, 50)), "solve_p99_ms": float(np.percentile(a, 99)),
+            "step_p50_ms": float(np.percentile(b, 50)), "step_p99_ms": float(np.percentile(b, 99)),
+            "samples": int(a.size)}
+
+
+def mixed_error(size: str, steps: int, stream) -> dict:
+    """The mixed form against the FP64 form solved tightly (CG rtol 1e-13),
+    both on this GPU from the slab's initial state, on the FP64 form's dt
+    sequence, never re-synced (``frehg_b200.accuracy``)."""
+    from frehg_b200 import accuracy, workloads
+    from frehg_b200.gw import RichardsSolver
+
+    nx, ny, nz = (int(v) for v in size.split(","))
+    cfg = workloads.hillslope(nx, ny, nz)
+    m = RichardsSolver(accuracy.mixed(cfg), stream=stream.cuda_stream)
+    ref = RichardsSolver(accuracy.tight_fp64(cfg), stream=stream.cuda_stream)
+    try:
+        s = accuracy.trajectory(m, ref, steps, cfg.domain.dx, cfg.domain.dy)
+    finally:
+        m.close()
+        ref.close()
+    per = s.pop("per_step")
+    s["head_per_step"] = [p["head"] for p in per]
+    s["reference"] = "FP64 form, Jacobi CG to rtol 1e-13, same dt sequence, no re-sync"
+    s["scales"] = {"head": "max(max|h|, 1 m)", "flux": "K A of the face direction",
+                   "storage": "owned volume", "audit": "owned volume"}
+    return s
 
 
 def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
@@ -244,6 +341,7 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
     gw.setProfiling(True)
     launches0 = gw.kernelLaunches()
     iters, outer, solve_ms = 0, 0, 0.0
+    solve_list, step_list = [], []
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -255,7 +353,10 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
             gw.advance()
             iters += gw.lastSolve()[0]
             outer += gw._info["outer_iterations"]
-            solve_ms += gw.phaseTimes()["solve"]
+            ph = gw.phaseTimes()
+            solve_ms += ph["solve"]
+            solve_list.append(ph["solve"])
+            step_list.append(sum(ph.values()))
         end.record(stream)
         torch.cuda.synchronize()
     launches = gw.kernelLaunches() - launches0
@@ -270,7 +371,7 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
         total_cells = float(a.item())
     out = dict(value=total_cells * args.steps / (ms / 1e3), ms=ms, iters=iters, outer=outer,
                solve_ms=solve_ms, launches=launches, clocks=clocks.summary(), active=active,
-               e2e=None)
+               e2e=None, latency=latency_summary(solve_list, step_list))
     if e2e_steps:
         e2e_steps = args.steps if e2e_steps < 0 else e2e_steps
         gw.restore(ck)
@@ -297,6 +398,62 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
     return out
 
 
+def ensemble_forms(members, steps, warmup, seq_steps, rank):
+    """Both forms of an ensemble of ``members`` seeded domains: autotune,
+    ``warmup`` batch steps, ``steps`` timed batch steps, then ``seq_steps``
+    member-by-member steps for comparison."""
+    import torch
+
+    from frehg_b200 import workloads
+    from frehg_b200.batch import RichardsBatch
+    from frehg_b200.gw import RichardsSolver
+
+    forms = {}
+    for prec in ("mixed", "fp64"):
+        cfgs = workloads.ensemble(members, seed=20261204 + rank, precision=prec)
+        solvers = [RichardsSolver(c) for c in cfgs]
+        cells = float(sum(s.activeCells() for s in solvers))
+        batch = RichardsBatch(solvers)
+        tuned, tune_ms = batch.autotune(trials=1)
+        for _ in range(warmup):
+            batch.step()
+        st0 = batch.stats()
+        torch.cuda.synchronize()
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+            t0 = time.perf_counter()
+            iters = 0
+            for _ in range(steps):
+                infos = batch.step()
+                iters += sum(i["cg_iterations"] for i in infos)
+            sec = time.perf_counter() - t0
+        st = batch.stats()
+        batch.close()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(seq_steps):
+            for s in solvers:
+                s.advance()
+        seq_sec = time.perf_counter() - t1
+        for s in solvers:
+            s.close()
+        forms[prec] = {
+            "value": cells * steps / sec, "ms_per_step": 1e3 * sec / steps,
+            "members": len(cfgs), "active_cells": cells,
+            "solve_iterations_per_member_step": iters / (steps * len(cfgs)),
+            "kernels_per_step": st["kernels_per_step"],
+            "kernel_launches": st["kernel_launches"] - st0["kernel_launches"],
+            "solve_launches_per_step": st["solve_launches"], "solve_blocks": st["solve_blocks"],
+            "graph_replay": bool(st["uses_graph"]), "autotuned": tuned,
+            "autotune_best_step_ms": tune_ms, "clocks": clocks.summary(),
+            "member_by_member": {"value": cells * seq_steps / seq_sec,
+                                 "ms_per_step": 1e3 * seq_sec / seq_steps,
+                                 "steps": seq_steps},
+            "batch_over_member_by_member": (cells * steps / sec) /
+                                           (cells * seq_steps / seq_sec),
+        }
+    return forms
+
+
 def run_ensemble(args, rank, world):
     """Many uneven domains stepped as one batch (frehg_gw_batch_*), each form.
 
@@ -309,55 +466,7 @@ def run_ensemble(args, rank, world):
     another through frehg_gw_step for ``--seq-steps`` steps.  Under torchrun
     every rank steps its own ensemble (seed + rank); no collective.
     """
-    import torch
-
-    from frehg_b200 import workloads
-    from frehg_b200.batch import RichardsBatch
-    from frehg_b200.gw import RichardsSolver
-
-    forms = {}
-    for prec in ("mixed", "fp64"):
-        cfgs = workloads.ensemble(args.members, seed=20261204 + rank, precision=prec)
-        solvers = [RichardsSolver(c) for c in cfgs]
-        cells = float(sum(s.activeCells() for s in solvers))
-        batch = RichardsBatch(solvers)
-        tuned, tune_ms = batch.autotune(trials=1)
-        for _ in range(args.warmup):
-            batch.step()
-        st0 = batch.stats()
-        torch.cuda.synchronize()
-        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
-            t0 = time.perf_counter()
-            iters = 0
-            for _ in range(args.steps):
-                infos = batch.step()
-                iters += sum(i["cg_iterations"] for i in infos)
-            sec = time.perf_counter() - t0
-        st = batch.stats()
-        batch.close()
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        for _ in range(args.seq_steps):
-            for s in solvers:
-                s.advance()
-        seq_sec = time.perf_counter() - t1
-        for s in solvers:
-            s.close()
-        forms[prec] = {
-            "value": cells * args.steps / sec, "ms_per_step": 1e3 * sec / args.steps,
-            "members": len(cfgs), "active_cells": cells,
-            "solve_iterations_per_member_step": iters / (args.steps * len(cfgs)),
-            "kernels_per_step": st["kernels_per_step"],
-            "kernel_launches": st["kernel_launches"] - st0["kernel_launches"],
-            "solve_launches_per_step": st["solve_launches"], "solve_blocks": st["solve_blocks"],
-            "graph_replay": bool(st["uses_graph"]), "autotuned": tuned,
-            "autotune_best_step_ms": tune_ms, "clocks": clocks.summary(),
-            "member_by_member": {"value": cells * args.seq_steps / seq_sec,
-                                 "ms_per_step": 1e3 * seq_sec / args.seq_steps,
-                                 "steps": args.seq_steps},
-            "batch_over_member_by_member": (cells * args.steps / sec) /
-                                           (cells * args.seq_steps / seq_sec),
-        }
+    forms = ensemble_forms(args.members, args.steps, args.warmup, args.seq_steps, rank)
     if rank != 0:
         return
     line = {
@@ -392,6 +501,22 @@ def serve_requests(n, seed):
         cfg = workloads.ensemble_member(rng, "mixed", (side, side), (nz, nz))
         out.append((cfg, int(rng.integers(20, 201))))
     return out
+
+
+def serve_summary(n_requests: int, rate: float, rank: int) -> dict:
+    """A short served stream (``n_requests`` of :func:`serve_requests`,
+    Poisson arrivals at ``rate`` req/s): p50 / p99 request latency and
+    cell-steps/s, for the headline line."""
+    from frehg_b200.serve import PreparedRequest, RichardsServer, run_stream
+
+    reqs = [PreparedRequest(c, n) for c, n in serve_requests(n_requests, 20261205 + rank)]
+    rng = np.random.default_rng(7 + rank)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    with RichardsServer() as srv:
+        res = run_stream(srv, reqs, arrivals)
+    res["rate_req_per_s"] = rate
+    res["requested_cell_steps"] = int(sum(r.nx * r.ny * r.nz * r.steps for r in reqs))
+    return res
 
 
 def run_serve(args, rank, world):
@@ -498,34 +623,51 @@ def main():
     forms = {
         "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms"] / args.steps,
                  "cg_iterations_per_step": fp64["iters"] / args.steps,
-                 "solve_ms_per_step": fp64["solve_ms"] / args.steps, "roofline": roof_fp64},
+                 "solve_ms_per_step": fp64["solve_ms"] / args.steps, "roofline": roof_fp64,
+                 "latency": fp64["latency"]},
         "mixed": {"value": mixed["value"], "ms_per_step": mixed["ms"] / args.steps,
                   "inner_iterations_per_step": mixed["iters"] / args.steps,
                   "outer_sweeps_per_step": mixed["outer"] / args.steps,
-                  "solve_ms_per_step": mixed["solve_ms"] / args.steps, "roofline": roof_mixed},
+                  "solve_ms_per_step": mixed["solve_ms"] / args.steps, "roofline": roof_mixed,
+                  "latency": mixed["latency"]},
         "mixed_over_fp64": mixed["value"] / fp64["value"] if fp64["value"] else None,
     }
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
+    extras = {}
+    if world == 1:
+        # Driver-visible summaries of the rest of the metric (N = 1 only):
+        # the mixed form's error against the tight FP64 form over a
+        # trajectory, a short served stream (p50 / p99 request latency) and a
+        # smaller ensemble batch, each outside the timed region.
+        if args.error_steps > 0:
+            extras["mixed_error"] = mixed_error(args.size, args.error_steps, stream)
+        if args.summary_requests > 0:
+            extras["serve"] = serve_summary(args.summary_requests, args.summary_rate, rank)
+        if args.summary_members > 0:
+            extras["ensemble"] = ensemble_forms(args.summary_members, 5, 3, 2, rank)
+            extras["ensemble"]["config"] = (f"{args.summary_members} independent boxes of "
+                                            "workloads.ensemble (seeded), 3 warm-up + 5 timed "
+                                            "batch steps, 2 member-by-member steps")
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        cpu = cpu_baseline(args.cpu_sample, os.cpu_count() or 1)
-    nx, ny, nz = (int(v) for v in args.size.split(","))
+        cpu = cpu_baseline(os.cpu_count() or 1)
+    cfg_line = slab_config(args.size)
+    cfg_line["active_cells_per_gpu"] = res["active"]
     line = {
         "metric": METRIC, "value": res["value"], "unit": "cell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32-inner/f64",
         "data": "synthetic",
-        "config": {"workload": f"terrain-following heterogeneous slab {nx}x{ny}x{nz} "
-                               f"(hillslope, seeded), dt0 60 s adaptive, {args.precision} solve",
-                   "active_cells_per_gpu": res["active"], "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (13 GB working set)"},
+        "config": cfg_line, "form": args.precision, "parallelism": f"replicas x{world}",
         "roofline": roof, "forms": forms, "cpu_baseline": cpu, "e2e": res["e2e"],
         "gpu_launches": res["launches"], "clocks": res["clocks"],
+        "latency": res["latency"],
     }
+    line.update(extras)
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -111,6 +111,7 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     if (!coop) return fail(FREHG_GW_ECUDA, "device lacks cooperative launch");
 
     auto* hnd = new frehg_gw_handle();
+    hnd->device = dev;
     fgw::Device& D = hnd->D;
     CUDA_TRY(cudaDeviceGetAttribute(&D.sm_count, cudaDevAttrMultiProcessorCount, dev), "sm");
     CUDA_TRY(cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking), "stream");
@@ -168,6 +169,10 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
       if (e == cudaSuccess && !D.arena_plan)
         e = cudaMemcpy(D.codes, H.codes.data(), H.codes.size() * sizeof(int), cudaMemcpyHostToDevice);
       if (e == cudaSuccess) e = dalloc(D, &D.values, 6 * static_cast<size_t>(d.ncol));
+      // Zero like the host staging copy: every later upload keeps the two
+      // equal entry for entry (frehg_gw_set_bc_values relies on it).
+      if (e == cudaSuccess && !D.arena_plan)
+        e = cudaMemset(D.values, 0, 6 * static_cast<size_t>(d.ncol) * sizeof(double));
       for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
         e = dalloc(D, &D.h[b], n3);
         if (e == cudaSuccess) e = dalloc(D, &D.wc[b], n3);
@@ -292,6 +297,7 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
 
 int frehg_gw_destroy(frehg_gw_handle* h) {
   if (!h) return FREHG_GW_OK;
+  FGW_ON_DEVICE(h);
   cudaStreamSynchronize(h->D.stream);
   for (cudaEvent_t& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -303,6 +309,7 @@ int frehg_gw_destroy(frehg_gw_handle* h) {
 
 int frehg_gw_set_stream(frehg_gw_handle* h, void* stream) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   CUDA_TRY(cudaStreamSynchronize(h->D.stream), "set_stream");
   if (h->D.own_stream) cudaStreamDestroy(h->D.stream);
   if (stream) {
@@ -318,6 +325,7 @@ int frehg_gw_set_stream(frehg_gw_handle* h, void* stream) {
 int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* bot,
                            const double* xm, const double* xp, const double* ym, const double* yp) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   fgw::Device& D = h->D;
   const fgw::Dims& d = D.d;
   const long long nc = d.ncol;
@@ -353,7 +361,20 @@ int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* 
     if (ym) put(4, fgw::col2(d, 1, i), ym[i - 1]);
     if (yp) put(5, fgw::col2(d, d.ny, i), yp[i - 1]);
   }
-  if (bad) return fail(FREHG_GW_EINVAL, "non-finite boundary value");
+  if (bad) {
+    // A rejected call changes nothing: the touched slots of the staging copy
+    // are read back from the device, which holds the last accepted values
+    // (the two are equal entry for entry after every accepted call).
+    const double* src[6] = {top, bot, xm, xp, ym, yp};
+    for (int slot = 0; slot < 6; ++slot) {
+      if (!src[slot]) continue;
+      CUDA_TRY(cudaMemcpyAsync(h->values.data() + slot * nc, D.values + slot * nc,
+                               static_cast<size_t>(nc) * sizeof(double), cudaMemcpyDeviceToHost,
+                               D.stream), "set_bc_values");
+    }
+    CUDA_TRY(cudaStreamSynchronize(D.stream), "set_bc_values");
+    return fail(FREHG_GW_EINVAL, "non-finite boundary value");
+  }
   // Upload what the kernels read: the top and bottom slots whole, the side
   // slots' edge entries (a column of the x edges, a row of the y edges).
   const size_t w = sizeof(double), pitch = static_cast<size_t>(d.nx2) * w;
@@ -380,6 +401,7 @@ int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* 
 
 int frehg_gw_init_state(frehg_gw_handle* h, int form, double constant, const double* field) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   if (form < FREHG_GW_IC_MOISTURE || form > FREHG_GW_IC_WATER_TABLE)
     return fail(FREHG_GW_EINVAL, "unknown initial-condition form");
   fgw::Device& D = h->D;
@@ -409,6 +431,7 @@ int frehg_gw_init_state(frehg_gw_handle* h, int form, double constant, const dou
 
 int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc) {
   if (!h || !head || !wc) return fail(FREHG_GW_EINVAL, "null argument");
+  FGW_ON_DEVICE(h);
   fgw::Device& D = h->D;
   const fgw::Dims& d = D.d;
   std::vector<double> hh(static_cast<size_t>(d.ncell)), ww(static_cast<size_t>(d.ncell));
@@ -440,6 +463,7 @@ int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc)
 int frehg_gw_restore(frehg_gw_handle* h, const double* head, const double* wc,
                      const double* vloss, double dtg) {
   if (!h || !head || !wc) return fail(FREHG_GW_EINVAL, "null argument");
+  FGW_ON_DEVICE(h);
   if (!(dtg > 0.0) || !std::isfinite(dtg)) return fail(FREHG_GW_EINVAL, "dtg must be positive");
   const int rc = frehg_gw_set_state(h, head, wc);
   if (rc != FREHG_GW_OK) return rc;
@@ -546,6 +570,7 @@ extern "C" {
 int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* info) {
   (void)t;  // boundary values arrive through frehg_gw_set_bc_values
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   if (!h->have_state) return fail(FREHG_GW_ESTATE, "frehg_gw_step before frehg_gw_init_state");
   if (!(dtg > 0.0) || !std::isfinite(dtg)) return fail(FREHG_GW_EINVAL, "dtg must be positive");
   fgw::Device& D = h->D;
@@ -619,6 +644,7 @@ size_t frehg_gw_field_size(const frehg_gw_handle* h, int field) {
 
 int frehg_gw_get_field(frehg_gw_handle* h, int field, double* out) {
   if (!h || !out) return fail(FREHG_GW_EINVAL, "null argument");
+  FGW_ON_DEVICE(h);
   fgw::Device& D = h->D;
   const fgw::Dims& d = D.d;
   const double* src = nullptr;
@@ -693,6 +719,7 @@ int frehg_gw_get_field(frehg_gw_handle* h, int field, double* out) {
 
 int frehg_gw_enable_transport_window(frehg_gw_handle* h) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   fgw::Device& D = h->D;
   if (D.win_x) return FREHG_GW_OK;
   const size_t n3 = static_cast<size_t>(D.d.ncell), nf = static_cast<size_t>(D.d.ncol) * (D.d.nz + 1);
@@ -716,6 +743,7 @@ int frehg_gw_enable_transport_window(frehg_gw_handle* h) {
 
 int frehg_gw_reset_transport_window(frehg_gw_handle* h) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   fgw::Device& D = h->D;
   if (!D.win_x) return FREHG_GW_OK;  // as the reference: a no-op until enabled
   const size_t n3 = static_cast<size_t>(D.d.ncell), nf = static_cast<size_t>(D.d.ncol) * (D.d.nz + 1);
@@ -730,6 +758,7 @@ int frehg_gw_reset_transport_window(frehg_gw_handle* h) {
 
 int frehg_gw_owned_volume(frehg_gw_handle* h, double* out) {
   if (!h || !out) return fail(FREHG_GW_EINVAL, "null argument");
+  FGW_ON_DEVICE(h);
   fgw::Device& D = h->D;
   fgw::launch_volume(D, D.wc[D.cur]);
   CUDA_TRY(cudaMemcpyAsync(D.out_host, D.out, sizeof(fgw::StepOut), cudaMemcpyDeviceToHost,
@@ -741,8 +770,11 @@ int frehg_gw_owned_volume(frehg_gw_handle* h, double* out) {
 
 long long frehg_gw_active_cells(const frehg_gw_handle* h) { return h ? h->nactive : 0; }
 
+int frehg_gw_device(const frehg_gw_handle* h) { return h ? h->device : -1; }
+
 int frehg_gw_set_profiling(frehg_gw_handle* h, int on) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   if (on && !h->ev[0]) {
     for (cudaEvent_t& e : h->ev) CUDA_TRY(cudaEventCreate(&e), "set_profiling");
   }
@@ -807,6 +839,7 @@ int static_field_address(double** out) {
 int frehg_gw_init_state_static(frehg_gw_handle* h, int form, double constant,
                                const double* field) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   if (form < FREHG_GW_IC_MOISTURE || form > FREHG_GW_IC_WATER_TABLE)
     return fail(FREHG_GW_EINVAL, "unknown initial-condition form");
   double* scratch = nullptr;

@@ -149,6 +149,7 @@ cudaError_t solve_group_launch(const SolveGroup& g, cudaStream_t s) {
 // ---------------------------------------------------------------- the batch
 struct frehg_gw_batch {
   std::vector<frehg_gw_handle*> m;
+  int device = 0;                   // the members' device
   frehg_gw_batch_opts opts{};
   cudaStream_t stream = nullptr;
   std::vector<cudaStream_t> pool;
@@ -501,6 +502,8 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
   for (int i = 0; i < n; ++i) {
     if (!members[i]) return fail(FREHG_GW_EINVAL, "batch: null member");
     if (!members[i]->have_state) return fail(FREHG_GW_ESTATE, "batch: member without state");
+    if (members[i]->device != members[0]->device)
+      return fail(FREHG_GW_EINVAL, "batch: members on different devices");
     if (members[i]->D.f.cpl)
       return fail(FREHG_GW_EUNSUPPORTED, "batch: a coupled-top member steps on its own");
     if (members[i]->D.win_x)
@@ -510,7 +513,9 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
     for (int j = 0; j < i; ++j)
       if (members[j] == members[i]) return fail(FREHG_GW_EINVAL, "batch: member given twice");
   }
+  FGW_ON_DEVICE(members[0]);
   auto* b = new frehg_gw_batch;
+  b->device = members[0]->device;
   b->m.assign(members, members + n);
   if (opts) b->opts = *opts;
   else b->opts.use_graph = 1;
@@ -543,9 +548,12 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
 
 int frehg_gw_batch_set_members(frehg_gw_batch* b, frehg_gw_handle* const* members, int n) {
   if (!b || !members || n < 1) return fail(FREHG_GW_EINVAL, "batch: null argument or n < 1");
+  FGW_ON_DEVICE(b);
   for (int i = 0; i < n; ++i) {
     if (!members[i]) return fail(FREHG_GW_EINVAL, "batch: null member");
     if (!members[i]->have_state) return fail(FREHG_GW_ESTATE, "batch: member without state");
+    if (members[i]->device != b->device)
+      return fail(FREHG_GW_EINVAL, "batch: members on different devices");
     if (members[i]->D.f.cpl)
       return fail(FREHG_GW_EUNSUPPORTED, "batch: a coupled-top member steps on its own");
     if (members[i]->D.win_x)
@@ -561,6 +569,7 @@ int frehg_gw_batch_set_members(frehg_gw_batch* b, frehg_gw_handle* const* member
 
 int frehg_gw_batch_destroy(frehg_gw_batch* b) {
   if (!b) return FREHG_GW_OK;
+  FGW_ON_DEVICE(b);
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graphs(b);
   free_groups(b);
@@ -579,6 +588,7 @@ int frehg_gw_batch_destroy(frehg_gw_batch* b) {
 
 int frehg_gw_batch_step(frehg_gw_batch* b, frehg_gw_step_info* infos) {
   if (!b) return fail(FREHG_GW_EINVAL, "null batch");
+  FGW_ON_DEVICE(b);
   for (auto* h : b->m)
     if (!(h->next_dt > 0.0) || !std::isfinite(h->next_dt))
       return fail(FREHG_GW_EINVAL, "batch: member dt must be positive");
@@ -608,6 +618,7 @@ int frehg_gw_batch_set_dt(frehg_gw_batch* b, int i, double dtg) {
 int frehg_gw_batch_autotune(frehg_gw_batch* b, int trials, frehg_gw_batch_opts* chosen,
                             double* best_ms) {
   if (!b) return fail(FREHG_GW_EINVAL, "null batch");
+  FGW_ON_DEVICE(b);
   if (trials < 1) trials = 1;
   const std::string key = tune_key(b);
   {

@@ -38,6 +38,7 @@ extern "C" {
 
 int frehg_gw_attach_coupling(frehg_gw_handle* h, const frehg_gw_coupling* c) {
   if (!h || !c) return fail(FREHG_GW_EINVAL, "attach_coupling: null argument");
+  FGW_ON_DEVICE(h);
   if (!(c->min_depth >= 0.0) || !std::isfinite(c->min_depth))
     return fail(FREHG_GW_EINVAL, "attach_coupling: min_depth must be finite and >= 0");
   fgw::Device& D = h->D;
@@ -101,6 +102,7 @@ int frehg_gw_attach_coupling(frehg_gw_handle* h, const frehg_gw_coupling* c) {
 
 int frehg_gw_get_surface(frehg_gw_handle* h, int which, double* host_out) {
   if (int rc = need_coupling(h)) return rc;
+  FGW_ON_DEVICE(h);
   if (!host_out) return fail(FREHG_GW_EINVAL, "get_surface: null output");
   fgw::Device& D = h->D;
   const size_t n2 = static_cast<size_t>(D.d.ncol);
@@ -121,6 +123,7 @@ int frehg_gw_get_surface(frehg_gw_handle* h, int which, double* host_out) {
 
 int frehg_gw_set_surface(frehg_gw_handle* h, int which, const double* host_in) {
   if (int rc = need_coupling(h)) return rc;
+  FGW_ON_DEVICE(h);
   if (!host_in) return fail(FREHG_GW_EINVAL, "set_surface: null input");
   if (which < 0 || which >= kSurfFields)
     return fail(FREHG_GW_EINVAL, "set_surface: bad or read-only field");
@@ -150,6 +153,7 @@ double frehg_gw_elevation_offset(const frehg_gw_handle* h) { return h ? h->offse
 
 int frehg_gw_coupler_init(frehg_gw_handle* h, const frehg_gw_coupler_opts* o) {
   if (int rc = need_coupling(h)) return rc;
+  FGW_ON_DEVICE(h);
   if (!o) return fail(FREHG_GW_EINVAL, "coupler_init: null options");
   const double first = o->sync ? o->dt : o->dt_init;
   if (!(o->dt > 0.0) || !(first > 0.0))
@@ -164,6 +168,7 @@ int frehg_gw_coupler_init(frehg_gw_handle* h, const frehg_gw_coupler_opts* o) {
 
 int frehg_gw_coupler_step(frehg_gw_handle* h, double t, double dt, frehg_gw_window_audit* out) {
   if (int rc = need_coupling(h)) return rc;
+  FGW_ON_DEVICE(h);
   if (!h->coupler) return fail(FREHG_GW_ESTATE, "coupler_step before frehg_gw_coupler_init");
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(FREHG_GW_EINVAL, "coupler_step: dt <= 0");
   fgw::Device& D = h->D;
@@ -230,6 +235,7 @@ int frehg_gw_coupler_state(frehg_gw_handle* h, double t, double* next_dt, double
 
 int frehg_gw_coupler_restore(frehg_gw_handle* h, double t, double dtg, double lag) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  FGW_ON_DEVICE(h);
   if (!h->coupler) return fail(FREHG_GW_ESTATE, "coupler_restore before frehg_gw_coupler_init");
   if (!(dtg > 0.0)) return fail(FREHG_GW_EINVAL, "coupler_restore: dtg must be positive");
   h->cdtg = dtg;

@@ -194,6 +194,7 @@ extern "C" {
 int frehg_gw_attach_density(frehg_gw_handle* h, int saline, int thermal,
                             const frehg_gw_density* c) {
   if (!h || !c) return fail(FREHG_GW_EINVAL, "attach_density: null argument");
+  FGW_ON_DEVICE(h);
   if (!saline && !thermal) return fail(FREHG_GW_EINVAL, "attach_density: no scalar");
   const double co[4] = {c->beta_saline, c->beta_saline_visc, c->thermal_expansion,
                         c->reference_temperature};
@@ -260,6 +261,7 @@ int frehg_gw_attach_density(frehg_gw_handle* h, int saline, int thermal,
 
 int frehg_gw_set_scalar(frehg_gw_handle* h, int which, const double* values) {
   if (int rc = need_density(h)) return rc;
+  FGW_ON_DEVICE(h);
   if (which < 0 || which > 3 || !h->D.scal[which])
     return fail(FREHG_GW_EINVAL, "set_scalar: scalar not attached");
   if (!values) return fail(FREHG_GW_EINVAL, "set_scalar: null values");
@@ -273,6 +275,7 @@ int frehg_gw_set_scalar(frehg_gw_handle* h, int which, const double* values) {
 
 int frehg_gw_get_scalar(frehg_gw_handle* h, int which, double* out) {
   if (int rc = need_density(h)) return rc;
+  FGW_ON_DEVICE(h);
   if (which < 0 || which > 3 || !h->D.scal[which])
     return fail(FREHG_GW_EINVAL, "get_scalar: scalar not attached");
   if (!out) return fail(FREHG_GW_EINVAL, "get_scalar: null output");

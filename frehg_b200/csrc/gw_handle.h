@@ -12,6 +12,7 @@
 
 struct frehg_gw_handle {
   fgw::Device D;
+  int device = 0;  // the CUDA device the handle's memory and stream live on
   double offset = 0.0;
   long long nactive = 0;
   double* bath_dev = nullptr;
@@ -39,6 +40,31 @@ struct frehg_gw_handle {
 
 namespace fgw_api {
 
+// Makes `dev` the calling thread's current device for the scope of one ABI
+// call and gives the caller's own back at the end, so that a thread driving
+// handles on several GPUs reaches each handle's memory and stream whatever
+// device it had selected.
+struct DeviceGuard {
+  int prev = -1;
+  bool switched = false;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      ok = false;
+      return;
+    }
+    if (prev != dev) {
+      ok = cudaSetDevice(dev) == cudaSuccess;
+      switched = ok;
+    }
+  }
+  ~DeviceGuard() {
+    if (switched) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 // Records `msg` as the calling thread's last error and returns `status`.
 int fail(int status, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
@@ -55,3 +81,10 @@ int finish_step(frehg_gw_handle* h, frehg_gw_step_info* info);
 cudaError_t upload_next_dt(frehg_gw_handle* h);
 
 }  // namespace fgw_api
+
+// Every ABI call on a handle runs on the handle's device (first statement
+// after the handle's null check).
+#define FGW_ON_DEVICE(h)                                 \
+  fgw_api::DeviceGuard fgw_device_guard_((h)->device);   \
+  if (!fgw_device_guard_.ok)                             \
+  return fgw_api::fail(FREHG_GW_ECUDA, "cannot make the handle's device current")

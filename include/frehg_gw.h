@@ -239,6 +239,13 @@ int frehg_gw_owned_volume(frehg_gw_handle* h, double* out);
 /* Number of active cells. */
 long long frehg_gw_active_cells(const frehg_gw_handle* h);
 
+/* The CUDA device ordinal the handle lives on: the calling thread's current
+ * device when frehg_gw_create ran.  Every call on the handle makes that
+ * device current for its duration and restores the caller's afterwards, so
+ * one thread may drive handles on several GPUs.  -1 for a null handle.  (The
+ * reference has one device per MPI rank, chosen by Kokkos at start-up.) */
+int frehg_gw_device(const frehg_gw_handle* h);
+
 /* Tracing (no counterpart in the reference, whose Timer sections do not
  * fence the device): with profiling on, each step records CUDA events around
  * its phases; frehg_gw_phase_times returns the last step's device times in

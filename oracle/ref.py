@@ -142,11 +142,29 @@ class RefSolver:
             c.bath = f64(np.full(d.ny * d.nx, float(d.bottom_elevation)))
         else:
             c.bath = f64(np.asarray(d.bottom_elevation).reshape(-1))
-        st = np.array([[s.ksx, s.ksy, s.ksz, s.theta_s, s.theta_r, s.vg_alpha, s.vg_n, s.aev]
-                       for s in cfg.soil_types], dtype=np.float64)
-        c.n_soil_types = len(cfg.soil_types)
-        c.soil_types = f64(st.reshape(-1))
-        c.soil_map = i32(np.asarray(cfg.soil_map).reshape(-1)) if cfg.soil_map is not None else None
+        cols = ("ksx", "ksy", "ksz", "theta_s", "theta_r", "vg_alpha", "vg_n", "aev")
+        if cfg.cell_soil is not None and cfg.soil_map is None:
+            # Per-cell soil reaches the reference the only way it takes it:
+            # one soil type per cell and the id map 0..ncell-1 in the
+            # reference's (j*nx + i)*nz + k order.  Built from the arrays
+            # directly (a 512x512x128 slab has 33.5M types).
+            ncell = d.nx * d.ny * d.nz
+            base = cfg.soil_types[0]
+            st = np.empty((ncell, 8), dtype=np.float64)
+            for n, name in enumerate(cols):
+                v = cfg.cell_soil.get(name, getattr(base, name))
+                st[:, n] = np.broadcast_to(np.asarray(v, np.float64),
+                                           (d.ny, d.nx, d.nz)).reshape(-1)
+            c.n_soil_types = ncell
+            c.soil_types = f64(st.reshape(-1))
+            c.soil_map = i32(np.arange(ncell, dtype=np.int32))
+        else:
+            st = np.array([[getattr(s, name) for name in cols] for s in cfg.soil_types],
+                          dtype=np.float64)
+            c.n_soil_types = len(cfg.soil_types)
+            c.soil_types = f64(st.reshape(-1))
+            c.soil_map = (i32(np.asarray(cfg.soil_map).reshape(-1))
+                          if cfg.soil_map is not None else None)
         ic = cfg.initial
         c.ic_form = _IC[ic.form]
         if np.isscalar(ic.value):

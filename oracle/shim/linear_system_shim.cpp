@@ -71,7 +71,21 @@ double nowSeconds() {
   return std::chrono::duration<double>(clock::now().time_since_epoch()).count();
 }
 
+// The OpenMP build (the CPU-baseline timing lane) runs the vector kernels
+// of the solve -- SpMV, dot products, AXPYs, the Jacobi apply -- across the
+// host threads, as PETSc's aijkokkos does on a Kokkos-OpenMP host; the ICC(0)
+// triangular solves stay serial, as PETSc's are.  The serial build (the
+// parity oracle) keeps one fixed summation order.
+#ifdef FREHG_SHIM_OPENMP
+#define SHIM_PAR_FOR _Pragma("omp parallel for schedule(static)")
+#define SHIM_PAR_SUM _Pragma("omp parallel for schedule(static) reduction(+ : s)")
+#else
+#define SHIM_PAR_FOR
+#define SHIM_PAR_SUM
+#endif
+
 void spmv(const Csr& a, const double* x, double* y) {
+  SHIM_PAR_FOR
   for (int m = 0; m < a.n; ++m) {
     double s = 0.0;
     for (int q = a.rowPtr[m]; q < a.rowPtr[m + 1]; ++q) s += a.val[q] * x[a.col[q]];
@@ -81,13 +95,16 @@ void spmv(const Csr& a, const double* x, double* y) {
 
 double dot(const std::vector<double>& u, const std::vector<double>& v) {
   double s = 0.0;
-  for (std::size_t n = 0; n < u.size(); ++n) s += u[n] * v[n];
+  const long nn = static_cast<long>(u.size());
+  SHIM_PAR_SUM
+  for (long n = 0; n < nn; ++n) s += u[n] * v[n];
   return s;
 }
 
 void applyPc(const ShimState& st, const std::vector<double>& r, std::vector<double>& z) {
   const int n = st.a.n;
   if (st.jacobi) {
+    SHIM_PAR_FOR
     for (int m = 0; m < n; ++m) z[m] = r[m] * st.diagInv[m];
     return;
   }
@@ -256,6 +273,7 @@ PetscInt LinearSystem::solveOnce(KSPConvergedReason& reason, PetscReal& residual
         p = z;
       } else {
         const double bb = beta / betaold;
+        SHIM_PAR_FOR
         for (int m = 0; m < n; ++m) p[m] = z[m] + bb * p[m];
       }
       dpiold = dpi;
@@ -267,7 +285,9 @@ PetscInt LinearSystem::solveOnce(KSPConvergedReason& reason, PetscReal& residual
         break;
       }
       const double a = beta / dpi;
+      SHIM_PAR_FOR
       for (int m = 0; m < n; ++m) x[m] += a * p[m];
+      SHIM_PAR_FOR
       for (int m = 0; m < n; ++m) r[m] -= a * w[m];
       applyPc(st, r, z);
       dp = std::sqrt(dot(z, z));

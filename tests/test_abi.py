@@ -108,3 +108,12 @@ def test_restore_rejects_bad_arguments_without_a_gpu():
     lib.frehg_gw_restore.restype = ctypes.c_int
     lib.frehg_gw_restore.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_double]
     assert lib.frehg_gw_restore(None, None, None, None, 1.0) == 1  # FREHG_GW_EINVAL
+
+
+def test_device_ordinal_of_a_null_handle_without_a_gpu():
+    if not os.path.exists(LIB):
+        pytest.skip("libfrehg_gw.so not built")
+    lib = ctypes.CDLL(LIB)
+    lib.frehg_gw_device.restype = ctypes.c_int
+    lib.frehg_gw_device.argtypes = [ctypes.c_void_p]
+    assert lib.frehg_gw_device(None) == -1

@@ -1,27 +1,43 @@
 """The mixed-precision form: FP32 inner line-preconditioned CG inside FP64
 defect correction (true residual <= 1e-11 ||b||), started from h^n.
 
-Its reference is the FP64 oracle solved tightly (Jacobi CG, rtol 1e-13) from
-the same state each step: the default oracle stops its CG at a
-preconditioned rtol of 1e-8, which leaves the head itself 1e-7..1e-6 away
-from the linear system's solution, so a tighter form is measured against the
-tight solve.  Bars: head within 1e-8 relative L-inf per step, the GPU's own
-mass audit closing to 1e-12 of the total storage, and the head within the
-default oracle's own solve error of the default oracle.
+Its reference is the FP64 step solved tightly (Jacobi CG, rtol 1e-13): the
+default oracle stops its CG at a preconditioned rtol of 1e-8, which leaves
+the head itself 1e-7..1e-6 away from the linear system's solution, so a
+tighter form is measured against the tight solve.  Two kinds of test:
+
+* one step at a time: the oracle is re-synced to the GPU state before every
+  step, so each step's error is measured alone (every scenario);
+* trajectories: the two forms step from the same initial state on the same
+  dt sequence and are never re-synced, so the error is that of a run -- on a
+  64x64x128 crop of the benchmark slab against the tight oracle, and on the
+  full 512x512x128 slab against the tight FP64 GPU form.
+
+Bars: head within 1e-8 relative L-inf, the GPU's own mass audit closing to
+1e-12 of the total storage.  The trajectories also bound the flux error (on
+the gravity scale K A of each direction) and the owned volume's relative
+error, and report the iteration counts.
 """
 import copy
+import json
+import os
 
 import numpy as np
 import pytest
 
 import cases
-from frehg_b200 import workloads
+from frehg_b200 import accuracy, workloads
 from frehg_b200.gw import RichardsSolver
 from oracle.gw import OracleSolver
 
 pytestmark = pytest.mark.gpu
 
 H_TOL = 1e-8
+AUDIT_TOL = 1e-12
+# Trajectory bars for the fluxes (gravity scale) and the owned volume: the
+# measured errors sit orders of magnitude below these.
+FLUX_TOL = 1e-6
+STORAGE_TOL = 1e-10
 
 
 def rel_linf(a, b):
@@ -87,3 +103,45 @@ def test_mixed_hillslope_crop_nz128():
 def test_mixed_deep_columns_tiled_solve():
     # Columns deeper than 256 cells take the shared-memory tiled line solve.
     run(workloads.column_32x32x50(nx=4, ny=3, nz=300), 3)
+
+
+def check_trajectory(s, name):
+    out = os.environ.get("FREHG_ACCURACY_OUT")
+    if out:
+        with open(os.path.join(out, f"mixed_error_{name}.json"), "w") as f:
+            json.dump(s, f, indent=1)
+    print(name, json.dumps({k: v for k, v in s.items() if k != "per_step"}))
+    assert all(p["status"] == 0 for p in s["per_step"])
+    assert s["head"] <= H_TOL, s["head"]
+    assert s["audit"] <= AUDIT_TOL, s["audit"]
+    assert s["flux"] <= FLUX_TOL, s["flux"]
+    assert s["storage"] <= STORAGE_TOL, s["storage"]
+
+
+def test_mixed_trajectory_slab_crop_vs_oracle():
+    # 64x64x128 crop of the benchmark slab, 10 steps, never re-synced,
+    # against the oracle solved tightly.
+    cfg = workloads.hillslope(64, 64, 128)
+    m = RichardsSolver(accuracy.mixed(cfg))
+    ref = OracleSolver(accuracy.tight_fp64(cfg))
+    try:
+        s = accuracy.trajectory(m, ref, 10, cfg.domain.dx, cfg.domain.dy)
+    finally:
+        m.close()
+        ref.close()
+    check_trajectory(s, "slab_64x64x128_vs_oracle")
+
+
+def test_mixed_trajectory_full_slab_vs_fp64():
+    # The benchmark's 512x512x128 slab, 10 steps, the mixed form against the
+    # FP64 GPU form solved tightly (both on one device, ~29 GB), never
+    # re-synced.
+    cfg = workloads.hillslope(512, 512, 128)
+    m = RichardsSolver(accuracy.mixed(cfg))
+    ref = RichardsSolver(accuracy.tight_fp64(cfg))
+    try:
+        s = accuracy.trajectory(m, ref, 10, cfg.domain.dx, cfg.domain.dy)
+    finally:
+        m.close()
+        ref.close()
+    check_trajectory(s, "slab_512x512x128_vs_fp64")
