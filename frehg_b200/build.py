@@ -15,7 +15,8 @@ OUT = os.path.join(HERE, "libfrehg_gw.so")
 SOURCES = ["gw_api.cu", "gw_kernels.cu", "gw_cg.cu", "gw_cg_mixed.cu", "gw_batch.cu", "gw_serve.cu",
            "gw_couple.cu", "gw_density.cu",
            "gw_setup.cpp"]
-HEADERS = ["gw_device.cuh", "gw_internal.h", "gw_setup.h", "gw_coop.cuh", "gw_handle.h"]
+HEADERS = ["gw_device.cuh", "gw_internal.h", "gw_setup.h", "gw_coop.cuh", "gw_handle.h",
+           "gw_linefactor.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -43,21 +44,39 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in deps if os.path.exists(p))
 
 
+def _compile(src: str, obj: str, ptxas_info: bool) -> subprocess.CompletedProcess:
+    cmd = [nvcc_path(), "-ccbin", host_compiler(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
+           "-Xcompiler", "-fPIC", "-c", "-o", obj, src]
+    if ptxas_info:
+        cmd[1:1] = ["-Xptxas", "-v"]
+    return subprocess.run(cmd, capture_output=True, text=True)
+
+
 def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> str:
+    """Compiles every source to an object in parallel (no cross-file device
+    code, so no device link), then links the shared library."""
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc_path(), "-ccbin", host_compiler(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
-           "-Xcompiler", "-fPIC", "-shared", "-o", OUT + ".tmp"]
-    if ptxas_info:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose or ptxas_info:
-        sys.stderr.write(res.stderr)
+    import concurrent.futures
+    import tempfile
+
+    with tempfile.TemporaryDirectory(prefix="frehg_build_") as tmp:
+        objs = [os.path.join(tmp, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+        jobs = max(1, min(len(SOURCES), os.cpu_count() or 1))
+        with concurrent.futures.ThreadPoolExecutor(jobs) as ex:
+            results = list(ex.map(lambda so: _compile(os.path.join(CSRC, so[0]), so[1], ptxas_info),
+                                  zip(SOURCES, objs)))
+        for src, res in zip(SOURCES, results):
+            if res.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {src}:\n" + res.stdout + res.stderr)
+            if verbose or ptxas_info:
+                sys.stderr.write(res.stderr)
+        cmd = [nvcc_path(), "-ccbin", host_compiler(), *ARCH, "-shared", "-o", OUT + ".tmp", *objs]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

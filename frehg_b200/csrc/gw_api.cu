@@ -496,9 +496,11 @@ cudaError_t enqueue_predictor(frehg_gw_handle* h) {
   if (D.f.baro) fgw::launch_baro(D);
   fgw::launch_ghosts(D, hn, wcn);
   if (D.f.cpl) fgw::launch_cpl_mode(D, hn);
+  const bool mixed = h->precision == FREHG_GW_PRECISION_MIXED;
+  if (h->fused && fgw::launch_predict(D, hn, wcn, mixed)) return cudaGetLastError();
   fgw::launch_closure_pred(D, hn);
-  fgw::launch_assemble(D, hn, wcn, h->precision == FREHG_GW_PRECISION_MIXED);
-  if (h->precision == FREHG_GW_PRECISION_MIXED) return fgw::launch_line_factor(D);
+  fgw::launch_assemble(D, hn, wcn, mixed);
+  if (mixed) return fgw::launch_line_factor(D);
   return cudaGetLastError();
 }
 
@@ -779,6 +781,12 @@ int frehg_gw_set_profiling(frehg_gw_handle* h, int on) {
     for (cudaEvent_t& e : h->ev) CUDA_TRY(cudaEventCreate(&e), "set_profiling");
   }
   h->profiling = on != 0;
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_set_fused(frehg_gw_handle* h, int on) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  h->fused = on != 0;
   return FREHG_GW_OK;
 }
 

@@ -140,6 +140,9 @@ void launch_ghosts(const Device& D, double* h, double* wc);
 void launch_closure_pred(const Device& D, const double* h);
 // warm: also write the mixed solve's starting iterate x = h^n (active cells).
 void launch_assemble(const Device& D, const double* hn, const double* wcn, bool warm);
+// The predictor in one fused pass (closures, faces, rows and, mixed, the
+// column factors) where it applies; false: use the separate passes.
+bool launch_predict(const Device& D, const double* hn, const double* wcn, bool mixed);
 void launch_closure_corr(const Device& D, const double* hn);
 void launch_flux(const Device& D, const double* wcn);
 void launch_update_wc(const Device& D, const double* hn, const double* wcn);

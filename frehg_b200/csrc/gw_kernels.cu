@@ -20,6 +20,7 @@
 
 #include "gw_coop.cuh"
 #include "gw_internal.h"
+#include "gw_linefactor.cuh"
 
 namespace fgw {
 
@@ -227,6 +228,233 @@ __global__ void __launch_bounds__(kBlock) k_closure_corr(Dims d, Fields f,
 }
 
 // ---------------------------------------------------------------- assembly
+// Everything the row of one active cell depends on, gathered before any
+// arithmetic: the six face conductivities, activity of the upper neighbours
+// and of the cells above and below, metrics, step-start state, BC data and
+// (density) the ratios.  Shared by k_assemble and the fused predictor.
+struct AsmIn {
+  double kxp, kxm, kyp, kym, kzm, kzp;
+  double dzc, dzu, dzl, wcnc, wcsc;
+  double cosxc, cosxw, axc, axw, cosyc, cosys, ayc, ays;
+  double chc, hnc, hne, hnw, hnn, hns;
+  double vxp, vxm, vyp, vym, vbot, vtop;
+  double botc_, bote, botw, botn, bots, sinxc, sinxw, sinyc, sinys;
+  // density: r v of the lateral faces (bx*, by*), the z faces' r and v, the
+  // lateral faces' r and the cell's r_rho; all 1 without density coupling
+  double bxc, bxw, byc, bys, rzpf, rzmf, vzpf, vzmf, rxc, rxw, ryc, rys, rrc;
+  // coupled top cell: exchange mode, surface depth, window budget, theta_r
+  double dep, avl, wcrc;
+  int cm;
+  int cxp, cxm, cyp, cym, botc, topc;
+  int8_t ae, an, au, al;
+};
+
+struct AsmOut {
+  double diag, gxp, gyp, gzp, rhs;  // gxp, gyp, gzp: the stored upper legs
+};
+
+// The arithmetic of the row of active cell (j, i, k) from gathered values
+// (assembleSystemImpl, Predictor.cpp:474-698).
+template <bool CPL, bool BARO>
+__device__ __forceinline__ AsmOut assemble_math(const Dims& d, const AsmIn& a, double dtg, int j,
+                                                int i, int k) {
+  const bool east = i == d.nx, west = i == 1, north = j == d.ny, south = j == 1;
+  const bool top = (k == 0) || !a.au;
+  const double volume = d.az * a.dzc;
+  // The reference's legs K dt cos / dx^2 * (A dx) and K dt / (dz dzf) *
+  // volume, and its RHS terms dt volume (...) / dz, with the lengths
+  // cancelled: K dt cos A (1/dx), K dt az / dzf and dt az (...) (equal up
+  // to rounding; three divisions per cell instead of nine).
+  double gxp = -a.kxp * dtg * a.cosxc * (a.axc * d.idx);
+  double gxm = -a.kxm * dtg * a.cosxw * (a.axw * d.idx);
+  double gyp = -a.kyp * dtg * a.cosyc * (a.ayc * d.idy);
+  double gym = -a.kym * dtg * a.cosys * (a.ays * d.idy);
+  if (BARO) {
+    gxp *= a.bxc;
+    gxm *= a.bxw;
+    gyp *= a.byc;
+    gym *= a.bys;
+  }
+  if (east && is_head(a.cxp)) gxp *= 2.0;
+  if (west && is_head(a.cxm)) gxm *= 2.0;
+  if (north && is_head(a.cyp)) gyp *= 2.0;
+  if (south && is_head(a.cym)) gym *= 2.0;
+  const double kdt = dtg * d.az;  // dt * volume / dz
+  // the z faces' K with their r v (and the gravity terms' r^2 v)
+  const double kzpb = BARO ? a.kzp * a.rzpf * a.vzpf : a.kzp;
+  const double kzmb = BARO ? a.kzm * a.rzmf * a.vzmf : a.kzm;
+  double dzf = (k == d.nz - 1) ? 0.5 * a.dzc : 0.5 * (a.dzc + a.dzl);
+  const double gzp = -kzpb * kdt / dzf;
+  dzf = top ? 0.5 * a.dzc : 0.5 * (a.dzc + a.dzu);
+  const double gzm = -kzmb * kdt / dzf;
+
+  const double storage =
+      BARO ? (a.chc + d.ss * a.wcnc / a.wcsc) * a.rrc : a.chc + d.ss * a.wcnc / a.wcsc;
+  double gct = storage * volume - (gxp + gxm + gyp + gym);
+  if (east && a.cxp == kFlux) gct += gxp;
+  if (west && a.cxm == kFlux) gct += gxm;
+  if (north && a.cyp == kFlux) gct += gyp;
+  if (south && a.cym == kFlux) gct += gym;
+  if (!(k == d.nz - 1 && a.botc != kHead)) gct -= gzp;
+  // Coupled top (Predictor.cpp:527-547): the exchange mode decides the
+  // Dirichlet leg, the surface depth and window budget feed the RHS.
+  const int cm = (CPL && top) ? a.cm : 0;
+  const bool dirichlet_top = CPL ? (cm == 1 || (d.pc && cm == 3)) : (a.topc == kHead);
+  if (!top || dirichlet_top) gct -= gzm;
+
+  double b = storage * a.hnc * volume;
+  b -= kdt * (BARO ? kzpb * a.rzpf : a.kzp);
+  b += kdt * (BARO ? kzmb * a.rzmf : a.kzm);
+  if (d.terrain) {
+    // along-layer gravity; the consistent form carries r^2 v of the face
+    const bool rb = BARO && d.pc;
+    double sg = (a.bote > a.botc_) ? 1.0 : -1.0;
+    b += sg * dtg * a.axc * a.kxp * a.sinxc * (rb ? a.bxc * a.rxc : 1.0);
+    sg = (a.botc_ > a.botw) ? -1.0 : 1.0;
+    b += sg * dtg * a.axw * a.kxm * a.sinxw * (rb ? a.bxw * a.rxw : 1.0);
+    sg = (a.botn > a.botc_) ? 1.0 : -1.0;
+    b += sg * dtg * a.ayc * a.kyp * a.sinyc * (rb ? a.byc * a.ryc : 1.0);
+    sg = (a.botc_ > a.bots) ? -1.0 : 1.0;
+    b += sg * dtg * a.ays * a.kym * a.sinys * (rb ? a.bys * a.rys : 1.0);
+  }
+  if (east) {
+    if (a.cxp == kFlux) b += a.axc * a.vxp * dtg * a.rxc;
+    else b -= gxp * a.hne;
+  }
+  if (west) {
+    if (a.cxm == kFlux) b += a.axw * a.vxm * dtg * a.rxw;
+    else b -= gxm * a.hnw;
+  }
+  if (north) {
+    if (a.cyp == kFlux) b += a.ayc * a.vyp * dtg * a.ryc;
+    else b -= gyp * a.hnn;
+  }
+  if (south) {
+    if (a.cym == kFlux) b += a.ays * a.vym * dtg * a.rys;
+    else b -= gym * a.hns;
+  }
+  if (k == d.nz - 1) {
+    if (a.botc == kFlux) b += kdt * a.rzpf * (a.vbot + kzpb);
+    else if (a.botc == kHead) b -= gzp * a.vbot;
+  }
+  if (top && CPL) {  // Predictor.cpp:627-674
+    if (cm == 1) {
+      b -= gzm * a.dep;
+    } else if (d.pc && cm == 3) {
+      // the ghost head is 0: the leg sits in the diagonal only
+    } else if (cm == 2) {
+      const double roomTop = fmax(0.0, (0.9999 * a.wcsc - a.wcnc) * a.dzc);
+      const double take = fmin(a.avl, roomTop);
+      const double qsup = -take / dtg;
+      b += -kdt * a.rzmf * (qsup + kzmb);
+    } else {
+      double qtop = 0.0;
+      if (a.topc == kFlux &&
+          ((a.vtop > 0.0 && a.wcnc < a.wcsc) || (a.vtop < 0.0 && a.wcnc > a.wcrc)))
+        qtop = a.vtop;
+      b += -kdt * a.rzmf * (qtop + kzmb);
+    }
+  } else if (top) {
+    if (a.topc == kHead) b -= gzm * a.vtop;
+    else if (a.topc == kFlux) b += -kdt * a.rzmf * (a.vtop + kzmb);
+  }
+  AsmOut o;
+  o.diag = gct;
+  o.gxp = (!east && a.ae) ? gxp : 0.0;
+  o.gyp = (!north && a.an) ? gyp : 0.0;
+  o.gzp = (k + 1 < d.nz && a.al) ? gzp : 0.0;
+  o.rhs = b;
+  return o;
+}
+
+// The per-cell data of the row other than the face conductivities (the
+// caller fills kxp .. kzp): metrics, state, BC data, ratios.
+template <bool CPL, bool BARO>
+__device__ __forceinline__ void assemble_gather(const Dims& d, const Fields& f,
+                                                const double* __restrict__ hn,
+                                                const double* __restrict__ wcn, double chc,
+                                                long long c, int j, int i, int k, AsmIn& a) {
+  const long long cw = c - d.sx, ce = c + d.sx, cs = c - d.sy, cn = c + d.sy;
+  const long long cu = (k >= 1) ? c - 1 : c, cl = (k + 1 < d.nz) ? c + 1 : c;
+  const long long col = col2(d, j, i);
+  a.ae = f.act[ce];
+  a.an = f.act[cn];
+  a.au = (k >= 1) ? f.act[cu] : int8_t(0);
+  a.al = (k + 1 < d.nz) ? f.act[cl] : int8_t(0);
+  a.dzc = f.dz[c];
+  a.dzu = f.dz[cu];
+  a.dzl = f.dz[cl];
+  a.wcnc = wcn[c];
+  a.wcsc = f.wcs[c];
+  a.cosxc = f.cosx[c];
+  a.cosxw = f.cosx[cw];
+  a.axc = f.ax[c];
+  a.axw = f.ax[cw];
+  a.cosyc = f.cosy[c];
+  a.cosys = f.cosy[cs];
+  a.ayc = f.ay[c];
+  a.ays = f.ay[cs];
+  a.chc = chc;
+  a.hnc = hn[c];
+  a.hne = hn[ce];
+  a.hnw = hn[cw];
+  a.hnn = hn[cn];
+  a.hns = hn[cs];
+  a.cxp = f.xpc[col];
+  a.cxm = f.xmc[col];
+  a.cyp = f.ypc[col];
+  a.cym = f.ymc[col];
+  a.botc = f.botc[col];
+  a.topc = f.topc[col];
+  a.vxp = f.xpv[col];
+  a.vxm = f.xmv[col];
+  a.vyp = f.ypv[col];
+  a.vym = f.ymv[col];
+  a.vbot = f.botv[col];
+  a.vtop = f.topv[col];
+  a.botc_ = a.bote = a.botw = a.botn = a.bots = 0.0;
+  a.sinxc = a.sinxw = a.sinyc = a.sinys = 0.0;
+  if (d.terrain) {
+    a.botc_ = f.bot[c];
+    a.bote = f.bot[ce];
+    a.botw = f.bot[cw];
+    a.botn = f.bot[cn];
+    a.bots = f.bot[cs];
+    a.sinxc = f.sinx[c];
+    a.sinxw = f.sinx[cw];
+    a.sinyc = f.siny[c];
+    a.sinys = f.siny[cs];
+  }
+  a.bxc = a.bxw = a.byc = a.bys = a.rzpf = a.rzmf = 1.0;
+  a.vzpf = a.vzmf = a.rxc = a.rxw = a.ryc = a.rys = a.rrc = 1.0;
+  if (BARO) {
+    const long long fz = fidx(d, j, i, k);
+    const BaroDev& B = *f.baro;
+    a.rxc = B.rxp[c];
+    a.rxw = B.rxp[cw];
+    a.ryc = B.ryp[c];
+    a.rys = B.ryp[cs];
+    a.bxc = a.rxc * B.vxp[c];
+    a.bxw = a.rxw * B.vxp[cw];
+    a.byc = a.ryc * B.vyp[c];
+    a.bys = a.rys * B.vyp[cs];
+    a.rzmf = B.rzp[fz];
+    a.rzpf = B.rzp[fz + 1];
+    a.vzmf = B.vzp[fz];
+    a.vzpf = B.vzp[fz + 1];
+    a.rrc = B.rrho[c];
+  }
+  a.cm = 0;
+  a.dep = a.avl = a.wcrc = 0.0;
+  const bool top = (k == 0) || !a.au;
+  if (CPL && top) {
+    a.cm = f.cpl->cmode[col];
+    a.dep = f.cpl->dept[col];
+    a.avl = f.cpl->avail[col];
+    a.wcrc = f.wcr[c];
+  }
+}
+
 // The 7-point head system of one active cell (assembleSystemImpl,
 // Predictor.cpp:400-698, uncoupled, density ratios 1): storage
 // C(h^n) + Ss theta^n / theta_s, the six legs with the head-edge doubling,
@@ -253,60 +481,19 @@ __device__ __forceinline__ void assemble_body(
       if (xw) xw[c] = 0.0;
       continue;
     }
-    const long long cw = c - d.sx, ce = c + d.sx, cs = c - d.sy, cn = c + d.sy;
-    const long long cu = (k >= 1) ? c - 1 : c, cl = (k + 1 < d.nz) ? c + 1 : c;
-    const long long col = col2(d, j, i);
     // Gather: the six face conductivities (k_faces), the cell's metrics,
     // heads and BC data.
     const long long fz = fidx(d, j, i, k);
-    const double kxp = kxf[c], kxm = kxf[cw], kyp = kyf[c], kym = kyf[cs];
-    const double kzm = kzff[fz], kzp = kzff[fz + 1];
-    const int8_t ac = f.act[c], ae = f.act[ce], an = f.act[cn];
-    const int8_t au = (k >= 1) ? f.act[cu] : int8_t(0), al = (k + 1 < d.nz) ? f.act[cl] : int8_t(0);
-    const double dzc = f.dz[c], dzu = f.dz[cu], dzl = f.dz[cl];
-    const double wcnc = wcn[c], wcsc = f.wcs[c];
-    const double cosxc = f.cosx[c], cosxw = f.cosx[cw], axc = f.ax[c], axw = f.ax[cw];
-    const double cosyc = f.cosy[c], cosys = f.cosy[cs], ayc = f.ay[c], ays = f.ay[cs];
-    const double chc = ch[c], hnc = hn[c], hne = hn[ce], hnw = hn[cw], hnn = hn[cn],
-                 hns = hn[cs];
-    const int cxp = f.xpc[col], cxm = f.xmc[col], cyp = f.ypc[col], cym = f.ymc[col];
-    const int botc = f.botc[col], topc = f.topc[col];
-    const double vxp = f.xpv[col], vxm = f.xmv[col], vyp = f.ypv[col], vym = f.ymv[col];
-    const double vbot = f.botv[col], vtop = f.topv[col];
-    double botc_ = 0.0, bote = 0.0, botw = 0.0, botn = 0.0, bots = 0.0;
-    double sinxc = 0.0, sinxw = 0.0, sinyc = 0.0, sinys = 0.0;
-    if (d.terrain) {
-      botc_ = f.bot[c];
-      bote = f.bot[ce];
-      botw = f.bot[cw];
-      botn = f.bot[cn];
-      bots = f.bot[cs];
-      sinxc = f.sinx[c];
-      sinxw = f.sinx[cw];
-      sinyc = f.siny[c];
-      sinys = f.siny[cs];
-    }
-    // Density coupling (the reference's assembly with its ratios): r v of each
-    // face for the legs, the cell's r_rho for the storage; 1 without.
-    double bxc = 1.0, bxw = 1.0, byc = 1.0, bys = 1.0, rzpf = 1.0, rzmf = 1.0;
-    double vzpf = 1.0, vzmf = 1.0, rxc = 1.0, rxw = 1.0, ryc = 1.0, rys = 1.0, rrc = 1.0;
-    if (BARO) {
-      const BaroDev& B = *f.baro;
-      rxc = B.rxp[c];
-      rxw = B.rxp[cw];
-      ryc = B.ryp[c];
-      rys = B.ryp[cs];
-      bxc = rxc * B.vxp[c];
-      bxw = rxw * B.vxp[cw];
-      byc = ryc * B.vyp[c];
-      bys = rys * B.vyp[cs];
-      rzmf = B.rzp[fz];
-      rzpf = B.rzp[fz + 1];
-      vzmf = B.vzp[fz];
-      vzpf = B.vzp[fz + 1];
-      rrc = B.rrho[c];
-    }
-    if (xw) xw[c] = ac ? hnc : 0.0;  // the mixed solve's starting iterate
+    AsmIn a;
+    a.kxp = kxf[c];
+    a.kxm = kxf[c - d.sx];
+    a.kyp = kyf[c];
+    a.kym = kyf[c - d.sy];
+    a.kzm = kzff[fz];
+    a.kzp = kzff[fz + 1];
+    const int8_t ac = f.act[c];
+    assemble_gather<CPL, BARO>(d, f, hn, wcn, ch[c], c, j, i, k, a);
+    if (xw) xw[c] = ac ? a.hnc : 0.0;  // the mixed solve's starting iterate
     if (!ac) {
       diag[c] = 1.0;
       gxps[c] = 0.0;
@@ -315,116 +502,12 @@ __device__ __forceinline__ void assemble_body(
       rhs[c] = 0.0;
       continue;
     }
-    const bool east = i == d.nx, west = i == 1, north = j == d.ny, south = j == 1;
-    const bool top = (k == 0) || !au;
-    const double volume = d.az * dzc;
-    // The reference's legs K dt cos / dx^2 * (A dx) and K dt / (dz dzf) *
-    // volume, and its RHS terms dt volume (...) / dz, with the lengths
-    // cancelled: K dt cos A (1/dx), K dt az / dzf and dt az (...) (equal up
-    // to rounding; three divisions per cell instead of nine).
-    double gxp = -kxp * dtg * cosxc * (axc * d.idx);
-    double gxm = -kxm * dtg * cosxw * (axw * d.idx);
-    double gyp = -kyp * dtg * cosyc * (ayc * d.idy);
-    double gym = -kym * dtg * cosys * (ays * d.idy);
-    if (BARO) {
-      gxp *= bxc;
-      gxm *= bxw;
-      gyp *= byc;
-      gym *= bys;
-    }
-    if (east && is_head(cxp)) gxp *= 2.0;
-    if (west && is_head(cxm)) gxm *= 2.0;
-    if (north && is_head(cyp)) gyp *= 2.0;
-    if (south && is_head(cym)) gym *= 2.0;
-    const double kdt = dtg * d.az;  // dt * volume / dz
-    // the z faces' K with their r v (and the gravity terms' r^2 v)
-    const double kzpb = BARO ? kzp * rzpf * vzpf : kzp, kzmb = BARO ? kzm * rzmf * vzmf : kzm;
-    double dzf = (k == d.nz - 1) ? 0.5 * dzc : 0.5 * (dzc + dzl);
-    const double gzp = -kzpb * kdt / dzf;
-    dzf = top ? 0.5 * dzc : 0.5 * (dzc + dzu);
-    const double gzm = -kzmb * kdt / dzf;
-
-    const double storage = BARO ? (chc + d.ss * wcnc / wcsc) * rrc : chc + d.ss * wcnc / wcsc;
-    double gct = storage * volume - (gxp + gxm + gyp + gym);
-    if (east && cxp == kFlux) gct += gxp;
-    if (west && cxm == kFlux) gct += gxm;
-    if (north && cyp == kFlux) gct += gyp;
-    if (south && cym == kFlux) gct += gym;
-    if (!(k == d.nz - 1 && botc != kHead)) gct -= gzp;
-    // Coupled top (Predictor.cpp:527-547): the exchange mode decides the
-    // Dirichlet leg, the surface depth and window budget feed the RHS.
-    int cm = 0;
-    double dep = 0.0, avl = 0.0, wcrc = 0.0;
-    if (CPL && top) {
-      cm = f.cpl->cmode[col];
-      dep = f.cpl->dept[col];
-      avl = f.cpl->avail[col];
-      wcrc = f.wcr[c];
-    }
-    const bool dirichlet_top = CPL ? (cm == 1 || (d.pc && cm == 3)) : (topc == kHead);
-    if (!top || dirichlet_top) gct -= gzm;
-
-    double b = storage * hnc * volume;
-    b -= kdt * (BARO ? kzpb * rzpf : kzp);
-    b += kdt * (BARO ? kzmb * rzmf : kzm);
-    if (d.terrain) {
-      // along-layer gravity; the consistent form carries r^2 v of the face
-      const bool rb = BARO && d.pc;
-      double sg = (bote > botc_) ? 1.0 : -1.0;
-      b += sg * dtg * axc * kxp * sinxc * (rb ? bxc * rxc : 1.0);
-      sg = (botc_ > botw) ? -1.0 : 1.0;
-      b += sg * dtg * axw * kxm * sinxw * (rb ? bxw * rxw : 1.0);
-      sg = (botn > botc_) ? 1.0 : -1.0;
-      b += sg * dtg * ayc * kyp * sinyc * (rb ? byc * ryc : 1.0);
-      sg = (botc_ > bots) ? -1.0 : 1.0;
-      b += sg * dtg * ays * kym * sinys * (rb ? bys * rys : 1.0);
-    }
-    if (east) {
-      if (cxp == kFlux) b += axc * vxp * dtg * rxc;
-      else b -= gxp * hne;
-    }
-    if (west) {
-      if (cxm == kFlux) b += axw * vxm * dtg * rxw;
-      else b -= gxm * hnw;
-    }
-    if (north) {
-      if (cyp == kFlux) b += ayc * vyp * dtg * ryc;
-      else b -= gyp * hnn;
-    }
-    if (south) {
-      if (cym == kFlux) b += ays * vym * dtg * rys;
-      else b -= gym * hns;
-    }
-    if (k == d.nz - 1) {
-      if (botc == kFlux) b += kdt * rzpf * (vbot + kzpb);
-      else if (botc == kHead) b -= gzp * vbot;
-    }
-    if (top && CPL) {  // Predictor.cpp:627-674
-      if (cm == 1) {
-        b -= gzm * dep;
-      } else if (d.pc && cm == 3) {
-        // the ghost head is 0: the leg sits in the diagonal only
-      } else if (cm == 2) {
-        const double roomTop = fmax(0.0, (0.9999 * wcsc - wcnc) * dzc);
-        const double take = fmin(avl, roomTop);
-        const double qsup = -take / dtg;
-        b += -kdt * rzmf * (qsup + kzmb);
-      } else {
-        double qtop = 0.0;
-        if (topc == kFlux &&
-            ((vtop > 0.0 && wcnc < wcsc) || (vtop < 0.0 && wcnc > wcrc)))
-          qtop = vtop;
-        b += -kdt * rzmf * (qtop + kzmb);
-      }
-    } else if (top) {
-      if (topc == kHead) b -= gzm * vtop;
-      else if (topc == kFlux) b += -kdt * rzmf * (vtop + kzmb);
-    }
-    diag[c] = gct;
-    gxps[c] = (!east && ae) ? gxp : 0.0;
-    gyps[c] = (!north && an) ? gyp : 0.0;
-    gzps[c] = (k + 1 < d.nz && al) ? gzp : 0.0;
-    rhs[c] = b;
+    const AsmOut o = assemble_math<CPL, BARO>(d, a, dtg, j, i, k);
+    diag[c] = o.diag;
+    gxps[c] = o.gxp;
+    gyps[c] = o.gyp;
+    gzps[c] = o.gzp;
+    rhs[c] = o.rhs;
   }
 }
 
@@ -489,6 +572,175 @@ template <bool CPL>
 __global__ void __launch_bounds__(kBlock, 4) k_faces(Dims d, Fields f, PassK pk, double* kx,
                                                      double* ky, double* kzf) {
   faces_body<CPL>(d, f, pk, kx, ky, kzf, blockIdx.x, gridDim.x);
+}
+
+// ---------------------------------------------------------------- fused predictor
+// The whole predictor of a groundwater-only domain (no coupled top, no
+// density coupling; nz <= 32 E) in one pass: the closures of h^n, the face
+// conductivities, the row assembly and, for the mixed form, the FP32 casts
+// and the column LDL^T factors -- the work of k_closure_pred, k_faces,
+// k_assemble and k_line_factor_warp without their intermediate arrays (per
+// cell K x3 and C, the three face arrays, the FP64 re-read by the factor).
+//
+// A block owns a strip of kPredCols interior columns along i plus one halo
+// column on each side, one warp per column, lane l holding the E consecutive
+// cells k = l E + e of it, and marches j over kPredRows rows.  At row j it
+// evaluates the closures of row j + 1 (K along x for the strip and its
+// halo, K along y for the strip into shared memory; K along z and C(h^n)
+// stay in registers for the next row), then every interior warp takes its
+// cell's six faces -- x from the shared row, y from the shared rows j - 1,
+// j, j + 1, z by shuffles along its own column -- and the row.  K along x
+// lives in three row slots and K along y in four, so a slot is rewritten
+// only after every warp has passed the barrier that follows its last
+// reader: one __syncthreads per row.  Halo columns cost 2 / kPredCols more
+// closures and each segment one more row; the closures are cheap against
+// the memory traffic.  The values are those of the separate passes: the
+// same closure, face-rule and row functions on the same inputs.
+constexpr int kPredWarps = 8;
+constexpr int kPredCols = kPredWarps - 2;
+constexpr int kPredRows = 16;
+
+// Shared memory of one block: K along x in three row slots for every warp,
+// K along y in four row slots and K along z and C(h^n) in two row slots for
+// the interior warps.
+__host__ __device__ inline size_t pred_smem_bytes(int E) {
+  return static_cast<size_t>(3 * kPredWarps + 4 * kPredCols + 4 * kPredCols) * 32 * E *
+         sizeof(double);
+}
+
+// Two blocks per SM up to 128 cells a column; deeper columns need 147 KB of
+// shared memory a block, one block per SM, with the registers that frees.
+template <int E, bool MIXED>
+__global__ void __launch_bounds__(kPredWarps * 32, (E >= 8) ? 1 : 2) k_predict(
+    Dims d, Fields f, const double* __restrict__ hn, const double* __restrict__ wcn,
+    const double* __restrict__ dtgp, double* __restrict__ diag, double* __restrict__ gxps,
+    double* __restrict__ gyps, double* __restrict__ gzps, double* __restrict__ rhs,
+    double* __restrict__ xw, float* __restrict__ diag32, float* __restrict__ gxp32,
+    float* __restrict__ gyp32, float* __restrict__ gzp32, float* __restrict__ dinv32,
+    float* __restrict__ l32) {
+  extern __shared__ __align__(16) double psm[];
+  constexpr int NZP = 32 * E;
+  double* skx = psm;                                // [3][kPredWarps][NZP]
+  double* sky = skx + 3 * kPredWarps * NZP;         // [4][kPredCols][NZP]
+  double* skz = sky + 4 * kPredCols * NZP;          // [2][kPredCols][NZP]
+  double* sch = skz + 2 * kPredCols * NZP;          // [2][kPredCols][NZP]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, k0 = lane * E;
+  const int i = blockIdx.x * kPredCols + w;  // this warp's column (warp 0: the west halo)
+  const bool has_col = i <= d.nx + 1;
+  const bool inner = w >= 1 && w <= kPredCols && i <= d.nx;
+  const int iw = w - 1;  // index among the interior columns
+  const int jb = 1 + blockIdx.y * kPredRows;
+  const int je = min(d.ny, jb + kPredRows - 1);
+  const int nz = d.nz;
+  const double dtg = *dtgp;
+
+  // Closures of row jj for this warp's column (Predictor.cpp:127-232,
+  // 445-452): K along x into its slot; for interior warps K along y, and
+  // with `full` K along z and C.
+  auto closures = [&](int jj, bool full) {
+    double* kxs = skx + ((jj % 3) * kPredWarps + w) * NZP;
+    double* kys = sky + ((jj & 3) * kPredCols + iw) * NZP;
+    double* kzs = skz + ((jj & 1) * kPredCols + iw) * NZP;
+    double* chs = sch + ((jj & 1) * kPredCols + iw) * NZP;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int k = k0 + e;
+      if (k < nz) {
+        const long long c = cidx(d, jj, i, k);
+        const double hc = hn[c];
+        const Soil so = soil_at(f, c);
+        const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
+        const VgParts v = vg_parts(so, hc);
+        const KrParts p = vg_kr_from(v, hc);
+        kxs[k] = vg_k_from(p, ksx);
+        if (inner) kys[k] = vg_k_from(p, ksy);
+        if (full) {
+          kzs[k] = vg_k_from(p, ksz);
+          chs[k] = vg_capacity_from(so, v, hc);
+        }
+      }
+    }
+  };
+
+  if (has_col) {
+    if (inner) closures(jb - 1, false);  // K along y of row jb - 1
+    closures(jb, inner);
+  }
+  for (int j = jb; j <= je; ++j) {
+    if (has_col) closures(j + 1, inner);
+    __syncthreads();
+    if (inner) {
+      const double* kx0 = skx + ((j % 3) * kPredWarps) * NZP;
+      const double* kyS = sky + (((j - 1) & 3) * kPredCols + iw) * NZP;
+      const double* kyC = sky + ((j & 3) * kPredCols + iw) * NZP;
+      const double* kyN = sky + (((j + 1) & 3) * kPredCols + iw) * NZP;
+      const double* kzC = skz + ((j & 1) * kPredCols + iw) * NZP;
+      const double* chC = sch + ((j & 1) * kPredCols + iw) * NZP;
+      const long long col = col2(d, j, i), cb = cidx(d, j, i, 0);
+      const int topc = f.topc[col], botc = f.botc[col];
+      const int xcode_m = (i == 1) ? f.xmc[col2(d, j, 1)] : f.xpc[col2(d, j, d.nx)];
+      const int xcode_p = f.xpc[col2(d, j, d.nx)];
+      const int ycode_m = (j == 1) ? f.ymc[col2(d, 1, i)] : f.ypc[col2(d, d.ny, i)];
+      const int ycode_p = f.ypc[col2(d, d.ny, i)];
+      double av[E], ev[E], xv[E], yv[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = k0 + e;
+        av[e] = 1.0;
+        ev[e] = xv[e] = yv[e] = 0.0;
+        if (k < nz) {
+          const long long c = cb + k;
+          const long long ce = c + d.sx, cw = c - d.sx, cn = c + d.sy, cs = c - d.sy;
+          const long long cu = (k >= 1) ? c - 1 : c, cl = (k + 1 < nz) ? c + 1 : c;
+          const double wcc = wcn[c], wsc = f.wcs[c];
+          const int8_t ac = f.act[c];
+          const Flank fc_x{kx0[w * NZP + k], f.ksx[c], wcc, wsc, ac};
+          const Flank fe_x{kx0[(w + 1) * NZP + k], f.ksx[ce], wcn[ce], f.wcs[ce], f.act[ce]};
+          const Flank fw_x{kx0[(w - 1) * NZP + k], f.ksx[cw], wcn[cw], f.wcs[cw], f.act[cw]};
+          const Flank fc_y{kyC[k], f.ksy[c], wcc, wsc, ac};
+          const Flank fn_y{kyN[k], f.ksy[cn], wcn[cn], f.wcs[cn], f.act[cn]};
+          const Flank fs_y{kyS[k], f.ksy[cs], wcn[cs], f.wcs[cs], f.act[cs]};
+          const ZFlank zu{(k >= 1) ? kzC[k - 1] : kzC[k], f.ksz[cu], f.dz[cu],
+                          (k >= 1) ? f.act[cu] : int8_t(0)};
+          const ZFlank zc{kzC[k], f.ksz[c], f.dz[c], ac};
+          const ZFlank zl{(k + 1 < nz) ? kzC[k + 1] : 0.0, f.ksz[cl], f.dz[cl],
+                          (k + 1 < nz) ? f.act[cl] : int8_t(0)};
+          AsmIn a;
+          a.kxp = face_lat(d, fc_x, fe_x, false, i == d.nx, xcode_p);
+          a.kxm = face_lat(d, fw_x, fc_x, i == 1, false, xcode_m);
+          a.kyp = face_lat(d, fc_y, fn_y, false, j == d.ny, ycode_p);
+          a.kym = face_lat(d, fs_y, fc_y, j == 1, false, ycode_m);
+          a.kzm = face_z<false>(d, zu, zc, k, topc, botc, 0.0);
+          if (k + 1 < nz) {
+            a.kzp = face_z<false>(d, zc, zl, k + 1, topc, botc, 0.0);
+          } else {
+            const ZFlank none{0.0, 0.0, 0.0, 0};
+            a.kzp = face_z<false>(d, zc, none, nz, topc, botc, 0.0);
+          }
+          assemble_gather<false, false>(d, f, hn, wcn, chC[k], c, j, i, k, a);
+          if (MIXED) xw[c] = ac ? a.hnc : 0.0;  // the mixed solve's starting iterate
+          double rv = 0.0;
+          if (ac) {
+            const AsmOut o = assemble_math<false, false>(d, a, dtg, j, i, k);
+            av[e] = o.diag;
+            xv[e] = o.gxp;
+            yv[e] = o.gyp;
+            ev[e] = o.gzp;
+            rv = o.rhs;
+          }
+          diag[c] = av[e];
+          gxps[c] = xv[e];
+          gyps[c] = yv[e];
+          gzps[c] = ev[e];
+          rhs[c] = rv;
+        }
+      }
+      if (MIXED) factor_column<E>(nz, cb, av, ev, xv, yv, diag32, gxp32, gyp32, gzp32, dinv32, l32);
+    }
+    // The next row's closures rewrite this warp's K along z and C slots
+    // that other lanes of the warp have just read.
+    __syncwarp();
+  }
 }
 
 // ---------------------------------------------------------------- fluxes
@@ -2024,6 +2276,33 @@ void launch_assemble(const Device& D, const double* hn, const double* wcn, bool 
                                                      dtg_slot(D), D.diag, D.gxp, D.gyp, D.gzp,
                                                      D.rhs, warm ? D.x : nullptr);
   D.launches += 2;
+}
+
+// The fused predictor where it applies (groundwater-only domain, nz <= 256);
+// false: the caller launches the separate passes.
+bool launch_predict(const Device& D, const double* hn, const double* wcn, bool mixed) {
+  if (D.f.cpl != nullptr || D.f.baro != nullptr || D.d.nz > 256) return false;
+  const int E = D.d.nz <= 32 ? 1 : D.d.nz <= 64 ? 2 : D.d.nz <= 128 ? 4 : 8;
+  using Kern = void (*)(Dims, Fields, const double*, const double*, const double*, double*,
+                        double*, double*, double*, double*, double*, float*, float*, float*,
+                        float*, float*, float*);
+  Kern k;
+  if (mixed) k = E == 1 ? k_predict<1, true> : E == 2 ? k_predict<2, true>
+               : E == 4 ? k_predict<4, true> : k_predict<8, true>;
+  else k = E == 1 ? k_predict<1, false> : E == 2 ? k_predict<2, false>
+         : E == 4 ? k_predict<4, false> : k_predict<8, false>;
+  const size_t smem = pred_smem_bytes(E);
+  if (raise_smem_limit(reinterpret_cast<const void*>(k), smem) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const dim3 grid((D.d.nx + kPredCols - 1) / kPredCols, (D.d.ny + kPredRows - 1) / kPredRows);
+  k<<<grid, kPredWarps * 32, smem, D.stream>>>(D.d, D.f, hn, wcn, dtg_slot(D), D.diag, D.gxp,
+                                                D.gyp, D.gzp, D.rhs, mixed ? D.x : nullptr,
+                                                D.diag32, D.gxp32, D.gyp32, D.gzp32, D.dinv32,
+                                                D.l32);
+  ++D.launches;
+  return true;
 }
 
 void launch_closure_corr(const Device& D, const double* hn) {

@@ -65,6 +65,8 @@ def load_library(path: str = LIB_PATH):
     lib.frehg_gw_set_profiling.restype = C.c_int
     lib.frehg_gw_phase_times.argtypes = [H, _dp]
     lib.frehg_gw_phase_times.restype = C.c_int
+    lib.frehg_gw_set_fused.argtypes = [H, C.c_int]
+    lib.frehg_gw_set_fused.restype = C.c_int
     lib.frehg_gw_kernel_launches.argtypes = [H]
     lib.frehg_gw_kernel_launches.restype = C.c_longlong
     lib.frehg_gw_attach_coupling.argtypes = [H, C.POINTER(Coupling)]
@@ -267,6 +269,10 @@ class RichardsSolver:
 
     def setProfiling(self, on: bool = True) -> None:
         _check(self.lib, self.lib.frehg_gw_set_profiling(self.h, int(bool(on))))
+
+    def setFused(self, on: bool = True) -> None:
+        """Fused phase kernels (default) or every phase as separate passes."""
+        _check(self.lib, self.lib.frehg_gw_set_fused(self.h, int(bool(on))))
 
     def phaseTimes(self) -> dict:
         """Device ms per phase of the last step (profiling on)."""

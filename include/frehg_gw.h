@@ -255,6 +255,13 @@ int frehg_gw_device(const frehg_gw_handle* h);
 int frehg_gw_set_profiling(frehg_gw_handle* h, int on);
 int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5);
 
+/* Kernel selection (no counterpart in the reference): on (the default), a
+ * groundwater-only domain with nz <= 256 runs each phase that has one as a
+ * single fused pass (the predictor: closures, faces, rows and the mixed
+ * form's column factors); off, every phase runs as its separate passes.  The
+ * arithmetic is the same either way. */
+int frehg_gw_set_fused(frehg_gw_handle* h, int on);
+
 /* The transport window (RichardsSolver::enableTransportWindow,
  * resetTransportWindow, windowVolumeX/Y/Z, windowVentVolume,
  * src/gw/RichardsSolver.hpp:229-248; accumulateTransportWindow,

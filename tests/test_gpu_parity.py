@@ -39,7 +39,8 @@ def rel_linf(a, b, floor=0.0):
     return float(np.max(np.abs(a - b)) / scale)
 
 
-def compare(cfg, steps, fields=("h", "wc", "qx", "qy", "qz", "kx", "ky", "kz"), t_end=None):
+def compare(cfg, steps, fields=("h", "wc", "qx", "qy", "qz", "kx", "ky", "kz"), t_end=None,
+            dt_rtol=1e-9):
     """Steps the B200 form and the oracle in lockstep on the oracle's dt
     sequence: ``steps`` steps, or, with ``t_end``, the reference driver's
     loop to that time (``Simulation::runGroundwaterLoop``,
@@ -60,7 +61,7 @@ def compare(cfg, steps, fields=("h", "wc", "qx", "qy", "qz", "kx", "ky", "kz"), 
         n = 0
         while (n < steps) if t_end is None else (cpu.t < t_end - 1.0e-9):
             dtg = cpu.next_dt()
-            assert gpu.nextDt() == pytest.approx(dtg, rel=1e-9), f"step {n}"
+            assert gpu.nextDt() == pytest.approx(dtg, rel=dt_rtol), f"step {n}"
             cpu.t += dtg
             cpu.step(cpu.t, dtg)
             info = gpu.step(cpu.t, dtg)
@@ -107,8 +108,12 @@ def test_hillslope_crop_parity():
 
 def test_box_32x32x50_to_end_time():
     # The homogeneous box case as described: 1 h of simulated time from
-    # dt0 = 10 s (about 300 adaptive steps, 8 to 40 CG iterations each).
-    its = compare(workloads.column_32x32x50(), 0, t_end=3600.0)
+    # dt0 = 10 s (about 300 adaptive steps, 8 to 40 CG iterations each).  Once
+    # the wetting front nears saturation the controller's Courant cap
+    # Co dz / (dK/dtheta) sets dt, and dK/dtheta there amplifies the last
+    # bits of theta by 1 / (1 - Se^(1/m)): the GPU's own next dt (from its own
+    # state; the steps themselves take the oracle's) is held to 1e-8 here.
+    its = compare(workloads.column_32x32x50(), 0, t_end=3600.0, dt_rtol=1e-8)
     assert len(its) > 100
 
 
