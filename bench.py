@@ -288,6 +288,17 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+def reduce_over_ranks(dist, ms: float, active: int, device) -> tuple:
+    """The job's time (the slowest rank's) and the cells all ranks stepped:
+    every rank calls it once after its timed region, in the same order."""
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    a = torch.tensor([float(active)], device=device, dtype=torch.float64)
+    dist.all_reduce(a)
+    return float(t.item()), float(a.item())
+
+
 def latency_summary(solve_ms, step_ms) -> dict:
     """p50 / p99 of the per-step device times (CUDA events around each phase
     of every timed step): the predictor solve alone and the whole step."""
@@ -363,12 +374,7 @@ def timed_form(args, precision, rank, local, dist, stream, e2e_steps):
     ms = start.elapsed_time(end)
     total_cells = float(active)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        a = torch.tensor([float(active)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(a)
-        total_cells = float(a.item())
+        ms, total_cells = reduce_over_ranks(dist, ms, active, "cuda")
     out = dict(value=total_cells * args.steps / (ms / 1e3), ms=ms, iters=iters, outer=outer,
                solve_ms=solve_ms, launches=launches, clocks=clocks.summary(), active=active,
                e2e=None, latency=latency_summary(solve_list, step_list))

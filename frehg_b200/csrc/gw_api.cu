@@ -509,10 +509,12 @@ void enqueue_corrector(frehg_gw_handle* h) {
   const int nxt = 1 - D.cur;
   double* hn = D.h[D.cur];
   double* wcn = D.wc[D.cur];
-  fgw::launch_closure_corr(D, hn);
-  fgw::launch_flux(D, wcn);
-  if (D.f.cpl) fgw::launch_cpl_book(D, wcn);
-  fgw::launch_update_wc(D, hn, wcn);
+  if (!(h->fused && fgw::launch_correct(D, hn, wcn))) {
+    fgw::launch_closure_corr(D, hn);
+    fgw::launch_flux(D, wcn);
+    if (D.f.cpl) fgw::launch_cpl_book(D, wcn);
+    fgw::launch_update_wc(D, hn, wcn);
+  }
   if (h->profiling) cudaEventRecord(h->ev[3], D.stream);
   fgw::launch_classify(D, D.wc[nxt], D.h[nxt]);
   fgw::launch_walk(D, D.wc[nxt]);

@@ -143,6 +143,9 @@ void launch_assemble(const Device& D, const double* hn, const double* wcn, bool 
 // The predictor in one fused pass (closures, faces, rows and, mixed, the
 // column factors) where it applies; false: use the separate passes.
 bool launch_predict(const Device& D, const double* hn, const double* wcn, bool mixed);
+// The corrector (head scatter, closures, faces, fluxes, theta update) in one
+// fused pass where it applies; false: use the separate passes.
+bool launch_correct(const Device& D, const double* hn, const double* wcn);
 void launch_closure_corr(const Device& D, const double* hn);
 void launch_flux(const Device& D, const double* wcn);
 void launch_update_wc(const Device& D, const double* hn, const double* wcn);

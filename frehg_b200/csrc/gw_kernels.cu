@@ -166,6 +166,43 @@ __global__ void __launch_bounds__(kBlock) k_closure_pred(Dims d, Fields f,
   closure_pred_body(d, f, h, kcx, kcy, kcz, ch, blockIdx.x, gridDim.x);
 }
 
+// The predicted head of cell c = (j, i, k): the solution of an active
+// interior cell, h^n of an inactive one (fillAndSolve's gw_scatter_head,
+// Predictor.cpp:745-754), the head BC's ghost of an edge ghost
+// (enforceHeadBc, RichardsSolver.cpp:762), 0 in the four corner columns.
+__device__ __forceinline__ double predicted_head(const Dims& d, const Fields& f,
+                                                 const double* __restrict__ x,
+                                                 const double* __restrict__ hn, long long c, int j,
+                                                 int i) {
+  const bool jin = j >= 1 && j <= d.ny, iin = i >= 1 && i <= d.nx;
+  double hv = 0.0;
+  if (jin && iin) {
+    const int8_t ac = f.act[c];
+    const double xc = x[c], hc = hn[c];
+    hv = ac ? xc : hc;
+  } else if (jin && (i == 0 || i == d.nx + 1)) {
+    const long long ci = (i == 0) ? c + d.sx : c - d.sx;
+    const long long cc = col2(d, j, i == 0 ? 1 : d.nx);
+    const int8_t ai = f.act[ci];
+    const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
+    const int code = i == 0 ? f.xmc[cc] : f.xpc[cc];
+    const double val = i == 0 ? f.xmv[cc] : f.xpv[cc];
+    // the edge face's density ratio: the ghost's slot west, the edge cell's east
+    const double r = (f.baro == nullptr) ? 1.0 : f.baro->rxp[i == 0 ? c : ci];
+    hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc, r, i != 0);
+  } else if (iin && (j == 0 || j == d.ny + 1)) {
+    const long long ci = (j == 0) ? c + d.sy : c - d.sy;
+    const long long cc = col2(d, j == 0 ? 1 : d.ny, i);
+    const int8_t ai = f.act[ci];
+    const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
+    const int code = j == 0 ? f.ymc[cc] : f.ypc[cc];
+    const double val = j == 0 ? f.ymv[cc] : f.ypv[cc];
+    const double r = (f.baro == nullptr) ? 1.0 : f.baro->ryp[j == 0 ? c : ci];
+    hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc, r, j != 0);
+  }
+  return hv;
+}
+
 // Corrector pass: scatter the solved heads (fillAndSolve's gw_scatter_head,
 // Predictor.cpp:745-754), re-impose the ghost heads (enforceHeadBc after the
 // solve, RichardsSolver.cpp:762) and evaluate the per-cell conductivities of
@@ -181,34 +218,9 @@ __device__ __forceinline__ void closure_corr_body(Dims d, Fields f,
        c += static_cast<long long>(G) * blockDim.x) {
     int j, i, k;
     unflatten(d, c, j, i, k);
-    const bool jin = j >= 1 && j <= d.ny, iin = i >= 1 && i <= d.nx;
     const Soil so = soil_at(f, c);
     const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
-    double hv = 0.0;
-    if (jin && iin) {
-      const int8_t ac = f.act[c];
-      const double xc = x[c], hc = hn[c];
-      hv = ac ? xc : hc;
-    } else if (jin && (i == 0 || i == d.nx + 1)) {
-      const long long ci = (i == 0) ? c + d.sx : c - d.sx;
-      const long long cc = col2(d, j, i == 0 ? 1 : d.nx);
-      const int8_t ai = f.act[ci];
-      const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
-      const int code = i == 0 ? f.xmc[cc] : f.xpc[cc];
-      const double val = i == 0 ? f.xmv[cc] : f.xpv[cc];
-      // the edge face's density ratio: the ghost's slot west, the edge cell's east
-      const double r = (f.baro == nullptr) ? 1.0 : f.baro->rxp[i == 0 ? c : ci];
-      hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc, r, i != 0);
-    } else if (iin && (j == 0 || j == d.ny + 1)) {
-      const long long ci = (j == 0) ? c + d.sy : c - d.sy;
-      const long long cc = col2(d, j == 0 ? 1 : d.ny, i);
-      const int8_t ai = f.act[ci];
-      const double xi = x[ci], hi0 = hn[ci], zc = f.bot[ci] + 0.5 * f.dz[ci];
-      const int code = j == 0 ? f.ymc[cc] : f.ypc[cc];
-      const double val = j == 0 ? f.ymv[cc] : f.ypv[cc];
-      const double r = (f.baro == nullptr) ? 1.0 : f.baro->ryp[j == 0 ? c : ci];
-      hv = ghost_head_at(d, f, code, val, ai ? xi : hi0, zc, cc, r, j != 0);
-    }
+    const double hv = predicted_head(d, f, x, hn, c, j, i);
     const KrParts p = vg_kr_parts(so, hv);
     hp[c] = hv;
     kcx[c] = vg_k_from(p, ksx);
@@ -763,7 +775,7 @@ struct LatFlux {
 
 __device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux& v, double ih,
                                   bool lo_edge, bool hi_edge, int code, double value, long long b,
-                                  const double* __restrict__ hp, double rf, double vf) {
+                                  double rf, double vf) {
   double q;
   if (lo_edge) {
     q = v.area * v.kcb * vf * v.cosv * (v.hpb - v.hpa) * (2.0 * ih);
@@ -780,7 +792,7 @@ __device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux&
     if (d.pc) {
       kf = d.harm ? face_harm(v.kca, v.ksa, 1.0, v.kcb, v.ksb, 1.0) : 0.5 * (v.kca + v.kcb);
     } else {
-      kf = 0.5 * (v.kca + vg_k(soil_at(f, b), hp[b], v.ksa));
+      kf = 0.5 * (v.kca + vg_k(soil_at(f, b), v.hpb, v.ksa));
     }
     if (!v.acta || !v.actb) kf = 0.0;
   }
@@ -800,8 +812,7 @@ __device__ inline double flux_lat(const Dims& d, const Fields& f, const LatFlux&
 // conductance's v.
 __device__ inline double flux_zv(const Dims& d, const Fields& f, const ZFlank& u, const ZFlank& l,
                                  double hpu, double hpl, int k, int topc, double topv, int botc,
-                                 double botv, long long cu, const double* __restrict__ hp,
-                                 double rz, double vz) {
+                                 double botv, long long cu, double rz, double vz) {
   const bool below = (k < d.nz) && l.act;
   const bool above = (k >= 1) && u.act;
   if (below && !above) {  // face above a column's top cell
@@ -827,7 +838,7 @@ __device__ inline double flux_zv(const Dims& d, const Fields& f, const ZFlank& u
     if (d.pc) {
       kf = d.harm ? face_harm(u.kc, u.ks, u.dz, l.kc, l.ks, l.dz) : 0.5 * (u.kc + l.kc);
     } else {
-      kf = 0.5 * (vg_k(soil_at(f, cu), hp[cu], l.ks) + l.kc);
+      kf = 0.5 * (vg_k(soil_at(f, cu), hpu, l.ks) + l.kc);
     }
     const double delta = 0.5 * (u.dz + l.dz);
     return d.az * kf * vz * ((hpl - hpu) / delta - rz);
@@ -944,14 +955,14 @@ __device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
       const Flank a{vx.kca, vx.ksa, vx.wa, vx.wsa, vx.acta};
       const Flank b{vx.kcb, vx.ksb, vx.wb, vx.wsb, vx.actb};
       kx[c] = face_lat(d, a, b, i == 0, i == d.nx, codex);
-      qx[c] = flux_lat(d, f, vx, d.idx, i == 0, i == d.nx, codex, valx, e, hp,
+      qx[c] = flux_lat(d, f, vx, d.idx, i == 0, i == d.nx, codex, valx, e,
                        BARO ? f.baro->rxp[c] : 1.0, BARO ? f.baro->vxp[c] : 1.0);
     }
     if (doY) {
       const Flank a{vy.kca, vy.ksa, vy.wa, vy.wsa, vy.acta};
       const Flank b{vy.kcb, vy.ksb, vy.wb, vy.wsb, vy.actb};
       ky[c] = face_lat(d, a, b, j == 0, j == d.ny, codey);
-      qy[c] = flux_lat(d, f, vy, d.idy, j == 0, j == d.ny, codey, valy, n, hp,
+      qy[c] = flux_lat(d, f, vy, d.idy, j == 0, j == d.ny, codey, valy, n,
                        BARO ? f.baro->ryp[c] : 1.0, BARO ? f.baro->vyp[c] : 1.0);
     }
     if (doZ) {
@@ -962,11 +973,11 @@ __device__ __forceinline__ void flux_body(Dims d, Fields f, PassK pk,
       if (CPL && zc.act && !(k >= 1 && zu.act))
         qzf[fz] = flux_top_coupled(d, f, col, c, hpc, wcn[c], dtg, rz, vz);
       else
-        qzf[fz] = flux_zv(d, f, zu, zc, hpu, hpc, k, topc, topv, botc, botv, cu, hp, rz, vz);
+        qzf[fz] = flux_zv(d, f, zu, zc, hpu, hpc, k, topc, topv, botc, botv, cu, rz, vz);
       if (k == d.nz - 1) {
         const ZFlank none{0.0, 0.0, 0.0, 0};
         kzf[fz + 1] = face_z<CPL>(d, zc, none, d.nz, topc, botc, 0.0);
-        qzf[fz + 1] = flux_zv(d, f, zc, none, hpc, 0.0, d.nz, topc, topv, botc, botv, c, hp,
+        qzf[fz + 1] = flux_zv(d, f, zc, none, hpc, 0.0, d.nz, topc, topv, botc, botv, c,
                               BARO ? f.baro->rzp[fz + 1] : 1.0,
                               BARO ? f.baro->vzp[fz + 1] : 1.0);
       }
@@ -1001,6 +1012,23 @@ __global__ void __launch_bounds__(kBlock, 2) k_flux(Dims d, Fields f, PassK pk,
 // branch on loaded data, so one memory round trip serves the cell.
 // BARO: density coupling (updateWaterContent with its ratios): the storage
 // weighs by the cell's r_rho, each face flux by its face's r.
+// theta of an active cell from its six face fluxes (density ratios 1);
+// adds the cell's Ss storage term to acc.
+__device__ __forceinline__ double theta_update(const Dims& d, double dtg, double w0, double hpc,
+                                               double hnc, double dzc, double ts, double qxp,
+                                               double qxm, double qyp, double qym, double qzt,
+                                               double qzb, double& acc) {
+  const double volume = d.az * dzc;
+  const double dh = hpc - hnc;
+  const double coeff = volume * (1.0 + d.ss * dh / ts);
+  const double dqx = dtg * (qxp - qxm);
+  const double dqy = dtg * (qyp - qym);
+  const double dqz = dtg * (qzb - qzt);
+  const double upd = (w0 * volume + dqx + dqy + dqz) / coeff;
+  acc += upd * volume * d.ss * dh / ts;
+  return upd;
+}
+
 template <bool BARO>
 __device__ __forceinline__ void update_wc_body(
     Dims d, Fields f, const double* __restrict__ hp, const double* __restrict__ hn,
@@ -1035,14 +1063,7 @@ __device__ __forceinline__ void update_wc_body(
         upd = (w0 * r * volume + dqx + dqy + dqz) / coeff;
         acc += upd * volume * r * d.ss * dh / ts;
       } else if (ac) {
-        const double volume = d.az * dzc;
-        const double dh = hpc - hnc;
-        const double coeff = volume * (1.0 + d.ss * dh / ts);
-        const double dqx = dtg * (qxp - qxm);
-        const double dqy = dtg * (qyp - qym);
-        const double dqz = dtg * (qzb - qzt);
-        upd = (w0 * volume + dqx + dqy + dqz) / coeff;
-        acc += upd * volume * d.ss * dh / ts;
+        upd = theta_update(d, dtg, w0, hpc, hnc, dzc, ts, qxp, qxm, qyp, qym, qzt, qzb, acc);
       }
     }
     wcu[c] = upd;
@@ -1061,6 +1082,217 @@ __global__ void __launch_bounds__(kBlock, 4) k_update_wc(
     uint8_t* __restrict__ satf, int* __restrict__ colflag, double* partial) {
   update_wc_body<BARO>(d, f, hp, hn, wcn, qx, qy, qzf, dtgp, wcu, satf, colflag, partial,
                        blockIdx.x, gridDim.x);
+}
+
+// ---------------------------------------------------------------- fused corrector
+// The corrector of a groundwater-only domain (no coupled top, no density
+// coupling; nz <= 32 E) in one pass: the head scatter with its ghosts and
+// the closures of the predicted head (k_closure_corr), the corrector's face
+// conductivities and Darcy fluxes (k_flux) and the theta update with the
+// saturation flags and the Ss audit partials (k_update_wc), without the
+// per-cell K arrays between them.  The same strip and row march as
+// k_predict: at row j the closures of row j + 1 fill the shared rows (the
+// predicted head and K along x for the strip and its halo, K along y for
+// the strip, K along z per warp), then every interior warp takes its cell's
+// six fluxes -- the x- and y- ones evaluated again from the same inputs as
+// the neighbour that owns and stores them -- and theta.  Ghost cells'
+// outputs (predicted head, theta, flags) are stored by the block that owns
+// the strip and rows they border, once.  The grid is the domain's reducing
+// grid (D.nblk blocks) walking the (strip, segment) items, so each block
+// leaves one Ss partial.
+constexpr int kCorrWarps = 8;
+constexpr int kCorrCols = kCorrWarps - 2;
+constexpr int kCorrRows = 16;
+
+__host__ __device__ inline size_t corr_smem_bytes(int E) {
+  // K along x [3][warps], head [4][warps], K along y [4][cols], K along z [2][cols]
+  return static_cast<size_t>(3 * kCorrWarps + 4 * kCorrWarps + 4 * kCorrCols + 2 * kCorrCols) *
+         32 * E * sizeof(double);
+}
+
+template <int E>
+__global__ void __launch_bounds__(kCorrWarps * 32, (E >= 8) ? 1 : 2) k_correct(
+    Dims d, Fields f, const double* __restrict__ x, const double* __restrict__ hn,
+    const double* __restrict__ wcn, const double* __restrict__ dtgp, double* __restrict__ hp,
+    double* __restrict__ kx, double* __restrict__ ky, double* __restrict__ kzf,
+    double* __restrict__ qx, double* __restrict__ qy, double* __restrict__ qzf,
+    double* __restrict__ wcu, uint8_t* __restrict__ satf, int* __restrict__ colflag,
+    double* __restrict__ partial) {
+  extern __shared__ __align__(16) double csm[];
+  constexpr int NZP = 32 * E;
+  double* skx = csm;                               // [3][kCorrWarps][NZP]
+  double* shp = skx + 3 * kCorrWarps * NZP;        // [4][kCorrWarps][NZP]
+  double* sky = shp + 4 * kCorrWarps * NZP;        // [4][kCorrCols][NZP]
+  double* skz = sky + 4 * kCorrCols * NZP;         // [2][kCorrCols][NZP]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, k0 = lane * E;
+  const int iw = w - 1;
+  const int nz = d.nz;
+  const double dtg = *dtgp;
+  const int nstrips = (d.nx + kCorrCols - 1) / kCorrCols;
+  const int nitems = nstrips * ((d.ny + kCorrRows - 1) / kCorrRows);
+  double acc = 0.0;
+
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int strip = item % nstrips, seg = item / nstrips;
+    const int i0 = 1 + strip * kCorrCols;
+    const int i = i0 - 1 + w;
+    const bool has_col = i <= d.nx + 1;
+    const bool inner = w >= 1 && w <= kCorrCols && i <= d.nx;
+    const int jb = 1 + seg * kCorrRows;
+    const int je = min(d.ny, jb + kCorrRows - 1);
+    // the columns and rows whose ghost cells this item stores
+    const int ilo = (strip == 0) ? 0 : i0, ihi = min(d.nx, i0 + kCorrCols - 1);
+    const int ihi_g = (ihi == d.nx) ? d.nx + 1 : ihi;
+    const int jlo_g = (jb == 1) ? 0 : jb, jhi_g = (je == d.ny) ? d.ny + 1 : je;
+    const bool own_i = i >= ilo && i <= ihi_g;
+
+    // Closures of row jj for this warp's column: the predicted head and K
+    // along x into their slots; interior warps also K along y and, with
+    // `full`, K along z.  Ghost cells owned by this item get their outputs.
+    auto closures = [&](int jj, bool full) {
+      double* kxs = skx + ((jj % 3) * kCorrWarps + w) * NZP;
+      double* hps = shp + ((jj & 3) * kCorrWarps + w) * NZP;
+      double* kys = sky + ((jj & 3) * kCorrCols + iw) * NZP;
+      double* kzs = skz + ((jj & 1) * kCorrCols + iw) * NZP;
+      const bool ghost = jj == 0 || jj == d.ny + 1 || i == 0 || i == d.nx + 1;
+      const bool store = ghost && own_i && jj >= jlo_g && jj <= jhi_g;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = k0 + e;
+        if (k < nz) {
+          const long long c = cidx(d, jj, i, k);
+          const Soil so = soil_at(f, c);
+          const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
+          const double hv = predicted_head(d, f, x, hn, c, jj, i);
+          const KrParts p = vg_kr_parts(so, hv);
+          hps[k] = hv;
+          kxs[k] = vg_k_from(p, ksx);
+          if (inner) kys[k] = vg_k_from(p, ksy);
+          if (full) kzs[k] = vg_k_from(p, ksz);
+          if (store) {
+            const double w0 = wcn[c];
+            hp[c] = hv;
+            wcu[c] = w0;
+            satf[c] = (w0 >= so.ts || hv > so.aev) ? 1 : 0;
+            if (k == 0) colflag[col2(d, jj, i)] = 0;
+          }
+        }
+      }
+    };
+
+    __syncthreads();  // the previous item's last row is read before the slots are rewritten
+    if (has_col) {
+      closures(jb - 1, false);
+      closures(jb, inner);
+    }
+    for (int j = jb; j <= je; ++j) {
+      if (has_col) closures(j + 1, inner);
+      __syncthreads();
+      if (inner) {
+        const double* kx0 = skx + ((j % 3) * kCorrWarps) * NZP;
+        const double* hp0 = shp + ((j & 3) * kCorrWarps) * NZP;
+        const double* hpS = shp + (((j - 1) & 3) * kCorrWarps + w) * NZP;
+        const double* hpN = shp + (((j + 1) & 3) * kCorrWarps + w) * NZP;
+        const double* kyS = sky + (((j - 1) & 3) * kCorrCols + iw) * NZP;
+        const double* kyC = sky + ((j & 3) * kCorrCols + iw) * NZP;
+        const double* kyN = sky + (((j + 1) & 3) * kCorrCols + iw) * NZP;
+        const double* kzC = skz + ((j & 1) * kCorrCols + iw) * NZP;
+        const long long col = col2(d, j, i), cb = cidx(d, j, i, 0), fb = fidx(d, j, i, 0);
+        const int topc = f.topc[col], botc = f.botc[col];
+        const double topv = f.topv[col], botv = f.botv[col];
+        const long long exm = col2(d, j, 1), exp_ = col2(d, j, d.nx);
+        const long long eym = col2(d, 1, i), eyp = col2(d, d.ny, i);
+        const int cxm = (i == 1) ? f.xmc[exm] : f.xpc[exp_], cxp = f.xpc[exp_];
+        const double vxm = (i == 1) ? f.xmv[exm] : f.xpv[exp_], vxp = f.xpv[exp_];
+        const int cym = (j == 1) ? f.ymc[eym] : f.ypc[eyp], cyp = f.ypc[eyp];
+        const double vym = (j == 1) ? f.ymv[eym] : f.ypv[eyp], vyp = f.ypv[eyp];
+        // one cell at a time: a cell's loads fill the registers
+#pragma unroll 1
+        for (int e = 0; e < E; ++e) {
+          const int k = k0 + e;
+          if (k >= nz) break;
+          const long long c = cb + k, fz = fb + k;
+          const long long ce = c + d.sx, cw = c - d.sx, cn = c + d.sy, cs = c - d.sy;
+          const long long cu = (k >= 1) ? c - 1 : c, cl = (k + 1 < nz) ? c + 1 : c;
+          const double hpc = hp0[w * NZP + k];
+          const double w0 = wcn[c], ts = f.wcs[c];
+          const int8_t ac = f.act[c];
+          const double botc_ = f.bot[c];
+          // lateral faces: c with its east / north neighbour (stored here),
+          // west / south neighbour with c (evaluated again)
+          const LatFlux vxe{kx0[w * NZP + k], kx0[(w + 1) * NZP + k], f.ksx[c], f.ksx[ce], hpc,
+                            hp0[(w + 1) * NZP + k], w0, wcn[ce], ts, f.wcs[ce], botc_, f.bot[ce],
+                            f.ax[c], f.cosx[c], f.sinx[c], ac, f.act[ce]};
+          const LatFlux vxw{kx0[(w - 1) * NZP + k], kx0[w * NZP + k], f.ksx[cw], f.ksx[c],
+                            hp0[(w - 1) * NZP + k], hpc, wcn[cw], w0, f.wcs[cw], ts, f.bot[cw],
+                            botc_, f.ax[cw], f.cosx[cw], f.sinx[cw], f.act[cw], ac};
+          const LatFlux vyn{kyC[k], kyN[k], f.ksy[c], f.ksy[cn], hpc, hpN[k], w0, wcn[cn], ts,
+                            f.wcs[cn], botc_, f.bot[cn], f.ay[c], f.cosy[c], f.siny[c], ac,
+                            f.act[cn]};
+          const LatFlux vys{kyS[k], kyC[k], f.ksy[cs], f.ksy[c], hpS[k], hpc, wcn[cs], w0,
+                            f.wcs[cs], ts, f.bot[cs], botc_, f.ay[cs], f.cosy[cs], f.siny[cs],
+                            f.act[cs], ac};
+          const double qxp = flux_lat(d, f, vxe, d.idx, false, i == d.nx, cxp, vxp, ce, 1.0, 1.0);
+          const double qxm = flux_lat(d, f, vxw, d.idx, i == 1, false, cxm, vxm, c, 1.0, 1.0);
+          const double qyp = flux_lat(d, f, vyn, d.idy, false, j == d.ny, cyp, vyp, cn, 1.0, 1.0);
+          const double qym = flux_lat(d, f, vys, d.idy, j == 1, false, cym, vym, c, 1.0, 1.0);
+          kx[c] = face_lat(d, Flank{vxe.kca, vxe.ksa, vxe.wa, vxe.wsa, vxe.acta},
+                           Flank{vxe.kcb, vxe.ksb, vxe.wb, vxe.wsb, vxe.actb}, false, i == d.nx,
+                           cxp);
+          qx[c] = qxp;
+          ky[c] = face_lat(d, Flank{vyn.kca, vyn.ksa, vyn.wa, vyn.wsa, vyn.acta},
+                           Flank{vyn.kcb, vyn.ksb, vyn.wb, vyn.wsb, vyn.actb}, false, j == d.ny,
+                           cyp);
+          qy[c] = qyp;
+          if (i == 1) {  // the west boundary face, in the ghost column's slot
+            kx[cw] = face_lat(d, Flank{vxw.kca, vxw.ksa, vxw.wa, vxw.wsa, vxw.acta},
+                              Flank{vxw.kcb, vxw.ksb, vxw.wb, vxw.wsb, vxw.actb}, true, false,
+                              cxm);
+            qx[cw] = qxm;
+          }
+          if (j == 1) {  // the south boundary face, in the ghost row's slot
+            ky[cs] = face_lat(d, Flank{vys.kca, vys.ksa, vys.wa, vys.wsa, vys.acta},
+                              Flank{vys.kcb, vys.ksb, vys.wb, vys.wsb, vys.actb}, true, false,
+                              cym);
+            qy[cs] = qym;
+          }
+          // z faces: above c (stored here) and below c (stored by the cell
+          // below, or here for the bottom face)
+          const double hpu = (k >= 1) ? hp0[w * NZP + k - 1] : hpc;
+          const ZFlank zu{(k >= 1) ? kzC[k - 1] : kzC[k], f.ksz[cu], f.dz[cu],
+                          (k >= 1) ? f.act[cu] : int8_t(0)};
+          const ZFlank zc{kzC[k], f.ksz[c], f.dz[c], ac};
+          kzf[fz] = face_z<false>(d, zu, zc, k, topc, botc, 0.0);
+          const double qzt = flux_zv(d, f, zu, zc, hpu, hpc, k, topc, topv, botc, botv, cu, 1.0, 1.0);
+          qzf[fz] = qzt;
+          double qzb;
+          if (k + 1 < nz) {
+            const ZFlank zl{kzC[k + 1], f.ksz[cl], f.dz[cl], f.act[cl]};
+            qzb = flux_zv(d, f, zc, zl, hpc, hp0[w * NZP + k + 1], k + 1, topc, topv, botc, botv,
+                          c, 1.0, 1.0);
+          } else {
+            const ZFlank none{0.0, 0.0, 0.0, 0};
+            kzf[fz + 1] = face_z<false>(d, zc, none, nz, topc, botc, 0.0);
+            qzb = flux_zv(d, f, zc, none, hpc, 0.0, nz, topc, topv, botc, botv, c, 1.0, 1.0);
+            qzf[fz + 1] = qzb;
+          }
+          double upd = w0;
+          if (ac)
+            upd = theta_update(d, dtg, w0, hpc, hn[c], zc.dz, ts, qxp, qxm, qyp, qym, qzt, qzb,
+                               acc);
+          hp[c] = hpc;
+          wcu[c] = upd;
+          satf[c] = (upd >= ts || hpc > f.aev[c]) ? 1 : 0;
+          if (k == 0) colflag[col] = 0;  // the walk's column flags start clear
+        }
+      }
+      // The next row's closures rewrite this warp's K along z slot, which
+      // other lanes of the warp have just read.
+      __syncwarp();
+    }
+  }
+  const double s = block_reduce(acc, SumOp(), 0.0);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
 // ---------------------------------------------------------------- post-allocation
@@ -2301,6 +2533,25 @@ bool launch_predict(const Device& D, const double* hn, const double* wcn, bool m
                                                 D.gyp, D.gzp, D.rhs, mixed ? D.x : nullptr,
                                                 D.diag32, D.gxp32, D.gyp32, D.gzp32, D.dinv32,
                                                 D.l32);
+  ++D.launches;
+  return true;
+}
+
+// The fused corrector where it applies (groundwater-only domain, nz <= 256);
+// false: the caller launches the separate passes.
+bool launch_correct(const Device& D, const double* hn, const double* wcn) {
+  if (D.f.cpl != nullptr || D.f.baro != nullptr || D.d.nz > 256) return false;
+  const int E = D.d.nz <= 32 ? 1 : D.d.nz <= 64 ? 2 : D.d.nz <= 128 ? 4 : 8;
+  const auto k = E == 1 ? k_correct<1> : E == 2 ? k_correct<2> : E == 4 ? k_correct<4>
+                                                                  : k_correct<8>;
+  const size_t smem = corr_smem_bytes(E);
+  if (raise_smem_limit(reinterpret_cast<const void*>(k), smem) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  k<<<cells_grid(D), kCorrWarps * 32, smem, D.stream>>>(
+      D.d, D.f, D.x, hn, wcn, dtg_slot(D), D.hp, D.kx, D.ky, D.kzf, D.qx, D.qy, D.qzf, D.wcu,
+      D.satf, D.colflag, D.partial + kPSs * D.nblk);
   ++D.launches;
   return true;
 }
