@@ -9,7 +9,7 @@
 // frehg::FatalError (src/core/Types.hpp:53-62), so driver-side error
 // semantics are unchanged.  Fields come back in the ABI shapes (interior
 // cells, k fastest); a driver that keeps the reference's halo-layout views
-// copies them in (INTEGRATION.md shows the wiring).
+// copies them into their interiors.
 #pragma once
 
 #include <array>
