@@ -620,10 +620,45 @@ __host__ __device__ inline size_t pred_smem_bytes(int E) {
          sizeof(double);
 }
 
+// Closures of row jj for warp w's column i (Predictor.cpp:127-232,
+// 445-452): K along x into its slot; with `ky` K along y, with `full` K
+// along z and C(h^n) into the interior column iw's slots.
+template <int E>
+__device__ __forceinline__ void pred_closures(const Dims& d, const Fields& f,
+                                              const double* __restrict__ hn, double* psm, int w,
+                                              int iw, int i, int jj, bool ky, bool full) {
+  constexpr int NZP = 32 * E;
+  double* kxs = psm + ((jj % 3) * kPredWarps + w) * NZP;
+  double* kys = psm + 3 * kPredWarps * NZP + ((jj & 3) * kPredCols + iw) * NZP;
+  double* kzs = psm + (3 * kPredWarps + 4 * kPredCols) * NZP + ((jj & 1) * kPredCols + iw) * NZP;
+  double* chs = psm + (3 * kPredWarps + 6 * kPredCols) * NZP + ((jj & 1) * kPredCols + iw) * NZP;
+  const int k0 = (threadIdx.x & 31) * E, nz = d.nz;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int k = k0 + e;
+    if (k < nz) {
+      const long long c = cidx(d, jj, i, k);
+      const double hc = hn[c];
+      const Soil so = soil_at(f, c);
+      const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
+      const VgParts v = vg_parts(so, hc);
+      const KrParts p = vg_kr_from(v, hc);
+      kxs[k] = vg_k_from(p, ksx);
+      if (ky) kys[k] = vg_k_from(p, ksy);
+      if (full) {
+        kzs[k] = vg_k_from(p, ksz);
+        chs[k] = vg_capacity_from(so, v, hc);
+      }
+    }
+  }
+}
+
 // Two blocks per SM up to 128 cells a column; deeper columns need 147 KB of
 // shared memory a block, one block per SM, with the registers that frees.
+// The kernel body takes the domain's Dims and Fields by value, as the other
+// cell kernels' bodies do.
 template <int E, bool MIXED>
-__global__ void __launch_bounds__(kPredWarps * 32, (E >= 8) ? 1 : 2) k_predict(
+__device__ __forceinline__ void predict_body(
     Dims d, Fields f, const double* __restrict__ hn, const double* __restrict__ wcn,
     const double* __restrict__ dtgp, double* __restrict__ diag, double* __restrict__ gxps,
     double* __restrict__ gyps, double* __restrict__ gzps, double* __restrict__ rhs,
@@ -646,40 +681,12 @@ __global__ void __launch_bounds__(kPredWarps * 32, (E >= 8) ? 1 : 2) k_predict(
   const int nz = d.nz;
   const double dtg = *dtgp;
 
-  // Closures of row jj for this warp's column (Predictor.cpp:127-232,
-  // 445-452): K along x into its slot; for interior warps K along y, and
-  // with `full` K along z and C.
-  auto closures = [&](int jj, bool full) {
-    double* kxs = skx + ((jj % 3) * kPredWarps + w) * NZP;
-    double* kys = sky + ((jj & 3) * kPredCols + iw) * NZP;
-    double* kzs = skz + ((jj & 1) * kPredCols + iw) * NZP;
-    double* chs = sch + ((jj & 1) * kPredCols + iw) * NZP;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int k = k0 + e;
-      if (k < nz) {
-        const long long c = cidx(d, jj, i, k);
-        const double hc = hn[c];
-        const Soil so = soil_at(f, c);
-        const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
-        const VgParts v = vg_parts(so, hc);
-        const KrParts p = vg_kr_from(v, hc);
-        kxs[k] = vg_k_from(p, ksx);
-        if (inner) kys[k] = vg_k_from(p, ksy);
-        if (full) {
-          kzs[k] = vg_k_from(p, ksz);
-          chs[k] = vg_capacity_from(so, v, hc);
-        }
-      }
-    }
-  };
-
   if (has_col) {
-    if (inner) closures(jb - 1, false);  // K along y of row jb - 1
-    closures(jb, inner);
+    if (inner) pred_closures<E>(d, f, hn, psm, w, iw, i, jb - 1, true, false);  // K along y
+    pred_closures<E>(d, f, hn, psm, w, iw, i, jb, inner, inner);
   }
   for (int j = jb; j <= je; ++j) {
-    if (has_col) closures(j + 1, inner);
+    if (has_col) pred_closures<E>(d, f, hn, psm, w, iw, i, j + 1, inner, inner);
     __syncthreads();
     if (inner) {
       const double* kx0 = skx + ((j % 3) * kPredWarps) * NZP;
@@ -1084,6 +1091,18 @@ __global__ void __launch_bounds__(kBlock, 4) k_update_wc(
                        blockIdx.x, gridDim.x);
 }
 
+template <int E, bool MIXED>
+__global__ void __launch_bounds__(kPredWarps * 32, (E >= 8) ? 1 : 2) k_predict(
+    Dims d, Fields f, const double* __restrict__ hn, const double* __restrict__ wcn,
+    const double* __restrict__ dtgp, double* __restrict__ diag, double* __restrict__ gxps,
+    double* __restrict__ gyps, double* __restrict__ gzps, double* __restrict__ rhs,
+    double* __restrict__ xw, float* __restrict__ diag32, float* __restrict__ gxp32,
+    float* __restrict__ gyp32, float* __restrict__ gzp32, float* __restrict__ dinv32,
+    float* __restrict__ l32) {
+  predict_body<E, MIXED>(d, f, hn, wcn, dtgp, diag, gxps, gyps, gzps, rhs, xw, diag32, gxp32,
+                         gyp32, gzp32, dinv32, l32);
+}
+
 // ---------------------------------------------------------------- fused corrector
 // The corrector of a groundwater-only domain (no coupled top, no density
 // coupling; nz <= 32 E) in one pass: the head scatter with its ghosts and
@@ -1110,8 +1129,60 @@ __host__ __device__ inline size_t corr_smem_bytes(int E) {
          32 * E * sizeof(double);
 }
 
+// The ghost cells an item of k_correct stores: its columns [.., ..] (own_i
+// for this warp's column) and rows [jlo, jhi].
+struct CorrOwn {
+  bool own_i;
+  int jlo, jhi;
+};
+
+// Closures of row jj for warp w's column i of k_correct: the predicted head
+// and K along x into their slots; with `ky` K along y, with `full` K along z
+// (interior column iw).  Ghost cells the item owns get their outputs (head,
+// theta^n as theta, the saturation flag, a cleared column flag).
 template <int E>
-__global__ void __launch_bounds__(kCorrWarps * 32, (E >= 8) ? 1 : 2) k_correct(
+__device__ __forceinline__ void corr_closures(const Dims& d, const Fields& f,
+                                              const double* __restrict__ x,
+                                              const double* __restrict__ hn,
+                                              const double* __restrict__ wcn, double* csm, int w,
+                                              int iw, int i, int jj, bool ky, bool full,
+                                              CorrOwn own, double* __restrict__ hp,
+                                              double* __restrict__ wcu, uint8_t* __restrict__ satf,
+                                              int* __restrict__ colflag) {
+  constexpr int NZP = 32 * E;
+  double* kxs = csm + ((jj % 3) * kCorrWarps + w) * NZP;
+  double* hps = csm + 3 * kCorrWarps * NZP + ((jj & 3) * kCorrWarps + w) * NZP;
+  double* kys = csm + 7 * kCorrWarps * NZP + ((jj & 3) * kCorrCols + iw) * NZP;
+  double* kzs = csm + (7 * kCorrWarps + 4 * kCorrCols) * NZP + ((jj & 1) * kCorrCols + iw) * NZP;
+  const bool ghost = jj == 0 || jj == d.ny + 1 || i == 0 || i == d.nx + 1;
+  const bool store = ghost && own.own_i && jj >= own.jlo && jj <= own.jhi;
+  const int k0 = (threadIdx.x & 31) * E, nz = d.nz;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int k = k0 + e;
+    if (k < nz) {
+      const long long c = cidx(d, jj, i, k);
+      const Soil so = soil_at(f, c);
+      const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
+      const double hv = predicted_head(d, f, x, hn, c, jj, i);
+      const KrParts p = vg_kr_parts(so, hv);
+      hps[k] = hv;
+      kxs[k] = vg_k_from(p, ksx);
+      if (ky) kys[k] = vg_k_from(p, ksy);
+      if (full) kzs[k] = vg_k_from(p, ksz);
+      if (store) {
+        const double w0 = wcn[c];
+        hp[c] = hv;
+        wcu[c] = w0;
+        satf[c] = (w0 >= so.ts || hv > so.aev) ? 1 : 0;
+        if (k == 0) colflag[col2(d, jj, i)] = 0;
+      }
+    }
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void correct_body(
     Dims d, Fields f, const double* __restrict__ x, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ dtgp, double* __restrict__ hp,
     double* __restrict__ kx, double* __restrict__ ky, double* __restrict__ kzf,
@@ -1146,47 +1217,18 @@ __global__ void __launch_bounds__(kCorrWarps * 32, (E >= 8) ? 1 : 2) k_correct(
     const int jlo_g = (jb == 1) ? 0 : jb, jhi_g = (je == d.ny) ? d.ny + 1 : je;
     const bool own_i = i >= ilo && i <= ihi_g;
 
-    // Closures of row jj for this warp's column: the predicted head and K
-    // along x into their slots; interior warps also K along y and, with
-    // `full`, K along z.  Ghost cells owned by this item get their outputs.
-    auto closures = [&](int jj, bool full) {
-      double* kxs = skx + ((jj % 3) * kCorrWarps + w) * NZP;
-      double* hps = shp + ((jj & 3) * kCorrWarps + w) * NZP;
-      double* kys = sky + ((jj & 3) * kCorrCols + iw) * NZP;
-      double* kzs = skz + ((jj & 1) * kCorrCols + iw) * NZP;
-      const bool ghost = jj == 0 || jj == d.ny + 1 || i == 0 || i == d.nx + 1;
-      const bool store = ghost && own_i && jj >= jlo_g && jj <= jhi_g;
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const int k = k0 + e;
-        if (k < nz) {
-          const long long c = cidx(d, jj, i, k);
-          const Soil so = soil_at(f, c);
-          const double ksx = f.ksx[c], ksy = f.ksy[c], ksz = f.ksz[c];
-          const double hv = predicted_head(d, f, x, hn, c, jj, i);
-          const KrParts p = vg_kr_parts(so, hv);
-          hps[k] = hv;
-          kxs[k] = vg_k_from(p, ksx);
-          if (inner) kys[k] = vg_k_from(p, ksy);
-          if (full) kzs[k] = vg_k_from(p, ksz);
-          if (store) {
-            const double w0 = wcn[c];
-            hp[c] = hv;
-            wcu[c] = w0;
-            satf[c] = (w0 >= so.ts || hv > so.aev) ? 1 : 0;
-            if (k == 0) colflag[col2(d, jj, i)] = 0;
-          }
-        }
-      }
-    };
-
     __syncthreads();  // the previous item's last row is read before the slots are rewritten
+    const CorrOwn own{own_i, jlo_g, jhi_g};
     if (has_col) {
-      closures(jb - 1, false);
-      closures(jb, inner);
+      corr_closures<E>(d, f, x, hn, wcn, csm, w, iw, i, jb - 1, inner, false, own, hp, wcu, satf,
+                       colflag);
+      corr_closures<E>(d, f, x, hn, wcn, csm, w, iw, i, jb, inner, inner, own, hp, wcu, satf,
+                       colflag);
     }
     for (int j = jb; j <= je; ++j) {
-      if (has_col) closures(j + 1, inner);
+      if (has_col)
+        corr_closures<E>(d, f, x, hn, wcn, csm, w, iw, i, j + 1, inner, inner, own, hp, wcu,
+                         satf, colflag);
       __syncthreads();
       if (inner) {
         const double* kx0 = skx + ((j % 3) * kCorrWarps) * NZP;
@@ -1293,6 +1335,18 @@ __global__ void __launch_bounds__(kCorrWarps * 32, (E >= 8) ? 1 : 2) k_correct(
   }
   const double s = block_reduce(acc, SumOp(), 0.0);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+template <int E>
+__global__ void __launch_bounds__(kCorrWarps * 32, (E >= 8) ? 1 : 2) k_correct(
+    Dims d, Fields f, const double* __restrict__ x, const double* __restrict__ hn,
+    const double* __restrict__ wcn, const double* __restrict__ dtgp, double* __restrict__ hp,
+    double* __restrict__ kx, double* __restrict__ ky, double* __restrict__ kzf,
+    double* __restrict__ qx, double* __restrict__ qy, double* __restrict__ qzf,
+    double* __restrict__ wcu, uint8_t* __restrict__ satf, int* __restrict__ colflag,
+    double* __restrict__ partial) {
+  correct_body<E>(d, f, x, hn, wcn, dtgp, hp, kx, ky, kzf, qx, qy, qzf, wcu, satf, colflag,
+                  partial);
 }
 
 // ---------------------------------------------------------------- post-allocation
