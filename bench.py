@@ -595,6 +595,8 @@ def main():
     stream = torch.cuda.Stream()
     other = "fp64" if args.precision == "mixed" else "mixed"
     res_other = timed_form(args, other, rank, local, dist, stream, 0)
+    # The mixed form's algorithm with FP64 inner iterations: what FP32 buys.
+    res_line = timed_form(args, "fp64_line", rank, local, dist, stream, 0)
     res = timed_form(args, args.precision, rank, local, dist, stream, args.e2e_steps)
     fp64 = res if args.precision == "fp64" else res_other
     mixed = res if args.precision == "mixed" else res_other
@@ -636,7 +638,22 @@ def main():
                   "outer_sweeps_per_step": mixed["outer"] / args.steps,
                   "solve_ms_per_step": mixed["solve_ms"] / args.steps, "roofline": roof_mixed,
                   "latency": mixed["latency"]},
+        "fp64_line": {"value": res_line["value"], "ms_per_step": res_line["ms"] / args.steps,
+                      "inner_iterations_per_step": res_line["iters"] / args.steps,
+                      "outer_sweeps_per_step": res_line["outer"] / args.steps,
+                      "solve_ms_per_step": res_line["solve_ms"] / args.steps,
+                      "solve_alg_bytes_per_cell_inner": 128,
+                      "latency": res_line["latency"]},
         "mixed_over_fp64": mixed["value"] / fp64["value"] if fp64["value"] else None,
+        # the split of mixed / FP64: precision alone (same algorithm, FP64
+        # inner iterations) and the algorithm (line preconditioner + warm
+        # start against point Jacobi from x = 0), for the step and the solve
+        "mixed_over_fp64_line": mixed["value"] / res_line["value"] if res_line["value"] else None,
+        "fp64_line_over_fp64": res_line["value"] / fp64["value"] if fp64["value"] else None,
+        "solve_fp64_line_over_mixed": (res_line["solve_ms"] / mixed["solve_ms"]
+                                       if mixed["solve_ms"] else None),
+        "solve_fp64_over_fp64_line": (fp64["solve_ms"] / res_line["solve_ms"]
+                                      if res_line["solve_ms"] else None),
     }
     if rank != 0:
         if dist:

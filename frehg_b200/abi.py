@@ -23,7 +23,7 @@ FIELD = {
     "rho": 22, "visc": 23, "rho_x": 24, "rho_y": 25, "rho_z": 26, "visc_x": 27, "visc_y": 28,
     "visc_z": 29,
 }
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "fp64_line": 2}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)

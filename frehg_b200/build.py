@@ -12,11 +12,12 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libfrehg_gw.so")
-SOURCES = ["gw_api.cu", "gw_kernels.cu", "gw_cg.cu", "gw_cg_mixed.cu", "gw_batch.cu", "gw_serve.cu",
+SOURCES = ["gw_api.cu", "gw_kernels.cu", "gw_cg.cu", "gw_cg_mixed.cu", "gw_cg_line64.cu",
+           "gw_batch.cu", "gw_serve.cu",
            "gw_couple.cu", "gw_density.cu",
            "gw_setup.cpp"]
 HEADERS = ["gw_device.cuh", "gw_internal.h", "gw_setup.h", "gw_coop.cuh", "gw_handle.h",
-           "gw_linefactor.cuh"]
+           "gw_linefactor.cuh", "gw_linesolve.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -504,6 +504,8 @@ int frehg_gw_batch_create(frehg_gw_handle* const* members, int n,
     if (!members[i]->have_state) return fail(FREHG_GW_ESTATE, "batch: member without state");
     if (members[i]->device != members[0]->device)
       return fail(FREHG_GW_EINVAL, "batch: members on different devices");
+    if (members[i]->precision == FREHG_GW_PRECISION_FP64_LINE)
+      return fail(FREHG_GW_EUNSUPPORTED, "batch: the FP64 line form steps on its own");
     if (members[i]->D.f.cpl)
       return fail(FREHG_GW_EUNSUPPORTED, "batch: a coupled-top member steps on its own");
     if (members[i]->D.win_x)
@@ -554,6 +556,8 @@ int frehg_gw_batch_set_members(frehg_gw_batch* b, frehg_gw_handle* const* member
     if (!members[i]->have_state) return fail(FREHG_GW_ESTATE, "batch: member without state");
     if (members[i]->device != b->device)
       return fail(FREHG_GW_EINVAL, "batch: members on different devices");
+    if (members[i]->precision == FREHG_GW_PRECISION_FP64_LINE)
+      return fail(FREHG_GW_EUNSUPPORTED, "batch: the FP64 line form steps on its own");
     if (members[i]->D.f.cpl)
       return fail(FREHG_GW_EUNSUPPORTED, "batch: a coupled-top member steps on its own");
     if (members[i]->D.win_x)

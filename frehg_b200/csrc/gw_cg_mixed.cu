@@ -40,6 +40,7 @@
 #include "gw_coop.cuh"
 #include "gw_internal.h"
 #include "gw_linefactor.cuh"
+#include "gw_linesolve.cuh"
 
 namespace fgw {
 
@@ -192,153 +193,6 @@ __device__ inline void column_solve(const float* r, const float* __restrict__ di
   for (int k = nz - 2; k >= 0; --k) {
     zk = z[k] * __ldg(dinv + k) - __ldg(l + k) * zk;
     z[k] = zk;
-  }
-}
-
-// Warp-per-column LDL^T solve (nz <= 32 * kMaxE).  Lane `lane` holds the
-// E consecutive cells k = lane * E + e of the column (E a power of two with
-// 32 E >= nz).  With the unit lower bidiagonal factor L (subdiagonal l) and
-// pivots 1/dinv, z = T^-1 r is
-//   y_k = r_k - l_{k-1} y_{k-1}            (k ascending, y_0 = r_0)
-//   z_k = dinv_k y_k - l_k z_{k+1}         (k descending, z_{nz-1} = dinv y)
-// Each step is an affine map of its predecessor.  A lane composes its E maps,
-// a Hillis-Steele scan over the 32 lanes composes the lane maps (inclusive
-// for the forward sweep, suffix for the backward one), and each lane then
-// replays its E steps from its exclusive prefix.  Cells past nz hold the
-// identity map.  FP32 throughout: this is the inner preconditioner, whose
-// rounding the FP64 outer residual absorbs.
-//
-// Every load of a column is issued before any of its stores: the arrays are
-// distinct, but the compiler cannot prove it, and loads placed after a store
-// would wait for it.
-constexpr int kMaxE = 8;
-constexpr unsigned kFull = 0xffffffffu;
-
-__device__ inline void scan_affine_up(float& A, float& B, int lane) {
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const float Ap = __shfl_up_sync(kFull, A, off);
-    const float Bp = __shfl_up_sync(kFull, B, off);
-    if (lane >= off) {
-      B = fmaf(A, Bp, B);
-      A *= Ap;
-    }
-  }
-}
-
-__device__ inline void scan_affine_down(float& C, float& Dv, int lane) {
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const float Cn = __shfl_down_sync(kFull, C, off);
-    const float Dn = __shfl_down_sync(kFull, Dv, off);
-    if (lane + off < 32) {
-      Dv = fmaf(C, Dn, Dv);
-      C *= Cn;
-    }
-  }
-}
-
-// Load / store a lane's E cells of the column starting at cb.  `vec` (nz a
-// multiple of E) makes every lane all-in or all-out, with E-aligned addresses.
-template <int E>
-__device__ inline void ld_col(const float* p, long long cb, int lane, int nz, bool vec,
-                              float (&v)[E]) {
-  const int k0 = lane * E;
-  if (vec) {
-    if (k0 < nz) {
-      const float* q = p + cb + k0;
-      if constexpr (E == 1) {
-        v[0] = q[0];
-      } else if constexpr (E == 2) {
-        const float2 t = *reinterpret_cast<const float2*>(q);
-        v[0] = t.x;
-        v[1] = t.y;
-      } else {
-#pragma unroll
-        for (int e = 0; e < E; e += 4) {
-          const float4 t = *reinterpret_cast<const float4*>(q + e);
-          v[e] = t.x;
-          v[e + 1] = t.y;
-          v[e + 2] = t.z;
-          v[e + 3] = t.w;
-        }
-      }
-    } else {
-#pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = 0.0f;
-    }
-  } else {
-#pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = (k0 + e < nz) ? p[cb + k0 + e] : 0.0f;
-  }
-}
-
-template <int E>
-__device__ inline void st_col(float* p, long long cb, int lane, int nz, bool vec,
-                              const float (&v)[E]) {
-  const int k0 = lane * E;
-  if (vec) {
-    if (k0 < nz) {
-      float* q = p + cb + k0;
-      if constexpr (E == 1) {
-        q[0] = v[0];
-      } else if constexpr (E == 2) {
-        *reinterpret_cast<float2*>(q) = make_float2(v[0], v[1]);
-      } else {
-#pragma unroll
-        for (int e = 0; e < E; e += 4)
-          *reinterpret_cast<float4*>(q + e) = make_float4(v[e], v[e + 1], v[e + 2], v[e + 3]);
-      }
-    }
-  } else {
-#pragma unroll
-    for (int e = 0; e < E; ++e)
-      if (k0 + e < nz) p[cb + k0 + e] = v[e];
-  }
-}
-
-// z = T^-1 r for the column whose factors this lane holds (lk = l_k,
-// di = dinv_k of its E cells).
-template <int E>
-__device__ inline void warp_column_solve(const float (&lk)[E], const float (&di)[E], int lane,
-                                         int nz, const float (&r)[E], float (&z)[E]) {
-  const int k0 = lane * E;
-  const float lprev = __shfl_up_sync(kFull, lk[E - 1], 1);  // l_{k0-1}
-  float a[E];
-  float A = 1.0f, B = 0.0f;
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const int k = k0 + e;
-    a[e] = (k >= nz) ? 1.0f : (k == 0) ? 0.0f : -(e == 0 ? lprev : lk[e - 1]);
-    const float b = (k < nz) ? r[e] : 0.0f;
-    B = fmaf(a[e], B, b);
-    A *= a[e];
-  }
-  scan_affine_up(A, B, lane);
-  float y = __shfl_up_sync(kFull, B, 1);
-  if (lane == 0) y = 0.0f;
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    y = fmaf(a[e], y, (k0 + e < nz) ? r[e] : 0.0f);
-    z[e] = y;
-  }
-  float c[E];
-  float C = 1.0f, Dv = 0.0f;
-#pragma unroll
-  for (int e = E - 1; e >= 0; --e) {
-    const int k = k0 + e;
-    c[e] = (k >= nz) ? 1.0f : (k + 1 < nz) ? -lk[e] : 0.0f;
-    z[e] = (k < nz) ? di[e] * z[e] : 0.0f;
-    Dv = fmaf(c[e], Dv, z[e]);
-    C *= c[e];
-  }
-  scan_affine_down(C, Dv, lane);
-  float zn = __shfl_down_sync(kFull, Dv, 1);
-  if (lane == 31) zn = 0.0f;
-#pragma unroll
-  for (int e = E - 1; e >= 0; --e) {
-    zn = fmaf(c[e], zn, z[e]);
-    z[e] = zn;
   }
 }
 

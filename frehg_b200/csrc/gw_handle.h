@@ -26,7 +26,7 @@ struct frehg_gw_handle {
   bool have_state = false;
   int start_buf = 0;  // ping-pong index of the last step's theta^n
   bool profiling = false;
-  bool fused = true;  // fused phase kernels where they apply (frehg_gw_set_fused)
+  bool fused = false;  // fused phase kernels where they apply (frehg_gw_set_fused)
   cudaEvent_t ev[6] = {};
   double phase_ms[5] = {0, 0, 0, 0, 0};
   // coupled top: the last step's books and the cumulative mode-3 clamp

@@ -116,7 +116,9 @@ struct Device {
   float *dinv32 = nullptr, *l32 = nullptr;  // LDL^T factors of the column blocks
   float *r32 = nullptr, *z32 = nullptr, *d32 = nullptr, *p032 = nullptr, *p132 = nullptr,
         *w32 = nullptr;
-  double* xalt = nullptr;  // FP64 ping-pong partner of x (mixed outer sweeps)
+  double* xalt = nullptr;  // FP64 ping-pong partner of x (mixed / FP64 line outer sweeps)
+  // FP64 line form: the column factors in FP64 and the correction d
+  double *dinv64 = nullptr, *l64 = nullptr, *d64 = nullptr;
   // reductions
   double* partial = nullptr;   // kPSlots x nblk
   double* cgpart = nullptr;    // 4 x cg grid
@@ -176,6 +178,10 @@ cudaError_t launch_line_factor(Device& D);
 cudaError_t launch_cg_mixed(Device& D, double rtol, double atol, int maxit, double outer_rtol,
                             int max_outer);
 int cg64_grid(int sm_count, long long ncell);
+// FP64 line form (nz <= 256): FP64 column factors, then the FP64 line-PCG
+// defect-correction solve (the mixed form's algorithm in FP64).
+cudaError_t launch_line_factor64(Device& D);
+cudaError_t launch_cg_line64(Device& D, double atol, int maxit, double outer_rtol, int max_outer);
 
 // Raises (never lowers) a kernel's opt-in dynamic shared-memory limit to
 // `bytes`.  Only raising keeps every launch recorded earlier (in a captured

@@ -98,4 +98,49 @@ __device__ __forceinline__ void factor_column(int nz, long long cb, const double
   }
 }
 
+// The same factorization for the FP64 line form: FP64 factors (1/d_k, l_k),
+// no casts.
+template <int E>
+__device__ __forceinline__ void factor_column64(int nz, long long cb, const double (&av)[E],
+                                                const double (&ev)[E], double* __restrict__ dinv,
+                                                double* __restrict__ l) {
+  const int lane = threadIdx.x & 31, k0 = lane * E;
+  const double eprev_lane = __shfl_up_sync(0xffffffffu, ev[E - 1], 1);
+  M2 L{1.0, 0.0, 0.0, 1.0};
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int k = k0 + e;
+    if (k < nz) {
+      const double ep = (k == 0) ? 0.0 : (e == 0 ? eprev_lane : ev[e - 1]);
+      L = m2_mul(M2{av[e], -ep * ep, 1.0, 0.0}, L);
+    }
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const M2 q = m2_shfl_up(L, off);
+    if (lane >= off) L = m2_mul(L, q);
+  }
+  M2 X = m2_shfl_up(L, 1);
+  if (lane == 0) X = M2{1.0, 0.0, 0.0, 1.0};
+  double n = X.a, m = X.c;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int k = k0 + e;
+    if (k >= nz) break;
+    const long long c = cb + k;
+    const double ep = (k == 0) ? 0.0 : (e == 0 ? eprev_lane : ev[e - 1]);
+    const double n2 = av[e] * n - ep * ep * m;
+    m = n;
+    n = n2;
+    const double s = fmax(fabs(n), fabs(m));
+    if (s > 0.0 && isfinite(s)) {
+      n /= s;
+      m /= s;
+    }
+    const double dk = n / m;
+    dinv[c] = (dk > 0.0 && isfinite(dk)) ? 1.0 / dk : 1.0 / av[e];
+    l[c] = (k + 1 < nz) ? ev[e] / dk : 0.0;
+  }
+}
+
 }  // namespace fgw

@@ -258,6 +258,7 @@ size_t frehg_gw_device_bytes(const frehg_gw_desc* d) {
   b += r(4 * ncol);                         // column flags
   b += 11 * r(8 * ns);                      // FP64 solver vectors with margins
   if (d->precision == FREHG_GW_PRECISION_MIXED) b += 12 * r(4 * ns) + r(8 * ns);
+  if (d->precision == FREHG_GW_PRECISION_FP64_LINE) b += 4 * r(8 * ns);
   const size_t nblk = std::min<size_t>((n3 + 255) / 256, 512 * 8);
   const size_t cg = std::max<size_t>((n3 + 255) / 256, 512 * 4);
   b += r(8 * fgw::kPSlots * nblk) + r(8 * 4 * cg) + r(sizeof(fgw::StepOut));

@@ -79,7 +79,11 @@ enum { FREHG_GW_IC_MOISTURE = 0, FREHG_GW_IC_HEAD = 1, FREHG_GW_IC_WATER_TABLE =
 /* Arithmetic of the predictor's linear solve. */
 enum {
   FREHG_GW_PRECISION_FP64 = 0, /* FP64 Jacobi-PCG, PETSc KSPCG semantics */
-  FREHG_GW_PRECISION_MIXED = 1 /* FP32 inner PCG inside FP64 defect correction */
+  FREHG_GW_PRECISION_MIXED = 1, /* FP32 inner PCG inside FP64 defect correction */
+  /* The mixed form's algorithm (line-preconditioned CG in defect correction,
+   * started from h^n) with FP64 inner iterations, nz <= 256: the comparison
+   * that isolates what FP32 buys.  Not in batches. */
+  FREHG_GW_PRECISION_FP64_LINE = 2
 };
 
 /* Fields for frehg_gw_get_field. */
@@ -153,8 +157,8 @@ typedef struct frehg_gw_desc {
   double rtol, atol;
   int max_iterations;
   int precision;      /* FREHG_GW_PRECISION_* */
-  double outer_rtol;  /* mixed: ||b - A x|| / ||b|| target of the FP64 outer loop
-                         (0 = 1e-11) */
+  double outer_rtol;  /* mixed / FP64 line: ||b - A x|| / ||b|| target of the FP64
+                         outer loop (0 = 3e-12) */
   int max_outer;      /* mixed: outer-iteration cap */
 } frehg_gw_desc;
 
@@ -255,11 +259,13 @@ int frehg_gw_device(const frehg_gw_handle* h);
 int frehg_gw_set_profiling(frehg_gw_handle* h, int on);
 int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5);
 
-/* Kernel selection (no counterpart in the reference): on (the default), a
- * groundwater-only domain with nz <= 256 runs each phase that has one as a
- * single fused pass (the predictor: closures, faces, rows and the mixed
- * form's column factors); off, every phase runs as its separate passes.  The
- * arithmetic is the same either way. */
+/* Kernel selection (no counterpart in the reference).  The fused predictor
+ * (closures, faces, rows and the mixed form's column factors in one pass) and
+ * fused corrector (head scatter, closures, faces, fluxes, theta update) for
+ * groundwater-only domains with nz <= 256 raised a misaligned-address error
+ * on the B200 whose cause is not yet found, so they are disabled: on = 1
+ * returns FREHG_GW_EUNSUPPORTED, on = 0 (every phase as its separate passes,
+ * the default) succeeds. */
 int frehg_gw_set_fused(frehg_gw_handle* h, int on);
 
 /* The transport window (RichardsSolver::enableTransportWindow,

@@ -10,8 +10,8 @@ of their scale (fluxes on the gravity scale), CG iterations within +-2 and
 the next dt within 1e-9.  The mixed form is compared against the FP64 oracle
 solved tightly (rtol 1e-13) from the GPU's state each step: head within
 1e-8, fields within 1e-6, with the outer target at 1e-12 (on the small
-hydrostatic-side column the default 1e-11 residual leaves the head 1.2e-8
-from the tight solve: the column's conditioning, not the coupling).  The audit terms follow the oracle's (1e-9 / 1e-6
+hydrostatic-side column a residual of 1e-11 left the head 1.2e-8 from the
+tight solve: the column's conditioning, not the coupling).  The audit terms follow the oracle's (1e-9 / 1e-6
 of their scale).  The volume audit of the groundwater-only step does not
 close under density coupling (the theta update conserves r-weighted mass,
 face by face): in the FP64 form the GPU's closure residual must equal the
