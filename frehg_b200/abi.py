@@ -21,7 +21,7 @@ FIELD = {
     "siny": 15, "cosy": 16, "vloss": 17,
     "win_x": 18, "win_y": 19, "win_z": 20, "win_vent": 21,
     "rho": 22, "visc": 23, "rho_x": 24, "rho_y": 25, "rho_z": 26, "visc_x": 27, "visc_y": 28,
-    "visc_z": 29,
+    "visc_z": 29, "h_prev": 30,
 }
 PRECISION = {"fp64": 0, "mixed": 1, "fp64_line": 2}
 

@@ -410,6 +410,7 @@ int frehg_gw_set_bc_values(frehg_gw_handle* h, const double* top, const double* 
 int frehg_gw_init_state(frehg_gw_handle* h, int form, double constant, const double* field) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
   FGW_ON_DEVICE(h);
+  h->have_prev = false;
   if (form < FREHG_GW_IC_MOISTURE || form > FREHG_GW_IC_WATER_TABLE)
     return fail(FREHG_GW_EINVAL, "unknown initial-condition form");
   fgw::Device& D = h->D;
@@ -440,6 +441,7 @@ int frehg_gw_init_state(frehg_gw_handle* h, int form, double constant, const dou
 int frehg_gw_set_state(frehg_gw_handle* h, const double* head, const double* wc) {
   if (!h || !head || !wc) return fail(FREHG_GW_EINVAL, "null argument");
   FGW_ON_DEVICE(h);
+  h->have_prev = false;
   fgw::Device& D = h->D;
   const fgw::Dims& d = D.d;
   std::vector<double> hh(static_cast<size_t>(d.ncell)), ww(static_cast<size_t>(d.ncell));
@@ -472,6 +474,7 @@ int frehg_gw_restore(frehg_gw_handle* h, const double* head, const double* wc,
                      const double* vloss, double dtg) {
   if (!h || !head || !wc) return fail(FREHG_GW_EINVAL, "null argument");
   FGW_ON_DEVICE(h);
+  h->have_prev = false;
   if (!(dtg > 0.0) || !std::isfinite(dtg)) return fail(FREHG_GW_EINVAL, "dtg must be positive");
   const int rc = frehg_gw_set_state(h, head, wc);
   if (rc != FREHG_GW_OK) return rc;
@@ -495,7 +498,7 @@ int frehg_gw_restore(frehg_gw_handle* h, const double* head, const double* wc,
 
 namespace fgw_api {
 
-cudaError_t enqueue_predictor(frehg_gw_handle* h) {
+cudaError_t enqueue_predictor(frehg_gw_handle* h, double dtg) {
   fgw::Device& D = h->D;
   double* hn = D.h[D.cur];
   double* wcn = D.wc[D.cur];
@@ -508,7 +511,13 @@ cudaError_t enqueue_predictor(frehg_gw_handle* h) {
   const bool line64 = h->precision == FREHG_GW_PRECISION_FP64_LINE;
   if (!line64 && h->fused && fgw::launch_predict(D, hn, wcn, mixed)) return cudaGetLastError();
   fgw::launch_closure_pred(D, hn);
-  fgw::launch_assemble(D, hn, wcn, mixed || line64);  // both start from x = h^n
+  // Both warm-started forms begin from h^n, or, when the previous step's
+  // start state h^(n-1) is still in the other state buffer, from the linear
+  // extrapolation of the two to this step's end.
+  const bool extrap = (mixed || line64) && h->extrapolate && h->have_prev && dtg > 0.0 &&
+                      h->prev_dtg > 0.0;
+  fgw::launch_assemble(D, hn, wcn, mixed || line64, extrap ? D.h[1 - D.cur] : nullptr,
+                       extrap ? dtg / h->prev_dtg : 0.0);
   if (mixed) return fgw::launch_line_factor(D);
   if (line64) return fgw::launch_line_factor64(D);
   return cudaGetLastError();
@@ -598,7 +607,7 @@ int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* 
   CUDA_TRY(cudaMemcpyAsync(&D.out->next_dt, &D.out_host->next_dt, sizeof(double),
                            cudaMemcpyHostToDevice, D.stream), "step dtg");
   mark(0);
-  cudaError_t e = fgw_api::enqueue_predictor(h);
+  cudaError_t e = fgw_api::enqueue_predictor(h, dtg);
   if (e != cudaSuccess) return cuda_fail(e, "predictor launch");
   mark(1);
   if (h->precision == FREHG_GW_PRECISION_MIXED) {
@@ -623,7 +632,12 @@ int frehg_gw_step(frehg_gw_handle* h, double t, double dtg, frehg_gw_step_info* 
       h->phase_ms[n] = ms;
     }
   }
-  return fgw_api::finish_step(h, info);
+  const int rc = fgw_api::finish_step(h, info);
+  // The state buffer not holding the new h^n now holds this step's start
+  // state: the next single step may extrapolate from the pair.
+  h->have_prev = rc == FREHG_GW_OK;
+  h->prev_dtg = dtg;
+  return rc;
 }
 
 int frehg_gw_next_dt(frehg_gw_handle* h, double* out) {
@@ -696,6 +710,10 @@ int frehg_gw_get_field(frehg_gw_handle* h, int field, double* out) {
     case FREHG_GW_FIELD_VISC_Y: src = D.vyp; kind = 2; break;
     case FREHG_GW_FIELD_RHO_Z: src = D.rzp; kind = 3; break;
     case FREHG_GW_FIELD_VISC_Z: src = D.vzp; kind = 3; break;
+    case FREHG_GW_FIELD_HEAD_PREV:
+      if (!h->have_prev) return fail(FREHG_GW_ESTATE, "get_field: no previous step start");
+      src = D.h[1 - D.cur];
+      break;
     default: return fail(FREHG_GW_EINVAL, "unknown field");
   }
   if (!src && field >= FREHG_GW_FIELD_RHO) {  // no density coupling: every ratio is 1
@@ -807,6 +825,41 @@ int frehg_gw_set_fused(frehg_gw_handle* h, int on) {
   return FREHG_GW_OK;
 }
 
+int frehg_gw_prev_dt(frehg_gw_handle* h, double* out) {
+  if (!h || !out) return fail(FREHG_GW_EINVAL, "null argument");
+  *out = h->have_prev ? h->prev_dtg : 0.0;
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_restore_prev(frehg_gw_handle* h, const double* head_prev, double prev_dt) {
+  if (!h || !head_prev) return fail(FREHG_GW_EINVAL, "null argument");
+  FGW_ON_DEVICE(h);
+  if (!(prev_dt > 0.0) || !std::isfinite(prev_dt))
+    return fail(FREHG_GW_EINVAL, "restore_prev: prev_dt must be positive");
+  if (!h->have_state) return fail(FREHG_GW_ESTATE, "restore_prev before a state");
+  fgw::Device& D = h->D;
+  const fgw::Dims& d = D.d;
+  // Only the interior heads are read (the extrapolated start of active cells).
+  std::vector<double> full(static_cast<size_t>(d.ncell), 0.0);
+  CUDA_TRY(cudaStreamSynchronize(D.stream), "restore_prev");
+  size_t q = 0;
+  for (int j = 1; j <= d.ny; ++j)
+    for (int i = 1; i <= d.nx; ++i)
+      for (int k = 0; k < d.nz; ++k) full[fgw::cidx(d, j, i, k)] = head_prev[q++];
+  CUDA_TRY(cudaMemcpy(D.h[1 - D.cur], full.data(), full.size() * sizeof(double),
+                      cudaMemcpyHostToDevice), "restore_prev");
+  h->have_prev = true;
+  h->prev_dtg = prev_dt;
+  return FREHG_GW_OK;
+}
+
+int frehg_gw_set_warm_start(frehg_gw_handle* h, int mode) {
+  if (!h) return fail(FREHG_GW_EINVAL, "null handle");
+  if (mode != 0 && mode != 1) return fail(FREHG_GW_EINVAL, "set_warm_start: mode 0 or 1");
+  h->extrapolate = mode == 1;
+  return FREHG_GW_OK;
+}
+
 int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5) {
   if (!h || !ms5) return fail(FREHG_GW_EINVAL, "null argument");
   for (int n = 0; n < 5; ++n) ms5[n] = h->phase_ms[n];
@@ -865,6 +918,7 @@ int frehg_gw_init_state_static(frehg_gw_handle* h, int form, double constant,
                                const double* field) {
   if (!h) return fail(FREHG_GW_EINVAL, "null handle");
   FGW_ON_DEVICE(h);
+  h->have_prev = false;
   if (form < FREHG_GW_IC_MOISTURE || form > FREHG_GW_IC_WATER_TABLE)
     return fail(FREHG_GW_EINVAL, "unknown initial-condition form");
   double* scratch = nullptr;

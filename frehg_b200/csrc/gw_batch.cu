@@ -602,6 +602,7 @@ int frehg_gw_batch_step(frehg_gw_batch* b, frehg_gw_step_info* infos) {
   std::string msg;
   for (size_t i = 0; i < b->m.size(); ++i) {
     const int s = fgw_api::finish_step(b->m[i], infos ? &infos[i] : nullptr);
+    b->m[i]->have_prev = false;  // batched steps start from h^n
     if (s != FREHG_GW_OK && first_bad == FREHG_GW_OK) {
       first_bad = s;
       msg = "batch member " + std::to_string(i) + ": " + frehg_gw_last_error();

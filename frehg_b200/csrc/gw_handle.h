@@ -27,6 +27,12 @@ struct frehg_gw_handle {
   int start_buf = 0;  // ping-pong index of the last step's theta^n
   bool profiling = false;
   bool fused = false;  // fused phase kernels where they apply (frehg_gw_set_fused)
+  // Starting iterate of the mixed / FP64 line solves (frehg_gw_set_warm_start):
+  // extrapolated from the previous step's start state when it is at hand
+  // (have_prev: the last call stepped this handle alone from that state).
+  bool extrapolate = true;
+  bool have_prev = false;
+  double prev_dtg = 0.0;
   cudaEvent_t ev[6] = {};
   double phase_ms[5] = {0, 0, 0, 0, 0};
   // coupled top: the last step's books and the cumulative mode-3 clamp
@@ -73,7 +79,9 @@ int cuda_fail(cudaError_t e, const char* what);
 // The kernels of one step before and after the predictor solve, on the
 // handle's stream; every kernel reads the step's dtg from the device step
 // record.
-cudaError_t enqueue_predictor(frehg_gw_handle* h);
+// dtg: the step's dt, for the extrapolated starting iterate of a single
+// step (0: start from h^n, as the batched steps do).
+cudaError_t enqueue_predictor(frehg_gw_handle* h, double dtg = 0.0);
 void enqueue_corrector(frehg_gw_handle* h);
 // Interprets the step record read back into D.out_host: fills *info (may be
 // null) and, on success, flips the state buffers and takes the next dt.

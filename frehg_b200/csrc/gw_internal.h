@@ -140,8 +140,10 @@ struct Device {
 // ---------------------------------------------------------------- launchers
 void launch_ghosts(const Device& D, double* h, double* wc);
 void launch_closure_pred(const Device& D, const double* h);
-// warm: also write the mixed solve's starting iterate x = h^n (active cells).
-void launch_assemble(const Device& D, const double* hn, const double* wcn, bool warm);
+// warm: also write the mixed / FP64 line solves' starting iterate x (active
+// cells): h^n, or with hprev = h^(n-1) h^n + ratio (h^n - h^(n-1)).
+void launch_assemble(const Device& D, const double* hn, const double* wcn, bool warm,
+                     const double* hprev = nullptr, double ratio = 0.0);
 // The predictor in one fused pass (closures, faces, rows and, mixed, the
 // column factors) where it applies; false: use the separate passes.
 bool launch_predict(const Device& D, const double* hn, const double* wcn, bool mixed);

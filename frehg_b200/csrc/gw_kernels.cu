@@ -482,8 +482,8 @@ __device__ __forceinline__ void assemble_body(
     const double* __restrict__ kzff, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ ch, const double* __restrict__ dtgp,
     double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
-    double* __restrict__ gzps, double* __restrict__ rhs, double* __restrict__ xw, const int bid,
-    const int G) {
+    double* __restrict__ gzps, double* __restrict__ rhs, double* __restrict__ xw,
+    const double* __restrict__ hprev, double ratio, const int bid, const int G) {
   const double dtg = *dtgp;
   for (long long c = bid * static_cast<long long>(blockDim.x) + threadIdx.x; c < d.ncell;
        c += static_cast<long long>(G) * blockDim.x) {
@@ -505,7 +505,10 @@ __device__ __forceinline__ void assemble_body(
     a.kzp = kzff[fz + 1];
     const int8_t ac = f.act[c];
     assemble_gather<CPL, BARO>(d, f, hn, wcn, ch[c], c, j, i, k, a);
-    if (xw) xw[c] = ac ? a.hnc : 0.0;  // the mixed solve's starting iterate
+    // The mixed / FP64 line solves' starting iterate: h^n, or with hprev
+    // (h^(n-1)) its linear extrapolation to the step's end,
+    // h^n + (dt_n / dt_(n-1)) (h^n - h^(n-1)).
+    if (xw) xw[c] = ac ? (hprev ? a.hnc + ratio * (a.hnc - hprev[c]) : a.hnc) : 0.0;
     if (!ac) {
       diag[c] = 1.0;
       gxps[c] = 0.0;
@@ -529,9 +532,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_assemble(
     const double* __restrict__ kzff, const double* __restrict__ hn,
     const double* __restrict__ wcn, const double* __restrict__ ch, const double* __restrict__ dtgp,
     double* __restrict__ diag, double* __restrict__ gxps, double* __restrict__ gyps,
-    double* __restrict__ gzps, double* __restrict__ rhs, double* __restrict__ xw) {
+    double* __restrict__ gzps, double* __restrict__ rhs, double* __restrict__ xw,
+    const double* __restrict__ hprev, double ratio) {
   assemble_body<CPL, BARO>(d, f, kxf, kyf, kzff, hn, wcn, ch, dtgp, diag, gxps, gyps, gzps, rhs,
-                           xw, blockIdx.x, gridDim.x);
+                           xw, hprev, ratio, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- predictor faces
@@ -2420,7 +2424,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_assemble_batch(const StepArgs* ta
   int bid, G;
   load_member(tab, first, n, sa, bid, G);
   assemble_body<false, false>(sa.d, sa.f, sa.kx, sa.ky, sa.kzf, sa.hn, sa.wcn, sa.ch, &sa.dtg, sa.diag, sa.gxp,
-                sa.gyp, sa.gzp, sa.rhs, sa.mixed ? sa.x : nullptr, bid, G);
+                sa.gyp, sa.gzp, sa.rhs, sa.mixed ? sa.x : nullptr, nullptr, 0.0, bid, G);
 }
 
 __global__ void __launch_bounds__(kBlock, 4) k_faces_batch(const StepArgs* tab, const int* first,
@@ -2551,7 +2555,8 @@ void launch_closure_pred(const Device& D, const double* h) {
 }
 
 // The predictor's faces go through D.kx, D.ky, D.kzf (free until k_flux).
-void launch_assemble(const Device& D, const double* hn, const double* wcn, bool warm) {
+void launch_assemble(const Device& D, const double* hn, const double* wcn, bool warm,
+                     const double* hprev, double ratio) {
   const PassK pk{D.kcx, D.kcy, D.kcz, wcn};
   const auto faces = (D.f.cpl != nullptr) ? k_faces<true> : k_faces<false>;
   const bool cpl = D.f.cpl != nullptr, baro = D.f.baro != nullptr;
@@ -2560,7 +2565,8 @@ void launch_assemble(const Device& D, const double* hn, const double* wcn, bool 
   faces<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, pk, D.kx, D.ky, D.kzf);
   assemble<<<cells_grid(D), kBlock, 0, D.stream>>>(D.d, D.f, D.kx, D.ky, D.kzf, hn, wcn, D.ch,
                                                      dtg_slot(D), D.diag, D.gxp, D.gyp, D.gzp,
-                                                     D.rhs, warm ? D.x : nullptr);
+                                                     D.rhs, warm ? D.x : nullptr,
+                                                     warm ? hprev : nullptr, ratio);
   D.launches += 2;
 }
 

@@ -67,6 +67,12 @@ def load_library(path: str = LIB_PATH):
     lib.frehg_gw_phase_times.restype = C.c_int
     lib.frehg_gw_set_fused.argtypes = [H, C.c_int]
     lib.frehg_gw_set_fused.restype = C.c_int
+    lib.frehg_gw_set_warm_start.argtypes = [H, C.c_int]
+    lib.frehg_gw_set_warm_start.restype = C.c_int
+    lib.frehg_gw_prev_dt.argtypes = [H, _dp]
+    lib.frehg_gw_prev_dt.restype = C.c_int
+    lib.frehg_gw_restore_prev.argtypes = [H, _dp, C.c_double]
+    lib.frehg_gw_restore_prev.restype = C.c_int
     lib.frehg_gw_kernel_launches.argtypes = [H]
     lib.frehg_gw_kernel_launches.restype = C.c_longlong
     lib.frehg_gw_attach_coupling.argtypes = [H, C.POINTER(Coupling)]
@@ -185,8 +191,17 @@ class RichardsSolver:
         (``Simulation::checkpointFields3`` and the ``dtg`` scalar,
         driver/Simulation.cpp:707-722, 1211-1216): interior h, wc, the
         cumulative clamp loss, the next dt, and the time reached."""
-        return {"t": self.t, "dtg": self.nextDt(), "h": self.field("h"),
-                "wc": self.field("wc"), "vloss": self.field("vloss")}
+        ck = {"t": self.t, "dtg": self.nextDt(), "h": self.field("h"),
+              "wc": self.field("wc"), "vloss": self.field("vloss")}
+        # The mixed and FP64 line forms start each step from an extrapolation
+        # of the last two start heads: keeping the older one makes a restart
+        # take the same steps bit for bit.
+        prev = C.c_double()
+        _check(self.lib, self.lib.frehg_gw_prev_dt(self.h, C.byref(prev)))
+        if prev.value > 0.0:
+            ck["dtg_prev"] = prev.value
+            ck["h_prev"] = self.field("h_prev")
+        return ck
 
     def restore(self, ck: dict) -> None:
         """``Simulation::restoreFromCheckpoint`` for the groundwater step
@@ -199,20 +214,29 @@ class RichardsSolver:
         _check(self.lib, self.lib.frehg_gw_restore(
             self.h, hh.ctypes.data_as(_dp), ww.ctypes.data_as(_dp),
             None if vv is None else vv.ctypes.data_as(_dp), float(ck["dtg"])))
+        if ck.get("h_prev") is not None and ck.get("dtg_prev"):
+            hp = np.ascontiguousarray(ck["h_prev"], np.float64)
+            _check(self.lib, self.lib.frehg_gw_restore_prev(self.h, hp.ctypes.data_as(_dp),
+                                                            float(ck["dtg_prev"])))
         self.t = float(ck["t"])
 
     def save_checkpoint(self, path: str) -> None:
         """Writes :meth:`checkpoint` to ``path`` (numpy .npz, exact values)."""
         ck = self.checkpoint()
+        extra = {"h_prev": ck["h_prev"], "dtg_prev": ck["dtg_prev"]} if "h_prev" in ck else {}
         np.savez(path, t=ck["t"], dtg=ck["dtg"], h=ck["h"], wc=ck["wc"], vloss=ck["vloss"],
-                 shape=np.array([self.nx, self.ny, self.nz]))
+                 shape=np.array([self.nx, self.ny, self.nz]), **extra)
 
     def load_checkpoint(self, path: str) -> None:
         with np.load(path) as z:
             if tuple(z["shape"]) != (self.nx, self.ny, self.nz):
                 raise FatalError(1, f"checkpoint {path} is for a {tuple(z['shape'])} domain")
-            self.restore({"t": float(z["t"]), "dtg": float(z["dtg"]), "h": z["h"],
-                          "wc": z["wc"], "vloss": z["vloss"]})
+            ck = {"t": float(z["t"]), "dtg": float(z["dtg"]), "h": z["h"], "wc": z["wc"],
+                  "vloss": z["vloss"]}
+            if "h_prev" in z.files:
+                ck["h_prev"] = z["h_prev"]
+                ck["dtg_prev"] = float(z["dtg_prev"])
+            self.restore(ck)
 
     def setState(self, head: np.ndarray, wc: np.ndarray) -> None:
         """Restart read + ``refreshDerivedState``."""
@@ -273,6 +297,11 @@ class RichardsSolver:
     def setFused(self, on: bool = True) -> None:
         """Fused phase kernels (default) or every phase as separate passes."""
         _check(self.lib, self.lib.frehg_gw_set_fused(self.h, int(bool(on))))
+
+    def setWarmStart(self, extrapolate: bool = True) -> None:
+        """Mixed / FP64 line solves: start from the extrapolated head (default)
+        or from h^n."""
+        _check(self.lib, self.lib.frehg_gw_set_warm_start(self.h, int(bool(extrapolate))))
 
     def phaseTimes(self) -> dict:
         """Device ms per phase of the last step (profiling on)."""

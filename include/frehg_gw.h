@@ -121,7 +121,11 @@ enum {
   FREHG_GW_FIELD_VISC_X = 27,   /* r_visc face means, like QX */
   FREHG_GW_FIELD_VISC_Y = 28,   /* like QY */
   FREHG_GW_FIELD_VISC_Z = 29,   /* like QZ */
-  FREHG_GW_FIELD_COUNT = 30
+  /* The last step's start head h^(n-1), like HEAD: with the next dt it is
+   * the state the mixed / FP64 line forms' extrapolated start needs
+   * (frehg_gw_set_warm_start); ESTATE when the handle has none. */
+  FREHG_GW_FIELD_HEAD_PREV = 30,
+  FREHG_GW_FIELD_COUNT = 31
 };
 
 /* Static description of one domain.  Host pointers; the library copies what
@@ -267,6 +271,26 @@ int frehg_gw_phase_times(frehg_gw_handle* h, double* ms5);
  * returns FREHG_GW_EUNSUPPORTED, on = 0 (every phase as its separate passes,
  * the default) succeeds. */
 int frehg_gw_set_fused(frehg_gw_handle* h, int on);
+
+/* Starting iterate of the mixed and FP64 line solves (no counterpart in the
+ * reference, whose KSP starts from 0): mode 1 (the default) starts a step
+ * from the linear extrapolation of the last two step-start heads,
+ * h^n + (dt_n / dt_(n-1)) (h^n - h^(n-1)), when the handle's previous call was
+ * a step of its own from h^(n-1) (after init_state, set_state, restore or a
+ * batched step it starts from h^n); mode 0 always starts from h^n.  The
+ * solution's accuracy is set by the outer residual target either way; the
+ * start changes the iteration count.  The FP64 Jacobi form keeps PETSc's
+ * x0 = 0. */
+int frehg_gw_set_warm_start(frehg_gw_handle* h, int mode);
+
+/* The extrapolated start's history, for checkpoints that must restart bit
+ * for bit (no counterpart in the reference, whose start is x0 = 0):
+ * frehg_gw_prev_dt gives the last step's dt (0 when the handle has no
+ * history), FREHG_GW_FIELD_HEAD_PREV its start head; after frehg_gw_restore,
+ * frehg_gw_restore_prev(h, head_prev, prev_dt) puts both back (head_prev in
+ * the HEAD shape). */
+int frehg_gw_prev_dt(frehg_gw_handle* h, double* out);
+int frehg_gw_restore_prev(frehg_gw_handle* h, const double* head_prev, double prev_dt);
 
 /* The transport window (RichardsSolver::enableTransportWindow,
  * resetTransportWindow, windowVolumeX/Y/Z, windowVentVolume,
