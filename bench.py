@@ -13,7 +13,9 @@ step's own controller from dt0 = 60 s.
 At N = 1 the line also carries, each measured outside the timed region:
 ``latency`` (p50 / p99 of the per-step solve and step device times),
 ``mixed_error`` (the mixed form against the tight FP64 form over a 10-step
-trajectory: head, flux, storage, audit, iteration counts), ``serve`` (a
+trajectory: head, flux, storage, audit, iteration counts, cells whose
+theta took the other post-allocation branch; beside it the FP64 form at its
+configured rtol against the same tight solve), ``serve`` (a
 short Poisson stream through the serving loop: p50 / p99 request latency,
 cell-steps/s), ``ensemble`` (a 64-member batch, both forms, against stepping
 the members one by one) and ``cpu_baseline`` (the reference's step on
@@ -311,24 +313,42 @@ def latency_summary(solve_ms, step_ms) -> dict:
 def mixed_error(size: str, steps: int, stream) -> dict:
     """The mixed form against the FP64 form solved tightly (CG rtol 1e-13),
     both on this GPU from the slab's initial state, on the FP64 form's dt
-    sequence, never re-synced (``frehg_b200.accuracy``)."""
+    sequence, never re-synced (``frehg_b200.accuracy``).  Beside it, the
+    same comparison for the FP64 form at its configured rtol (the
+    reference's own solve, the one the reference ships): the spread the
+    reference's tolerance itself allows on this trajectory."""
+    import copy
+
     from frehg_b200 import accuracy, workloads
     from frehg_b200.gw import RichardsSolver
 
     nx, ny, nz = (int(v) for v in size.split(","))
     cfg = workloads.hillslope(nx, ny, nz)
-    m = RichardsSolver(accuracy.mixed(cfg), stream=stream.cuda_stream)
+    own = copy.deepcopy(cfg)
+    own.solver.precision = "fp64"
+    forms = {"mixed": RichardsSolver(accuracy.mixed(cfg), stream=stream.cuda_stream),
+             "fp64": RichardsSolver(own, stream=stream.cuda_stream)}
     ref = RichardsSolver(accuracy.tight_fp64(cfg), stream=stream.cuda_stream)
     try:
-        s = accuracy.trajectory(m, ref, steps, cfg.domain.dx, cfg.domain.dy)
+        res = accuracy.trajectories(forms, ref, steps, cfg.domain.dx, cfg.domain.dy)
     finally:
-        m.close()
+        for m in forms.values():
+            m.close()
         ref.close()
+    s = res["mixed"]
     per = s.pop("per_step")
     s["head_per_step"] = [p["head"] for p in per]
+    s["theta_cells_per_step"] = [p["theta_cells"] for p in per]
+    env = res["fp64"]
+    env.pop("per_step")
+    s["fp64_rtol_envelope"] = {
+        "rtol": cfg.solver.rtol,
+        **{k: env[k] for k in ("head", "flux", "storage", "storage_unflipped", "theta_cells",
+                               "audit", "inner_iterations_per_step")}}
     s["reference"] = "FP64 form, Jacobi CG to rtol 1e-13, same dt sequence, no re-sync"
     s["scales"] = {"head": "max(max|h|, 1 m)", "flux": "K A of the face direction",
-                   "storage": "owned volume", "audit": "owned volume"}
+                   "storage": "owned volume", "audit": "owned volume",
+                   "theta_cells": "cells with |theta - theta_ref| > 1e-6"}
     return s
 
 

@@ -13,6 +13,11 @@ below are those of a run, not of one step.  Per step it records:
   Darcy flux near equilibrium cancels to the solve's residual, so it has
   no scale of its own);
 * storage: the owned volume's relative difference, and theta's L-inf;
+* theta_cells: how many cells' theta differs by more than 1e-6, and
+  storage_unflipped, the relative volume difference over the other cells
+  (a cell at theta_s whose net flux cancels to the solve's residual stays
+  saturated or drains by the sign of that residual, a difference of order
+  theta_s - theta_r in that cell that no tolerance on the solve removes);
 * the mixed form's own mass audit, |dV - (in - ss + realloc - vloss)| / V;
 * iterations: the mixed form's inner and outer counts, the FP64 form's CG
   count.
@@ -75,34 +80,57 @@ def trajectory(m, ref, steps: int, dx: float, dy: float, t0: float = 0.0) -> dic
     (its step record carries the iteration counts and the audit terms);
     ``ref`` anything with ``step(t, dtg)``, ``next_dt()``, ``field(name)``,
     ``owned_volume()`` and an ``info`` dict or step record."""
+    return trajectories({"m": m}, ref, steps, dx, dy, t0)["m"]
+
+
+def trajectories(forms: dict, ref, steps: int, dx: float, dy: float, t0: float = 0.0) -> dict:
+    """:func:`trajectory` for several solvers at once (name -> solver), all
+    on ``ref``'s dt sequence; returns name -> summary.  Besides the errors,
+    each step counts the cells whose theta differs from ``ref``'s by more
+    than 1e-6 (``theta_cells``): the branches of the post-allocation (a
+    cell at theta_s stays saturated or drains to theta(h) by the sign of its
+    net inflow) turn a residual-sized difference in a cell whose net flux
+    cancels into a difference of order theta_s - theta_r in that one cell,
+    and ``storage`` then carries that cell's volume.  ``storage_unflipped``
+    is the relative volume difference over the other cells."""
     t = t0
-    prev_m = m.owned_volume()
-    per_step = []
+    prev = {n: m.owned_volume() for n, m in forms.items()}
+    cell_volume = dx * dy * next(iter(forms.values())).field("dz3d")
+    per_step = {n: [] for n in forms}
     for _ in range(steps):
         dtg = ref.next_dt()
         t += dtg
         info_ref = ref.step(t, dtg)
-        info = m.step(t, dtg)
         if info_ref is None:
             info_ref = getattr(ref, "info", {})
-        e = step_errors(m, ref, dx, dy)
-        v_m, v_ref = m.owned_volume(), ref.owned_volume()
-        e["storage"] = abs(v_m - v_ref) / max(abs(v_ref), 1e-300)
-        resid = (v_m - prev_m) - (info["boundary_in"] - info["ss_storage"] +
-                                  info["realloc_adjust"] - info["vloss"])
-        e["audit"] = abs(resid) / max(v_m, 1.0)
-        prev_m = v_m
-        e["inner_iterations"] = int(info["cg_iterations"])
-        e["outer_iterations"] = int(info["outer_iterations"])
-        e["fp64_iterations"] = int(info_ref["cg_iterations"])
-        e["status"] = int(info["status"])
-        e["dtg"] = dtg
-        per_step.append(e)
-    return summarize(per_step)
+        wc_ref = ref.field("wc")
+        v_ref = ref.owned_volume()
+        for n, m in forms.items():
+            info = m.step(t, dtg)
+            e = step_errors(m, ref, dx, dy)
+            dwc = m.field("wc") - wc_ref
+            kept = np.abs(dwc) <= 1e-6
+            e["theta_cells"] = int(dwc.size - np.count_nonzero(kept))
+            v_m = m.owned_volume()
+            e["storage"] = abs(v_m - v_ref) / max(abs(v_ref), 1e-300)
+            e["storage_unflipped"] = (abs(float(np.sum(dwc[kept] * cell_volume[kept]))) /
+                                      max(abs(v_ref), 1e-300))
+            resid = (v_m - prev[n]) - (info["boundary_in"] - info["ss_storage"] +
+                                       info["realloc_adjust"] - info["vloss"])
+            e["audit"] = abs(resid) / max(v_m, 1.0)
+            prev[n] = v_m
+            e["inner_iterations"] = int(info["cg_iterations"])
+            e["outer_iterations"] = int(info["outer_iterations"])
+            e["fp64_iterations"] = int(info_ref["cg_iterations"])
+            e["status"] = int(info["status"])
+            e["dtg"] = dtg
+            per_step[n].append(e)
+    return {n: summarize(p) for n, p in per_step.items()}
 
 
 def summarize(per_step: list) -> dict:
-    keys = ("head", "theta", "qx", "qy", "qz", "flux", "storage", "audit")
+    keys = ("head", "theta", "qx", "qy", "qz", "flux", "storage", "storage_unflipped", "audit",
+            "theta_cells")
     s = {k: max(p[k] for p in per_step) for k in keys}
     n = len(per_step)
     s["steps"] = n

@@ -38,6 +38,16 @@ AUDIT_TOL = 1e-12
 # measured errors sit orders of magnitude below these.
 FLUX_TOL = 1e-6
 STORAGE_TOL = 1e-10
+# Cells whose theta may take the other post-allocation branch: a cell at
+# theta_s whose net flux cancels to the solve's residual stays saturated or
+# drains to theta(h) by that residual's sign, so any two solves that differ
+# by a residual can part there (one cell in ten full-slab steps measured;
+# the reference's own FP64 solve at its configured rtol parts in ~38000).
+# The volume bar applies to the other cells.
+FLIP_MAX = 4
+# The mixed form's errors against the tight solve, as a fraction of those of
+# the reference's own FP64 solve at its configured rtol.
+ENVELOPE_FRAC = 1e-2
 
 
 def rel_linf(a, b):
@@ -115,7 +125,8 @@ def check_trajectory(s, name):
     assert s["head"] <= H_TOL, s["head"]
     assert s["audit"] <= AUDIT_TOL, s["audit"]
     assert s["flux"] <= FLUX_TOL, s["flux"]
-    assert s["storage"] <= STORAGE_TOL, s["storage"]
+    assert s["theta_cells"] <= FLIP_MAX, s["theta_cells"]
+    assert s["storage_unflipped"] <= STORAGE_TOL, s["storage_unflipped"]
 
 
 def test_mixed_trajectory_slab_crop_vs_oracle():
@@ -134,17 +145,24 @@ def test_mixed_trajectory_slab_crop_vs_oracle():
 
 def test_mixed_trajectory_full_slab_vs_fp64():
     # The benchmark's 512x512x128 slab, 10 steps, the mixed form against the
-    # FP64 GPU form solved tightly (both on one device, ~29 GB), never
-    # re-synced.
+    # FP64 GPU form solved tightly, never re-synced; beside it the FP64 form
+    # at its configured rtol against the same tight solve (three solvers on
+    # one device, ~45 GB).
     cfg = workloads.hillslope(512, 512, 128)
-    m = RichardsSolver(accuracy.mixed(cfg))
+    own = copy.deepcopy(cfg)
+    own.solver.precision = "fp64"
+    forms = {"mixed": RichardsSolver(accuracy.mixed(cfg)), "fp64": RichardsSolver(own)}
     ref = RichardsSolver(accuracy.tight_fp64(cfg))
     try:
-        s = accuracy.trajectory(m, ref, 10, cfg.domain.dx, cfg.domain.dy)
+        res = accuracy.trajectories(forms, ref, 10, cfg.domain.dx, cfg.domain.dy)
     finally:
-        m.close()
+        for m in forms.values():
+            m.close()
         ref.close()
+    s, env = res["mixed"], res["fp64"]
     check_trajectory(s, "slab_512x512x128_vs_fp64")
+    for k in ("head", "flux", "storage", "theta_cells"):
+        assert s[k] <= ENVELOPE_FRAC * env[k], (k, s[k], env[k])
 
 
 @pytest.mark.parametrize("name", ["head_top", "gravity_bottom", "side_flux", "mixed_box",
