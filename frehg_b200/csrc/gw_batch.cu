@@ -9,9 +9,11 @@
 //          single-domain block count
 
 //   2.     the predictor solves of all members in one cooperative launch per
-//          kernel class (FP64 / mixed, column layout), each member on its own
-//          block range with its own CG state, reductions and barrier; a
-//          member's blocks leave as soon as its solve has converged
+//          kernel class (FP64 / mixed, column layout) of at most the device's
+//          co-resident blocks, each member on its own block count with its
+//          own CG state, reductions and barrier; the blocks take the members'
+//          block slots from a queue, so the blocks of a member whose solve has
+//          converged go straight on to the next waiting member's slots
 //   3.     corrector, post-allocation, clamp, audit and controller of all
 //          members, one launch per phase, and one read-back of all step
 //          records; one synchronisation for the whole batch
@@ -49,7 +51,8 @@ namespace fgw {
 
 namespace {
 
-__global__ void k_zero_states(CgState** st, int n) {
+__global__ void k_zero_states(CgState** st, int n, int* queue) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *queue = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     CgState* s = st[i];
     s->dp = 0.0;
@@ -97,12 +100,13 @@ int solve_max_blocks(const Device& D, const SolveClass& c) {
 
 size_t solve_group_bytes(const SolveClass& c, int n) {
   auto r = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
-  return r(args_bytes(c) * n) + r(sizeof(int) * (n + 1)) + r(sizeof(CgState*) * n);
+  return r(args_bytes(c) * n) + r(sizeof(int) * (n + 1)) + r(sizeof(CgState*) * n) +
+         r(sizeof(int));
 }
 
 cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
                               const std::vector<int>& nb, const std::vector<SolveParams>& p,
-                              void* mem) {
+                              int max_grid, void* mem) {
   g.cls = c;
   g.n = static_cast<int>(ds.size());
   const size_t ab = args_bytes(c);
@@ -117,12 +121,15 @@ cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vec
     st[i] = &ds[i]->out->cg;
     if (c.kind == 1) g.smem = std::max(g.smem, mixed_batch_smem(*ds[i], c.variant));
   }
-  g.grid = first.back();
+  g.slots = first.back();
+  g.grid = std::min(g.slots, max_grid);
   auto r = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   char* base = static_cast<char*>(mem);
   g.tab = base;
   g.first = reinterpret_cast<int*>(base + r(tab.size()));
   g.states = reinterpret_cast<CgState**>(base + r(tab.size()) + r(first.size() * sizeof(int)));
+  g.queue = reinterpret_cast<int*>(base + r(tab.size()) + r(first.size() * sizeof(int)) +
+                                   r(st.size() * sizeof(CgState*)));
   cudaError_t e = cudaMemcpy(g.tab, tab.data(), tab.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(g.first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice);
@@ -134,11 +141,12 @@ cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vec
 }
 
 cudaError_t solve_group_launch(const SolveGroup& g, cudaStream_t s) {
-  k_zero_states<<<(g.n + 255) / 256, 256, 0, s>>>(g.states, g.n);
+  k_zero_states<<<(g.n + 255) / 256, 256, 0, s>>>(g.states, g.n, g.queue);
   void* tab = g.tab;
   int* first = g.first;
   int n = g.n;
-  void* args[] = {&tab, &first, &n};
+  int* queue = g.queue;
+  void* args[] = {&tab, &first, &n, &queue};
   return cudaLaunchCooperativeKernel(batch_kernel(g.cls), dim3(g.grid), dim3(coop::kCgBlock), args,
                                      g.smem, s);
 }
@@ -198,10 +206,12 @@ int build_groups(frehg_gw_batch* b) {
     b->nb[i] = static_cast<int>(std::max(1LL, std::min<long long>(
                                                   want, fgw::solve_max_blocks(h->D, cls[i]))));
   }
-  // Members of one class share a launch while their blocks fit the device
-  // co-resident; a class that needs more takes several launches in turn.
+  // The members of one class share one launch of at most the device's
+  // co-resident blocks; they queue for those blocks, largest block count
+  // first (the longest solves start first, the small ones fill the tail).
   struct Spec {
     fgw::SolveClass c;
+    int cap = 0;
     std::vector<fgw::Device*> ds;
     std::vector<int> nbs;
     std::vector<fgw::SolveParams> ps;
@@ -218,23 +228,21 @@ int build_groups(frehg_gw_batch* b) {
     const int per_sm = fgw::solve_blocks_per_sm(c, smem);
     if (per_sm < 1) return fail(FREHG_GW_ECUDA, "batch: solve kernel cannot be resident");
     const int cap = per_sm * b->m[i]->D.sm_count;
-    Spec cur{c, {}, {}, {}};
-    int used = 0;
+    Spec cur{c, cap, {}, {}, {}};
+    std::vector<int> order;
     for (int j = i; j < n; ++j) {
       if (done[j] || !(cls[j] == c)) continue;
-      const int take = std::min(b->nb[j], cap);
-      b->nb[j] = take;
-      if (used + take > cap) {
-        specs.push_back(cur);
-        cur = Spec{c, {}, {}, {}};
-        used = 0;
-      }
+      b->nb[j] = std::min(b->nb[j], cap);
+      order.push_back(j);
+      done[j] = true;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int u, int v) { return b->nb[u] > b->nb[v]; });
+    for (const int j : order) {
       frehg_gw_handle* h = b->m[j];
       cur.ds.push_back(&h->D);
-      cur.nbs.push_back(take);
+      cur.nbs.push_back(b->nb[j]);
       cur.ps.push_back(fgw::SolveParams{h->rtol, h->atol, h->outer_rtol, h->maxit, h->max_outer});
-      used += take;
-      done[j] = true;
     }
     if (!cur.ds.empty()) specs.push_back(cur);
   }
@@ -253,7 +261,7 @@ int build_groups(frehg_gw_batch* b) {
   size_t off = 0;
   for (const auto& sp : specs) {
     fgw::SolveGroup g;
-    const cudaError_t e = fgw::solve_group_build(g, sp.c, sp.ds, sp.nbs, sp.ps,
+    const cudaError_t e = fgw::solve_group_build(g, sp.c, sp.ds, sp.nbs, sp.ps, sp.cap,
                                                  static_cast<char*>(b->group_mem) + off);
     if (e != cudaSuccess) return cuda_fail(e, "batch: solve group");
     off += fgw::solve_group_bytes(sp.c, static_cast<int>(sp.ds.size()));

@@ -174,20 +174,30 @@ __global__ void __launch_bounds__(kCgBlock, 2) k_cg64(Cg64Args a) {
   cg64_body(a, blockIdx.x, gridDim.x);
 }
 
-// One cooperative launch over several domains: instance i owns blocks
-// [first[i], first[i+1]) and runs its own solve on them.
+// One cooperative launch over several domains: instance i owns block slots
+// [first[i], first[i+1]) and runs its own solve on them; each block takes the
+// next slot from `queue` (zeroed before the launch) until all are handed out,
+// so a block whose instance has converged goes on to a waiting instance.  The
+// slot, not the block, fixes the block's share of its instance's cells.
 __global__ void __launch_bounds__(kCgBlock, 3)
-    k_cg64_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n) {
+    k_cg64_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n, int* queue) {
   __shared__ Cg64Args sa;
-  __shared__ int sb, sg;
-  if (threadIdx.x == 0) {
-    const int i = instance_of(first, n, blockIdx.x);
-    sa = tab[i];
-    sb = blockIdx.x - first[i];
-    sg = first[i + 1] - first[i];
+  __shared__ int sb, sg, slot;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      slot = atomicAdd(queue, 1);
+      if (slot < first[n]) {
+        const int i = instance_of(first, n, slot);
+        sa = tab[i];
+        sb = slot - first[i];
+        sg = first[i + 1] - first[i];
+      }
+    }
+    __syncthreads();
+    if (slot >= first[n]) break;
+    cg64_body(sa, sb, sg);
+    __syncthreads();  // every thread is done with sa before the next slot's
   }
-  __syncthreads();
-  cg64_body(sa, sb, sg);
 }
 
 
@@ -352,20 +362,30 @@ __global__ void __launch_bounds__(kCgBlock, 2) k_cg64v(Cg64Args a) {
   cg64v_body(a, blockIdx.x, gridDim.x);
 }
 
-// One cooperative launch over several domains: instance i owns blocks
-// [first[i], first[i+1]) and runs its own solve on them.
+// One cooperative launch over several domains: instance i owns block slots
+// [first[i], first[i+1]) and runs its own solve on them; each block takes the
+// next slot from `queue` (zeroed before the launch) until all are handed out,
+// so a block whose instance has converged goes on to a waiting instance.  The
+// slot, not the block, fixes the block's share of its instance's cells.
 __global__ void __launch_bounds__(kCgBlock, 3)
-    k_cg64v_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n) {
+    k_cg64v_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n, int* queue) {
   __shared__ Cg64Args sa;
-  __shared__ int sb, sg;
-  if (threadIdx.x == 0) {
-    const int i = instance_of(first, n, blockIdx.x);
-    sa = tab[i];
-    sb = blockIdx.x - first[i];
-    sg = first[i + 1] - first[i];
+  __shared__ int sb, sg, slot;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      slot = atomicAdd(queue, 1);
+      if (slot < first[n]) {
+        const int i = instance_of(first, n, slot);
+        sa = tab[i];
+        sb = slot - first[i];
+        sg = first[i + 1] - first[i];
+      }
+    }
+    __syncthreads();
+    if (slot >= first[n]) break;
+    cg64v_body(sa, sb, sg);
+    __syncthreads();  // every thread is done with sa before the next slot's
   }
-  __syncthreads();
-  cg64v_body(sa, sb, sg);
 }
 
 }  // namespace

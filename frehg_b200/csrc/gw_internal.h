@@ -267,19 +267,25 @@ int solve_max_blocks(const Device& D, const SolveClass& c);
 struct SolveGroup {
   SolveClass cls{0, 0};
   int n = 0, grid = 0;
+  int slots = 0;                 // the members' blocks in total (first[n])
   size_t smem = 0;
   void* tab = nullptr;           // device table of per-member kernel arguments
   int* first = nullptr;          // device block offsets, n + 1
   CgState** states = nullptr;    // device array of the members' CG states
+  int* queue = nullptr;          // device counter of the slots handed out
 };
 // Device bytes a group of n members of class c needs for its tables.
 size_t solve_group_bytes(const SolveClass& c, int n);
 // Builds a group over `ds` with `nb[i]` blocks each (all of class `c`), its
 // tables placed in `mem` (solve_group_bytes of device memory the caller owns).
+// The launch takes min(sum nb, max_grid) co-resident blocks (max_grid at
+// least every nb[i]); each block takes the members' block slots from a queue
+// in table order, so a member's slots go out together and the blocks of a
+// converged member go on to the next member's.
 cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
                               const std::vector<int>& nb, const std::vector<SolveParams>& p,
-                              void* mem);
-// Zeroes the members' CG states and launches the group on `s`.
+                              int max_grid, void* mem);
+// Zeroes the members' CG states and the slot queue and launches the group on `s`.
 cudaError_t solve_group_launch(const SolveGroup& g, cudaStream_t s);
 
 // Per-kind pieces of the batched solves (gw_cg.cu, gw_cg_mixed.cu).

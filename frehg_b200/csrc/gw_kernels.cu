@@ -1794,7 +1794,7 @@ __device__ inline void walk_take(double& dv, int m, double* rs, double* ws, cons
                                  double* qs, unsigned* rbits, int face, bool plus, double idtg,
                                  double* pc, int from) {
   const double take = (rs[m] > dv) ? dv : rs[m];
-  ws[m] += take * ivs[m];
+  ws[m] = __fma_rn(take, ivs[m], ws[m]);
   rs[m] -= take;
   // The rate is rounded on its own (no fused multiply-add), so every kernel
   // that inlines this walk -- with or without the path record that reuses
@@ -1866,6 +1866,116 @@ __device__ inline void walk_cell(const Dims& d, int kk, double upv, double dnv, 
   }
 }
 
+// Stages flagged column `base` for the walk: room, theta and the face fluxes
+// into shared memory and the room bits; with `all` also the reciprocal cell
+// volumes and the inactive bits (a restage keeps those).
+__device__ inline void walk_stage(const Dims& d, const Fields& f, long long base, long long fb,
+                                  int nz, int lane, const double* __restrict__ room,
+                                  const double* wc, const double* qzf, double* rs, double* ws,
+                                  double* ivs, double* qs, unsigned* rbits, unsigned* ibits,
+                                  bool all) {
+  for (int k0 = 0; k0 < nz; k0 += 32) {
+    const int k = k0 + lane;
+    double r = 0.0;
+    bool inact = false;
+    if (k < nz) {
+      r = room[base + k];
+      rs[k] = r;
+      ws[k] = wc[base + k];
+      if (all) ivs[k] = 1.0 / (d.az * f.dz[base + k]);
+      inact = !f.act[base + k];
+    }
+    const unsigned rb = __ballot_sync(0xffffffffu, r > 0.0);
+    const unsigned ib = __ballot_sync(0xffffffffu, inact);
+    if (lane == 0) {
+      rbits[k0 >> 5] = rb;
+      if (all) ibits[k0 >> 5] = ib;
+    }
+  }
+  for (int k = lane; k <= nz; k += 32) qs[k] = qzf[fb + k];
+  __syncwarp();
+}
+
+// The walk of a staged column in the common case, where no deposit changes
+// where a later one goes: every surplus cell's upward send finds a cell with
+// room between it and the first inactive cell above it, and every deposit
+// leaves its cell some room (rs > dv before the deposit), so the room bits
+// never change.  Each lane resolves the targets of its own cells from the
+// bits (the nearest cell with room above within the active run; the nearest
+// below, or none: lost), and lane 0 applies the deposits in the general
+// walk's order -- cells ascending, each one's upward send before its
+// downward one -- with walk_take's arithmetic, so the result is the general
+// walk's bit for bit.  Returns 0 when the column is walked; 2 when a send
+// fell outside the case (no target above, or a deposit that would use up
+// its cell's room): the shared column is then partly updated and `lost` is
+// restored, the caller restages the column and runs the general walk.
+__device__ inline int walk_fast(const Fields& f, long long base, int nz, int lane, double* rs,
+                                double* ws, const double* ivs, double* qs, const unsigned* rbits,
+                                const unsigned* ibits, const double* __restrict__ sup,
+                                const double* __restrict__ sdn, double idtg, double& lost) {
+  const double lost0 = lost;
+  for (int k0 = 0; k0 < nz; k0 += 32) {
+    const int k = k0 + lane;
+    double su = 0.0, sd = 0.0;
+    int mu = -1, md = -1;
+    bool any = false, bad = false;
+    if (k < nz && f.act[base + k]) {
+      su = sup[base + k];
+      sd = sdn[base + k];
+      any = su > 0.0 || sd > 0.0;
+      if (su > 0.0) {
+        mu = bits_highest(rbits, bits_highest(ibits, 0, k - 1) + 1, k - 1);
+        bad = mu < 0;
+      }
+      if (sd > 0.0) md = bits_lowest(rbits, k + 1, nz - 1);
+    }
+    if (__any_sync(0xffffffffu, bad)) {
+      lost = lost0;
+      __syncwarp();
+      return 2;
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, any);
+    int fail = 0;
+    while (mask) {
+      const int b = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const double upv = __shfl_sync(0xffffffffu, su, b);
+      const double dnv = __shfl_sync(0xffffffffu, sd, b);
+      const int tu = __shfl_sync(0xffffffffu, mu, b);
+      const int td = __shfl_sync(0xffffffffu, md, b);
+      if (lane == 0 && !fail) {
+        if (upv > 0.0) {
+          if (rs[tu] > upv) {
+            ws[tu] = __fma_rn(upv, ivs[tu], ws[tu]);
+            rs[tu] -= upv;
+            qs[tu + 1] += __dmul_rn(upv, idtg);
+          } else {
+            fail = 1;
+          }
+        }
+        if (!fail && dnv > 0.0) {
+          if (td < 0) {
+            lost -= dnv;
+          } else if (rs[td] > dnv) {
+            ws[td] = __fma_rn(dnv, ivs[td], ws[td]);
+            rs[td] -= dnv;
+            qs[td] -= __dmul_rn(dnv, idtg);
+          } else {
+            fail = 1;
+          }
+        }
+      }
+    }
+    if (__shfl_sync(0xffffffffu, fail, 0)) {
+      lost = lost0;
+      __syncwarp();
+      return 2;
+    }
+    __syncwarp();
+  }
+  return 0;
+}
+
 template <bool CPL>
 __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
                                                  const double* __restrict__ room,
@@ -1900,26 +2010,18 @@ __device__ __forceinline__ void walk_body(Dims d, Fields f, double* wc,
     double* pc = pcorr ? pcorr + fb : nullptr;  // transport window: this column's path records
     if (pc)
       for (int q = lane; q <= nz; q += 32) pc[q] = 0.0;
-    for (int k0 = 0; k0 < nz; k0 += 32) {
-      const int k = k0 + lane;
-      double r = 0.0;
-      bool inact = false;
-      if (k < nz) {
-        r = room[base + k];
-        rs[k] = r;
-        ws[k] = wc[base + k];
-        ivs[k] = 1.0 / (d.az * f.dz[base + k]);
-        inact = !f.act[base + k];
-      }
-      const unsigned rb = __ballot_sync(0xffffffffu, r > 0.0);
-      const unsigned ib = __ballot_sync(0xffffffffu, inact);
-      if (lane == 0) {
-        rbits[k0 >> 5] = rb;
-        ibits[k0 >> 5] = ib;
-      }
+    walk_stage(d, f, base, fb, nz, lane, room, wc, qzf, rs, ws, ivs, qs, rbits, ibits, true);
+    int how = 1;
+    if (!CPL && !pc)
+      how = walk_fast(f, base, nz, lane, rs, ws, ivs, qs, rbits, ibits, sup, sdn, idtg, lost);
+    if (how == 0) {
+      for (int k = lane; k < nz; k += 32) wc[base + k] = ws[k];
+      for (int k = lane; k <= nz; k += 32) qzf[fb + k] = qs[k];
+      __syncwarp();
+      continue;
     }
-    for (int k = lane; k <= nz; k += 32) qs[k] = qzf[fb + k];
-    __syncwarp();
+    if (how == 2) walk_stage(d, f, base, fb, nz, lane, room, wc, qzf, rs, ws, ivs, qs, rbits, ibits,
+                             false);
     for (int k0 = 0; k0 < nz; k0 += 32) {
       const int k = k0 + lane;
       double su = 0.0, sd = 0.0;
