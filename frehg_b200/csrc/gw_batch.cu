@@ -51,9 +51,57 @@ namespace fgw {
 
 namespace {
 
-__global__ void k_zero_states(CgState** st, int n, int* queue) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *queue = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+// Before a group's solve launch, one block: ranks the members by estimated
+// work, nb (iterations of the previous solve + 4), largest first, ties by
+// table index (up to kRankMax members; beyond, table order), writes the queue
+// order and its slot offsets, then zeroes the members' CG states and the
+// slot counter.  The order only decides which member's slots go out first;
+// a member's arithmetic depends on its own block count alone.
+constexpr int kRankMax = 1024;
+
+__global__ void k_queue_setup(CgState** st, const int* __restrict__ first, int n, int* queue,
+                              int* order, int* ofirst) {
+  __shared__ int part[256];
+  const int t = threadIdx.x;
+  if (n <= kRankMax) {
+    for (int i = t; i < n; i += blockDim.x) {
+      const long long wi = static_cast<long long>(first[i + 1] - first[i]) * (st[i]->its + 4);
+      int rank = 0;
+      for (int j = 0; j < n; ++j) {
+        const long long wj = static_cast<long long>(first[j + 1] - first[j]) * (st[j]->its + 4);
+        rank += (wj > wi || (wj == wi && j < i)) ? 1 : 0;
+      }
+      order[rank] = i;
+    }
+  } else {
+    for (int i = t; i < n; i += blockDim.x) order[i] = i;
+  }
+  __syncthreads();
+  // ofirst: exclusive prefix of the block counts in queue order, by chunks
+  // of blockDim.x members (a thread sums its chunk, the block scans the sums).
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int lo = t * per, hi = min(n, lo + per);
+  int sum = 0;
+  for (int q = lo; q < hi; ++q) sum += first[order[q] + 1] - first[order[q]];
+  part[t] = sum;
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+    for (int u = 0; u < static_cast<int>(blockDim.x); ++u) {
+      const int v = part[u];
+      part[u] = run;
+      run += v;
+    }
+    ofirst[n] = run;
+  }
+  __syncthreads();
+  int run = part[t];
+  for (int q = lo; q < hi; ++q) {
+    ofirst[q] = run;
+    run += first[order[q] + 1] - first[order[q]];
+  }
+  __syncthreads();
+  for (int i = t; i < n; i += blockDim.x) {
     CgState* s = st[i];
     s->dp = 0.0;
     s->rnorm0 = 0.0;
@@ -64,6 +112,7 @@ __global__ void k_zero_states(CgState** st, int n, int* queue) {
     s->bar_count = 0u;
     s->bar_gen = 0u;
   }
+  if (t == 0) *queue = 0;
 }
 
 size_t args_bytes(const SolveClass& c) {
@@ -101,7 +150,7 @@ int solve_max_blocks(const Device& D, const SolveClass& c) {
 size_t solve_group_bytes(const SolveClass& c, int n) {
   auto r = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   return r(args_bytes(c) * n) + r(sizeof(int) * (n + 1)) + r(sizeof(CgState*) * n) +
-         r(sizeof(int));
+         r(sizeof(int)) + r(sizeof(int) * n) + r(sizeof(int) * (n + 1));
 }
 
 cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
@@ -128,8 +177,11 @@ cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vec
   g.tab = base;
   g.first = reinterpret_cast<int*>(base + r(tab.size()));
   g.states = reinterpret_cast<CgState**>(base + r(tab.size()) + r(first.size() * sizeof(int)));
-  g.queue = reinterpret_cast<int*>(base + r(tab.size()) + r(first.size() * sizeof(int)) +
-                                   r(st.size() * sizeof(CgState*)));
+  char* q = base + r(tab.size()) + r(first.size() * sizeof(int)) +
+            r(st.size() * sizeof(CgState*));
+  g.queue = reinterpret_cast<int*>(q);
+  g.order = reinterpret_cast<int*>(q + r(sizeof(int)));
+  g.ofirst = reinterpret_cast<int*>(q + r(sizeof(int)) + r(sizeof(int) * ds.size()));
   cudaError_t e = cudaMemcpy(g.tab, tab.data(), tab.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(g.first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice);
@@ -141,12 +193,14 @@ cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vec
 }
 
 cudaError_t solve_group_launch(const SolveGroup& g, cudaStream_t s) {
-  k_zero_states<<<(g.n + 255) / 256, 256, 0, s>>>(g.states, g.n, g.queue);
+  k_queue_setup<<<1, 256, 0, s>>>(g.states, g.first, g.n, g.queue, g.order, g.ofirst);
   void* tab = g.tab;
   int* first = g.first;
   int n = g.n;
   int* queue = g.queue;
-  void* args[] = {&tab, &first, &n, &queue};
+  int* order = g.order;
+  int* ofirst = g.ofirst;
+  void* args[] = {&tab, &first, &n, &queue, &order, &ofirst};
   return cudaLaunchCooperativeKernel(batch_kernel(g.cls), dim3(g.grid), dim3(coop::kCgBlock), args,
                                      g.smem, s);
 }
@@ -207,8 +261,9 @@ int build_groups(frehg_gw_batch* b) {
                                                   want, fgw::solve_max_blocks(h->D, cls[i]))));
   }
   // The members of one class share one launch of at most the device's
-  // co-resident blocks; they queue for those blocks, largest block count
-  // first (the longest solves start first, the small ones fill the tail).
+  // co-resident blocks; they queue for those blocks, largest estimated work
+  // first (k_queue_setup), so the longest solves start first and the small
+  // ones fill the tail.
   struct Spec {
     fgw::SolveClass c;
     int cap = 0;
@@ -236,8 +291,6 @@ int build_groups(frehg_gw_batch* b) {
       order.push_back(j);
       done[j] = true;
     }
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int u, int v) { return b->nb[u] > b->nb[v]; });
     for (const int j : order) {
       frehg_gw_handle* h = b->m[j];
       cur.ds.push_back(&h->D);

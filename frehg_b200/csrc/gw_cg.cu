@@ -174,22 +174,26 @@ __global__ void __launch_bounds__(kCgBlock, 2) k_cg64(Cg64Args a) {
   cg64_body(a, blockIdx.x, gridDim.x);
 }
 
-// One cooperative launch over several domains: instance i owns block slots
-// [first[i], first[i+1]) and runs its own solve on them; each block takes the
-// next slot from `queue` (zeroed before the launch) until all are handed out,
-// so a block whose instance has converged goes on to a waiting instance.  The
-// slot, not the block, fixes the block's share of its instance's cells.
+// One cooperative launch over several domains: instance i owns
+// first[i+1] - first[i] block slots and runs its own solve on them; each block
+// takes the next slot from `queue` (zeroed before the launch) until all are
+// handed out, the instances' slots in queue order (`order`, slot offsets
+// `ofirst`), so a block whose instance has converged goes on to a waiting
+// instance.  The slot's index within its instance, not the block, fixes the
+// block's share of the instance's cells.
 __global__ void __launch_bounds__(kCgBlock, 3)
-    k_cg64_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n, int* queue) {
+    k_cg64_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n, int* queue,
+           const int* __restrict__ order, const int* __restrict__ ofirst) {
   __shared__ Cg64Args sa;
   __shared__ int sb, sg, slot;
   for (;;) {
     if (threadIdx.x == 0) {
       slot = atomicAdd(queue, 1);
       if (slot < first[n]) {
-        const int i = instance_of(first, n, slot);
+        const int q = instance_of(ofirst, n, slot);
+        const int i = order[q];
         sa = tab[i];
-        sb = slot - first[i];
+        sb = slot - ofirst[q];
         sg = first[i + 1] - first[i];
       }
     }
@@ -362,22 +366,26 @@ __global__ void __launch_bounds__(kCgBlock, 2) k_cg64v(Cg64Args a) {
   cg64v_body(a, blockIdx.x, gridDim.x);
 }
 
-// One cooperative launch over several domains: instance i owns block slots
-// [first[i], first[i+1]) and runs its own solve on them; each block takes the
-// next slot from `queue` (zeroed before the launch) until all are handed out,
-// so a block whose instance has converged goes on to a waiting instance.  The
-// slot, not the block, fixes the block's share of its instance's cells.
+// One cooperative launch over several domains: instance i owns
+// first[i+1] - first[i] block slots and runs its own solve on them; each block
+// takes the next slot from `queue` (zeroed before the launch) until all are
+// handed out, the instances' slots in queue order (`order`, slot offsets
+// `ofirst`), so a block whose instance has converged goes on to a waiting
+// instance.  The slot's index within its instance, not the block, fixes the
+// block's share of the instance's cells.
 __global__ void __launch_bounds__(kCgBlock, 3)
-    k_cg64v_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n, int* queue) {
+    k_cg64v_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n, int* queue,
+           const int* __restrict__ order, const int* __restrict__ ofirst) {
   __shared__ Cg64Args sa;
   __shared__ int sb, sg, slot;
   for (;;) {
     if (threadIdx.x == 0) {
       slot = atomicAdd(queue, 1);
       if (slot < first[n]) {
-        const int i = instance_of(first, n, slot);
+        const int q = instance_of(ofirst, n, slot);
+        const int i = order[q];
         sa = tab[i];
-        sb = slot - first[i];
+        sb = slot - ofirst[q];
         sg = first[i + 1] - first[i];
       }
     }

@@ -611,20 +611,22 @@ __global__ void __launch_bounds__(kCgBlock, mixed_min_blocks<V, E>(false)) k_cg_
 }
 
 // One cooperative launch over several domains of the same (V, E) class:
-// instance i owns block slots [first[i], first[i+1]) and runs its own solve;
-// the blocks take the slots from `queue` in order (as k_cg64_batch).
+// instance i owns first[i+1] - first[i] block slots and runs its own solve;
+// the blocks take the slots from `queue` in queue order (as k_cg64_batch).
 template <int V, int E>
 __global__ void __launch_bounds__(kCgBlock, mixed_min_blocks<V, E>(true))
-    k_cg_mixed_batch(const MixedArgs* __restrict__ tab, const int* __restrict__ first, int n, int* queue) {
+    k_cg_mixed_batch(const MixedArgs* __restrict__ tab, const int* __restrict__ first, int n, int* queue,
+           const int* __restrict__ order, const int* __restrict__ ofirst) {
   __shared__ MixedArgs sa;
   __shared__ int sb, sg, slot;
   for (;;) {
     if (threadIdx.x == 0) {
       slot = atomicAdd(queue, 1);
       if (slot < first[n]) {
-        const int i = instance_of(first, n, slot);
+        const int q = instance_of(ofirst, n, slot);
+        const int i = order[q];
         sa = tab[i];
-        sb = slot - first[i];
+        sb = slot - ofirst[q];
         sg = first[i + 1] - first[i];
       }
     }
@@ -784,7 +786,7 @@ size_t mixed_batch_smem(const Device& D, int variant) {
 }
 
 const void* mixed_batch_kernel(int variant) {
-  using Kern = void (*)(const MixedArgs*, const int*, int, int*);
+  using Kern = void (*)(const MixedArgs*, const int*, int, int*, const int*, const int*);
   static const Kern table[2][5] = {
       {k_cg_mixed_batch<1, 0>, k_cg_mixed_batch<1, 1>, k_cg_mixed_batch<1, 2>,
        k_cg_mixed_batch<1, 4>, k_cg_mixed_batch<1, 8>},

@@ -273,15 +273,19 @@ struct SolveGroup {
   int* first = nullptr;          // device block offsets, n + 1
   CgState** states = nullptr;    // device array of the members' CG states
   int* queue = nullptr;          // device counter of the slots handed out
+  int* order = nullptr;          // device queue order of the members, n
+  int* ofirst = nullptr;         // device slot offsets in queue order, n + 1
 };
 // Device bytes a group of n members of class c needs for its tables.
 size_t solve_group_bytes(const SolveClass& c, int n);
 // Builds a group over `ds` with `nb[i]` blocks each (all of class `c`), its
 // tables placed in `mem` (solve_group_bytes of device memory the caller owns).
 // The launch takes min(sum nb, max_grid) co-resident blocks (max_grid at
-// least every nb[i]); each block takes the members' block slots from a queue
-// in table order, so a member's slots go out together and the blocks of a
-// converged member go on to the next member's.
+// least every nb[i]); each block takes the members' block slots from a queue,
+// so a member's slots go out together and the blocks of a converged member go
+// on to the next member's.  The queue holds the members by estimated work,
+// largest first (nb times the iterations of the member's previous solve),
+// re-ranked on the device before every launch.
 cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
                               const std::vector<int>& nb, const std::vector<SolveParams>& p,
                               int max_grid, void* mem);

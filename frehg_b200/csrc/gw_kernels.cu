@@ -2863,6 +2863,19 @@ void launch_volume(const Device& D, const double* wc) {
 }
 
 // ---------------------------------------------------------------- batched phases (host)
+// Blocks of a member in the batched cell passes: a block per 8 cells a thread
+// (at most the member's own single-domain count).  Many members share each
+// launch, so the single-domain count (up to 8 blocks per SM for every
+// member, one or two cells a thread on small members) only added blocks and
+// their reductions; the member's arithmetic per cell does not depend on it,
+// its partial sums' order does (on its own size only).
+constexpr int kBatchCellsPerThread = 8;
+int batch_cell_blocks(const Device& D) {
+  const long long per = static_cast<long long>(kBlock) * kBatchCellsPerThread;
+  const long long want = (D.d.ncell + per - 1) / per;
+  return static_cast<int>(std::max(1LL, std::min<long long>(want, D.nblk)));
+}
+
 void fill_step_args(const Device& D, bool mixed, double dtg, double co_max, double dq_grow,
                     double dq_shrink, double dt_min, double dt_max, StepArgs& a) {
   std::memset(&a, 0, sizeof(a));
@@ -2911,7 +2924,7 @@ void fill_step_args(const Device& D, bool mixed, double dtg, double co_max, doub
   a.dq_shrink = dq_shrink;
   a.dt_min = dt_min;
   a.dt_max = dt_max;
-  a.nblk = D.nblk;
+  a.nblk = batch_cell_blocks(D);
   a.tc = line_tile_cols(D.d.nz);
   a.mixed = mixed ? 1 : 0;
   const size_t smem = kWalkWarps * walk_warp_bytes(D.d.nz);
@@ -2941,7 +2954,7 @@ cudaError_t phase_tables_build(PhaseTables& t, const std::vector<const Device*>&
   t.factor_smem = 0;
   for (int i = 0; i < t.n; ++i) {
     const Device& D = *ds[i];
-    fc[i + 1] = fc[i] + D.nblk;
+    fc[i + 1] = fc[i] + batch_cell_blocks(D);
     fg[i + 1] = fg[i] + ghost_blocks(D);
     ff[i + 1] = ff[i] + (mixed[i] ? line_factor_blocks(D) : 0);
     const size_t ws = kWalkWarps * walk_warp_bytes(D.d.nz);
