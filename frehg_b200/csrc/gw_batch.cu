@@ -9,11 +9,12 @@
 //          single-domain block count
 
 //   2.     the predictor solves of all members in one cooperative launch per
-//          kernel class (FP64 / mixed, column layout) of at most the device's
-//          co-resident blocks, each member on its own block count with its
-//          own CG state, reductions and barrier; the blocks take the members'
-//          block slots from a queue, so the blocks of a member whose solve has
-//          converged go straight on to the next waiting member's slots
+//          solve kind (FP64, mixed) of at most the device's co-resident
+//          blocks, each member in its own class's form (column layout, vector
+//          width) on its own block count with its own CG state, reductions
+//          and barrier; the blocks take the members' block slots from a queue
+//          ordered by estimated work, so the blocks of a member whose solve
+//          has converged go straight on to the next waiting member's slots
 //   3.     corrector, post-allocation, clamp, audit and controller of all
 //          members, one launch per phase, and one read-back of all step
 //          records; one synchronisation for the whole batch
@@ -120,7 +121,7 @@ size_t args_bytes(const SolveClass& c) {
 }
 
 const void* batch_kernel(const SolveClass& c) {
-  return c.kind == 0 ? cg64_batch_kernel(c.variant) : mixed_batch_kernel(c.variant);
+  return c.kind == 0 ? cg64_batch_kernel() : mixed_batch_kernel();
 }
 
 }  // namespace
@@ -154,8 +155,8 @@ size_t solve_group_bytes(const SolveClass& c, int n) {
 }
 
 cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
-                              const std::vector<int>& nb, const std::vector<SolveParams>& p,
-                              int max_grid, void* mem) {
+                              const std::vector<int>& variants, const std::vector<int>& nb,
+                              const std::vector<SolveParams>& p, int max_grid, void* mem) {
   g.cls = c;
   g.n = static_cast<int>(ds.size());
   const size_t ab = args_bytes(c);
@@ -164,11 +165,11 @@ cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vec
   std::vector<CgState*> st(ds.size());
   g.smem = 0;
   for (size_t i = 0; i < ds.size(); ++i) {
-    if (c.kind == 0) cg64_fill_args(*ds[i], p[i], tab.data() + i * ab);
-    else mixed_fill_args(*ds[i], p[i], tab.data() + i * ab);
+    if (c.kind == 0) cg64_fill_args(*ds[i], p[i], variants[i], tab.data() + i * ab);
+    else mixed_fill_args(*ds[i], p[i], variants[i], tab.data() + i * ab);
     first[i + 1] = first[i] + nb[i];
     st[i] = &ds[i]->out->cg;
-    if (c.kind == 1) g.smem = std::max(g.smem, mixed_batch_smem(*ds[i], c.variant));
+    if (c.kind == 1) g.smem = std::max(g.smem, mixed_batch_smem(*ds[i], variants[i]));
   }
   g.slots = first.back();
   g.grid = std::min(g.slots, max_grid);
@@ -260,44 +261,43 @@ int build_groups(frehg_gw_batch* b) {
     b->nb[i] = static_cast<int>(std::max(1LL, std::min<long long>(
                                                   want, fgw::solve_max_blocks(h->D, cls[i]))));
   }
-  // The members of one class share one launch of at most the device's
-  // co-resident blocks; they queue for those blocks, largest estimated work
-  // first (k_queue_setup), so the longest solves start first and the small
-  // ones fill the tail.
+  // The members of one solve kind (FP64, mixed) share one launch of at most
+  // the device's co-resident blocks, each in its own class's form; they
+  // queue for those blocks, largest estimated work first (k_queue_setup), so
+  // the longest solves start first and the small ones fill the tail.
   struct Spec {
     fgw::SolveClass c;
     int cap = 0;
     std::vector<fgw::Device*> ds;
+    std::vector<int> variants;
     std::vector<int> nbs;
     std::vector<fgw::SolveParams> ps;
   };
   std::vector<Spec> specs;
-  std::vector<bool> done(n, false);
-  for (int i = 0; i < n; ++i) {
-    if (done[i]) continue;
-    const fgw::SolveClass c = cls[i];
+  for (int kind = 0; kind < 2; ++kind) {
     size_t smem = 0;
-    for (int j = i; j < n; ++j)
-      if (cls[j] == c && c.kind == 1)
-        smem = std::max(smem, fgw::mixed_batch_smem(b->m[j]->D, c.variant));
+    bool any = false;
+    for (int j = 0; j < n; ++j) {
+      if (cls[j].kind != kind) continue;
+      any = true;
+      if (kind == 1) smem = std::max(smem, fgw::mixed_batch_smem(b->m[j]->D, cls[j].variant));
+    }
+    if (!any) continue;
+    const fgw::SolveClass c{kind, 0};
     const int per_sm = fgw::solve_blocks_per_sm(c, smem);
     if (per_sm < 1) return fail(FREHG_GW_ECUDA, "batch: solve kernel cannot be resident");
-    const int cap = per_sm * b->m[i]->D.sm_count;
-    Spec cur{c, cap, {}, {}, {}};
-    std::vector<int> order;
-    for (int j = i; j < n; ++j) {
-      if (done[j] || !(cls[j] == c)) continue;
-      b->nb[j] = std::min(b->nb[j], cap);
-      order.push_back(j);
-      done[j] = true;
-    }
-    for (const int j : order) {
+    Spec cur{c, 0, {}, {}, {}, {}};
+    for (int j = 0; j < n; ++j) {
+      if (cls[j].kind != kind) continue;
       frehg_gw_handle* h = b->m[j];
+      cur.cap = per_sm * h->D.sm_count;
+      b->nb[j] = std::min(b->nb[j], cur.cap);
       cur.ds.push_back(&h->D);
+      cur.variants.push_back(cls[j].variant);
       cur.nbs.push_back(b->nb[j]);
       cur.ps.push_back(fgw::SolveParams{h->rtol, h->atol, h->outer_rtol, h->maxit, h->max_outer});
     }
-    if (!cur.ds.empty()) specs.push_back(cur);
+    specs.push_back(cur);
   }
   // One device allocation for every group's tables, kept while it fits.
   size_t need = 0;
@@ -314,8 +314,8 @@ int build_groups(frehg_gw_batch* b) {
   size_t off = 0;
   for (const auto& sp : specs) {
     fgw::SolveGroup g;
-    const cudaError_t e = fgw::solve_group_build(g, sp.c, sp.ds, sp.nbs, sp.ps, sp.cap,
-                                                 static_cast<char*>(b->group_mem) + off);
+    const cudaError_t e = fgw::solve_group_build(g, sp.c, sp.ds, sp.variants, sp.nbs, sp.ps,
+                                                 sp.cap, static_cast<char*>(b->group_mem) + off);
     if (e != cudaSuccess) return cuda_fail(e, "batch: solve group");
     off += fgw::solve_group_bytes(sp.c, static_cast<int>(sp.ds.size()));
     b->groups.push_back(g);

@@ -45,6 +45,7 @@ struct Cg64Args {
   CgState* st;
   double rtol, atol;
   int maxit;
+  int variant;  // batched solves: 1 = the two-cell form (nz even), 0 = the scalar one
 };
 
 __device__ inline int sgn(double v) { return (v > 0.0) - (v < 0.0); }
@@ -173,37 +174,6 @@ __device__ __forceinline__ void cg64_body(const Cg64Args& a, const int bid, cons
 __global__ void __launch_bounds__(kCgBlock, 2) k_cg64(Cg64Args a) {
   cg64_body(a, blockIdx.x, gridDim.x);
 }
-
-// One cooperative launch over several domains: instance i owns
-// first[i+1] - first[i] block slots and runs its own solve on them; each block
-// takes the next slot from `queue` (zeroed before the launch) until all are
-// handed out, the instances' slots in queue order (`order`, slot offsets
-// `ofirst`), so a block whose instance has converged goes on to a waiting
-// instance.  The slot's index within its instance, not the block, fixes the
-// block's share of the instance's cells.
-__global__ void __launch_bounds__(kCgBlock, 3)
-    k_cg64_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n, int* queue,
-           const int* __restrict__ order, const int* __restrict__ ofirst) {
-  __shared__ Cg64Args sa;
-  __shared__ int sb, sg, slot;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      slot = atomicAdd(queue, 1);
-      if (slot < first[n]) {
-        const int q = instance_of(ofirst, n, slot);
-        const int i = order[q];
-        sa = tab[i];
-        sb = slot - ofirst[q];
-        sg = first[i + 1] - first[i];
-      }
-    }
-    __syncthreads();
-    if (slot >= first[n]) break;
-    cg64_body(sa, sb, sg);
-    __syncthreads();  // every thread is done with sa before the next slot's
-  }
-}
-
 
 // The same solve with two consecutive k-cells per thread and 16-byte loads
 // and stores (used when nz is even, so every pair and every i/j-neighbour pair
@@ -367,15 +337,16 @@ __global__ void __launch_bounds__(kCgBlock, 2) k_cg64v(Cg64Args a) {
 }
 
 // One cooperative launch over several domains: instance i owns
-// first[i+1] - first[i] block slots and runs its own solve on them; each block
-// takes the next slot from `queue` (zeroed before the launch) until all are
-// handed out, the instances' slots in queue order (`order`, slot offsets
-// `ofirst`), so a block whose instance has converged goes on to a waiting
-// instance.  The slot's index within its instance, not the block, fixes the
-// block's share of the instance's cells.
+// first[i+1] - first[i] block slots and runs its own solve on them, in the
+// scalar or the two-cell form by its `variant`; each block takes the next
+// slot from `queue` (zeroed before the launch) until all are handed out, the
+// instances' slots in queue order (`order`, slot offsets `ofirst`), so a
+// block whose instance has converged goes on to a waiting instance.  The
+// slot's index within its instance, not the block, fixes the block's share
+// of the instance's cells.
 __global__ void __launch_bounds__(kCgBlock, 3)
-    k_cg64v_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n, int* queue,
-           const int* __restrict__ order, const int* __restrict__ ofirst) {
+    k_cg64_batch(const Cg64Args* __restrict__ tab, const int* __restrict__ first, int n,
+                 int* queue, const int* __restrict__ order, const int* __restrict__ ofirst) {
   __shared__ Cg64Args sa;
   __shared__ int sb, sg, slot;
   for (;;) {
@@ -391,7 +362,11 @@ __global__ void __launch_bounds__(kCgBlock, 3)
     }
     __syncthreads();
     if (slot >= first[n]) break;
-    cg64v_body(sa, sb, sg);
+    if (sa.variant) {
+      cg64v_body(sa, sb, sg);
+    } else {
+      cg64_body(sa, sb, sg);
+    }
     __syncthreads();  // every thread is done with sa before the next slot's
   }
 }
@@ -449,14 +424,12 @@ cudaError_t launch_cg64(Device& D, double rtol, double atol, int maxit) {
 
 size_t cg64_args_bytes() { return sizeof(Cg64Args); }
 
-void cg64_fill_args(const Device& D, const SolveParams& p, void* dst) {
-  const Cg64Args a = make_cg64_args(D, p.rtol, p.atol, p.maxit);
+void cg64_fill_args(const Device& D, const SolveParams& p, int variant, void* dst) {
+  Cg64Args a = make_cg64_args(D, p.rtol, p.atol, p.maxit);
+  a.variant = variant;
   std::memcpy(dst, &a, sizeof(a));
 }
 
-const void* cg64_batch_kernel(int variant) {
-  return variant ? reinterpret_cast<const void*>(k_cg64v_batch)
-                 : reinterpret_cast<const void*>(k_cg64_batch);
-}
+const void* cg64_batch_kernel() { return reinterpret_cast<const void*>(k_cg64_batch); }
 
 }  // namespace fgw

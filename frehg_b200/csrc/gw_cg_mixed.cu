@@ -173,7 +173,8 @@ struct MixedArgs {
   double outer_rtol, inner_rtol, atol;
   int max_inner, max_outer, max_total;
   int tc;
-  int warm;  // x0 holds the starting iterate (h^n, written by the assembly)
+  int warm;     // x0 holds the starting iterate (h^n, written by the assembly)
+  int variant;  // batched solves: 16 V + E (mixed_variant)
 };
 
 // Forward/backward LDL^T sweeps of one column: z = T^-1 r.  r and z live in
@@ -610,13 +611,26 @@ __global__ void __launch_bounds__(kCgBlock, mixed_min_blocks<V, E>(false)) k_cg_
   cg_mixed_body<V, E>(a, blockIdx.x, gridDim.x);
 }
 
-// One cooperative launch over several domains of the same (V, E) class:
-// instance i owns first[i+1] - first[i] block slots and runs its own solve;
-// the blocks take the slots from `queue` in queue order (as k_cg64_batch).
-template <int V, int E>
-__global__ void __launch_bounds__(kCgBlock, mixed_min_blocks<V, E>(true))
-    k_cg_mixed_batch(const MixedArgs* __restrict__ tab, const int* __restrict__ first, int n, int* queue,
-           const int* __restrict__ order, const int* __restrict__ ofirst) {
+// One cooperative launch over several domains of every (V, E) class:
+// instance i owns first[i+1] - first[i] block slots and runs its own solve in
+// its class's form (`variant`); the blocks take the slots from `queue` in
+// queue order (as k_cg64_batch).  One launch for all classes, so the classes
+// share the device instead of following one another; the dynamic shared
+// memory is the largest any member needs.
+template <int V>
+__device__ __forceinline__ void cg_mixed_any(const MixedArgs& a, int e, int sb, int sg) {
+  switch (e) {
+    case 0: cg_mixed_body<V, 0>(a, sb, sg); break;
+    case 1: cg_mixed_body<V, 1>(a, sb, sg); break;
+    case 2: cg_mixed_body<V, 2>(a, sb, sg); break;
+    case 4: cg_mixed_body<V, 4>(a, sb, sg); break;
+    default: cg_mixed_body<V, 8>(a, sb, sg); break;
+  }
+}
+
+__global__ void __launch_bounds__(kCgBlock, 2)
+    k_cg_mixed_batch(const MixedArgs* __restrict__ tab, const int* __restrict__ first, int n,
+                     int* queue, const int* __restrict__ order, const int* __restrict__ ofirst) {
   __shared__ MixedArgs sa;
   __shared__ int sb, sg, slot;
   for (;;) {
@@ -632,7 +646,11 @@ __global__ void __launch_bounds__(kCgBlock, mixed_min_blocks<V, E>(true))
     }
     __syncthreads();
     if (slot >= first[n]) break;
-    cg_mixed_body<V, E>(sa, sb, sg);
+    if (sa.variant / 16 == 4) {
+      cg_mixed_any<4>(sa, sa.variant % 16, sb, sg);
+    } else {
+      cg_mixed_any<1>(sa, sa.variant % 16, sb, sg);
+    }
     __syncthreads();  // every thread is done with sa before the next slot's
   }
 }
@@ -776,8 +794,9 @@ int mixed_variant(const Device& D, bool tiled) {
 
 size_t mixed_args_bytes() { return sizeof(MixedArgs); }
 
-void mixed_fill_args(const Device& D, const SolveParams& p, void* dst) {
-  const MixedArgs a = make_mixed_args(D, p.atol, p.maxit, p.outer_rtol, p.max_outer);
+void mixed_fill_args(const Device& D, const SolveParams& p, int variant, void* dst) {
+  MixedArgs a = make_mixed_args(D, p.atol, p.maxit, p.outer_rtol, p.max_outer);
+  a.variant = variant;
   std::memcpy(dst, &a, sizeof(a));
 }
 
@@ -785,17 +804,7 @@ size_t mixed_batch_smem(const Device& D, int variant) {
   return (variant % 16 == 0) ? mixed_smem(D.d.nz) : 0;
 }
 
-const void* mixed_batch_kernel(int variant) {
-  using Kern = void (*)(const MixedArgs*, const int*, int, int*, const int*, const int*);
-  static const Kern table[2][5] = {
-      {k_cg_mixed_batch<1, 0>, k_cg_mixed_batch<1, 1>, k_cg_mixed_batch<1, 2>,
-       k_cg_mixed_batch<1, 4>, k_cg_mixed_batch<1, 8>},
-      {k_cg_mixed_batch<4, 0>, k_cg_mixed_batch<4, 1>, k_cg_mixed_batch<4, 2>,
-       k_cg_mixed_batch<4, 4>, k_cg_mixed_batch<4, 8>}};
-  const int v = variant / 16, e = variant % 16;
-  const int slot = e == 0 ? 0 : e == 1 ? 1 : e == 2 ? 2 : e == 4 ? 3 : 4;
-  return reinterpret_cast<const void*>(table[v == 4 ? 1 : 0][slot]);
-}
+const void* mixed_batch_kernel() { return reinterpret_cast<const void*>(k_cg_mixed_batch); }
 
 // ---------------------------------------------------------------- batched line factor
 namespace {

@@ -278,7 +278,8 @@ struct SolveGroup {
 };
 // Device bytes a group of n members of class c needs for its tables.
 size_t solve_group_bytes(const SolveClass& c, int n);
-// Builds a group over `ds` with `nb[i]` blocks each (all of class `c`), its
+// Builds a group over `ds` with `nb[i]` blocks each (all of solve kind c.kind,
+// member i in class variants[i]), its
 // tables placed in `mem` (solve_group_bytes of device memory the caller owns).
 // The launch takes min(sum nb, max_grid) co-resident blocks (max_grid at
 // least every nb[i]); each block takes the members' block slots from a queue,
@@ -287,19 +288,19 @@ size_t solve_group_bytes(const SolveClass& c, int n);
 // largest first (nb times the iterations of the member's previous solve),
 // re-ranked on the device before every launch.
 cudaError_t solve_group_build(SolveGroup& g, const SolveClass& c, const std::vector<Device*>& ds,
-                              const std::vector<int>& nb, const std::vector<SolveParams>& p,
-                              int max_grid, void* mem);
+                              const std::vector<int>& variants, const std::vector<int>& nb,
+                              const std::vector<SolveParams>& p, int max_grid, void* mem);
 // Zeroes the members' CG states and the slot queue and launches the group on `s`.
 cudaError_t solve_group_launch(const SolveGroup& g, cudaStream_t s);
 
 // Per-kind pieces of the batched solves (gw_cg.cu, gw_cg_mixed.cu).
 size_t cg64_args_bytes();
-void cg64_fill_args(const Device& D, const SolveParams& p, void* dst);
-const void* cg64_batch_kernel(int variant);
+void cg64_fill_args(const Device& D, const SolveParams& p, int variant, void* dst);
+const void* cg64_batch_kernel();
 int mixed_variant(const Device& D, bool tiled);
 size_t mixed_args_bytes();
-void mixed_fill_args(const Device& D, const SolveParams& p, void* dst);
+void mixed_fill_args(const Device& D, const SolveParams& p, int variant, void* dst);
 size_t mixed_batch_smem(const Device& D, int variant);
-const void* mixed_batch_kernel(int variant);
+const void* mixed_batch_kernel();
 
 }  // namespace fgw
