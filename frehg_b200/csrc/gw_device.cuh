@@ -160,13 +160,16 @@ __device__ inline double vg_theta_fast(const Soil& s, double h) {
   return wc;
 }
 
+// h(theta) with 1/m = n / (n - 1) and 1/n taken before the logarithms, so
+// the chain log -> expm1 -> log -> exp holds multiplications, not divisions
+// (equal to the divided form up to rounding).
 __device__ inline double vg_head_fast(const Soil& s, double wc) {
-  const double m = 1.0 - 1.0 / s.vgn;
+  const double im = s.vgn / (s.vgn - 1.0), in = 1.0 / s.vgn;
   if (wc - s.tr < 1.0e-7) wc = s.tr + 1.0e-7;
   if (wc < s.ts) {
     const double ratio = (s.ts - s.tr) / (wc - s.tr);
-    const double x = expm1(log(ratio) / m);  // ratio^(1/m) - 1
-    return -(1.0 / s.vga) * exp(log(x) / s.vgn);
+    const double x = expm1(log(ratio) * im);  // ratio^(1/m) - 1
+    return -(1.0 / s.vga) * exp(log(x) * in);
   }
   return 0.0;
 }
@@ -247,9 +250,9 @@ __device__ inline double vg_k(const Soil& s, double h, double ks) {
 // (1 - Se^(1/m))^m / (1 - Se^(1/m)): 2 powers instead of 6.
 __device__ inline double vg_dkdtheta(const Soil& s, double wc, double ks) {
   if (wc > 0.9999 * s.ts && wc < s.ts) wc = 0.9999 * s.ts;
-  const double m = 1.0 - 1.0 / s.vgn;
+  const double m = 1.0 - 1.0 / s.vgn, im = s.vgn / (s.vgn - 1.0);
   const double se = (wc - s.tr) / (s.ts - s.tr);
-  const double s1m = exp(log(se) / m);  // Se^(1/m); Se = 0 gives 0
+  const double s1m = exp(log(se) * im);  // Se^(1/m); Se = 0 gives 0
   const double q = 1.0 - s1m;
   const double t0 = exp(m * log(q));     // (1 - Se^(1/m))^m
   const double rs = sqrt(se);

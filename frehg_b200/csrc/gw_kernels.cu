@@ -503,12 +503,15 @@ __device__ __forceinline__ void assemble_body(
     a.kym = kyf[c - d.sy];
     a.kzm = kzff[fz];
     a.kzp = kzff[fz + 1];
+    // h^(n-1) with the cell's other loads (behind the activity test it cost a
+    // memory round trip of its own: 0.2 ms a 512x512x128 step).
+    const double hpv = hprev ? hprev[c] : 0.0;
     const int8_t ac = f.act[c];
     assemble_gather<CPL, BARO>(d, f, hn, wcn, ch[c], c, j, i, k, a);
     // The mixed / FP64 line solves' starting iterate: h^n, or with hprev
     // (h^(n-1)) its linear extrapolation to the step's end,
     // h^n + (dt_n / dt_(n-1)) (h^n - h^(n-1)).
-    if (xw) xw[c] = ac ? (hprev ? a.hnc + ratio * (a.hnc - hprev[c]) : a.hnc) : 0.0;
+    if (xw) xw[c] = ac ? (hprev ? a.hnc + ratio * (a.hnc - hpv) : a.hnc) : 0.0;
     if (!ac) {
       diag[c] = 1.0;
       gxps[c] = 0.0;

@@ -8,7 +8,10 @@ bars are the single-domain parity bars: head within 1e-9 relative L-inf for
 the FP64 form and 1e-8 for the mixed form, CG iterations within +/-2, and each
 member's own mass audit closing to 1e-12 of its storage.  Within the batch
 path the arithmetic is fixed by the member alone: graph replay and direct
-launches agree bit for bit, and so does a member alone and in a mix.
+launches agree bit for bit, and so does a member alone and in a mix (the
+members' solves share one launch per solve kind, their blocks taking block
+slots from a queue ranked by the previous step's work, so a member's place in
+the queue changes which blocks run it, never its arithmetic).
 """
 import copy
 
@@ -76,6 +79,9 @@ def test_batch_members_match_single_domain_steps():
         assert st["members"] == len(cfgs)
         assert st["steps"] == 4
         assert st["kernels_per_step"] > 0
+        # Members of every column class share one solve launch per solve kind
+        # (FP64 and mixed here), whatever their depths.
+        assert st["solve_launches"] == 2, st
     finally:
         batch.close()
         for s in solo + mem:
