@@ -145,6 +145,9 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     d.redistribute = desc->surplus_redistribute ? 1 : 0;
     d.terrain = desc->follow_terrain ? 1 : 0;
 
+    int soil_kind[8];
+    double soil_u[8] = {};
+    for (int f = 0; f < 8; ++f) soil_kind[f] = fgw::soil_storage(*desc, f, &soil_u[f]);
     // Allocation sequence, run twice (see dalloc): plan, then slices.
     auto allocate = [&]() -> cudaError_t {
       const long long n3 = d.ncell, nf = d.ncol * (d.nz + 1), m = d.sy;
@@ -155,7 +158,12 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
       };
       cudaError_t e = cudaSuccess;
       double** soil[8] = {&D.ksx, &D.ksy, &D.ksz, &D.vga, &D.vgn, &D.wcs, &D.wcr, &D.aev};
-      for (int f = 0; f < 8 && e == cudaSuccess; ++f) e = up(soil[f], H.soil[f]);
+      for (int f = 0; f < 8 && e == cudaSuccess; ++f) {
+        const int g = soil_kind[f];
+        if (g == fgw::kSoilUniform) e = up(soil[f], std::vector<double>(1, soil_u[f]));
+        else if (g >= 0) *soil[f] = *soil[g];  // equal bytes: one array for both
+        else e = up(soil[f], H.soil[f]);
+      }
       if (e == cudaSuccess) e = up(&D.dz, H.dz);
       if (e == cudaSuccess) e = up(&D.bot, H.bot);
       if (e == cudaSuccess) e = up(&D.ax, H.ax);
@@ -244,14 +252,12 @@ int frehg_gw_create(const frehg_gw_desc* desc, frehg_gw_handle** out) {
     }
 
     fgw::Fields& f = D.f;
-    f.ksx = D.ksx;
-    f.ksy = D.ksy;
-    f.ksz = D.ksz;
-    f.vga = D.vga;
-    f.vgn = D.vgn;
-    f.wcs = D.wcs;
-    f.wcr = D.wcr;
-    f.aev = D.aev;
+    {
+      const double* sp[8] = {D.ksx, D.ksy, D.ksz, D.vga, D.vgn, D.wcs, D.wcr, D.aev};
+      fgw::SoilField* sf[8] = {&f.ksx, &f.ksy, &f.ksz, &f.vga, &f.vgn, &f.wcs, &f.wcr, &f.aev};
+      for (int q = 0; q < 8; ++q)
+        *sf[q] = fgw::SoilField{sp[q], soil_kind[q] == fgw::kSoilUniform ? 0LL : ~0LL};
+    }
     f.dz = D.dz;
     f.bot = D.bot;
     f.ax = D.ax;

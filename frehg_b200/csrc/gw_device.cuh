@@ -60,9 +60,20 @@ struct BaroDev {
 };
 
 // Device pointers of one domain (see gw_internal.h for ownership).
+// One soil parameter field, read as f.field[c] either way: per-cell values
+// in the halo layout (mirrored ghosts, m = ~0), or, for a field that is
+// uniform over the domain, one value in device memory (m = 0: every index
+// reads p[0], a broadcast from L1 instead of a stream from HBM).  The index
+// mask costs one integer AND; a branch on uniformity made the kernels spill.
+struct SoilField {
+  const double* p;
+  long long m;
+  __host__ __device__ double operator[](long long c) const { return p[c & m]; }
+};
+
 struct Fields {
-  // soil (halo layout, mirrored ghosts)
-  const double *ksx, *ksy, *ksz, *vga, *vgn, *wcs, *wcr, *aev;
+  // soil: ksx ksy ksz alpha n theta_s theta_r aev
+  SoilField ksx, ksy, ksz, vga, vgn, wcs, wcr, aev;
   // geometry
   const double *dz, *bot, *ax, *ay, *sinx, *cosx, *siny, *cosy;
   const int8_t* act;   // 1 = active cell (gid >= 0), 0 = inactive or ghost

@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "gw_handle.h"
+#include "gw_setup.h"
 
 using fgw_api::cuda_fail;
 using fgw_api::fail;
@@ -248,7 +249,13 @@ size_t frehg_gw_device_bytes(const frehg_gw_desc* d) {
   const size_t n3 = ncol * d->nz, nf = ncol * (d->nz + 1);
   const size_t m = static_cast<size_t>(d->nx + 2) * d->nz, ns = n3 + 2 * m;
   auto r = [](size_t bytes) { return (bytes + 255) & ~static_cast<size_t>(255); };
-  size_t b = 16 * r(8 * n3);               // soil and geometry
+  int arrays = 8, ones = 0;  // geometry; soil by fgw::soil_storage
+  for (int f = 0; f < 8; ++f) {
+    const int k = fgw::soil_storage(*d, f, nullptr);
+    arrays += k == fgw::kSoilOwn;
+    ones += k == fgw::kSoilUniform;
+  }
+  size_t b = arrays * r(8 * n3) + ones * r(8);  // soil and geometry
   b += r(8 * ncol);                         // bed raster
   b += r(n3) + r(n3);                       // activity mask, saturation flags
   b += r(4 * 6 * ncol) + r(8 * 6 * ncol);   // BC codes and values

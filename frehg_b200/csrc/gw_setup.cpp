@@ -10,6 +10,8 @@
 // 160-215).  Soil ghosts mirror the interior (RichardsSolver.cpp:24-57).
 #include "gw_setup.h"
 
+#include <cstring>
+
 #include <algorithm>
 #include <cmath>
 
@@ -43,6 +45,26 @@ void mirror_edges(std::vector<T>& f, int nx, int ny, int nzf) {
 bool valid_code(int c) { return c >= FREHG_GW_BC_NOFLUX && c <= FREHG_GW_BC_HEAD_HYDROSTATIC; }
 
 }  // namespace
+
+int soil_storage(const frehg_gw_desc& d, int f, double* u) {
+  const double* src[8] = {d.ksx, d.ksy, d.ksz, d.vg_alpha, d.vg_n, d.theta_s, d.theta_r, d.aev};
+  if (f < 0 || f > 7 || !src[f] || d.nx < 1 || d.ny < 1 || d.nz < 1) return kSoilOwn;
+  const size_t n = static_cast<size_t>(d.nx) * d.ny * d.nz;
+  const double* a = src[f];
+  bool uniform = true;
+  for (size_t c = 1; c < n && uniform; ++c) uniform = std::memcmp(a + c, a, sizeof(double)) == 0;
+  if (uniform) {
+    if (u) *u = a[0];
+    return kSoilUniform;
+  }
+  // the first earlier match is never itself shared: that field would have
+  // matched first; a uniform field is never equal to this non-uniform one
+  for (int g = 0; g < f; ++g) {
+    if (!src[g]) continue;
+    if (src[g] == a || std::memcmp(src[g], a, n * sizeof(double)) == 0) return g;
+  }
+  return kSoilOwn;
+}
 
 int build_host_domain(const frehg_gw_desc& d, HostDomain& o, std::string& err) {
   if (d.abi_version != FREHG_GW_ABI_VERSION) {

@@ -29,4 +29,16 @@ struct HostDomain {
 // frehg_gw_status; on failure `err` says why.
 int build_host_domain(const frehg_gw_desc& desc, HostDomain& out, std::string& err);
 
+// How soil field f (0..7: ksx ksy ksz alpha n theta_s theta_r aev) is kept
+// on the device: kSoilUniform when every cell of the descriptor's array holds
+// the same value (*u gets it; the device keeps that one value, not an
+// array), the index g < f of an earlier field whose array holds the
+// same bytes (an isotropic soil's ksx = ksy = ksz: one array serves both),
+// or kSoilOwn.  Soil never changes after frehg_gw_create, so a shared array is
+// never written.  The values the kernels read are the descriptor's either
+// way; what changes is the bytes they move.
+constexpr int kSoilOwn = -1;
+constexpr int kSoilUniform = -2;
+int soil_storage(const frehg_gw_desc& desc, int f, double* u);
+
 }  // namespace fgw

@@ -117,3 +117,33 @@ def test_device_ordinal_of_a_null_handle_without_a_gpu():
     lib.frehg_gw_device.restype = ctypes.c_int
     lib.frehg_gw_device.argtypes = [ctypes.c_void_p]
     assert lib.frehg_gw_device(None) == -1
+
+
+def test_soil_storage_shares_equal_arrays_and_keeps_uniform_fields_as_one_value():
+    """A soil field uniform over the domain takes no cell array on the
+    device, and equal ksx / ksy / ksz arrays are stored once: the estimate
+    of the domain's device memory counts only the arrays it keeps (to the
+    2 MiB page the arena rounds to)."""
+    if not os.path.exists(LIB):
+        pytest.skip("libfrehg_gw.so not built")
+    import numpy as np
+
+    from frehg_b200 import workloads
+    from frehg_b200.serve import PreparedRequest
+    nx, ny, nz = 64, 48, 96
+    rng = np.random.default_rng(7)
+    ks = np.exp(rng.normal(np.log(1e-5), 1.0, (ny, nx, nz)))
+    alpha = rng.uniform(0.5, 3.0, (ny, nx, nz))
+    vgn = rng.uniform(1.4, 2.5, (ny, nx, nz))
+
+    def need(cell_soil):
+        cfg = workloads.column_32x32x50(nx=nx, ny=ny, nz=nz)
+        cfg.cell_soil = cell_soil
+        return PreparedRequest(cfg, 1).device_bytes()
+
+    array = ((nx + 2) * (ny + 2) * nz * 8 + 255) // 256 * 256
+    uniform = need(None)  # every soil field uniform: no soil array
+    iso = need(dict(ksx=ks, ksy=ks.copy(), ksz=ks, vg_alpha=alpha, vg_n=vgn))  # 3 arrays
+    aniso = need(dict(ksx=ks, ksy=2.0 * ks, ksz=ks, vg_alpha=alpha, vg_n=vgn))  # 4 arrays
+    assert abs((iso - uniform) - 3 * array) <= 2 << 20, (iso - uniform, array)
+    assert abs((aniso - iso) - array) <= 2 << 20, (aniso - iso, array)
