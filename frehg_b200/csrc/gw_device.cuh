@@ -262,14 +262,15 @@ __device__ inline double vg_k(const Soil& s, double h, double ks) {
 __device__ inline double vg_dkdtheta(const Soil& s, double wc, double ks) {
   if (wc > 0.9999 * s.ts && wc < s.ts) wc = 0.9999 * s.ts;
   const double m = 1.0 - 1.0 / s.vgn, im = s.vgn / (s.vgn - 1.0);
-  const double se = (wc - s.tr) / (s.ts - s.tr);
+  const double idt = 1.0 / (s.ts - s.tr);
+  const double se = (wc - s.tr) * idt;
   const double s1m = exp(log(se) * im);  // Se^(1/m); Se = 0 gives 0
   const double q = 1.0 - s1m;
   const double t0 = exp(m * log(q));     // (1 - Se^(1/m))^m
-  const double rs = sqrt(se);
-  const double t1 = 0.5 * ks / rs * (1.0 - t0) * (1.0 - t0);
-  const double t2 = 2.0 * ks * (s1m / rs) * (1.0 - t0) * (t0 / q);
-  return (t1 + t2) / (s.ts - s.tr);
+  const double irs = rsqrt(se);          // Se^(-1/2)
+  const double t1 = 0.5 * ks * irs * (1.0 - t0) * (1.0 - t0);
+  const double t2 = 2.0 * ks * (s1m * irs) * (1.0 - t0) * (t0 / q);
+  return (t1 + t2) * idt;
 }
 
 // Harmonic-Ks x arithmetic-kr face rule (src/gw/FaceConductivity.hpp:48-59)

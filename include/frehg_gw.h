@@ -421,7 +421,11 @@ int frehg_gw_batch_stats(const frehg_gw_batch* b, frehg_gw_batch_stats_t* out);
 int frehg_gw_batch_solve_blocks(const frehg_gw_batch* b, int* nb);
 
 /* Device memory frehg_gw_create allocates for this descriptor (an upper
- * estimate including allocation rounding); no counterpart in the reference. */
+ * estimate including allocation rounding); no counterpart in the reference.
+ * It reads the soil arrays: a soil field uniform over the domain is kept as
+ * one value and one equal byte for byte to an earlier field (ksx = ksy = ksz
+ * of an isotropic soil) shares that field's array, so neither takes a cell
+ * array of device memory. */
 size_t frehg_gw_device_bytes(const frehg_gw_desc* desc);
 
 /* ---------------------------------------------------------------- serving

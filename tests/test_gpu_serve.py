@@ -95,8 +95,13 @@ def test_admission_keeps_within_the_memory_budget():
 
 def test_device_bytes_estimate_covers_the_allocation():
     import torch
-    for prec in ("fp64", "mixed"):
-        cfg = workloads.column_32x32x50(nx=64, ny=48, nz=96, precision=prec)
+    # A single-soil box (every soil field uniform: one value each) and a
+    # per-cell soil slab crop (ksx = ksy = ksz shared, alpha and n per cell).
+    cases = [workloads.column_32x32x50(nx=64, ny=48, nz=96, precision=prec)
+             for prec in ("fp64", "mixed")]
+    cases.append(workloads.hillslope(64, 48, 96, precision="mixed"))
+    for cfg in cases:
+        prec = cfg.solver.precision
         need = PreparedRequest(cfg, 1).device_bytes()
         torch.cuda.synchronize()
         free0, _ = torch.cuda.mem_get_info()
